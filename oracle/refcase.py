@@ -1,0 +1,147 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY: runs the reference's own pressure path (``oracle/_ref/ref_harness``, compiled
+from the reference sources by ``oracle/Makefile``) on one case and reads back what it computed.
+
+The case file format is documented at the top of ``oracle/ref_harness.cpp``.
+"""
+from __future__ import annotations
+
+import os
+import struct
+import subprocess
+import tempfile
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+HARNESS = os.path.join(_HERE, "_ref", "ref_harness")
+SOLVER_CG, SOLVER_AMG, SOLVER_BICGSTAB = 0, 1, 2
+
+
+def available() -> bool:
+    return os.path.exists(HARNESS)
+
+
+def build(ref_root: str = "/root/reference") -> bool:
+    """Compiles the harness when the reference sources are present; True when the binary exists afterwards."""
+    if os.path.isdir(ref_root):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "ref", "REF=" + ref_root, "-j8"])
+    return available()
+
+
+@dataclass
+class RefResult:
+    Nx: int
+    Ny: int
+    Nz: int
+    n: int
+    iters: int
+    singular: bool
+    threads: int
+    t_assemble: float
+    t_solve_cold: float
+    t_solve_warm: float
+    t_project: float
+    rel_res: float
+    max_div: float
+    dh: float
+    types: np.ndarray
+    idp: np.ndarray
+    rowptr: np.ndarray
+    col: np.ndarray
+    val: np.ndarray
+    b_raw: np.ndarray
+    b: np.ndarray
+    x: np.ndarray
+    p: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    width: list
+    gap: list
+    centre: list
+
+
+def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000,
+               threads=1, repeats=0):
+    g = case.grid
+    grid_mode = 0 if not g.nonuniform else 1
+    nxi, nyi = g.Nx - 2, g.Ny - 2
+    nzi = g.Nz - 2 if g.dim == 3 else 0
+    hdr = [g.dim, grid_mode, g.grid_size, nxi, nyi, nzi, label_mode, int(case.needs_compat), 0, solver, max_iters,
+           threads, case.method, repeats, g.Nx, g.Ny]
+    with open(path, "wb") as f:
+        f.write(b"NBCASE01")
+        f.write(struct.pack("<16i", *hdr))
+        f.write(struct.pack("<6d", *g.domain))
+        f.write(struct.pack("<4d", case.rho, case.dt, case.tol if tol is None else tol, 0.0))
+        if grid_mode == 1:
+            for a in range(g.dim):
+                f.write(np.ascontiguousarray(g.interior_widths[a], dtype="<f8").tobytes())
+        if label_mode == 0:
+            text = case.scene.to_text().encode()
+            f.write(struct.pack("<i", len(text)))
+            f.write(text)
+        else:
+            f.write(np.ascontiguousarray(types, dtype=np.uint8).tobytes())
+        f.write(np.ascontiguousarray(u, dtype="<f8").tobytes())
+        f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
+        if g.dim == 3:
+            f.write(np.ascontiguousarray(w, dtype="<f8").tobytes())
+
+
+def read_result(path, dim) -> RefResult:
+    with open(path, "rb") as f:
+        data = f.read()
+    assert data[:8] == b"NBRES001", "bad result file"
+    off = 8
+    Nx, Ny, Nz, n, nnz, iters, sing, thr = struct.unpack_from("<8i", data, off)
+    off += 32
+    tA, tC, tW, tP, rr, md, dh, _ = struct.unpack_from("<8d", data, off)
+    off += 64
+    cells = Nx * Ny * Nz
+
+    def take(dtype, count):
+        nonlocal off
+        a = np.frombuffer(data, dtype=dtype, count=count, offset=off).copy()
+        off += a.nbytes
+        return a
+
+    types = take(np.uint8, cells)
+    idp = take("<i4", cells)
+    rowptr = take("<i4", n + 1)
+    col = take("<i4", nnz)
+    val = take("<f8", nnz)
+    b_raw = take("<f8", n)
+    b = take("<f8", n)
+    x = take("<f8", n)
+    p = take("<f8", cells)
+    u = take("<f8", (Nx + 1) * Ny * Nz)
+    v = take("<f8", Nx * (Ny + 1) * Nz)
+    w = take("<f8", Nx * Ny * (Nz + 1)) if dim == 3 else np.zeros(0)
+    width, gap, centre = [], [], []
+    for _ in range(3):
+        (nw,) = struct.unpack_from("<i", data, off); off += 4
+        width.append(take("<f8", nw))
+        (ng,) = struct.unpack_from("<i", data, off); off += 4
+        gap.append(take("<f8", ng))
+        (nc,) = struct.unpack_from("<i", data, off); off += 4
+        centre.append(take("<f8", nc))
+    return RefResult(Nx, Ny, Nz, n, iters, bool(sing), thr, tA, tC, tW, tP, rr, md, dh, types, idp, rowptr, col, val,
+                     b_raw, b, x, p, u, v, w, width, gap, centre)
+
+
+def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000, threads=1,
+        repeats=0, timeout=3600) -> RefResult:
+    """Runs the reference on ``case`` with face velocities u, v, w; labels from the scene text (label_mode 0) or
+    the given ``types`` (label_mode 1)."""
+    if not available():
+        raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+    with tempfile.TemporaryDirectory() as td:
+        cp, rp = os.path.join(td, "case.bin"), os.path.join(td, "res.bin")
+        write_case(cp, case, u, v, w, label_mode, types, solver, tol, max_iters, threads, repeats)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([HARNESS, cp, rp], capture_output=True, text=True, timeout=timeout, env=env, cwd=td)
+        if r.returncode != 0:
+            raise RuntimeError("ref_harness failed (%d): %s %s" % (r.returncode, r.stdout[-2000:], r.stderr[-2000:]))
+        return read_result(rp, case.grid.dim)

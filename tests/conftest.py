@@ -1,0 +1,50 @@
+import glob
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (runs the CUDA path through the C ABI)")
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+
+def load_golden(name):
+    """A fixture plus its case, rebuilt from the stored builder name and arguments."""
+    from nereus_cfd_b200 import workloads as W
+
+    z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    case = getattr(W, meta["builder"])(**meta["kwargs"])
+    return case, meta, z
+
+
+def cuda_ok():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def nb():
+    """The B200 library through its C ABI; GPU tests only."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    from nereus_cfd_b200 import capi
+
+    return capi.load()

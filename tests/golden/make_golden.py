@@ -1,0 +1,73 @@
+"""Writes the golden fixtures under tests/golden/ from the NEREUS reference's own pressure path.
+
+Run in a checkout that has the reference sources (it builds oracle/_ref/ref_harness from them first):
+
+    python tests/golden/make_golden.py [REF_ROOT]
+
+Each fixture is one small case: the inputs both sides read (face velocities, the prescribed ring pressure) and what
+the reference computed from them (cell types, IDP, the CSR matrix, b before and after the compatibility step, the
+Eigen-CG solution, the pressure field, the projected velocities, iterations, relative residual, max |div u|, and its
+spacing tables). The case geometry itself is rebuilt from the builder name and arguments stored in ``meta``.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from nereus_cfd_b200 import workloads as W  # noqa: E402
+from oracle import refcase  # noqa: E402
+
+# (fixture name, builder, kwargs, solver tolerance or None for the case's own)
+CASES = [
+    ("closed_box_2d_16", "closed_box_2d", {"n": 16, "seed": 11}, 1e-12),
+    ("sphere_outlet_3d_12", "sphere_outlet_3d", {"n": 12, "seed": 12}, 1e-12),
+    ("stretched_cylinder_3d_24x16x16", "stretched_cylinder_3d", {"nx": 24, "ny": 16, "nz": 16, "seed": 13}, 1e-12),
+    ("flip_tank_3d_12", "flip_tank_3d", {"n": 12, "seed": 14}, 1e-12),
+    ("dirichlet_linear_2d_40", "dirichlet_linear_2d", {"n": 40}, None),
+    ("dirichlet_linear_3d_20", "dirichlet_linear_3d", {"n": 20}, None),
+    ("channel_2d_stretched_24x12", "channel_2d_stretched", {"nx": 24, "ny": 12, "seed": 15}, 1e-12),
+    ("inflow_outflow_3d_8", "inflow_outflow_3d", {"n": 8, "seed": 16}, 1e-12),
+    ("all_solid_3d_6", "all_solid_3d", {"n": 6, "seed": 17}, 1e-12),
+]
+
+
+def build_case(builder: str, kwargs: dict) -> W.Case:
+    return getattr(W, builder)(**kwargs)
+
+
+def main(ref_root: str = "/root/reference") -> None:
+    if not refcase.build(ref_root):
+        raise SystemExit("the reference harness could not be built from %s" % ref_root)
+    for name, builder, kwargs, tol in CASES:
+        case = build_case(builder, kwargs)
+        g = case.grid
+        # labels from the reference's own scene code (label_mode 0), then velocities from those labels
+        probe = refcase.run(case, *[np.zeros(int(np.prod(s))) if s != (0,) else np.zeros(0)
+                                    for s in (g.u_shape(), g.v_shape(), g.w_shape())], tol=1e-6)
+        types = probe.types
+        u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
+        ref = refcase.run(case, u, v, w, tol=tol if tol is not None else case.tol)
+        p_in = np.where(ref.types == W.PRESSURE, ref.p, 0.0)
+        meta = dict(name=name, builder=builder, kwargs=kwargs, tol=tol if tol is not None else case.tol,
+                    needs_compat=case.needs_compat, rho=case.rho, dt=case.dt, n=ref.n, iters=ref.iters,
+                    singular=ref.singular, rel_res=ref.rel_res, max_div=ref.max_div, dh=ref.dh)
+        out = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(
+            out, meta=np.array(json.dumps(meta)), u=u.ravel(), v=v.ravel(), w=w.ravel(), p_in=p_in,
+            types=ref.types, idp=ref.idp, rowptr=ref.rowptr, col=ref.col, val=ref.val, b_raw=ref.b_raw, b=ref.b,
+            x=ref.x, p=ref.p, u_out=ref.u, v_out=ref.v, w_out=ref.w,
+            **{"width%d" % a: ref.width[a] for a in range(3)}, **{"gap%d" % a: ref.gap[a] for a in range(3)},
+            **{"centre%d" % a: ref.centre[a] for a in range(3)})
+        print("%-36s n=%-6d iters=%-4d rel_res=%.2e max_div=%.2e  %d KB" % (
+            name, ref.n, ref.iters, ref.rel_res, ref.max_div, os.path.getsize(out) // 1024))
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])
