@@ -1,0 +1,190 @@
+/*
+ * nereus_b200.h -- the C ABI of the B200 pressure projection for NEREUS (RaphaelLaroca/NEREUS_CFD).
+ *
+ * It replaces the pressure step of the reference's PressureSolver2D / PressureSolver3D static classes
+ * (src/Methods/PPESolver/PressureSolver3D.h:49-75, PressureSolver2D.h:49-76): the divergence of the intermediate MAC
+ * face velocities, the Poisson system from the cell types and the (stretched) spacing tables, the solve, the
+ * constant level, the scatter and pressure ring, and the pressure-gradient velocity correction. One context serves
+ * one grid on one GPU; a batch and a serving queue advance many independent grids at once.
+ *
+ * Conventions
+ *   - Status codes (nb_status): 0 OK; no exception crosses the ABI.
+ *   - Fields are the MAC grid's (src/headers/Core/MAC.h:235-254, 369-374): cell (i,j,k) = (y,x,z) at
+ *     (i*Nx + j)*Nz + k, u with Nx+1 entries along x, v with Ny+1 along y, w with Nz+1 along z; Nx, Ny, Nz include
+ *     the one-cell border ring. In 2D pass Nz = 1 and w = NULL.
+ *   - Spacing tables are the reference's padded ones (MAC.h:439-448): width[a] has N_a + 2 entries
+ *     (width[a][n+1] = Width(a, n), n = -1..N_a), gap[a] has N_a + 1 (gap[a][n+1] = FaceGap(a, n), n = -1..N_a-1).
+ *     In 2D width[2]/gap[2] describe the single z cell and are not read.
+ *   - Host pointers unless the function name says _device. The library allocates its own device memory; it is not
+ *     reentrant across host threads for one context (one context per host thread, as the reference's statics are
+ *     one system per dimension).
+ */
+#ifndef NEREUS_B200_H
+#define NEREUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum nb_status
+{
+    NB_OK = 0,
+    NB_NOT_CONVERGED = 1, /* the solve hit its iteration caps; the result still holds the last iterate */
+    NB_BAD_INPUT = 2,     /* sizes, pointers, tables or cell types the call cannot take */
+    NB_OUT_OF_MEMORY = 3, /* device allocation failed, or a request exceeds the serving budget */
+    NB_DEVICE_ERROR = 4,  /* a CUDA call failed; nb_last_error() says which */
+    NB_NO_DEVICE = 5,     /* no CUDA device, or the library was not built for it */
+    NB_BUSY = 6           /* a serving slot/ticket is not ready yet */
+} nb_status;
+
+/* Cell types (src/headers/Core/Definitions.h:191-196). */
+enum { NB_FLUID = 0, NB_SOLID = 1, NB_EMPTY = 2, NB_INFLOW = 3, NB_PRESSURE = 4, NB_OUTFLOW = 5 };
+
+/* What solves: plain FP64 MG-PCG, or FP32 MG-PCG inside FP64 iterative refinement. */
+enum { NB_PRECISION_FP64 = 0, NB_PRECISION_MIXED = 1 };
+
+/* Pressure schemes (src/Methods/PPESolver/PressureSettings.h:260). */
+enum { NB_SCHEME_CHORIN = 0, NB_SCHEME_INCREMENTAL = 1 };
+
+typedef struct nb_options
+{
+    int device;          /* CUDA device ordinal */
+    int precision;       /* NB_PRECISION_FP64 or NB_PRECISION_MIXED */
+    int max_iters;       /* FP64: PCG iterations; mixed: inner PCG iterations per refinement step */
+    int max_outer;       /* mixed: refinement steps */
+    double inner_tol;    /* mixed: relative residual reduction asked of each inner solve */
+    int pre_sweeps;      /* red-black Gauss-Seidel sweeps before the coarse correction */
+    int post_sweeps;     /* ... and after it */
+    int coarse_sweeps;   /* symmetric sweep pairs on the coarsest level */
+    int max_levels;      /* multigrid levels at most (>= 1) */
+    void *stream;        /* cudaStream_t to launch on; NULL: the context makes its own */
+} nb_options;
+
+typedef struct nb_result
+{
+    int status;          /* nb_status of the solve */
+    int n;               /* unknowns: interior FLUID cells (SystemSize) */
+    int singular;        /* no Dirichlet neighbour anywhere */
+    int iters_outer;     /* refinement steps (mixed) or 1 (FP64) */
+    int iters_inner;     /* PCG iterations summed over all steps (LastIterations) */
+    int levels;          /* multigrid levels used */
+    double b_norm;       /* ||b||_2 after the compatibility step */
+    double rel_res;      /* ||b - A x||_2 / ||b||_2 in FP64, A the reference's matrix */
+    double max_div;      /* max |div u| over FLUID cells after the projection (-1 when not computed) */
+    double seconds;      /* device time of the call's solve + projection (CUDA events) */
+} nb_result;
+
+typedef struct nb_ctx nb_ctx;
+
+/* ---- library ---- */
+void nereus_b200_default_options(nb_options *opt);
+const char *nereus_b200_last_error(void);
+int nereus_b200_device_count(void);
+
+/* ---- context: replaces PressureSolver3D::InitializePressureSolver / DestroyPressureSolver / ReleasePressureSolver
+ *      (PressureSolver3D.h:52-54; PressureSolver3D.cpp:89-116) ---- */
+int nereus_b200_create(nb_ctx **ctx, const nb_options *opt);
+void nereus_b200_destroy(nb_ctx *ctx);
+
+/* The grid's layout: cell types and spacing tables. Replaces EnsureSystem / AssembleSystem
+ * (PressureSolver3D.cpp:120-178) and, like PressureLayoutChanged (PressureSettings.h:300-303), rebuilds the
+ * hierarchy only when the sizes or the cell-type bytes differ from the last call. dh is the uniform cell size
+ * (MAC::dh); nonUniform selects the stretched coefficients A_f/d_f (MatrixScale3D, PressureSolver3D.cpp:34-37). */
+int nereus_b200_set_layout(nb_ctx *ctx, int dim, int Nx, int Ny, int Nz, const uint8_t *cellTypes,
+                           const double *const width[3], const double *const gap[3], int nonUniform, double dh);
+
+/* The pressure step and the projection on host fields, in place: SolveChorin/SolvePressure followed by
+ * ProjectPressure (PressureSolver3D.cpp:279-345, 396-438). p carries the ring values MAC::EnforcePressureBC
+ * wrote on the host (prescribed PRESSURE cells); the call replays the rest of the ring (EMPTY 0, others copied)
+ * after the scatter, levels a singular system's mean to 0 when needsCompat is set, and corrects u, v, w on every
+ * face with no solid side. tol: relative residual ||b - A x|| / ||b||. scheme must be NB_SCHEME_CHORIN. */
+int nereus_b200_project(nb_ctx *ctx, double *u, double *v, double *w, double *p, double rho, double dt, int scheme,
+                        int needsCompat, double tol, nb_result *out);
+
+/* The reference's two registered steps separately. nereus_b200_solve_pressure is the "pressure" step alone
+ * (SolveScheme, PressureSolver3D.cpp:279-328): p is written (unknowns scattered, ring replayed), u, v, w are only
+ * read. nereus_b200_project_velocity is the "projection" step alone (ProjectPressure, PressureSolver3D.cpp:417-438)
+ * with the pressure p as given. Running the two in turn gives what nereus_b200_project gives. */
+int nereus_b200_solve_pressure(nb_ctx *ctx, const double *u, const double *v, const double *w, double *p, double rho,
+                               double dt, int scheme, int needsCompat, double tol, nb_result *out);
+int nereus_b200_project_velocity(nb_ctx *ctx, double *u, double *v, double *w, const double *p, double rho,
+                                 double dt);
+
+/* The same on fields already in device memory (sizes as above), in place; launches on the context's stream. */
+int nereus_b200_project_device(nb_ctx *ctx, double *d_u, double *d_v, double *d_w, double *d_p, double rho,
+                               double dt, int needsCompat, double tol, nb_result *out);
+
+/* SolveLaplacian (PressureSolver3D.h:64, PressureSolver3D.cpp:355-371): L x = f on the unknowns, f and x indexed
+ * like the matrix (IDP order, n = SystemSize entries); x = 0 at air and pressure cells, no flux at solids. */
+int nereus_b200_solve_laplacian(nb_ctx *ctx, const double *f, double *x, double tol, nb_result *out);
+
+/* SystemSize / LastIterations / GetIDP (PressureSolver3D.h:66-68, 75). idp: Nx*Ny*Nz entries, -1 off the system. */
+int nereus_b200_system_size(const nb_ctx *ctx);
+int nereus_b200_last_iterations(const nb_ctx *ctx);
+int nereus_b200_get_idp(nb_ctx *ctx, int32_t *idp);
+
+/* The assembled matrix as the reference's CSR (PressureSolver3D.cpp:128-178 + Eigen setFromTriplets): rows in IDP
+ * order, ascending columns, the diagonal only when non-zero; computed on the device by the same coefficient code
+ * the solver applies. rowptr: n+1 entries; col/val: up to 7n (3D) or 5n (2D). *nnz receives the count. */
+int nereus_b200_export_matrix(nb_ctx *ctx, int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singular);
+
+/* The right-hand side before the compatibility step (PressureSolver3D.cpp:288-298), in IDP order, from host fields
+ * (p carries the prescribed ring values; the ring is replayed first, as SolveScheme's EnforcePressureBC does). */
+int nereus_b200_rhs(nb_ctx *ctx, const double *u, const double *v, const double *w, const double *p, double rho,
+                    double dt, double *b);
+
+/* ---- measurement (the reference's per-step wall times, SimulationManager.h:343-353, at kernel granularity) ----
+ * With profiling on, the context brackets every launch of the selected kernels with CUDA events on its stream and
+ * keeps, per kernel, the launch count, the summed device time and the algorithmic bytes one launch must move
+ * (each array touched once). Kernel ids: */
+enum
+{
+    NB_K_SMOOTH0 = 0,   /* red-black Gauss-Seidel half-sweep on the finest level */
+    NB_K_RESIDUAL0 = 1, /* multigrid residual on the finest level */
+    NB_K_RESTRICT0 = 2, /* restriction from the finest level */
+    NB_K_PROLONG0 = 3,  /* prolongation + correction onto the finest level */
+    NB_K_PAPPLY = 4,    /* CG direction update fused with the stencil apply and p.Ap */
+    NB_K_XR = 5,        /* CG x, r update fused with r.r */
+    NB_K_DOT = 6,       /* r.z */
+    NB_K_REFINE = 7,    /* FP64 residual of the reference's matrix (+ correction in refinement) */
+    NB_K_RHS = 8,       /* divergence / right-hand side */
+    NB_K_PROJECT = 9,   /* velocity correction */
+    NB_K_COARSE = 10,   /* every kernel on the coarser levels */
+    NB_K_COUNT = 11
+};
+int nereus_b200_profile_enable(nb_ctx *ctx, unsigned kernelMask); /* bit k selects kernel id k; 0 turns it off */
+int nereus_b200_profile_read(nb_ctx *ctx, int kernelId, int *launches, double *totalMs, double *bytesPerLaunch);
+/* Kernel launches this library has made in this process (all contexts). */
+long long nereus_b200_kernel_launches(void);
+
+/* ---- scene labelling (Scene::CellTypeAt, src/headers/Core/Scene.h:639-686) on the device ---- */
+enum { NB_PRIM_BOX = 0, NB_PRIM_SPHERE = 1, NB_PRIM_CYLINDER = 2, NB_PRIM_PLANE = 3 };
+enum { NB_REGION_SOLID = 0, NB_REGION_FLUID = 1, NB_REGION_EMPTY = 2 };
+enum { NB_BC_NOSLIP = 0, NB_BC_SLIP, NB_BC_MOVING, NB_BC_INLET, NB_BC_PRESSURE_OUTLET, NB_BC_OUTFLOW };
+
+typedef struct nb_region
+{
+    int kind, region, axis, invert;
+    double p0[3], p1[3], radius;
+} nb_region;
+
+typedef struct nb_scene
+{
+    int face_kind[6];  /* BoundaryKind of xmin, xmax, ymin, ymax, zmin, zmax */
+    int face_has_p[6]; /* a pressure outlet with p= gives PRESSURE cells, without EMPTY */
+    int face_order[6]; /* declaration order, -1 unspecified (no-slip); the last declared wins at edges */
+    int nregions;      /* <= 16, applied in order */
+    nb_region regions[16];
+} nb_scene;
+
+/* cx[j], cy[i], cz[k]: each cell's sample coordinate (its centre, or its low face for corner sampling). */
+int nereus_b200_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
+                            const nb_scene *scene, uint8_t *cellTypes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

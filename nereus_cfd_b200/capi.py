@@ -1,0 +1,171 @@
+"""ctypes binding of the B200 library's C ABI (include/nereus_b200.h).
+
+The library is ``nereus_cfd_b200/libnereus_b200.so``, built in-tree by ``nereus_cfd_b200.build``. Loading fails with
+an error when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnereus_b200.so")
+
+NB_OK, NB_NOT_CONVERGED, NB_BAD_INPUT, NB_OUT_OF_MEMORY, NB_DEVICE_ERROR, NB_NO_DEVICE, NB_BUSY = range(7)
+STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BAD_INPUT", 3: "OUT_OF_MEMORY", 4: "DEVICE_ERROR",
+                5: "NO_DEVICE", 6: "BUSY"}
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+SCHEME_CHORIN, SCHEME_INCREMENTAL = 0, 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("max_iters", ctypes.c_int),
+                ("max_outer", ctypes.c_int), ("inner_tol", ctypes.c_double), ("pre_sweeps", ctypes.c_int),
+                ("post_sweeps", ctypes.c_int), ("coarse_sweeps", ctypes.c_int), ("max_levels", ctypes.c_int),
+                ("stream", ctypes.c_void_p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("n", ctypes.c_int), ("singular", ctypes.c_int),
+                ("iters_outer", ctypes.c_int), ("iters_inner", ctypes.c_int), ("levels", ctypes.c_int),
+                ("b_norm", ctypes.c_double), ("rel_res", ctypes.c_double), ("max_div", ctypes.c_double),
+                ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Region(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("region", ctypes.c_int), ("axis", ctypes.c_int), ("invert", ctypes.c_int),
+                ("p0", ctypes.c_double * 3), ("p1", ctypes.c_double * 3), ("radius", ctypes.c_double)]
+
+
+class SceneStruct(ctypes.Structure):
+    _fields_ = [("face_kind", ctypes.c_int * 6), ("face_has_p", ctypes.c_int * 6), ("face_order", ctypes.c_int * 6),
+                ("nregions", ctypes.c_int), ("regions", Region * 16)]
+
+
+# Every exported symbol of include/nereus_b200.h with its ctypes signature.
+SIGNATURES = {
+    "nereus_b200_default_options": (None, [ctypes.POINTER(Options)]),
+    "nereus_b200_last_error": (ctypes.c_char_p, []),
+    "nereus_b200_device_count": (ctypes.c_int, []),
+    "nereus_b200_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Options)]),
+    "nereus_b200_destroy": (None, [ctypes.c_void_p]),
+    "nereus_b200_set_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, _u8, _dp * 3, _dp * 3, ctypes.c_int, ctypes.c_double]),
+    "nereus_b200_project": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Result)]),
+    "nereus_b200_solve_pressure": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.POINTER(Result)]),
+    "nereus_b200_project_velocity": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                                    ctypes.c_double]),
+    "nereus_b200_project_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.POINTER(Result)]),
+    "nereus_b200_solve_laplacian": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_double,
+                                                   ctypes.POINTER(Result)]),
+    "nereus_b200_system_size": (ctypes.c_int, [ctypes.c_void_p]),
+    "nereus_b200_last_iterations": (ctypes.c_int, [ctypes.c_void_p]),
+    "nereus_b200_get_idp": (ctypes.c_int, [ctypes.c_void_p, _ip]),
+    "nereus_b200_export_matrix": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _dp, ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_int)]),
+    "nereus_b200_rhs": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                       _dp]),
+    "nereus_b200_label_cells": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                               _dp, ctypes.POINTER(SceneStruct), _u8]),
+    "nereus_b200_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint]),
+    "nereus_b200_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "nereus_b200_kernel_launches": (ctypes.c_longlong, []),
+}
+
+# kernel ids of nereus_b200_profile_* (include/nereus_b200.h)
+KERNEL_NAMES = ["smooth0", "residual0", "restrict0", "prolong0", "p_apply", "xr_update", "dot", "refine64", "rhs",
+                "project", "coarse_levels"]
+
+
+def profile_read(lib, ctx):
+    """{kernel name: (launches, total ms, algorithmic bytes per launch)} of the profiled kernels."""
+    out = {}
+    for k, name in enumerate(KERNEL_NAMES):
+        n, ms, by = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_double(0.0)
+        check(lib.nereus_b200_profile_read(ctx, k, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by)))
+        if n.value:
+            out[name] = (n.value, ms.value, by.value)
+    return out
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH):
+    """The loaded library with every signature declared. Raises when the shared object is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError("%s is not built: run `python -m nereus_cfd_b200.build` (no CPU fallback exists)" % path)
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class NBError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), msg))
+        self.status = status
+
+
+def check(status: int, allow=(NB_OK,)):
+    if status not in allow:
+        raise NBError(status, load().nereus_b200_last_error().decode(errors="replace"))
+    return status
+
+
+def ptr(a: np.ndarray, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    load().nereus_b200_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def scene_struct(scene) -> SceneStruct:
+    s = SceneStruct()
+    kind, has_p, order = scene.face_arrays()
+    for f in range(6):
+        s.face_kind[f], s.face_has_p[f], s.face_order[f] = kind[f], has_p[f], order[f]
+    s.nregions = len(scene.regions)
+    for n, r in enumerate(scene.regions):
+        s.regions[n].kind, s.regions[n].region, s.regions[n].axis = r.kind, r.region, r.axis
+        s.regions[n].invert = int(r.invert)
+        for a in range(3):
+            s.regions[n].p0[a], s.regions[n].p1[a] = r.p0[a], r.p1[a]
+        s.regions[n].radius = r.radius
+    return s
+
+
+def label_cells(grid, scene) -> np.ndarray:
+    """Scene::CellTypeAt for every cell, on the device."""
+    cx, cy, cz = [np.ascontiguousarray(c, dtype=np.float64) for c in grid.sample_coords(scene.at_centre)]
+    out = np.zeros(grid.cells, dtype=np.uint8)
+    s = scene_struct(scene)
+    check(load().nereus_b200_label_cells(grid.dim, grid.Nx, grid.Ny, grid.Nz, ptr(cx), ptr(cy), ptr(cz),
+                                         ctypes.byref(s), ptr(out, _u8)))
+    return out

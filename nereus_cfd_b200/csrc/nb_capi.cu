@@ -1,0 +1,324 @@
+// The extern "C" entry points of include/nereus_b200.h. Every call catches its own exceptions and turns them into an
+// nb_status; the message of the last failure on this host thread is kept for nereus_b200_last_error().
+#include "nb_solver.h"
+
+#include <memory>
+#include <new>
+#include <string>
+
+struct nb_ctx
+{
+    std::unique_ptr<nb::Context> c;
+};
+
+namespace
+{
+thread_local std::string g_error;
+
+int Fail(int code, const std::string &msg)
+{
+    g_error = msg;
+    return code;
+}
+
+template <typename F> int Guard(F &&f)
+{
+    try
+    {
+        return f();
+    }
+    catch (const nb::InputError &e)
+    {
+        return Fail(NB_BAD_INPUT, e.what());
+    }
+    catch (const nb::CudaError &e)
+    {
+        if (e.code == cudaErrorMemoryAllocation) return Fail(NB_OUT_OF_MEMORY, e.what());
+        if (e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver ||
+            e.code == cudaErrorNoKernelImageForDevice)
+            return Fail(NB_NO_DEVICE, e.what());
+        return Fail(NB_DEVICE_ERROR, e.what());
+    }
+    catch (const std::bad_alloc &)
+    {
+        return Fail(NB_OUT_OF_MEMORY, "host allocation failed");
+    }
+    catch (const std::exception &e)
+    {
+        return Fail(NB_DEVICE_ERROR, e.what());
+    }
+    catch (...)
+    {
+        return Fail(NB_DEVICE_ERROR, "unknown failure");
+    }
+}
+} // namespace
+
+extern "C" {
+
+void nereus_b200_default_options(nb_options *o)
+{
+    if (!o) return;
+    o->device = 0;
+    o->precision = NB_PRECISION_MIXED;
+    o->max_iters = 60;
+    o->max_outer = 12;
+    o->inner_tol = 1e-4;
+    o->pre_sweeps = 1;
+    o->post_sweeps = 1;
+    o->coarse_sweeps = 16;
+    o->max_levels = 16;
+    o->stream = nullptr;
+}
+
+const char *nereus_b200_last_error(void) { return g_error.c_str(); }
+
+int nereus_b200_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int nereus_b200_create(nb_ctx **ctx, const nb_options *opt)
+{
+    if (!ctx) return Fail(NB_BAD_INPUT, "ctx is null");
+    *ctx = nullptr;
+    return Guard([&] {
+        nb_options o;
+        nereus_b200_default_options(&o);
+        if (opt) o = *opt;
+        if (o.precision != NB_PRECISION_FP64 && o.precision != NB_PRECISION_MIXED)
+            throw nb::InputError("unknown precision");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+            return Fail(NB_NO_DEVICE, "no CUDA device");
+        if (o.device < 0 || o.device >= count) throw nb::InputError("device ordinal out of range");
+        auto *h = new nb_ctx;
+        try
+        {
+            h->c.reset(new nb::Context(o));
+        }
+        catch (...)
+        {
+            delete h;
+            throw;
+        }
+        *ctx = h;
+        return (int)NB_OK;
+    });
+}
+
+void nereus_b200_destroy(nb_ctx *ctx)
+{
+    if (!ctx) return;
+    try
+    {
+        if (ctx->c) cudaSetDevice(ctx->c->device);
+        ctx->c.reset();
+    }
+    catch (...)
+    {
+    }
+    delete ctx;
+}
+
+int nereus_b200_set_layout(nb_ctx *ctx, int dim, int Nx, int Ny, int Nz, const uint8_t *cellTypes,
+                           const double *const width[3], const double *const gap[3], int nonUniform, double dh)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    return Guard([&] {
+        NB_CK(cudaSetDevice(ctx->c->device));
+        ctx->c->SetLayout(dim, Nx, Ny, Nz, cellTypes, width, gap, nonUniform, dh);
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_project(nb_ctx *ctx, double *u, double *v, double *w, double *p, double rho, double dt, int scheme,
+                        int needsCompat, double tol, nb_result *out)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    if (scheme != NB_SCHEME_CHORIN) return Fail(NB_BAD_INPUT, "only the Chorin scheme is served");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        if (!C.built) throw nb::InputError("set_layout has not been called");
+        if (!u || !v || !p || (C.dim == 3 && !w)) throw nb::InputError("null field pointer");
+        nb_result local{};
+        nb_result *r = out ? out : &local;
+        C.du.upload(u, C.FieldSizeU(), C.st);
+        C.dv.upload(v, C.FieldSizeV(), C.st);
+        if (C.dim == 3) C.dw.upload(w, C.FieldSizeW(), C.st);
+        C.dp.upload(p, C.Cells(), C.st);
+        const int status = C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, rho, dt,
+                                           needsCompat, tol, r);
+        NB_CK(cudaMemcpyAsync(u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaMemcpyAsync(v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
+        if (C.dim == 3) NB_CK(cudaMemcpyAsync(w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaMemcpyAsync(p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaStreamSynchronize(C.st));
+        return status;
+    });
+}
+
+int nereus_b200_solve_pressure(nb_ctx *ctx, const double *u, const double *v, const double *w, double *p, double rho,
+                               double dt, int scheme, int needsCompat, double tol, nb_result *out)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    if (scheme != NB_SCHEME_CHORIN) return Fail(NB_BAD_INPUT, "only the Chorin scheme is served");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        if (!C.built) throw nb::InputError("set_layout has not been called");
+        if (!u || !v || !p || (C.dim == 3 && !w)) throw nb::InputError("null field pointer");
+        nb_result local{};
+        C.du.upload(u, C.FieldSizeU(), C.st);
+        C.dv.upload(v, C.FieldSizeV(), C.st);
+        if (C.dim == 3) C.dw.upload(w, C.FieldSizeW(), C.st);
+        C.dp.upload(p, C.Cells(), C.st);
+        const int status = C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, rho, dt,
+                                           needsCompat, tol, out ? out : &local, true, false);
+        NB_CK(cudaMemcpyAsync(p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaStreamSynchronize(C.st));
+        return status;
+    });
+}
+
+int nereus_b200_project_velocity(nb_ctx *ctx, double *u, double *v, double *w, const double *p, double rho,
+                                 double dt)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        if (!C.built) throw nb::InputError("set_layout has not been called");
+        if (!u || !v || !p || (C.dim == 3 && !w)) throw nb::InputError("null field pointer");
+        nb_result local{};
+        C.du.upload(u, C.FieldSizeU(), C.st);
+        C.dv.upload(v, C.FieldSizeV(), C.st);
+        if (C.dim == 3) C.dw.upload(w, C.FieldSizeW(), C.st);
+        C.dp.upload(p, C.Cells(), C.st);
+        C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, rho, dt, 0, 1.0, &local, false, true);
+        NB_CK(cudaMemcpyAsync(u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaMemcpyAsync(v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
+        if (C.dim == 3) NB_CK(cudaMemcpyAsync(w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaStreamSynchronize(C.st));
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_project_device(nb_ctx *ctx, double *d_u, double *d_v, double *d_w, double *d_p, double rho,
+                               double dt, int needsCompat, double tol, nb_result *out)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        nb_result local{};
+        return C.ProjectDevice(d_u, d_v, C.dim == 3 ? d_w : d_u, d_p, rho, dt, needsCompat, tol, out ? out : &local);
+    });
+}
+
+int nereus_b200_solve_laplacian(nb_ctx *ctx, const double *f, double *x, double tol, nb_result *out)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    if (!f || !x) return Fail(NB_BAD_INPUT, "null vector");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        nb_result local{};
+        return C.SolveLaplacian(f, x, tol, out ? out : &local);
+    });
+}
+
+int nereus_b200_system_size(const nb_ctx *ctx) { return ctx && ctx->c && ctx->c->built ? ctx->c->n : 0; }
+
+int nereus_b200_last_iterations(const nb_ctx *ctx) { return ctx && ctx->c ? ctx->c->lastIterations : 0; }
+
+int nereus_b200_get_idp(nb_ctx *ctx, int32_t *idp)
+{
+    if (!ctx || !ctx->c || !idp) return Fail(NB_BAD_INPUT, "null argument");
+    return Guard([&] {
+        NB_CK(cudaSetDevice(ctx->c->device));
+        ctx->c->GetIdp(idp);
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_export_matrix(nb_ctx *ctx, int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singular)
+{
+    if (!ctx || !ctx->c || !rowptr || !col || !val || !nnz || !singular) return Fail(NB_BAD_INPUT, "null argument");
+    return Guard([&] {
+        NB_CK(cudaSetDevice(ctx->c->device));
+        ctx->c->ExportMatrix(rowptr, col, val, nnz, singular);
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_rhs(nb_ctx *ctx, const double *u, const double *v, const double *w, const double *p, double rho,
+                    double dt, double *b)
+{
+    if (!ctx || !ctx->c || !u || !v || !p || !b) return Fail(NB_BAD_INPUT, "null argument");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        if (C.dim == 3 && !w) throw nb::InputError("null w");
+        C.Rhs(u, v, w, p, rho, dt, b);
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_profile_enable(nb_ctx *ctx, unsigned kernelMask)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    return Guard([&] {
+        NB_CK(cudaSetDevice(ctx->c->device));
+        NB_CK(cudaStreamSynchronize(ctx->c->st));
+        ctx->c->ProfClear();
+        ctx->c->profMask = kernelMask;
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_profile_read(nb_ctx *ctx, int kernelId, int *launches, double *totalMs, double *bytesPerLaunch)
+{
+    if (!ctx || !ctx->c || !launches || !totalMs || !bytesPerLaunch) return Fail(NB_BAD_INPUT, "null argument");
+    if (kernelId < 0 || kernelId >= NB_K_COUNT) return Fail(NB_BAD_INPUT, "kernel id out of range");
+    return Guard([&] {
+        NB_CK(cudaSetDevice(ctx->c->device));
+        ctx->c->ProfRead(kernelId, launches, totalMs, bytesPerLaunch);
+        return (int)NB_OK;
+    });
+}
+
+long long nereus_b200_kernel_launches(void) { return nb::g_launches.load(); }
+
+int nereus_b200_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
+                            const nb_scene *scene, uint8_t *cellTypes)
+{
+    if (!cx || !cy || !cz || !scene || !cellTypes) return Fail(NB_BAD_INPUT, "null argument");
+    if ((dim != 2 && dim != 3) || Nx < 1 || Ny < 1 || Nz < 1) return Fail(NB_BAD_INPUT, "bad sizes");
+    if (scene->nregions < 0 || scene->nregions > 16) return Fail(NB_BAD_INPUT, "at most 16 regions");
+    return Guard([&] {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return Fail(NB_NO_DEVICE, "no CUDA device");
+        const int nz = dim == 3 ? Nz : 1;
+        const size_t cells = (size_t)Nx * Ny * nz;
+        cudaStream_t st;
+        NB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        nb::DevArray<double> X, Y, Z;
+        nb::DevArray<uint8_t> T;
+        X.upload(cx, (size_t)Nx, st);
+        Y.upload(cy, (size_t)Ny, st);
+        Z.upload(cz, (size_t)nz, st);
+        T.alloc(cells);
+        nb::LaunchLabelCells(dim, Nx, Ny, nz, X.p, Y.p, Z.p, *scene, T.p, st);
+        NB_CK(cudaGetLastError());
+        NB_CK(cudaMemcpyAsync(cellTypes, T.p, cells, cudaMemcpyDeviceToHost, st));
+        NB_CK(cudaStreamSynchronize(st));
+        cudaStreamDestroy(st);
+        return (int)NB_OK;
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,780 @@
+// Kernels whose results must match the NEREUS reference bit for bit: scene labelling, IDP numbering, the assembled
+// matrix, the right-hand side, the FP64 residual, the scatter and pressure ring, and the projection.
+//
+// This file is compiled with -fmad=false: every expression rounds after each operation in the order the reference's
+// C++ writes it, as the host compiler (which emits no fused multiply-add for the default x86-64 target) does.
+#include "nb_kernels.h"
+
+#include <cub/device/device_scan.cuh>
+
+namespace nb
+{
+
+// ---------------------------------------------------------------------------------------------------------------
+// coefficients, exactly as the reference forms them
+// ---------------------------------------------------------------------------------------------------------------
+
+// FaceCoefs3D (PressureSolver3D.cpp:47-63); the 2D c[] table (PressureSolver2D.cpp:123-126).
+__device__ __forceinline__ void CoefsExact(const LevelView &v, int i, int j, int k, double c[6])
+{
+    if (v.dim == 2)
+    {
+        c[0] = Wd(v, 0, j) / Gp(v, 1, i);
+        c[1] = Wd(v, 0, j) / Gp(v, 1, i - 1);
+        c[2] = Wd(v, 1, i) / Gp(v, 0, j);
+        c[3] = Wd(v, 1, i) / Gp(v, 0, j - 1);
+        c[4] = c[5] = 0.0;
+        return;
+    }
+    if (!v.stretched)
+    {
+        for (int q = 0; q < 6; q++) c[q] = 1.0;
+        return;
+    }
+    const double ax = Wd(v, 1, i) * Wd(v, 2, k);
+    const double ay = Wd(v, 0, j) * Wd(v, 2, k);
+    const double az = Wd(v, 0, j) * Wd(v, 1, i);
+    c[0] = ay / Gp(v, 1, i);
+    c[1] = ay / Gp(v, 1, i - 1);
+    c[2] = ax / Gp(v, 0, j);
+    c[3] = ax / Gp(v, 0, j - 1);
+    c[4] = az / Gp(v, 2, k);
+    c[5] = az / Gp(v, 2, k - 1);
+}
+
+// DirichletRingFactor (PressureSettings.h:307-310).
+__device__ __forceinline__ double DRF(const LevelView &v, int a, int n, int s)
+{
+    return Gp(v, a, s < 0 ? n - 1 : n) / (0.5 * Wd(v, a, n));
+}
+
+// RingFactor3D (PressureSolver3D.cpp:80-87) / RingFactor2D (PressureSolver2D.cpp:55-60).
+__device__ __forceinline__ double RingFactorExact(const LevelView &v, int i, int j, int k, int q, int t)
+{
+    if (!IsDirichlet(t)) return 1.0;
+    const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3), nk = k + (q == 4) - (q == 5);
+    if (!OnRing(v, ni, nj, nk)) return 1.0;
+    const int s = (q % 2 == 0) ? 1 : -1;
+    return q < 2 ? DRF(v, 1, i, s) : (q < 4 ? DRF(v, 0, j, s) : DRF(v, 2, k, s));
+}
+
+// The diagonal of AssembleSystem before scaling (PressureSolver3D.cpp:151-166): fluid faces first, then the
+// Dirichlet faces with their ring factor, in q order. Also reports the neighbour types.
+__device__ __forceinline__ double DiagExact(const LevelView &v, int i, int j, int k, long long c, const double cq[6],
+                                            int t[6])
+{
+    const int nq = v.dim == 3 ? 6 : 4;
+    double diag = 0.0;
+    for (int q = 0; q < nq; q++)
+    {
+        t[q] = v.types[c + NbrOffset(v, q)];
+        if (t[q] == FLUID) diag -= cq[q];
+    }
+    for (int q = 0; q < nq; q++)
+        if (IsDirichlet(t[q])) diag -= cq[q] * RingFactorExact(v, i, j, k, q, t[q]);
+    return diag;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// scene labelling: Scene::CellTypeAt (Scene.h:639-673) with Primitive::Distance/Contains (Scene.h:265-366),
+// WinningFace (:566-575) and CellTypeOf (:677-686)
+// ---------------------------------------------------------------------------------------------------------------
+__device__ double PrimDistance(const nb_region &p, int dim, double x, double y, double z)
+{
+    const int axes = dim == 2 ? 2 : 3;
+    double d = 0.0;
+    if (p.kind == NB_PRIM_BOX)
+    {
+        const double c[3] = {x, y, z};
+        double outside = 0.0, inside = -1e30;
+        for (int a = 0; a < axes; a++)
+        {
+            const double dlo = p.p0[a] - c[a];
+            const double dhi = c[a] - p.p1[a];
+            const double dm = dlo > dhi ? dlo : dhi;
+            if (dm > 0.0) outside += dm * dm;
+            inside = inside > dm ? inside : dm;
+        }
+        d = outside > 0.0 ? sqrt(outside) : inside;
+    }
+    else if (p.kind == NB_PRIM_SPHERE)
+    {
+        const double dx = x - p.p0[0], dy = y - p.p0[1];
+        const double dz = axes == 3 ? (z - p.p0[2]) : 0.0;
+        d = sqrt(dx * dx + dy * dy + dz * dz) - p.radius;
+    }
+    else if (p.kind == NB_PRIM_CYLINDER)
+    {
+        double a1, a2;
+        if (p.axis == 0) { a1 = y - p.p0[1]; a2 = z - p.p0[2]; }
+        else if (p.axis == 1) { a1 = x - p.p0[0]; a2 = z - p.p0[2]; }
+        else { a1 = x - p.p0[0]; a2 = y - p.p0[1]; }
+        d = sqrt(a1 * a1 + a2 * a2) - p.radius;
+    }
+    else
+    {
+        const double nx = p.p1[0], ny = p.p1[1];
+        const double nz = axes == 3 ? p.p1[2] : 0.0;
+        const double len = sqrt(nx * nx + ny * ny + nz * nz);
+        const double inv = len > 0.0 ? 1.0 / len : 0.0;
+        const double dzc = axes == 3 ? (z - p.p0[2]) : 0.0;
+        d = ((x - p.p0[0]) * nx + (y - p.p0[1]) * ny + dzc * nz) * inv;
+    }
+    return p.invert ? -d : d;
+}
+
+__global__ void k_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
+                              nb_scene s, uint8_t *types)
+{
+    const long long cells = (long long)Nx * Ny * Nz;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int k = (int)(c % Nz);
+        const long long r = c / Nz;
+        const int j = (int)(r % Nx), i = (int)(r / Nx);
+        const double x = cx[j], y = cy[i], z = dim == 3 ? cz[k] : cz[0];
+        int type = FLUID;
+        for (int q = 0; q < s.nregions; q++)
+        {
+            const nb_region &p = s.regions[q];
+            if (!(PrimDistance(p, dim, x, y, z) < 0.0)) continue;
+            type = p.region == NB_REGION_SOLID ? SOLID : (p.region == NB_REGION_FLUID ? FLUID : EMPTY);
+        }
+        const bool on[6] = {j == 0, j == Nx - 1, i == 0, i == Ny - 1, k == 0, k == Nz - 1};
+        int best = -1, bestOrder = -2;
+        for (int f = 0; f < 6; f++)
+        {
+            if (!on[f] || (dim == 2 && f >= 4)) continue;
+            if (s.face_order[f] > bestOrder) { bestOrder = s.face_order[f]; best = f; }
+        }
+        if (best >= 0)
+        {
+            const int kind = s.face_kind[best];
+            type = kind == NB_BC_INLET ? INFLOW
+                 : kind == NB_BC_OUTFLOW ? OUTFLOW
+                 : kind == NB_BC_PRESSURE_OUTLET ? (s.face_has_p[best] ? PRESSURE : EMPTY) : SOLID;
+        }
+        types[c] = (uint8_t)type;
+    }
+}
+
+void LaunchLabelCells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
+                      const nb_scene &s, uint8_t *types, cudaStream_t st)
+{
+    const long long cells = (long long)Nx * Ny * Nz;
+    int blocks = (int)((cells + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    NB_COUNT_LAUNCH();
+    k_label_cells<<<blocks, 256, 0, st>>>(dim, Nx, Ny, Nz, cx, cy, cz, s, types);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// IDP numbering (PressureSolver3D.cpp:133-139): interior FLUID cells in (i, j, k) order = the order of lines, then
+// the fast axis. Count per line, exclusive scan, then a warp-ballot prefix inside each line.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_line_counts(LevelView v, int *counts)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int line = warp; line < v.nLines; line += nw)
+    {
+        int cnt = 0;
+        for (int f0 = 0; f0 < v.lineLen; f0 += 32)
+        {
+            const int f = f0 + lane;
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f < v.lineLen ? f : 0, i, j, k, c);
+            const bool fl = f < v.lineLen && v.types[c] == FLUID;
+            cnt += __popc(__ballot_sync(0xffffffffu, fl));
+        }
+        if (lane == 0) counts[line] = cnt;
+    }
+}
+
+__global__ void k_line_number(LevelView v, const int *offsets, int32_t *idp)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int line = warp; line < v.nLines; line += nw)
+    {
+        int base = offsets[line];
+        for (int f0 = 0; f0 < v.lineLen; f0 += 32)
+        {
+            const int f = f0 + lane;
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f < v.lineLen ? f : 0, i, j, k, c);
+            const bool fl = f < v.lineLen && v.types[c] == FLUID;
+            const unsigned m = __ballot_sync(0xffffffffu, fl);
+            if (fl) idp[c] = base + __popc(m & ((1u << lane) - 1u));
+            base += __popc(m);
+        }
+    }
+}
+
+int NumberUnknowns(const LevelView &v, int32_t *idp, int *lineCounts, int *lineOffsets, void *scanTmp,
+                   size_t scanTmpBytes, int *hostTotal, cudaStream_t st)
+{
+    cudaMemsetAsync(idp, 0xFF, sizeof(int32_t) * (size_t)v.cells, st);
+    if (v.nLines <= 0 || v.lineLen <= 0) { *hostTotal = 0; return 0; }
+    const int blocks = LineGrid(v.nLines, 148 * 8);
+    NB_COUNT_LAUNCH();
+    k_line_counts<<<blocks, kBlock, 0, st>>>(v, lineCounts);
+    size_t bytes = scanTmpBytes;
+    cub::DeviceScan::ExclusiveSum(scanTmp, bytes, lineCounts, lineOffsets, v.nLines + 1, st);
+    NB_COUNT_LAUNCH();
+    k_line_number<<<blocks, kBlock, 0, st>>>(v, lineOffsets, idp);
+    int total = 0;
+    cudaMemcpyAsync(&total, lineOffsets + v.nLines, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    *hostTotal = total;
+    return 0;
+}
+
+size_t ScanTempBytes(int n)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int *)nullptr, (int *)nullptr, n, (cudaStream_t)0);
+    return bytes;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// the assembled matrix, exported as CSR (AssembleSystem + setFromTriplets): row lengths, scan, fill
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_row_lengths(LevelView v, const int32_t *idp, int *rowLen, int *dirichletFlag)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    int dir = 0;
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            const int row = idp[c];
+            if (row < 0) continue;
+            double cq[6];
+            int t[6];
+            CoefsExact(v, i, j, k, cq);
+            const double diag = DiagExact(v, i, j, k, c, cq, t);
+            int len = diag != 0.0 ? 1 : 0;
+            const int nq = v.dim == 3 ? 6 : 4;
+            for (int q = 0; q < nq; q++)
+            {
+                if (t[q] == FLUID)
+                {
+                    if (idp[c + NbrOffset(v, q)] >= 0) len++;
+                    else dir = 1;
+                }
+                if (IsDirichlet(t[q])) dir = 1;
+            }
+            rowLen[row] = len;
+        }
+    if (dir) atomicOr(dirichletFlag, 1);
+}
+
+__global__ void k_row_fill(LevelView v, const int32_t *idp, const int *rowPtr, int32_t *col, double *val, double scale)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    // ascending column order = ascending linear offset: i-1, j-1, k-1, diagonal, k+1, j+1, i+1
+    const int order3[7] = {1, 3, 5, -1, 4, 2, 0};
+    const int order2[5] = {1, 3, -1, 2, 0};
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            const int row = idp[c];
+            if (row < 0) continue;
+            double cq[6];
+            int t[6];
+            CoefsExact(v, i, j, k, cq);
+            const double diag = DiagExact(v, i, j, k, c, cq, t);
+            int e = rowPtr[row];
+            const int ne = v.dim == 3 ? 7 : 5;
+            for (int s = 0; s < ne; s++)
+            {
+                const int q = v.dim == 3 ? order3[s] : order2[s];
+                if (q < 0)
+                {
+                    if (diag != 0.0) { col[e] = row; val[e] = scale * diag; e++; }
+                    continue;
+                }
+                if (t[q] != FLUID) continue;
+                const int cl = idp[c + NbrOffset(v, q)];
+                if (cl < 0) continue;
+                col[e] = cl;
+                val[e] = scale * cq[q];
+                e++;
+            }
+        }
+}
+
+int ExportMatrix(const LevelView &v, const int32_t *idp, int n, double scale, int *rowLen, int *rowPtr,
+                 int32_t *col, double *val, int *flag, void *scanTmp, size_t scanTmpBytes, int *hostNnz,
+                 int *hostSingular, cudaStream_t st)
+{
+    cudaMemsetAsync(flag, 0, sizeof(int), st);
+    cudaMemsetAsync(rowLen, 0, sizeof(int) * (size_t)(n + 1), st);
+    const int blocks = LineGrid(v.nLines, 148 * 8);
+    if (v.nLines > 0)
+    {
+        NB_COUNT_LAUNCH();
+        k_row_lengths<<<blocks, kBlock, 0, st>>>(v, idp, rowLen, flag);
+    }
+    size_t bytes = scanTmpBytes;
+    cub::DeviceScan::ExclusiveSum(scanTmp, bytes, rowLen, rowPtr, n + 1, st);
+    if (v.nLines > 0 && n > 0)
+    {
+        NB_COUNT_LAUNCH();
+        k_row_fill<<<blocks, kBlock, 0, st>>>(v, idp, rowPtr, col, val, scale);
+    }
+    int nnz = 0, dir = 0;
+    cudaMemcpyAsync(&nnz, rowPtr + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&dir, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    *hostNnz = nnz;
+    *hostSingular = dir ? 0 : 1;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// divergence and right-hand side: MAC::GetDivergencyAt (src/MAC.cpp:349-367, 443-456), DirichletSum
+// (PressureSolver3D.cpp:248-260) and SolveScheme's loop (:288-298)
+// ---------------------------------------------------------------------------------------------------------------
+struct Faces
+{
+    const double *u, *v, *w;
+    long long uI, uJ, vI, vJ, wI, wJ; // strides of i and j in u, v, w (k stride 1)
+};
+
+__device__ __forceinline__ double DivergenceAt(const LevelView &g, const Faces &F, int i, int j, int k, double dh)
+{
+    const long long cu = i * F.uI + j * F.uJ + k, cv = i * F.vI + j * F.vJ + k;
+    if (g.dim == 2)
+    {
+        if (g.stretched)
+        {
+            const double dx = Wd(g, 0, j), dy = Wd(g, 1, i);
+            const double fluxU = (F.u[cu + F.uJ] - F.u[cu]) * dy;
+            const double fluxV = (F.v[cv + F.vI] - F.v[cv]) * dx;
+            return (fluxU + fluxV) / (dx * dy);
+        }
+        const double divU = (F.u[cu + F.uJ] - F.u[cu]) / dh;
+        const double divV = (F.v[cv + F.vI] - F.v[cv]) / dh;
+        return divU + divV;
+    }
+    const long long cw = i * F.wI + j * F.wJ + k;
+    if (g.stretched)
+    {
+        const double dx = Wd(g, 0, j), dy = Wd(g, 1, i), dz = Wd(g, 2, k);
+        const double fluxU = (F.u[cu + F.uJ] - F.u[cu]) * dy * dz;
+        const double fluxV = (F.v[cv + F.vI] - F.v[cv]) * dx * dz;
+        const double fluxW = (F.w[cw + 1] - F.w[cw]) * dx * dy;
+        return (fluxU + fluxV + fluxW) / (dx * dy * dz);
+    }
+    const double divU = (F.u[cu + F.uJ] - F.u[cu]) / dh;
+    const double divV = (F.v[cv + F.vI] - F.v[cv]) / dh;
+    const double divW = (F.w[cw + 1] - F.w[cw]) / dh;
+    return divU + divV + divW;
+}
+
+__global__ void k_rhs(LevelView v, Faces F, const double *p, double rhoDt, double scale, double dh, double *b)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            if (v.types[c] != FLUID) continue;
+            double cq[6];
+            CoefsExact(v, i, j, k, cq);
+            double ds = 0.0;
+            const int nq = v.dim == 3 ? 6 : 4;
+            for (int q = 0; q < nq; q++)
+            {
+                const long long n = c + NbrOffset(v, q);
+                const int t = v.types[n];
+                if (t == PRESSURE) ds += cq[q] * RingFactorExact(v, i, j, k, q, t) * p[n];
+            }
+            double vol = 1.0;
+            if (v.stretched) vol = v.dim == 3 ? Wd(v, 0, j) * Wd(v, 1, i) * Wd(v, 2, k) : Wd(v, 0, j) * Wd(v, 1, i);
+            b[c] = rhoDt * DivergenceAt(v, F, i, j, k, dh) * vol - scale * ds;
+        }
+}
+
+Faces MakeFaces(const LevelView &v, const double *u, const double *vv, const double *w)
+{
+    Faces F;
+    F.u = u; F.v = vv; F.w = w;
+    const long long Nx = v.Nx, Ny = v.Ny, Nz = v.Nz;
+    (void)Ny;
+    F.uJ = Nz; F.uI = (Nx + 1) * Nz;
+    F.vJ = Nz; F.vI = Nx * Nz;
+    F.wJ = Nz + 1; F.wI = Nx * (Nz + 1);
+    return F;
+}
+
+void LaunchRhs(const LevelView &v, const double *u, const double *vv, const double *w, const double *p, double rhoDt,
+               double scale, double dh, double *b, cudaStream_t st)
+{
+    if (v.nLines <= 0) return;
+    NB_COUNT_LAUNCH();
+    k_rhs<<<LineGrid(v.nLines, 148 * 8), kBlock, 0, st>>>(v, MakeFaces(v, u, vv, w), p, rhoDt, scale, dh, b);
+}
+
+// max |div u| over FLUID cells (the post-projection check)
+__global__ void k_max_div(LevelView v, Faces F, double dh, Reducer R, int slot)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    double m[1] = {0.0};
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            if (v.types[c] != FLUID) continue;
+            m[0] = fmax(m[0], fabs(DivergenceAt(v, F, i, j, k, dh)));
+        }
+    GridReduce<1>(R, m, slot, 1);
+}
+
+void LaunchMaxDiv(const LevelView &v, const double *u, const double *vv, const double *w, double dh,
+                  const Reducer &R, int slot, cudaStream_t st)
+{
+    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
+    NB_COUNT_LAUNCH();
+    k_max_div<<<blocks, kBlock, 0, st>>>(v, MakeFaces(v, u, vv, w), dh, R, slot);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// FP64 residual of the reference's matrix: r = b - A x, A = scale * (off-diagonals c_q, diagonal DiagExact).
+// Writes the unit-form residual -r/scale in T for the solver, sums ||r||^2 (and r for a singular system).
+// The refinement form also adds a correction e first: x_out = x_in + e, r = b - A x_out, read from the
+// neighbours' x_in + e, so x_in and x_out are different arrays.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T, bool kAdd>
+__global__ void k_residual64(LevelView v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
+                             double scale, double sfac, Reducer R, int slot)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    double acc[2] = {0.0, 0.0};
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            if (v.types[c] != FLUID) continue;
+            double cq[6];
+            int t[6];
+            CoefsExact(v, i, j, k, cq);
+            const double diag = DiagExact(v, i, j, k, c, cq, t);
+            const double xc = kAdd ? xin[c] + (double)e[c] : xin[c];
+            double off = 0.0;
+            const int nq = v.dim == 3 ? 6 : 4;
+            for (int q = 0; q < nq; q++)
+                if (t[q] == FLUID)
+                {
+                    const long long n = c + NbrOffset(v, q);
+                    const double xn = kAdd ? xin[n] + (double)e[n] : xin[n];
+                    off += cq[q] * xn;
+                }
+            const double ax = scale * (off + diag * xc);
+            const double r = b[c] - ax;
+            if (kAdd) xout[c] = xc;
+            rOut[c] = (T)(r * sfac);
+            acc[0] += r * r;
+            acc[1] += r;
+        }
+    GridReduce<2>(R, acc, slot);
+}
+
+template <typename T>
+void LaunchResidual64(const LevelView &v, const double *b, const double *x, T *rOut, double scale, double sfac,
+                      const Reducer &R, int slot, cudaStream_t st)
+{
+    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
+    NB_COUNT_LAUNCH();
+    k_residual64<T, false><<<blocks, kBlock, 0, st>>>(v, b, x, (const T *)nullptr, nullptr, rOut, scale, sfac, R, slot);
+}
+
+template <typename T>
+void LaunchRefine64(const LevelView &v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
+                    double scale, double sfac, const Reducer &R, int slot, cudaStream_t st)
+{
+    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
+    NB_COUNT_LAUNCH();
+    k_residual64<T, true><<<blocks, kBlock, 0, st>>>(v, b, xin, e, xout, rOut, scale, sfac, R, slot);
+}
+
+template void LaunchResidual64<float>(const LevelView &, const double *, const double *, float *, double, double,
+                                      const Reducer &, int, cudaStream_t);
+template void LaunchResidual64<double>(const LevelView &, const double *, const double *, double *, double, double,
+                                       const Reducer &, int, cudaStream_t);
+template void LaunchRefine64<float>(const LevelView &, const double *, const double *, const float *, double *,
+                                    float *, double, double, const Reducer &, int, cudaStream_t);
+template void LaunchRefine64<double>(const LevelView &, const double *, const double *, const double *, double *,
+                                     double *, double, double, const Reducer &, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------------------------------------------
+// level, scatter, ring (PressureSolver3D.cpp:181-187, 321-328; MAC::EnforcePressureBC src/MAC.cpp:866-871 replaying
+// BuildRingList :1064-1096 -- y faces, then x, then z; EMPTY 0, PRESSURE kept, any other ring cell copies inward)
+// ---------------------------------------------------------------------------------------------------------------
+
+// sum of x over the unknowns, compensated (Neumaier) per thread, then the deterministic reduction of (sum, carry)
+__global__ void k_sum_unknowns(LevelView v, const double *x, Reducer R, int slot)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    double s = 0.0, comp = 0.0;
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            if (v.types[c] != FLUID) continue;
+            const double a = x[c];
+            const double t = s + a;
+            comp += fabs(s) >= fabs(a) ? (s - t) + a : (a - t) + s;
+            s = t;
+        }
+    double acc[2] = {s, comp};
+    GridReduce<2>(R, acc, slot);
+}
+
+// x -= (out[slot] + out[slot+1]) / n at the unknowns, then optionally scatter into p.
+__global__ void k_sub_mean_scatter(LevelView v, double *x, const double *sums, int n, int sub, double *p)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const double mean = sub ? (sums[0] + sums[1]) / (double)n : 0.0;
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            if (v.types[c] != FLUID) continue;
+            const double y = x[c] - mean;
+            x[c] = y;
+            if (p) p[c] = y;
+        }
+}
+
+void LaunchSumUnknowns(const LevelView &v, const double *x, const Reducer &R, int slot, cudaStream_t st)
+{
+    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
+    NB_COUNT_LAUNCH();
+    k_sum_unknowns<<<blocks, kBlock, 0, st>>>(v, x, R, slot);
+}
+
+void LaunchSubMeanScatter(const LevelView &v, double *x, const double *sums, int n, int sub, double *p, cudaStream_t st)
+{
+    if (v.nLines <= 0) return;
+    NB_COUNT_LAUNCH();
+    k_sub_mean_scatter<<<LineGrid(v.nLines, 148 * 8), kBlock, 0, st>>>(v, x, sums, n, sub, p);
+}
+
+__device__ __forceinline__ void RingEntry(const LevelView &v, double *p, long long d, long long s)
+{
+    const int t = v.types[d];
+    if (t == EMPTY) p[d] = 0.0;
+    else if (t != PRESSURE) p[d] = p[s];
+}
+
+// pass 0: y faces (i = 0, Ny-1) over (j, k); pass 1: x faces (j = 0, Nx-1) over (i, k); pass 2: z faces over (i, j)
+__global__ void k_ring(LevelView v, double *p, int pass)
+{
+    const int Nx = v.Nx, Ny = v.Ny, Nz = v.Nz;
+    const long long A = pass == 0 ? Nx : Ny;
+    const long long B = pass == 2 ? Nx : Nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < A * B;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int a = (int)(t / B), b = (int)(t % B);
+        long long lo, loSrc, hi, hiSrc;
+        if (pass == 0)
+        {
+            lo = (long long)a * v.sJ + b; loSrc = lo + v.sI;
+            hi = (long long)(Ny - 1) * v.sI + lo; hiSrc = hi - v.sI;
+        }
+        else if (pass == 1)
+        {
+            lo = (long long)a * v.sI + b; loSrc = lo + v.sJ;
+            hi = lo + (long long)(Nx - 1) * v.sJ; hiSrc = hi - v.sJ;
+        }
+        else
+        {
+            lo = (long long)a * v.sI + (long long)b * v.sJ; loSrc = lo + 1;
+            hi = lo + (Nz - 1); hiSrc = hi - 1;
+        }
+        RingEntry(v, p, lo, loSrc);
+        RingEntry(v, p, hi, hiSrc);
+    }
+}
+
+void LaunchRing(const LevelView &v, double *p, cudaStream_t st)
+{
+    const int passes = v.dim == 3 ? 3 : 2;
+    for (int pass = 0; pass < passes; pass++)
+    {
+        const long long A = pass == 0 ? v.Nx : v.Ny;
+        const long long B = pass == 2 ? v.Nx : v.Nz;
+        int blocks = (int)((A * B + 255) / 256);
+        if (blocks > 148 * 4) blocks = 148 * 4;
+        if (blocks < 1) blocks = 1;
+        NB_COUNT_LAUNCH();
+        k_ring<<<blocks, 256, 0, st>>>(v, p, pass);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// the projection: ProjectPressure (PressureSolver3D.cpp:417-438; 2D :382-395), ProjectionGradient
+// (PressureSolver3D.cpp:405-414; 2D :370-379), MAC::GetGradP (MAC.h:149-154) and FaceGate (MAC.h:271-274):
+// u -= dt/rho * grad p on every face whose two cells are not SOLID. One thread per cell (i, j, k) updates the
+// low u, v, w faces of that cell that lie in their component's loop range.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double ProjGrad(const LevelView &g, int a, int i, int j, int k, long long c, const double *p)
+{
+    double grad;
+    if (a == 0) grad = (p[c] - p[c - g.sJ]) / Gp(g, 0, j - 1);
+    else if (a == 1) grad = (p[c] - p[c - g.sI]) / Gp(g, 1, i - 1);
+    else grad = (p[c] - p[c - 1]) / Gp(g, 2, k - 1);
+    const int n = a == 0 ? j : (a == 1 ? i : k);
+    const int N = a == 0 ? g.Nx : (a == 1 ? g.Ny : g.Nz);
+    if (g.dim == 2)
+    {
+        if (n == 1 && IsDirichlet(a == 0 ? g.types[(long long)i * g.sI] : g.types[(long long)j * g.sJ]))
+            return grad * DRF(g, a, 1, -1);
+        if (n == N - 1 && IsDirichlet(a == 0 ? g.types[(long long)i * g.sI + (long long)(N - 1) * g.sJ]
+                                             : g.types[(long long)(N - 1) * g.sI + (long long)j * g.sJ]))
+            return grad * DRF(g, a, N - 2, +1);
+        return grad;
+    }
+    if (n != 1 && n != N - 1) return grad;
+    const int r = n == 1 ? 0 : N - 1;
+    const long long rc = a == 0 ? (long long)i * g.sI + (long long)r * g.sJ + k
+                       : (a == 1 ? (long long)r * g.sI + (long long)j * g.sJ + k
+                                 : (long long)i * g.sI + (long long)j * g.sJ + r);
+    if (!IsDirichlet(g.types[rc])) return grad;
+    return n == 1 ? grad * DRF(g, a, 1, -1) : grad * DRF(g, a, N - 2, +1);
+}
+
+__global__ void k_project(LevelView g, double *u, double *v, double *w, const double *p, double f)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + (g.dim == 3 ? 1 : 0);
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z + 1;
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
+    const int kEnd = g.dim == 3 ? Nz : 1; // w faces run to Nz-1; u, v stop at Nz-2
+    if (j > Nx - 1 || i > Ny - 1 || k >= kEnd) return;
+    const long long c = (long long)i * g.sI + (long long)j * g.sJ + k;
+    const int tc = g.types[c];
+    const bool kIn = g.dim == 2 || k <= Nz - 2;
+    // u face (i, j, k): i in [1, Ny-2], j in [1, Nx-1], k in [1, Nz-2]
+    if (i <= Ny - 2 && kIn)
+    {
+        if (!(tc == SOLID || g.types[c - g.sJ] == SOLID))
+        {
+            const long long fu = ((long long)i * (Nx + 1) + j) * Nz + k;
+            u[fu] = u[fu] - f * ProjGrad(g, 0, i, j, k, c, p);
+        }
+    }
+    // v face: i in [1, Ny-1], j in [1, Nx-2]
+    if (j <= Nx - 2 && kIn)
+    {
+        if (!(tc == SOLID || g.types[c - g.sI] == SOLID))
+        {
+            const long long fv = ((long long)i * Nx + j) * Nz + k;
+            v[fv] = v[fv] - f * ProjGrad(g, 1, i, j, k, c, p);
+        }
+    }
+    // w face: i in [1, Ny-2], j in [1, Nx-2], k in [1, Nz-1]
+    if (g.dim == 3 && i <= Ny - 2 && j <= Nx - 2)
+    {
+        if (!(tc == SOLID || g.types[c - 1] == SOLID))
+        {
+            const long long fw = ((long long)i * Nx + j) * (Nz + 1) + k;
+            w[fw] = w[fw] - f * ProjGrad(g, 2, i, j, k, c, p);
+        }
+    }
+}
+
+void LaunchProject(const LevelView &g, double *u, double *v, double *w, const double *p, double dtOverRho,
+                   cudaStream_t st)
+{
+    const int kCount = g.dim == 3 ? g.Nz - 1 : 1;
+    const int jCount = g.Nx - 1, iCount = g.Ny - 1;
+    if (kCount <= 0 || jCount <= 0 || iCount <= 0) return;
+    dim3 block(g.dim == 3 ? 32 : 1, g.dim == 3 ? 8 : 256);
+    dim3 grid((kCount + block.x - 1) / block.x, (jCount + block.y - 1) / block.y, iCount);
+    NB_COUNT_LAUNCH();
+    k_project<<<grid, block, 0, st>>>(g, u, v, w, p, dtOverRho);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// compact <-> grid through IDP, and the cell volume (SolveLaplacian, PressureSolver3D.cpp:355-371)
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_gather(LevelView v, const int32_t *idp, const double *grid, double *compact)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            const int r = idp[c];
+            if (r >= 0) compact[r] = grid[c];
+        }
+}
+
+__global__ void k_scatter_volume(LevelView v, const int32_t *idp, const double *compact, double *grid, int volume)
+{
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int line = warp; line < v.nLines; line += nw)
+        for (int f = lane; f < v.lineLen; f += 32)
+        {
+            int i, j, k;
+            long long c;
+            LineCell(v, line, f, i, j, k, c);
+            const int r = idp[c];
+            if (r < 0) continue;
+            double vol = 1.0;
+            if (volume && v.stretched)
+                vol = v.dim == 3 ? Wd(v, 0, j) * Wd(v, 1, i) * Wd(v, 2, k) : Wd(v, 0, j) * Wd(v, 1, i);
+            grid[c] = compact[r] * vol;
+        }
+}
+
+void LaunchGather(const LevelView &v, const int32_t *idp, const double *grid, double *compact, cudaStream_t st)
+{
+    if (v.nLines <= 0) return;
+    NB_COUNT_LAUNCH();
+    k_gather<<<LineGrid(v.nLines, 148 * 8), kBlock, 0, st>>>(v, idp, grid, compact);
+}
+
+void LaunchScatterVolume(const LevelView &v, const int32_t *idp, const double *compact, double *grid, int volume,
+                         cudaStream_t st)
+{
+    if (v.nLines <= 0) return;
+    NB_COUNT_LAUNCH();
+    k_scatter_volume<<<LineGrid(v.nLines, 148 * 8), kBlock, 0, st>>>(v, idp, compact, grid, volume);
+}
+
+} // namespace nb

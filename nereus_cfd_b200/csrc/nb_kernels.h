@@ -1,0 +1,80 @@
+// Host-side declarations of the B200 pressure-projection kernels' launchers.
+#pragma once
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/nereus_b200.h"
+#include "nb_device.cuh"
+
+namespace nb
+{
+
+// Kernel launches made by this library in this process (nereus_b200_kernel_launches).
+extern std::atomic<long long> g_launches;
+#define NB_COUNT_LAUNCH() ::nb::g_launches.fetch_add(1, std::memory_order_relaxed)
+
+// ---- nb_exact.cu: reference-exact kernels ----
+void LaunchLabelCells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
+                      const nb_scene &s, uint8_t *types, cudaStream_t st);
+int NumberUnknowns(const LevelView &v, int32_t *idp, int *lineCounts, int *lineOffsets, void *scanTmp,
+                   size_t scanTmpBytes, int *hostTotal, cudaStream_t st);
+size_t ScanTempBytes(int n);
+int ExportMatrix(const LevelView &v, const int32_t *idp, int n, double scale, int *rowLen, int *rowPtr,
+                 int32_t *col, double *val, int *flag, void *scanTmp, size_t scanTmpBytes, int *hostNnz,
+                 int *hostSingular, cudaStream_t st);
+void LaunchRhs(const LevelView &v, const double *u, const double *vv, const double *w, const double *p, double rhoDt,
+               double scale, double dh, double *b, cudaStream_t st);
+void LaunchMaxDiv(const LevelView &v, const double *u, const double *vv, const double *w, double dh,
+                  const Reducer &R, int slot, cudaStream_t st);
+template <typename T>
+void LaunchResidual64(const LevelView &v, const double *b, const double *x, T *rOut, double scale, double sfac,
+                      const Reducer &R, int slot, cudaStream_t st);
+template <typename T>
+void LaunchRefine64(const LevelView &v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
+                    double scale, double sfac, const Reducer &R, int slot, cudaStream_t st);
+void LaunchSumUnknowns(const LevelView &v, const double *x, const Reducer &R, int slot, cudaStream_t st);
+void LaunchSubMeanScatter(const LevelView &v, double *x, const double *sums, int n, int sub, double *p,
+                          cudaStream_t st);
+void LaunchRing(const LevelView &v, double *p, cudaStream_t st);
+void LaunchProject(const LevelView &g, double *u, double *v, double *w, const double *p, double dtOverRho,
+                   cudaStream_t st);
+void LaunchGather(const LevelView &v, const int32_t *idp, const double *grid, double *compact, cudaStream_t st);
+void LaunchScatterVolume(const LevelView &v, const int32_t *idp, const double *compact, double *grid, int volume,
+                         cudaStream_t st);
+
+// ---- nb_kernels.cu: multigrid and PCG kernels, T = float (inner solve) or double (plain FP64) ----
+void LaunchCoarsenTypes(const LevelView &fine, const LevelView &coarse, uint8_t *coarseTypes, cudaStream_t st);
+
+template <typename T> void LaunchSmoothFirst(const LevelView &v, const T *r, T *e, cudaStream_t st);
+template <typename T> void LaunchSmooth(const LevelView &v, const T *r, T *e, int colour, cudaStream_t st);
+template <typename T> void LaunchLevelResidual(const LevelView &v, const T *r, const T *e, T *res, cudaStream_t st);
+template <typename T>
+void LaunchRestrict(const LevelView &fine, const LevelView &coarse, const T *resFine, T *rCoarse, cudaStream_t st);
+template <typename T>
+void LaunchProlong(const LevelView &fine, const LevelView &coarse, const T *eCoarse, T *eFine, cudaStream_t st);
+template <typename T> void LaunchCoarseSolve(const LevelView &v, const T *r, T *e, int sweeps, cudaStream_t st);
+
+// PCG on the unit-form operator M = -A/scale of level 0. A singular (all-Neumann) system removes the mean of the
+// preconditioned residual z over the unknowns; its effect on r.z is carried in the scalars, so z itself is not
+// rewritten: with S[b..b+2] = (sum r.z, sum z, sum r), rz_eff = S[b] - (S[b+1]/n) S[b+2].
+//   dot:   out[base..base+2] = (sum r.z, sum z, sum r)
+//   pupd:  beta = first ? 0 : rz_eff(new)/rz_eff(old); pOut = (z - mean) + beta pIn; q = M pOut;
+//          out[slotPQ] = sum pOut.q
+//   xr:    alpha = rz_eff/S[pq]; x += alpha p; r -= alpha q; out[slotRR] = sum r.r
+template <typename T>
+void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, int base, cudaStream_t st);
+template <typename T>
+void LaunchUpdatePApply(const LevelView &v, const T *z, const T *pIn, T *pOut, T *q, const Reducer &R,
+                        const double *S, int first, int baseNew, int baseOld, int n, int singular, int slotPQ,
+                        int exact, cudaStream_t st);
+template <typename T>
+void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p, const T *q, const Reducer &R, const double *S,
+                    int baseRZ, int n, int singular, int slotPQ, int slotRR, cudaStream_t st);
+// y = s * x over the level's unknowns (x and y may alias)
+template <typename Tin, typename Tout>
+void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaStream_t st);
+
+} // namespace nb

@@ -1,0 +1,738 @@
+// Host orchestration of the B200 pressure projection (see nb_solver.h).
+//
+// The pressure step follows PressureSolver3D::SolveScheme + ProjectPressure (src/Methods/PPESolver/
+// PressureSolver3D.cpp:279-328, 417-438): ring, right-hand side, compatibility, solve, level, scatter, ring,
+// projection. The solve replaces Eigen's diagonal-preconditioned CG (PressureSettings.h:386-481) by a matrix-free
+// multigrid-preconditioned CG, in FP64 or as FP32 MG-PCG inside FP64 iterative refinement.
+#include "nb_solver.h"
+
+#include <algorithm>
+
+namespace nb
+{
+
+// ---------------------------------------------------------------------------------------------------------------
+// levels
+// ---------------------------------------------------------------------------------------------------------------
+LevelView LevelData::view() const
+{
+    LevelView v{};
+    v.dim = dim;
+    v.Nx = Nx;
+    v.Ny = Ny;
+    v.Nz = Nz;
+    v.cells = cells;
+    if (dim == 3)
+    {
+        v.sI = (long long)Nx * Nz;
+        v.sJ = Nz;
+        v.nLines = (Ny - 2) * (Nx - 2);
+        v.lineLen = Nz - 2;
+        v.lineDiv = Nx - 2;
+    }
+    else
+    {
+        v.sI = Nx;
+        v.sJ = 1;
+        v.nLines = Ny - 2;
+        v.lineLen = Nx - 2;
+        v.lineDiv = 1;
+    }
+    if (v.nLines < 0 || v.lineLen <= 0) v.nLines = 0;
+    if (v.lineDiv <= 0) v.lineDiv = 1;
+    v.types = types.p;
+    v.stretched = stretched ? 1 : 0;
+    v.gamma = gamma;
+    for (int a = 0; a < 3; a++)
+    {
+        v.w[a] = dw[a].p;
+        v.g[a] = dg[a].p;
+        v.w32[a] = dw32[a].p;
+        v.ig32[a] = dig32[a].p;
+    }
+    return v;
+}
+
+template <> float *LevelData::r<float>() { return r32.p; }
+template <> double *LevelData::r<double>() { return r64.p; }
+template <> float *LevelData::e<float>() { return e32.p; }
+template <> double *LevelData::e<double>() { return e64.p; }
+template <> float *LevelData::res<float>() { return res32.p; }
+template <> double *LevelData::res<double>() { return res64.p; }
+
+static void UploadTables(LevelData &Lv, cudaStream_t st)
+{
+    for (int a = 0; a < 3; a++)
+    {
+        Lv.dw[a].upload(Lv.w[a].data(), Lv.w[a].size(), st);
+        Lv.dg[a].upload(Lv.g[a].data(), Lv.g[a].size(), st);
+        std::vector<float> w32(Lv.w[a].begin(), Lv.w[a].end()), ig32(Lv.g[a].size());
+        for (size_t q = 0; q < ig32.size(); q++) ig32[q] = (float)(1.0 / Lv.g[a][q]);
+        Lv.dw32[a].upload(w32.data(), w32.size(), st);
+        Lv.dig32[a].upload(ig32.data(), ig32.size(), st);
+    }
+    NB_CK(cudaStreamSynchronize(st)); // the host vectors above are temporaries
+}
+
+// Coarse padded tables of one axis: interior widths summed in pairs, the ring mirroring its neighbour
+// (MAC::AddRing), padded and gapped like MAC::PadTable / MAC::GapTable.
+static void CoarseAxis(const std::vector<double> &wFine, int Nf, int Nc, std::vector<double> &wOut,
+                       std::vector<double> &gOut)
+{
+    // wFine is padded: Width(n) = wFine[n + 1], n = -1..Nf
+    const int nf = Nf - 2, m = Nc - 2;
+    std::vector<double> size(Nc);
+    for (int I = 1; I <= m; I++)
+    {
+        const int a = 2 * I - 1, b = 2 * I;
+        size[I] = wFine[a + 1] + (b <= nf ? wFine[b + 1] : 0.0);
+    }
+    size[0] = size[1];
+    size[Nc - 1] = size[m];
+    wOut.resize(Nc + 2);
+    for (int q = -1; q <= Nc; q++) wOut[q + 1] = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
+    gOut.resize(Nc + 1);
+    for (int q = -1; q <= Nc - 1; q++)
+    {
+        const double a = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
+        const double b = size[q + 1 >= Nc ? Nc - 1 : q + 1];
+        gOut[q + 1] = 0.5 * (a + b);
+    }
+}
+
+void Context::BuildHierarchy()
+{
+    L.clear();
+    L.reserve(32);
+    {
+        LevelData L0;
+        L0.dim = dim;
+        L0.Nx = Nx;
+        L0.Ny = Ny;
+        L0.Nz = Nz;
+        L0.cells = (long long)Nx * Ny * Nz;
+        L0.stretched = nonuniform;
+        L0.gamma = 1.0;
+        for (int a = 0; a < 3; a++) { L0.w[a] = wt[a]; L0.g[a] = gt[a]; }
+        L0.types.upload(layout.data(), layout.size(), st);
+        UploadTables(L0, st);
+        L.push_back(std::move(L0));
+    }
+    const int maxLevels = std::max(1, opt.max_levels);
+    while ((int)L.size() < maxLevels)
+    {
+        const LevelData &F = L.back();
+        const int nx = F.Nx - 2, ny = F.Ny - 2, nz = dim == 3 ? F.Nz - 2 : 1;
+        const int mn = dim == 3 ? std::min(nx, std::min(ny, nz)) : std::min(nx, ny);
+        const long long interior = (long long)nx * ny * nz;
+        if (mn < 8 || interior <= 512) break;
+        LevelData C;
+        C.dim = dim;
+        C.Nx = (nx + 1) / 2 + 2;
+        C.Ny = (ny + 1) / 2 + 2;
+        C.Nz = dim == 3 ? (nz + 1) / 2 + 2 : 1;
+        C.cells = (long long)C.Nx * C.Ny * C.Nz;
+        C.stretched = F.stretched;
+        C.gamma = F.gamma * (dim == 3 ? 2.0 : 1.0);
+        CoarseAxis(F.w[0], F.Nx, C.Nx, C.w[0], C.g[0]);
+        CoarseAxis(F.w[1], F.Ny, C.Ny, C.w[1], C.g[1]);
+        if (dim == 3) CoarseAxis(F.w[2], F.Nz, C.Nz, C.w[2], C.g[2]);
+        else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }
+        C.types.alloc((size_t)C.cells);
+        UploadTables(C, st);
+        LaunchCoarsenTypes(F.view(), C.view(), C.types.p, st);
+        L.push_back(std::move(C));
+    }
+    NB_CK(cudaGetLastError());
+}
+
+void Context::AllocVectors()
+{
+    const bool mixed = opt.precision == NB_PRECISION_MIXED;
+    for (size_t l = 0; l < L.size(); l++)
+    {
+        LevelData &Lv = L[l];
+        const size_t c = (size_t)Lv.cells;
+        const bool last = l + 1 == L.size();
+        if (mixed)
+        {
+            Lv.r32.alloc(c); Lv.r32.zero(st);
+            Lv.e32.alloc(c); Lv.e32.zero(st);
+            if (!last) { Lv.res32.alloc(c); Lv.res32.zero(st); }
+            Lv.r64.release(); Lv.e64.release(); Lv.res64.release();
+        }
+        else
+        {
+            Lv.r64.alloc(c); Lv.r64.zero(st);
+            Lv.e64.alloc(c); Lv.e64.zero(st);
+            if (!last) { Lv.res64.alloc(c); Lv.res64.zero(st); }
+            Lv.r32.release(); Lv.e32.release(); Lv.res32.release();
+        }
+    }
+    const size_t c = Cells();
+    b.alloc(c); b.zero(st);
+    xa.alloc(c); xa.zero(st);
+    xb.alloc(c); xb.zero(st);
+    if (mixed)
+    {
+        for (auto &a : p32) { a.alloc(c); a.zero(st); }
+        q32.alloc(c); q32.zero(st);
+        x32.alloc(c); x32.zero(st);
+        for (auto &a : p64) a.release();
+        q64.release();
+    }
+    else
+    {
+        for (auto &a : p64) { a.alloc(c); a.zero(st); }
+        q64.alloc(c); q64.zero(st);
+        for (auto &a : p32) a.release();
+        q32.release();
+        x32.release();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------------------------------------------
+Context::Context(const nb_options &o) : opt(o)
+{
+    device = o.device;
+    NB_CK(cudaSetDevice(device));
+    if (o.stream)
+        st = (cudaStream_t)o.stream;
+    else
+    {
+        NB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        ownStream = true;
+    }
+    red.maxBlocks = 148 * 8;
+    partials.alloc((size_t)red.maxBlocks * 4);
+    slots.alloc(S_COUNT);
+    slots.zero(st);
+    counter.alloc(1);
+    counter.zero(st);
+    red.partials = partials.p;
+    red.out = slots.p;
+    red.counter = counter.p;
+    NB_CK(cudaMallocHost((void **)&hostSlots, sizeof(double) * S_COUNT));
+    NB_CK(cudaEventCreate(&ev0));
+    NB_CK(cudaEventCreate(&ev1));
+}
+
+Context::~Context()
+{
+    if (st) cudaStreamSynchronize(st);
+    for (cudaEvent_t e : evPool) cudaEventDestroy(e);
+    if (hostSlots) cudaFreeHost(hostSlots);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    L.clear();
+    if (ownStream && st) cudaStreamDestroy(st);
+}
+
+// ---- per-kernel timing: events from a pool, bracketing launches of the selected kernel ids ----
+void Context::ProfBegin(int id, double bytes)
+{
+    if (!(profMask >> id & 1u)) return;
+    if (evUsed + 2 > evPool.size())
+        for (int q = 0; q < 256; q++)
+        {
+            cudaEvent_t e;
+            NB_CK(cudaEventCreate(&e));
+            evPool.push_back(e);
+        }
+    profA = evPool[evUsed++];
+    NB_CK(cudaEventRecord(profA, st));
+    profOpen = id;
+    profBytes = bytes;
+}
+
+void Context::ProfEnd()
+{
+    if (profOpen < 0) return;
+    cudaEvent_t b = evPool[evUsed++];
+    NB_CK(cudaEventRecord(b, st));
+    prof.push_back({profOpen, profA, b, profBytes});
+    profOpen = -1;
+}
+
+void Context::ProfClear()
+{
+    prof.clear();
+    evUsed = 0;
+    profOpen = -1;
+}
+
+void Context::ProfRead(int id, int *launches, double *ms, double *bytesPerLaunch)
+{
+    NB_CK(cudaStreamSynchronize(st));
+    int cnt = 0;
+    double t = 0.0, by = 0.0;
+    for (const ProfRecord &r : prof)
+        if (r.id == id)
+        {
+            float m = 0.0f;
+            NB_CK(cudaEventElapsedTime(&m, r.a, r.b));
+            t += m;
+            by += r.bytes;
+            cnt++;
+        }
+    *launches = cnt;
+    *ms = t;
+    *bytesPerLaunch = cnt ? by / cnt : 0.0;
+}
+
+double Context::ReadSlot(int s)
+{
+    NB_CK(cudaMemcpyAsync(hostSlots + s, slots.p + s, sizeof(double), cudaMemcpyDeviceToHost, st));
+    NB_CK(cudaStreamSynchronize(st));
+    return hostSlots[s];
+}
+
+void Context::ReadSlots(int s, int count)
+{
+    NB_CK(cudaMemcpyAsync(hostSlots + s, slots.p + s, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+    NB_CK(cudaStreamSynchronize(st));
+}
+
+void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *types, const double *const width[3],
+                        const double *const gap[3], int nonUniform, double dh_)
+{
+    if (dim_ != 2 && dim_ != 3) throw InputError("dim must be 2 or 3");
+    if (dim_ == 2) Nz_ = 1;
+    if (Nx_ < 2 || Ny_ < 2 || Nz_ < 1 || (dim_ == 3 && Nz_ < 2)) throw InputError("grid too small");
+    if (!types || !width || !gap) throw InputError("null layout pointer");
+    for (int a = 0; a < (dim_ == 3 ? 3 : 2); a++)
+        if (!width[a] || !gap[a]) throw InputError("null spacing table");
+    if (!nonUniform && !(dh_ > 0.0)) throw InputError("uniform grid needs dh > 0");
+    const size_t cells = (size_t)Nx_ * Ny_ * Nz_;
+    for (size_t c = 0; c < cells; c++)
+        if (types[c] > 5) throw InputError("cell type out of range");
+    const int N[3] = {Nx_, Ny_, Nz_};
+    bool same = built && dim_ == dim && Nx_ == Nx && Ny_ == Ny && Nz_ == Nz && (nonUniform != 0) == nonuniform &&
+                dh_ == dh && layout.size() == cells && std::memcmp(layout.data(), types, cells) == 0;
+    for (int a = 0; a < 3 && same; a++)
+    {
+        const size_t nw = (size_t)N[a] + 2, ng = (size_t)N[a] + 1;
+        if (a == 2 && dim_ == 2) continue;
+        same = wt[a].size() == nw && gt[a].size() == ng && std::memcmp(wt[a].data(), width[a], nw * 8) == 0 &&
+               std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
+    }
+    if (same) return; // PressureLayoutChanged: nothing moved
+    dim = dim_;
+    Nx = Nx_;
+    Ny = Ny_;
+    Nz = Nz_;
+    nonuniform = nonUniform != 0;
+    dh = dh_;
+    scale = nonuniform ? 1.0 : 1.0 / (dh * dh); // MatrixScale3D (PressureSolver3D.cpp:34-37)
+    layout.assign(types, types + cells);
+    for (int a = 0; a < 3; a++)
+    {
+        if (a == 2 && dim == 2)
+        {
+            const double w0 = width[2] ? width[2][1] : (width[0] ? width[0][1] : 1.0);
+            wt[2].assign(3, w0);
+            gt[2].assign(2, w0);
+            continue;
+        }
+        wt[a].assign(width[a], width[a] + N[a] + 2);
+        gt[a].assign(gap[a], gap[a] + N[a] + 1);
+        for (double x : wt[a])
+            if (!(x > 0.0) || !std::isfinite(x)) throw InputError("width table entries must be positive");
+        for (double x : gt[a])
+            if (!(x > 0.0) || !std::isfinite(x)) throw InputError("gap table entries must be positive");
+    }
+    built = false;
+    BuildHierarchy();
+    // IDP numbering and the singular flag
+    const LevelView v0 = L[0].view();
+    idp.alloc(cells);
+    lineCounts.alloc((size_t)std::max(v0.nLines, 0) + 1);
+    lineOffsets.alloc((size_t)std::max(v0.nLines, 0) + 1);
+    lineCounts.zero(st);
+    size_t need = std::max(ScanTempBytes(std::max(v0.nLines, 0) + 1), ScanTempBytes(1 << 20));
+    if (need > scanTmpBytes)
+    {
+        scanTmp.alloc(need);
+        scanTmpBytes = need;
+    }
+    int total = 0;
+    NumberUnknowns(v0, idp.p, lineCounts.p, lineOffsets.p, scanTmp.p, scanTmpBytes, &total, st);
+    n = total;
+    // singular: no FLUID row touches a Dirichlet neighbour or a FLUID ring cell (AssembleSystem's `dirichlet`)
+    {
+        bool dir = false;
+        const int nq = dim == 3 ? 6 : 4;
+        const long long sI = dim == 3 ? (long long)Nx * Nz : Nx, sJ = dim == 3 ? Nz : 1;
+        const long long off[6] = {sI, -sI, sJ, -sJ, 1, -1};
+        for (int i = 1; i < Ny - 1 && !dir; i++)
+            for (int j = 1; j < Nx - 1 && !dir; j++)
+                for (int k = dim == 3 ? 1 : 0; k < (dim == 3 ? Nz - 1 : 1) && !dir; k++)
+                {
+                    const long long c = (long long)i * sI + (long long)j * sJ + k;
+                    if (layout[c] != FLUID) continue;
+                    for (int q = 0; q < nq; q++)
+                    {
+                        const long long nb = c + off[q];
+                        const int t = layout[nb];
+                        if (IsDirichlet(t)) { dir = true; break; }
+                        if (t == FLUID)
+                        {
+                            const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3);
+                            const int nk = k + (q == 4) - (q == 5);
+                            const bool ring = ni == 0 || ni == Ny - 1 || nj == 0 || nj == Nx - 1 ||
+                                              (dim == 3 && (nk == 0 || nk == Nz - 1));
+                            if (ring) { dir = true; break; }
+                        }
+                    }
+                }
+        singular = !dir;
+    }
+    AllocVectors();
+    NB_CK(cudaStreamSynchronize(st));
+    built = true;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// multigrid V-cycle and PCG
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T> void Context::VCycle(int l, T *r, T *e)
+{
+    LevelData &Lv = L[l];
+    const LevelView v = Lv.view();
+    const double s = sizeof(T), cells = (double)Lv.cells;
+    // kernel id and algorithmic bytes per launch (each array touched once) for the finest level's kernels
+    auto prof = [&](int id, double bytesPerCell) {
+        ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
+    };
+    if (l + 1 == (int)L.size())
+    {
+        prof(NB_K_COARSE, 0.0);
+        LaunchCoarseSolve<T>(v, r, e, opt.coarse_sweeps, st);
+        ProfEnd();
+        return;
+    }
+    const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
+    const double half = (3.0 * s + 1.0) / 2.0; // one red-black sweep reads e, r, types and writes e: 3s + 1
+    prof(NB_K_SMOOTH0, 2.0 * s + 1.0);
+    LaunchSmoothFirst<T>(v, r, e, st);
+    ProfEnd();
+    prof(NB_K_SMOOTH0, half);
+    LaunchSmooth<T>(v, r, e, 1, st);
+    ProfEnd();
+    for (int q = 1; q < pre; q++)
+    {
+        prof(NB_K_SMOOTH0, half);
+        LaunchSmooth<T>(v, r, e, 0, st);
+        ProfEnd();
+        prof(NB_K_SMOOTH0, half);
+        LaunchSmooth<T>(v, r, e, 1, st);
+        ProfEnd();
+    }
+    T *res = Lv.res<T>();
+    prof(NB_K_RESIDUAL0, 3.0 * s + 1.0);
+    LaunchLevelResidual<T>(v, r, e, res, st);
+    ProfEnd();
+    LevelData &Lc = L[l + 1];
+    const LevelView vc = Lc.view();
+    prof(NB_K_RESTRICT0, s + s / 8.0);
+    LaunchRestrict<T>(v, vc, res, Lc.r<T>(), st);
+    ProfEnd();
+    VCycle<T>(l + 1, Lc.r<T>(), Lc.e<T>());
+    prof(NB_K_PROLONG0, 2.0 * s + s / 8.0 + 1.0);
+    LaunchProlong<T>(v, vc, Lc.e<T>(), e, st);
+    ProfEnd();
+    for (int q = 0; q < post; q++)
+    {
+        prof(NB_K_SMOOTH0, half);
+        LaunchSmooth<T>(v, r, e, 1, st);
+        ProfEnd();
+        prof(NB_K_SMOOTH0, half);
+        LaunchSmooth<T>(v, r, e, 0, st);
+        ProfEnd();
+    }
+}
+
+template <typename T>
+int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
+                    double *rrEnd)
+{
+    const LevelView v0 = L[0].view();
+    T *p[2] = {p0, p1};
+    NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * Cells(), st));
+    double rr = rrStart;
+    int it = 0;
+    while (it < maxIt && rr > rrTarget)
+    {
+        VCycle<T>(0, r, z);
+        const int baseNew = (it & 1) ? S_RZ1 : S_RZ0, baseOld = (it & 1) ? S_RZ0 : S_RZ1;
+        const double s = sizeof(T), cells = (double)Cells();
+        ProfBegin(NB_K_DOT, 2.0 * s * cells);
+        LaunchDot<T>(v0, r, z, red, baseNew, st);
+        ProfEnd();
+        T *pin = p[it & 1], *pout = p[(it + 1) & 1];
+        ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
+        LaunchUpdatePApply<T>(v0, z, pin, pout, q, red, slots.p, it == 0, baseNew, baseOld, n, singular ? 1 : 0,
+                              S_PQ, exact ? 1 : 0, st);
+        ProfEnd();
+        ProfBegin(NB_K_XR, 6.0 * s * cells);
+        LaunchUpdateXR<T>(v0, x, r, pout, q, red, slots.p, baseNew, n, singular ? 1 : 0, S_PQ, S_RR, st);
+        ProfEnd();
+        rr = ReadSlot(S_RR);
+        it++;
+        if (!std::isfinite(rr)) break;
+    }
+    NB_CK(cudaGetLastError());
+    *rrEnd = rr;
+    return it;
+}
+
+int Context::SolveMixed(double tol, double **xOut, nb_result *out)
+{
+    const LevelView v0 = L[0].view();
+    const double sfac = -1.0 / scale;
+    double *x = xa.p, *xo = xb.p;
+    xa.zero(st);
+    float *r32 = L[0].r32.p, *z32 = L[0].e32.p;
+    ProfBegin(NB_K_REFINE, (8.0 + 8.0 + 1.0 + 4.0) * (double)Cells());
+    LaunchResidual64<float>(v0, b.p, x, r32, scale, sfac, red, S_RES, st);
+    ProfEnd();
+    const double bn2 = ReadSlot(S_RES);
+    out->b_norm = std::sqrt(bn2);
+    int outer = 0, inner = 0, status = NB_OK;
+    double rr64 = bn2;
+    if (bn2 > 0.0)
+    {
+        const int maxOuter = std::max(1, opt.max_outer);
+        while (true)
+        {
+            if (std::sqrt(rr64 / bn2) <= tol) break;
+            if (outer >= maxOuter || !std::isfinite(rr64)) { status = NB_NOT_CONVERGED; break; }
+            x32.zero(st);
+            double rrEnd = 0.0;
+            const double rr0 = rr64 * sfac * sfac;
+            inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0,
+                                   rr0 * opt.inner_tol * opt.inner_tol, std::max(1, opt.max_iters), false, &rrEnd);
+            ProfBegin(NB_K_REFINE, (8.0 + 4.0 + 8.0 + 1.0 + 8.0 + 4.0) * (double)Cells());
+            LaunchRefine64<float>(v0, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);
+            ProfEnd();
+            std::swap(x, xo);
+            rr64 = ReadSlot(S_RES);
+            outer++;
+        }
+    }
+    out->iters_outer = outer;
+    out->iters_inner = inner;
+    out->rel_res = bn2 > 0.0 ? std::sqrt(rr64 / bn2) : 0.0;
+    *xOut = x;
+    return status;
+}
+
+int Context::SolveFP64(double tol, double **xOut, nb_result *out)
+{
+    const LevelView v0 = L[0].view();
+    const double sfac = -1.0 / scale;
+    double *x = xa.p;
+    xa.zero(st);
+    double *r = L[0].r64.p, *z = L[0].e64.p;
+    ProfBegin(NB_K_REFINE, (8.0 + 8.0 + 1.0 + 8.0) * (double)Cells());
+    LaunchResidual64<double>(v0, b.p, x, r, scale, sfac, red, S_RES, st);
+    ProfEnd();
+    const double bn2 = ReadSlot(S_RES);
+    out->b_norm = std::sqrt(bn2);
+    int its = 0, status = NB_OK, restarts = 0;
+    double rr = bn2;
+    if (bn2 > 0.0)
+    {
+        const int maxIt = std::max(1, opt.max_iters) * std::max(1, opt.max_outer);
+        while (true)
+        {
+            if (std::sqrt(rr / bn2) <= tol) break;
+            if (its >= maxIt || restarts > 4 || !std::isfinite(rr)) { status = NB_NOT_CONVERGED; break; }
+            double rrEnd = 0.0;
+            // the recursive residual is driven a little below the target, then checked against the true one
+            const double target = 0.25 * tol * tol * bn2 * sfac * sfac;
+            its += RunPCG<double>(x, r, z, p64[0].p, p64[1].p, q64.p, rr * sfac * sfac, target, maxIt - its, true,
+                                  &rrEnd);
+            ProfBegin(NB_K_REFINE, (8.0 + 8.0 + 1.0 + 8.0) * (double)Cells());
+            LaunchResidual64<double>(v0, b.p, x, r, scale, sfac, red, S_RES, st);
+            ProfEnd();
+            rr = ReadSlot(S_RES);
+            restarts++;
+        }
+    }
+    out->iters_outer = restarts;
+    out->iters_inner = its;
+    out->rel_res = bn2 > 0.0 ? std::sqrt(rr / bn2) : 0.0;
+    *xOut = x;
+    return status;
+}
+
+int Context::Solve(double tol, double **xOut, nb_result *out)
+{
+    if (!(tol > 0.0)) throw InputError("tolerance must be positive");
+    if (n == 0)
+    {
+        xa.zero(st);
+        *xOut = xa.p;
+        out->b_norm = 0.0;
+        out->rel_res = 0.0;
+        out->iters_inner = out->iters_outer = 0;
+        return NB_OK;
+    }
+    return opt.precision == NB_PRECISION_MIXED ? SolveMixed(tol, xOut, out) : SolveFP64(tol, xOut, out);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// the pressure step and projection
+// ---------------------------------------------------------------------------------------------------------------
+int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rho, double dt, int compat, double tol,
+                           nb_result *out, bool solve, bool correct)
+{
+    if (!built) throw InputError("set_layout has not been called");
+    if (!u || !v || !p || (dim == 3 && !w)) throw InputError("null field pointer");
+    if (!(rho > 0.0) || !(dt > 0.0)) throw InputError("rho and dt must be positive");
+    std::memset(out, 0, sizeof(*out));
+    out->n = n;
+    out->singular = singular ? 1 : 0;
+    out->levels = (int)L.size();
+    const LevelView v0 = L[0].view();
+    NB_CK(cudaEventRecord(ev0, st));
+    if (!solve)
+    {
+        ProfBegin(NB_K_PROJECT, (8.0 + 1.0 + 6.0 * 8.0) * (double)Cells());
+        LaunchProject(v0, u, v, w, p, dt / rho, st);
+        ProfEnd();
+        LaunchMaxDiv(v0, u, v, w, dh, red, S_DIV, st);
+        NB_CK(cudaEventRecord(ev1, st));
+        NB_CK(cudaGetLastError());
+        out->max_div = ReadSlot(S_DIV);
+        float ms = 0.0f;
+        NB_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        out->seconds = ms * 1e-3;
+        out->status = NB_OK;
+        return NB_OK;
+    }
+    LaunchRing(v0, p, st); // EnforcePressureBC at the start of SolveScheme
+    ProfBegin(NB_K_RHS, (3.0 * 8.0 + 1.0 + 8.0) * (double)Cells());
+    LaunchRhs(v0, u, v, w, p, rho / dt, scale, dh, b.p, st);
+    ProfEnd();
+    const bool compatOn = compat && singular && n > 0;
+    if (compatOn)
+        for (int pass = 0; pass < 2; pass++) // b -= mean(b), twice (PressureSolver3D.cpp:300-307)
+        {
+            LaunchSumUnknowns(v0, b.p, red, S_SUM, st);
+            LaunchSubMeanScatter(v0, b.p, slots.p + S_SUM, n, 1, nullptr, st);
+        }
+    double *x = nullptr;
+    const int status = Solve(tol, &x, out);
+    // LevelPressure's mean removal (PressureSolver3D.cpp:181-187), then the scatter into p
+    if (compatOn) LaunchSumUnknowns(v0, x, red, S_SUM, st);
+    LaunchSubMeanScatter(v0, x, slots.p + S_SUM, n, compatOn ? 1 : 0, p, st);
+    LaunchRing(v0, p, st);
+    if (correct)
+    {
+        ProfBegin(NB_K_PROJECT, (8.0 + 1.0 + 6.0 * 8.0) * (double)Cells());
+        LaunchProject(v0, u, v, w, p, dt / rho, st);
+        ProfEnd();
+        LaunchMaxDiv(v0, u, v, w, dh, red, S_DIV, st);
+    }
+    NB_CK(cudaEventRecord(ev1, st));
+    NB_CK(cudaGetLastError());
+    out->max_div = correct ? ReadSlot(S_DIV) : -1.0;
+    NB_CK(cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    NB_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    out->seconds = ms * 1e-3;
+    out->status = status;
+    lastIterations = out->iters_inner;
+    return status;
+}
+
+int Context::SolveLaplacian(const double *f, double *xh, double tol, nb_result *out)
+{
+    if (!built) throw InputError("set_layout has not been called");
+    std::memset(out, 0, sizeof(*out));
+    out->n = n;
+    out->singular = singular ? 1 : 0;
+    out->levels = (int)L.size();
+    out->max_div = -1.0;
+    if (n == 0) return NB_BAD_INPUT; // SolveLaplacian returns false on an empty system
+    const LevelView v0 = L[0].view();
+    DevArray<double> fc;
+    fc.upload(f, (size_t)n, st);
+    b.zero(st);
+    LaunchScatterVolume(v0, idp.p, fc.p, b.p, 1, st); // b = f * CellVolume (PressureSolver3D.cpp:360-369)
+    NB_CK(cudaEventRecord(ev0, st));
+    double *x = nullptr;
+    const int status = Solve(tol, &x, out);
+    NB_CK(cudaEventRecord(ev1, st));
+    LaunchGather(v0, idp.p, x, fc.p, st);
+    NB_CK(cudaMemcpyAsync(xh, fc.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    NB_CK(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    NB_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    out->seconds = ms * 1e-3;
+    out->status = status;
+    lastIterations = out->iters_inner;
+    return status;
+}
+
+void Context::Rhs(const double *u, const double *v, const double *w, const double *p, double rho, double dt,
+                  double *bOut)
+{
+    if (!built) throw InputError("set_layout has not been called");
+    const LevelView v0 = L[0].view();
+    DevArray<double> U, V, W, P, bc;
+    U.upload(u, FieldSizeU(), st);
+    V.upload(v, FieldSizeV(), st);
+    if (dim == 3) W.upload(w, FieldSizeW(), st);
+    P.upload(p, Cells(), st);
+    LaunchRing(v0, P.p, st);
+    b.zero(st);
+    LaunchRhs(v0, U.p, V.p, W.p, P.p, rho / dt, scale, dh, b.p, st);
+    bc.alloc((size_t)std::max(n, 1));
+    LaunchGather(v0, idp.p, b.p, bc.p, st);
+    if (n) NB_CK(cudaMemcpyAsync(bOut, bc.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    NB_CK(cudaStreamSynchronize(st));
+}
+
+void Context::ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnzOut, int *singularOut)
+{
+    if (!built) throw InputError("set_layout has not been called");
+    const LevelView v0 = L[0].view();
+    const size_t cap = (size_t)std::max(n, 1) * (dim == 3 ? 7 : 5);
+    DevArray<int> rowLen, rowPtr, flag;
+    DevArray<int32_t> c;
+    DevArray<double> vv;
+    rowLen.alloc((size_t)n + 1);
+    rowPtr.alloc((size_t)n + 1);
+    flag.alloc(1);
+    c.alloc(cap);
+    vv.alloc(cap);
+    int nnz = 0, sing = 0;
+    nb::ExportMatrix(v0, idp.p, n, scale, rowLen.p, rowPtr.p, c.p, vv.p, flag.p, scanTmp.p, scanTmpBytes, &nnz, &sing,
+                     st);
+    NB_CK(cudaMemcpyAsync(rowptr, rowPtr.p, sizeof(int) * ((size_t)n + 1), cudaMemcpyDeviceToHost, st));
+    if (nnz)
+    {
+        NB_CK(cudaMemcpyAsync(col, c.p, sizeof(int32_t) * (size_t)nnz, cudaMemcpyDeviceToHost, st));
+        NB_CK(cudaMemcpyAsync(val, vv.p, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToHost, st));
+    }
+    NB_CK(cudaStreamSynchronize(st));
+    *nnzOut = nnz;
+    *singularOut = sing;
+}
+
+void Context::GetIdp(int32_t *out)
+{
+    if (!built) throw InputError("set_layout has not been called");
+    NB_CK(cudaMemcpyAsync(out, idp.p, sizeof(int32_t) * Cells(), cudaMemcpyDeviceToHost, st));
+    NB_CK(cudaStreamSynchronize(st));
+}
+
+template void Context::VCycle<float>(int, float *, float *);
+template void Context::VCycle<double>(int, double *, double *);
+
+} // namespace nb

@@ -1,0 +1,200 @@
+// Host orchestration of the B200 pressure projection: the multigrid hierarchy, the PCG and refinement drivers, the
+// projection pipeline. One Context serves one grid on one device and stream.
+#pragma once
+
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nb_kernels.h"
+
+namespace nb
+{
+
+struct CudaError : std::runtime_error
+{
+    cudaError_t code;
+    CudaError(const char *what, cudaError_t c)
+        : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+struct InputError : std::runtime_error
+{
+    explicit InputError(const std::string &s) : std::runtime_error(s) {}
+};
+
+#define NB_CK(x)                                                                                                   \
+    do                                                                                                             \
+    {                                                                                                              \
+        cudaError_t e_ = (x);                                                                                      \
+        if (e_ != cudaSuccess) throw ::nb::CudaError(#x, e_);                                                      \
+    } while (0)
+
+template <typename T> struct DevArray
+{
+    T *p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray &) = delete;
+    DevArray &operator=(const DevArray &) = delete;
+    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevArray &operator=(DevArray &&o) noexcept
+    {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevArray() { release(); }
+    void alloc(size_t count)
+    {
+        if (count == n && p) return;
+        release();
+        if (count)
+        {
+            cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+            if (e != cudaSuccess) { p = nullptr; throw CudaError("cudaMalloc", e); }
+        }
+        n = count;
+    }
+    void zero(cudaStream_t st) { if (p && n) NB_CK(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
+    void upload(const T *h, size_t count, cudaStream_t st)
+    {
+        alloc(count);
+        if (count) NB_CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// scalar slots of the reducer
+enum : int
+{
+    S_RZ0 = 0,   // (r.z, sum z, sum r), even iterations
+    S_RZ1 = 3,   // ... odd iterations
+    S_PQ = 6,
+    S_RR = 7,
+    S_RES = 8,   // ||b - A x||^2, sum (b - A x)
+    S_SUM = 10,  // compensated sum (sum, carry)
+    S_DIV = 12,
+    S_COUNT = 16
+};
+
+struct LevelData
+{
+    int dim = 3, Nx = 0, Ny = 0, Nz = 1;
+    long long cells = 0;
+    bool stretched = false;
+    double gamma = 1.0;
+    std::vector<double> w[3], g[3];
+    DevArray<double> dw[3], dg[3];
+    DevArray<float> dw32[3], dig32[3];
+    DevArray<uint8_t> types;
+    DevArray<float> r32, e32, res32;
+    DevArray<double> r64, e64, res64;
+    LevelView view() const;
+    template <typename T> T *r();
+    template <typename T> T *e();
+    template <typename T> T *res();
+};
+
+struct Context
+{
+    nb_options opt{};
+    int device = 0;
+    cudaStream_t st = nullptr;
+    bool ownStream = false;
+
+    // layout
+    bool built = false;
+    int dim = 3, Nx = 0, Ny = 0, Nz = 1;
+    bool nonuniform = false;
+    double dh = 1.0, scale = 1.0;
+    std::vector<uint8_t> layout;
+    std::vector<double> wt[3], gt[3];
+    std::vector<LevelData> L;
+    DevArray<int32_t> idp;
+    int n = 0;
+    bool singular = false;
+    DevArray<int> lineCounts, lineOffsets;
+    DevArray<uint8_t> scanTmp;
+    size_t scanTmpBytes = 0;
+
+    // solver vectors on level 0 (grid layout)
+    DevArray<double> b, xa, xb;
+    DevArray<float> p32[2], q32, x32;
+    DevArray<double> p64[2], q64;
+
+    // fields for the host-buffer entry points
+    DevArray<double> du, dv, dw, dp;
+
+    // reductions
+    DevArray<double> partials, slots;
+    DevArray<unsigned> counter;
+    double *hostSlots = nullptr; // pinned
+    Reducer red{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    int lastIterations = 0;
+
+    // per-kernel device timing (nereus_b200_profile_*)
+    struct ProfRecord
+    {
+        int id;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    unsigned profMask = 0;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    std::vector<ProfRecord> prof;
+    int profOpen = -1;
+    cudaEvent_t profA = nullptr;
+    double profBytes = 0.0;
+    void ProfBegin(int id, double bytes);
+    void ProfEnd();
+    void ProfClear();
+    void ProfRead(int id, int *launches, double *ms, double *bytesPerLaunch);
+
+    Context(const nb_options &o);
+    ~Context();
+
+    void SetLayout(int dim, int Nx, int Ny, int Nz, const uint8_t *types, const double *const width[3],
+                   const double *const gap[3], int nonUniform, double dh);
+    // The pressure step and projection on device fields; returns the nb_status.
+    // solve: the pressure step (ring, RHS, compatibility, solve, level, scatter, ring); correct: the velocity
+    // correction with the p that results.
+    int ProjectDevice(double *u, double *v, double *w, double *p, double rho, double dt, int compat, double tol,
+                      nb_result *out, bool solve = true, bool correct = true);
+    int SolveLaplacian(const double *f, double *x, double tol, nb_result *out);
+    void Rhs(const double *u, const double *v, const double *w, const double *p, double rho, double dt, double *bOut);
+    void ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singularOut);
+    void GetIdp(int32_t *out);
+
+    LevelView View0() const { return L[0].view(); }
+    size_t FieldSizeU() const { return (size_t)(Nx + 1) * Ny * Nz; }
+    size_t FieldSizeV() const { return (size_t)Nx * (Ny + 1) * Nz; }
+    size_t FieldSizeW() const { return dim == 3 ? (size_t)Nx * Ny * (Nz + 1) : 0; }
+    size_t Cells() const { return (size_t)Nx * Ny * Nz; }
+
+  private:
+    void BuildHierarchy();
+    void AllocVectors();
+    double ReadSlot(int s);
+    void ReadSlots(int s, int count);
+    // Solve A x = b (b in this->b, grid layout); the solution ends in *xOut (xa or xb). Fills out->iters/rel_res.
+    int Solve(double tol, double **xOut, nb_result *out);
+    int SolveMixed(double tol, double **xOut, nb_result *out);
+    int SolveFP64(double tol, double **xOut, nb_result *out);
+    template <typename T> void VCycle(int l, T *r, T *e);
+    template <typename T>
+    int RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
+               double *rrEnd);
+};
+
+} // namespace nb

@@ -325,12 +325,14 @@ int main(int argc, char **argv)
     int iters = PRESSURE_TELEMETRY.lastIterations;
     const int repeats = h[13];
     double tWarm = 0.0;
+    std::vector<double> tEach(repeats > 0 ? repeats : 0);
     for (int r = 0; r < repeats; r++)
     {
         t1 = Now();
         if (dim == 3) PressureSolver3D::SolvePressure(nullptr, &grid, nullptr, time);
         else PressureSolver2D::SolvePressure(nullptr, &grid, nullptr, time);
-        tWarm += Now() - t1;
+        tEach[r] = Now() - t1;
+        tWarm += tEach[r];
     }
     if (repeats > 0) tWarm /= repeats;
 
@@ -394,6 +396,9 @@ int main(int argc, char **argv)
         const int32_t nc = (int32_t)grid.centreTable[a].size();
         WriteN(o, &nc, 1); WriteN(o, grid.centreTable[a].data(), nc);
     }
+    const int32_t nr = (int32_t)tEach.size();
+    WriteN(o, &nr, 1);
+    WriteN(o, tEach.data(), tEach.size());
     std::fclose(o);
     return 0;
 }

@@ -60,6 +60,7 @@ class RefResult:
     width: list
     gap: list
     centre: list
+    t_each: np.ndarray  # wall time of each warm repeat
 
 
 def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000,
@@ -127,8 +128,12 @@ def read_result(path, dim) -> RefResult:
         gap.append(take("<f8", ng))
         (nc,) = struct.unpack_from("<i", data, off); off += 4
         centre.append(take("<f8", nc))
+    t_each = np.zeros(0)
+    if off + 4 <= len(data):
+        (nr,) = struct.unpack_from("<i", data, off); off += 4
+        t_each = take("<f8", nr)
     return RefResult(Nx, Ny, Nz, n, iters, bool(sing), thr, tA, tC, tW, tP, rr, md, dh, types, idp, rowptr, col, val,
-                     b_raw, b, x, p, u, v, w, width, gap, centre)
+                     b_raw, b, x, p, u, v, w, width, gap, centre, t_each)
 
 
 def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000, threads=1,

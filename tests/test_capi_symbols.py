@@ -1,0 +1,72 @@
+"""The C ABI library (CPU side): it builds for sm_100a, loads, exports every entry point include/nereus_b200.h
+declares with the ctypes signature the bindings use, and refuses to run without a GPU instead of falling back."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT, cuda_ok
+from nereus_cfd_b200 import build, capi
+
+HEADER = os.path.join(ROOT, "include", "nereus_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nereus_b200_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return capi.load()
+
+
+def test_header_declares_the_survey_entry_points():
+    syms = declared_symbols()
+    for s in ["nereus_b200_create", "nereus_b200_destroy", "nereus_b200_set_layout", "nereus_b200_project",
+              "nereus_b200_solve_laplacian"]:
+        assert s in syms
+
+
+def test_every_declared_symbol_is_exported(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+        assert s in capi.SIGNATURES, "no ctypes signature for %s" % s
+    out = subprocess.run(["nm", "-D", "--defined-only", capi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\b(nereus_b200_\w+)\b", out))
+    assert set(syms) <= exported
+
+
+def test_built_for_sm100a_only():
+    flags = " ".join(build.ARCH)
+    assert "arch=compute_100a,code=sm_100a" in flags
+    assert len(re.findall(r"-gencode", flags)) == 1
+
+
+def test_default_options(lib):
+    o = capi.default_options()
+    assert o.precision == capi.PRECISION_MIXED
+    assert o.max_iters > 0 and o.max_outer > 0 and 0 < o.inner_tol < 1
+    assert o.pre_sweeps >= 1 and o.post_sweeps >= 1 and o.max_levels >= 1
+
+
+@pytest.mark.skipif(cuda_ok(), reason="checks the no-GPU behaviour")
+def test_no_device_is_an_error_not_a_fallback(lib):
+    ctx = ctypes.c_void_p()
+    st = lib.nereus_b200_create(ctypes.byref(ctx), None)
+    assert st == capi.NB_NO_DEVICE
+    assert not ctx
+    assert lib.nereus_b200_device_count() == 0
+
+
+def test_null_arguments_are_bad_input(lib):
+    assert lib.nereus_b200_create(None, None) == capi.NB_BAD_INPUT
+    assert lib.nereus_b200_project(None, None, None, None, None, 1.0, 1.0, 0, 0, 1e-8, None) == capi.NB_BAD_INPUT
+    assert lib.nereus_b200_system_size(None) == 0
+    lib.nereus_b200_destroy(None)  # a no-op
