@@ -1,0 +1,409 @@
+"""Benchmark of the B200 pressure projection: solves/s and p50/p99 latency at a 1e-8 relative residual.
+
+Workload (the configuration the metric is quoted on, one GPU): 3D 256^3 unit cube, uniform, a voxelised solid sphere
+at (0.5, 0.5, 0.5) radius 0.15 sampled at cell centres, no-slip walls, a p = 0 pressure outlet on x = 1; face
+velocities N(0,1) FP64 from a seeded SplitMix64/Box-Muller generator (synthetic data), zeroed on solid faces.
+A step is one pressure projection of that field: divergence/right-hand side, FP32 MG-PCG inside FP64 iterative
+refinement to ||b - A x|| / ||b|| <= 1e-8, level, scatter, ring, velocity correction. Each step restores the
+unprojected fields by a device copy first (inside the timed region), so every step solves the full problem; the
+552 MB of fields read per step are larger than the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank projects its own field (seeded per rank): weak scaling, no
+collective on the data path; the timing is the max over ranks.
+
+The JSON line also carries the plain single-solve FP64 MG-PCG form on the same workload, the roofline of the
+dominant kernel (CUDA events around its launches over the timed region, algorithmic bytes per launch), the end-to-end
+number through the C ABI with host buffers, the reference's CPU path timed on this host, clocks sampled during the
+timed region and the count of this library's kernel launches.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s, p50/p99 latency at 1e-8 rel residual: batched mixed vs plain FP64"
+TOL = 1e-8
+
+
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q
+    lo, hi = int(k), min(int(k) + 1, len(xs) - 1)
+    return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/*.md line
+    'traffic_bytes_per_launch <kernel> <bytes> <cells>'), scaled to the bench's cell count by the caller."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, fn)):
+            parts = line.strip().strip("`").split()
+            if len(parts) == 4 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                return float(parts[2]), float(parts[3])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, val in zip(names[1:], p[5:9]):
+                if val.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# the workload
+# ---------------------------------------------------------------------------------------------------------------------
+def make_workload(n: int, seed: int):
+    from nereus_cfd_b200 import capi, workloads as W
+
+    case = W.sphere_outlet_3d(n, seed=seed)
+    types = capi.label_cells(case.grid, case.scene)
+    u, v, w = W.face_velocities(case.grid, types, case.seed)
+    return case, types, u, v, w
+
+
+def run_b200(args, rank, world, dist):
+    import torch
+
+    from nereus_cfd_b200 import capi
+    from nereus_cfd_b200.pressure import MACGrid, PressureSolver
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = capi.load()
+    case, types, u, v, w = make_workload(args.size, seed=2 + 1000 * rank)
+    g = case.grid
+    stream = torch.cuda.current_stream()
+    td = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to("cuda")
+    U0, V0, W0 = td(u), td(v), td(w)
+    P0 = torch.zeros(g.cells, dtype=torch.float64, device="cuda")
+    U, V, Wf, P = U0.clone(), V0.clone(), W0.clone(), P0.clone()
+    mac = MACGrid.from_case(case, types, u, v, w)
+
+    def project_steps(solver, steps, times=None, start=None):
+        res = capi.Result()
+        for _ in range(steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            U.copy_(U0); V.copy_(V0); Wf.copy_(W0); P.copy_(P0)
+            st = lib.nereus_b200_project_device(solver.ctx, U.data_ptr(), V.data_ptr(), Wf.data_ptr(),
+                                                P.data_ptr(), case.rho, case.dt, 0, TOL, ctypes.byref(res))
+            capi.check(st)
+            e1.record(stream)
+            if times is not None:
+                times.append((e0, e1))
+        return res
+
+    def timed(solver, steps, warmup, profile_mask=0, clocks=False):
+        project_steps(solver, warmup)
+        capi.check(lib.nereus_b200_profile_enable(solver.ctx, profile_mask))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(dev) if clocks else None
+        if sampler:
+            sampler.start()
+        launches0 = lib.nereus_b200_kernel_launches()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        times = []
+        start.record(stream)
+        res = project_steps(solver, steps, times)
+        end.record(stream)
+        torch.cuda.synchronize()
+        launches = lib.nereus_b200_kernel_launches() - launches0
+        clk = sampler.stop() if sampler else None
+        if dist:
+            dist.barrier()
+        total_ms = start.elapsed_time(end)
+        lat = [a.elapsed_time(b) for a, b in times]
+        prof = capi.profile_read(lib, solver.ctx) if profile_mask else {}
+        capi.check(lib.nereus_b200_profile_enable(solver.ctx, 0))
+        return total_ms, lat, res, launches, clk, prof
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- the chosen form: FP32 MG-PCG inside FP64 refinement ----
+    mixed = PressureSolver("mixed", device=dev, stream=stream.cuda_stream)
+    mixed.InitializePressureSolver(mac)
+    total_ms, lat, res, launches, clk, prof = timed(mixed, args.steps, args.warmup,
+                                                   profile_mask=(1 << 11) - 1, clocks=True)
+    total_ms = max_over_ranks(total_ms)
+    value = world * args.steps / (total_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (largest summed device time over the timed region) ----
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if prof:
+        name, (cnt, ms, bpl) = max(((k, v) for k, v in prof.items() if v[2] > 0), key=lambda kv: kv[1][1])
+        per_launch_s = ms / cnt / 1e3
+        achieved = bpl / per_launch_s / 1e9
+        tr = ncu_traffic(name)
+        traffic = None
+        if tr:
+            traffic = tr[0] * (g.cells / tr[1])
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bpl, "launches": cnt, "avg_launch_us": round(per_launch_s * 1e6, 2),
+                "share_of_timed_region": round(ms / max(sum(x[1] for x in prof.values()), 1e-9), 4),
+                "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
+                                "GB/s": round(v[2] / (v[1] / v[0] / 1e3) / 1e9, 1) if v[2] else None}
+                            for k, v in prof.items()}}
+    mixed_res = res.as_dict()
+    mixed.DestroyPressureSolver()
+
+    # ---- the plain single-solve FP64 MG-PCG form on the same workload ----
+    fp64 = None
+    if not args.no_fp64:
+        plain = PressureSolver("fp64", device=dev, stream=stream.cuda_stream)
+        plain.InitializePressureSolver(mac)
+        ksteps = max(3, min(args.steps, args.fp64_steps))
+        t64, lat64, r64, _, _, _ = timed(plain, ksteps, 1)
+        t64 = max_over_ranks(t64)
+        v64 = world * ksteps / (t64 / 1e3)
+        fp64 = {"value": round(v64, 3), "unit": "solves/s", "steps": ksteps,
+                "p50_ms": round(percentile(lat64, 0.5), 3), "p99_ms": round(percentile(lat64, 0.99), 3),
+                "iters": r64.iters_inner, "rel_res": r64.rel_res, "speedup_mixed_over_fp64": round(value / v64, 3)}
+        plain.DestroyPressureSolver()
+
+    # ---- end to end through the C ABI with host buffers (pinned), H2D + D2H inside every step ----
+    e2e = None
+    if not args.no_e2e:
+        s = PressureSolver("mixed", device=dev)
+        s.InitializePressureSolver(mac)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).pin_memory().numpy()
+        hu0, hv0, hw0 = pin(u), pin(v), pin(w)
+        hp0 = np.zeros(g.cells)
+        hu, hv, hw, hp = pin(u), pin(v), pin(w), pin(hp0)
+        res = capi.Result()
+
+        def call():
+            np.copyto(hu, hu0); np.copyto(hv, hv0); np.copyto(hw, hw0); np.copyto(hp, hp0)
+            t0 = time.perf_counter()
+            capi.check(lib.nereus_b200_project(s.ctx, capi.ptr(hu), capi.ptr(hv), capi.ptr(hw), capi.ptr(hp),
+                                               case.rho, case.dt, 0, 0, TOL, ctypes.byref(res)))
+            return time.perf_counter() - t0
+
+        for _ in range(max(1, args.warmup)):
+            call()
+        ke = max(3, min(args.steps, args.e2e_steps))
+        if dist:
+            dist.barrier()
+        ts = [call() for _ in range(ke)]
+        tot = max_over_ranks(sum(ts))
+        nbytes = 8 * (hu.size + hv.size + hw.size + hp.size)
+        e2e = {"value": round(world * ke / tot, 3), "unit": "solves/s", "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": ke, "p50_ms": round(1e3 * percentile(ts, 0.5), 3),
+               "p99_ms": round(1e3 * percentile(ts, 0.99), 3), "api": "nereus_b200_project (host buffers)"}
+        s.DestroyPressureSolver()
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 MG-PCG in f64 refinement", "data": "synthetic",
+        "config": {"workload": "sphere_outlet_3d_%d" % args.size,
+                   "grid": "%dx%dx%d cells incl. ring, uniform, unit cube" % (g.Nx, g.Ny, g.Nz),
+                   "unknowns": mixed_res["n"], "tol": TOL, "precision": "mixed",
+                   "parallelism": "replicas x%d" % world, "levels": mixed_res["levels"],
+                   "l2": "inputs larger than L2 (552 MB of fields per step), restored by device copy in each step"},
+        "latency_ms": {"p50": round(percentile(lat, 0.5), 3), "p99": round(percentile(lat, 0.99), 3)},
+        "solve": {k: mixed_res[k] for k in ("iters_outer", "iters_inner", "rel_res", "max_div", "status")},
+        "fp64_plain": fp64, "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": int(launches),
+    }
+    return out
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# the reference's CPU path (oracle/_ref: the reference's own sources compiled here)
+# ---------------------------------------------------------------------------------------------------------------------
+def reference_cpu(size: int, steps: int, warmup: int, threads: int):
+    """Warm AMGCL solves (the reference's fastest CPU pressure path, SA + SPAI0 + CG, eigen_solver=AMG) of the
+    sphere-outlet workload at `size`^3 plus one projection, all host threads. Returns per-solve seconds."""
+    from nereus_cfd_b200 import workloads as W
+    from oracle import cpu, refcase
+
+    case = W.sphere_outlet_3d(size, seed=2)
+    types = cpu.label_cells(case.grid, case.scene)
+    u, v, w = W.face_velocities(case.grid, types, case.seed)
+    r = refcase.run(case, u, v, w, label_mode=1, types=types, solver=refcase.SOLVER_AMG, tol=TOL, threads=threads,
+                    repeats=steps + warmup, timeout=3600)
+    per = [float(t) + r.t_project for t in r.t_each[warmup:]]
+    return per, r
+
+
+def cpu_baseline_entry(args, scale_size):
+    from oracle import refcase
+
+    if not refcase.available():
+        return None
+    threads = os.cpu_count() or 1
+    per, r = reference_cpu(scale_size, max(2, min(args.steps, 5)), 1, threads)
+    ratio = ((scale_size + 2) ** 3) / float((args.size + 2) ** 3)
+    val = ratio / statistics.mean(per)
+    return {"value": round(val, 4), "unit": "solves/s", "cores": threads, "kind": "reference",
+            "sample": "reference AMGCL SA+SPAI0 CG (eigen_solver=AMG) warm solve to 1e-8 + ProjectPressure of the "
+                      "same sphere-outlet workload at %d^3 (%d solves, %.3f s each, %d iterations), scaled by the "
+                      "cell ratio %.4f to %d^3" % (scale_size, len(per), statistics.mean(per), r.iters, ratio,
+                                                   args.size)}
+
+
+def run_reference(args, rank, world):
+    from oracle import refcase
+
+    if rank != 0:
+        return None
+    if not refcase.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/ref_harness was not built (reference sources absent)"}
+    threads = os.cpu_count() or 1
+    sample = args.ref_size
+    per, r = reference_cpu(sample, args.steps, args.warmup, threads)
+    ratio = ((sample + 2) ** 3) / float((args.size + 2) ** 3)
+    lat = [t / ratio for t in per]  # seconds per full-size-equivalent solve
+    total = sum(lat)
+    value = args.steps / total
+    desc = ("reference AMGCL SA+SPAI0 CG (eigen_solver=AMG), warm, to 1e-8, + ProjectPressure; each step one solve "
+            "of the sphere-outlet workload at %d^3, scaled by the cell ratio %.4f to %d^3; %d host threads"
+            % (sample, ratio, args.size, threads))
+    return {"metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "sphere_outlet_3d_%d" % args.size, "tol": TOL, "precision": "fp64",
+                       "parallelism": "host threads x%d" % threads, "sample": desc},
+            "latency_ms": {"p50": round(1e3 * percentile(lat, 0.5), 3), "p99": round(1e3 * percentile(lat, 0.99), 3)},
+            "cpu_baseline": {"value": round(value, 4), "unit": "solves/s", "cores": threads, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": round(value, 4), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--ref-size", type=int, default=128, help="reference sample size (cells per side)")
+    ap.add_argument("--fp64-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = td
+    # the CPU baseline runs before any GPU work, on rank 0 at N = 1 only
+    cpu_base = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu_base = cpu_baseline_entry(args, args.ref_size)
+        except Exception as e:  # reported, never fatal to the GPU line
+            cpu_base = {"unavailable": str(e)[:200]}
+    out = run_b200(args, rank, world, dist)
+    out["cpu_baseline"] = cpu_base
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,132 @@
+// nereus_b200_solver.hpp -- C++ host side of the B200 pressure projection, shaped like the reference's
+// PressureSolver3D / PressureSolver2D static classes (src/Methods/PPESolver/PressureSolver3D.h:49-75) so that a NEREUS
+// build can route its pressure step through include/nereus_b200.h with the same calls, argument meaning and error
+// behaviour. Header-only; link with nereus_cfd_b200/libnereus_b200.so.
+//
+// The grid is passed as a view of the MAC's arrays (src/headers/Core/MAC.h:424-448): sizes with the ring, the cell
+// types, the padded Width / FaceGap tables and the four fields, all host memory owned by the caller.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nereus_b200.h"
+
+namespace nereus_b200
+{
+
+// What the pressure step reads and writes of a MAC grid.
+struct GridView
+{
+    int dim = 3;
+    int Nx = 0, Ny = 0, Nz = 1;     // ring included; Nz = 1 in 2D
+    bool nonUniform = false;
+    double dh = 0.0;                // MAC::dh (the uniform cell size)
+    const uint8_t *cellTypes = nullptr;
+    const double *width[3] = {nullptr, nullptr, nullptr}; // padded Width tables, N + 2 entries
+    const double *gap[3] = {nullptr, nullptr, nullptr};   // padded FaceGap tables, N + 1 entries
+    double *u = nullptr, *v = nullptr, *w = nullptr, *p = nullptr;
+};
+
+struct Error : std::runtime_error
+{
+    int status;
+    Error(int s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+inline void Check(int status)
+{
+    if (status != NB_OK && status != NB_NOT_CONVERGED) throw Error(status, nereus_b200_last_error());
+}
+
+// One pressure system on one GPU, the role the reference's static SYSTEM/IDP play per dimension.
+class PressureSolver
+{
+  public:
+    explicit PressureSolver(int precision = NB_PRECISION_MIXED, int device = 0)
+    {
+        nereus_b200_default_options(&opt_);
+        opt_.precision = precision;
+        opt_.device = device;
+    }
+    ~PressureSolver() { DestroyPressureSolver(); }
+    PressureSolver(const PressureSolver &) = delete;
+    PressureSolver &operator=(const PressureSolver &) = delete;
+
+    nb_options &Options() { return opt_; }
+
+    // InitializePressureSolver (PressureSolver3D.cpp:89-102): backend up, system assembled for this layout.
+    void InitializePressureSolver(const GridView &g, int scheme = NB_SCHEME_CHORIN)
+    {
+        if (scheme != NB_SCHEME_CHORIN) throw Error(NB_BAD_INPUT, "only the Chorin scheme is served");
+        if (!ctx_) Check(nereus_b200_create(&ctx_, &opt_));
+        EnsureSystem(g);
+    }
+
+    // EnsureSystem (PressureSolver3D.cpp:120-124): the library rebuilds only when the cell types changed.
+    void EnsureSystem(const GridView &g)
+    {
+        Check(nereus_b200_set_layout(ctx_, g.dim, g.Nx, g.Ny, g.dim == 3 ? g.Nz : 1, g.cellTypes, g.width, g.gap,
+                                     g.nonUniform ? 1 : 0, g.dh));
+    }
+
+    void DestroyPressureSolver()
+    {
+        if (ctx_) nereus_b200_destroy(ctx_);
+        ctx_ = nullptr;
+    }
+    void ReleasePressureSolver() { DestroyPressureSolver(); }
+
+    // SolveChorin / SolvePressure (PressureSolver3D.cpp:279-345) fused with ProjectPressure (:417-438): p must carry
+    // the ring values EnforcePressureBC(time) wrote. Returns the report; NOT_CONVERGED is reported, not thrown.
+    nb_result SolvePressure(const GridView &g, double rho, double dt, bool needsCompat, double tol)
+    {
+        EnsureSystem(g);
+        nb_result r{};
+        Check(nereus_b200_project(ctx_, g.u, g.v, g.w, g.p, rho, dt, NB_SCHEME_CHORIN, needsCompat ? 1 : 0, tol, &r));
+        lastIterations_ = r.iters_inner;
+        return r;
+    }
+
+    // The two registered steps separately, for a caller that keeps them apart.
+    nb_result SolvePressureOnly(const GridView &g, double rho, double dt, bool needsCompat, double tol)
+    {
+        EnsureSystem(g);
+        nb_result r{};
+        Check(nereus_b200_solve_pressure(ctx_, g.u, g.v, g.w, g.p, rho, dt, NB_SCHEME_CHORIN, needsCompat ? 1 : 0,
+                                         tol, &r));
+        lastIterations_ = r.iters_inner;
+        return r;
+    }
+    void ProjectPressure(const GridView &g, double rho, double dt)
+    {
+        Check(nereus_b200_project_velocity(ctx_, g.u, g.v, g.w, g.p, rho, dt));
+    }
+
+    // SolveLaplacian (PressureSolver3D.cpp:355-371): false when f's size is not SystemSize().
+    bool SolveLaplacian(const GridView &g, const std::vector<double> &f, std::vector<double> &x, double tol = 1e-12)
+    {
+        EnsureSystem(g);
+        const int n = SystemSize();
+        if (n == 0 || (int)f.size() != n) return false;
+        x.assign(n, 0.0);
+        nb_result r{};
+        Check(nereus_b200_solve_laplacian(ctx_, f.data(), x.data(), tol, &r));
+        return true;
+    }
+
+    int SystemSize() const { return ctx_ ? nereus_b200_system_size(ctx_) : 0; }
+    int LastIterations() const { return lastIterations_; }
+
+    // GetIDP for every cell at once: idp holds Nx*Ny*Nz entries, -1 off the system.
+    void GetIDP(int32_t *idp) { Check(nereus_b200_get_idp(ctx_, idp)); }
+
+  private:
+    nb_options opt_{};
+    nb_ctx *ctx_ = nullptr;
+    int lastIterations_ = 0;
+};
+
+} // namespace nereus_b200

@@ -241,8 +241,30 @@ template <typename T> void LaunchLevelResidual(const LevelView &v, const T *r, c
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// transfers
+// transfers. The prolongation is trilinear except at Neumann boundaries: a coarse contributor that is SOLID hands
+// its weight to the child's parent (a constant extrapolation across the wall, the reflection a zero-gradient
+// boundary asks for), a Dirichlet contributor keeps its zero. The restriction is the exact transpose.
 // ---------------------------------------------------------------------------------------------------------------
+
+// Weight the prolongation moves onto coarse cell (I,J,K) from the SOLID contributors of its child on side
+// (si, sj, sk): the sum of the trilinear weights of those contributors.
+template <typename T>
+__device__ __forceinline__ T SolidWeight(const LevelView &cv, int I, int J, int K, int si, int sj, int sk)
+{
+    const T wv[2] = {(T)0.75, (T)0.25};
+    const long long parent = (long long)I * cv.sI + (long long)J * cv.sJ + K;
+    T extra = (T)0;
+    const int nk = cv.dim == 3 ? 2 : 1;
+    for (int di = 0; di < 2; di++)
+        for (int dj = 0; dj < 2; dj++)
+            for (int dk = 0; dk < nk; dk++)
+            {
+                if (!(di | dj | dk)) continue;
+                const long long cc = parent + (long long)(di * si) * cv.sI + (long long)(dj * sj) * cv.sJ + dk * sk;
+                if (cv.types[cc] == SOLID) extra += wv[di] * wv[dj] * (cv.dim == 3 ? wv[dk] : (T)1);
+            }
+    return extra;
+}
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_restrict(LevelView fv, LevelView cv, const T *__restrict__ res,
                                                      T *__restrict__ rc)
@@ -280,6 +302,18 @@ __global__ void __launch_bounds__(kBlock) k_restrict(LevelView fv, LevelView cv,
                     s += wij * res[rowBase];
             }
         }
+        // the children of (I, J, K) also carry the weight the prolongation moved off their SOLID coarse contributors
+        const int nz = fv.dim == 3 ? 2 : 1;
+        for (int ci = 0; ci < 2; ci++)
+            for (int cj = 0; cj < 2; cj++)
+                for (int ck = 0; ck < nz; ck++)
+                {
+                    const int a = 2 * I - 1 + ci, b = 2 * J - 1 + cj, d = fv.dim == 3 ? 2 * K - 1 + ck : 0;
+                    if (a > fv.Ny - 2 || b > fv.Nx - 2 || (fv.dim == 3 && d > fv.Nz - 2)) continue;
+                    const int si = ci ? 1 : -1, sj = cj ? 1 : -1, sk = ck ? 1 : -1;
+                    const T extra = SolidWeight<T>(cv, I, J, K, si, sj, sk);
+                    if (extra != (T)0) s += extra * res[(long long)a * fv.sI + (long long)b * fv.sJ + d];
+                }
         rc[c] = s;
     }
 }
@@ -302,25 +336,22 @@ __global__ void __launch_bounds__(kBlock) k_prolong(LevelView fv, LevelView cv, 
         LineCell(fv, line, f, a, b, d, c);
         if (fv.types[c] != FLUID) continue;
         const int A = (a + 1) >> 1, B = (b + 1) >> 1;
-        const int A2 = (a & 1) ? A - 1 : A + 1, B2 = (b & 1) ? B - 1 : B + 1;
-        T s;
-        if (fv.dim == 3)
-        {
-            const int D = (d + 1) >> 1, D2 = (d & 1) ? D - 1 : D + 1;
-            auto at = [&](int I, int J, int K) { return ec[(long long)I * cv.sI + (long long)J * cv.sJ + K]; };
-            const T x00 = (T)0.75 * at(A, B, D) + (T)0.25 * at(A, B, D2);
-            const T x01 = (T)0.75 * at(A, B2, D) + (T)0.25 * at(A, B2, D2);
-            const T x10 = (T)0.75 * at(A2, B, D) + (T)0.25 * at(A2, B, D2);
-            const T x11 = (T)0.75 * at(A2, B2, D) + (T)0.25 * at(A2, B2, D2);
-            s = (T)0.75 * ((T)0.75 * x00 + (T)0.25 * x01) + (T)0.25 * ((T)0.75 * x10 + (T)0.25 * x11);
-        }
-        else
-        {
-            auto at = [&](int I, int J) { return ec[(long long)I * cv.sI + (long long)J * cv.sJ]; };
-            s = (T)0.75 * ((T)0.75 * at(A, B) + (T)0.25 * at(A, B2)) +
-                (T)0.25 * ((T)0.75 * at(A2, B) + (T)0.25 * at(A2, B2));
-        }
-        ef[c] += s;
+        const int D = fv.dim == 3 ? (d + 1) >> 1 : 0;
+        const int si = (a & 1) ? -1 : 1, sj = (b & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
+        const T wv[2] = {(T)0.75, (T)0.25};
+        const long long parent = (long long)A * cv.sI + (long long)B * cv.sJ + D;
+        T s = (T)0, extra = (T)0;
+        const int nk = fv.dim == 3 ? 2 : 1;
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < 2; dj++)
+                for (int dk = 0; dk < nk; dk++)
+                {
+                    const long long cc = parent + (long long)(di * si) * cv.sI + (long long)(dj * sj) * cv.sJ + dk * sk;
+                    const T w = wv[di] * wv[dj] * (fv.dim == 3 ? wv[dk] : (T)1);
+                    if ((di | dj | dk) && cv.types[cc] == SOLID) extra += w; // Neumann: the parent's value
+                    else s += w * ec[cc];
+                }
+        ef[c] += s + extra * ec[parent];
     }
 }
 
