@@ -61,6 +61,9 @@ typedef struct nb_options
     int coarse_sweeps;   /* symmetric sweep pairs on the coarsest level */
     int max_levels;      /* multigrid levels at most (>= 1) */
     void *stream;        /* cudaStream_t to launch on; NULL: the context makes its own */
+    int use_graphs;      /* 1: each CG iteration (V-cycle included) replays one captured CUDA graph; 0: launches */
+    int fused_sweeps;    /* 1: 3D levels smooth with one shared-memory tiled launch per red-black sweep, the
+                            prolongation and r.z fused in; 0 (default): one launch per colour */
 } nb_options;
 
 typedef struct nb_result

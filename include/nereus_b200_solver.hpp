@@ -49,6 +49,7 @@ class PressureSolver
     {
         nereus_b200_default_options(&opt_);
         opt_.precision = precision;
+        opt_.use_graphs = 1;
         opt_.device = device;
     }
     ~PressureSolver() { DestroyPressureSolver(); }

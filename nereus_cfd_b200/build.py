@@ -23,6 +23,8 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-
 SOURCES = {
     "nb_exact.cu": ["-fmad=false"],
     "nb_kernels.cu": [],
+    "nb_tail.cu": [],
+    "nb_fused.cu": [],
     "nb_solver.cu": [],
     "nb_capi.cu": [],
 }

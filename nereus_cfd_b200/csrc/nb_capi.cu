@@ -66,9 +66,11 @@ void nereus_b200_default_options(nb_options *o)
     o->inner_tol = 1e-4;
     o->pre_sweeps = 1;
     o->post_sweeps = 1;
-    o->coarse_sweeps = 16;
+    o->coarse_sweeps = 8;
     o->max_levels = 16;
     o->stream = nullptr;
+    o->use_graphs = 1;
+    o->fused_sweeps = 0;
 }
 
 const char *nereus_b200_last_error(void) { return g_error.c_str(); }

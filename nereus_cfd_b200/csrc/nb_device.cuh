@@ -34,7 +34,66 @@ struct LevelView
     const double *g[3]; // padded FaceGap tables, entry n at [n+1] (n = -1..N-1)
     const float *w32[3];
     const float *ig32[3]; // 1 / FaceGap, FP32
+    // Per-cell code of the level: bits 0-5 neighbour q is FLUID, bit 6 a neighbour is Dirichlet, bit 7 the cell is
+    // an unknown (interior FLUID). Built once per layout (k_build_codes).
+    const uint8_t *code;
+    // Tiled iteration over the interior: a block of 32 x 8 threads covers 32 cells along the fast axis and 8 along
+    // the mid axis and marches `slowChunk` steps along the slow axis. 3D: (fast, mid, slow) = (k, j, i);
+    // 2D: (j, i, -) with slowLen = 1.
+    int fastLen, midLen, slowLen, slowChunk;
 };
+
+enum : unsigned { CODE_FLUID_MASK = 0x3Fu, CODE_DIRICHLET = 0x40u, CODE_UNKNOWN = 0x80u };
+
+constexpr int kTileF = 32, kTileM = 8;
+
+// Coordinates of this thread's cell at slow step s (0-based); false outside the interior.
+__device__ __forceinline__ bool TileCell(const LevelView &v, int fo, int mo, int s, int &i, int &j, int &k,
+                                         long long &c)
+{
+    if (fo >= v.fastLen || mo >= v.midLen) return false;
+    if (v.dim == 3) { i = 1 + s; j = 1 + mo; k = 1 + fo; }
+    else { i = 1 + mo; j = 1 + fo; k = 0; }
+    c = (long long)i * v.sI + (long long)j * v.sJ + k;
+    return true;
+}
+
+// Cell of colour `colour` ((i+j+k)&1) number `ho` along the fast axis of its line; false past the line's end.
+__device__ __forceinline__ bool TileCellColour(const LevelView &v, int ho, int mo, int s, int colour, int &i, int &j,
+                                               int &k, long long &c)
+{
+    if (mo >= v.midLen) return false;
+    int f;
+    if (v.dim == 3)
+    {
+        i = 1 + s;
+        j = 1 + mo;
+        f = (((colour ^ (i + j)) & 1) ? 1 : 2) + 2 * ho; // k with (i + j + k) & 1 == colour
+        if (f > v.fastLen) return false;
+        k = f;
+    }
+    else
+    {
+        i = 1 + mo;
+        f = (((colour ^ i) & 1) ? 1 : 2) + 2 * ho;
+        if (f > v.fastLen) return false;
+        j = f;
+        k = 0;
+    }
+    c = (long long)i * v.sI + (long long)j * v.sJ + k;
+    return true;
+}
+
+inline dim3 TileGrid(const LevelView &v, bool half = false)
+{
+    const int f = half ? (v.fastLen + 1) / 2 : v.fastLen;
+    dim3 g((unsigned)((f + kTileF - 1) / kTileF), (unsigned)((v.midLen + kTileM - 1) / kTileM),
+           (unsigned)((v.slowLen + v.slowChunk - 1) / v.slowChunk));
+    if (g.x == 0) g.x = 1;
+    if (g.y == 0) g.y = 1;
+    if (g.z == 0) g.z = 1;
+    return g;
+}
 
 // Cell of interior line `line`, fast offset f (0-based).
 __device__ __forceinline__ void LineCell(const LevelView &v, int line, int f, int &i, int &j, int &k, long long &c)
@@ -149,6 +208,33 @@ __device__ __forceinline__ void LevelStencil(const LevelView &v, int i, int j, i
     fluidMask = m;
 }
 
+// The same stencil from the cell's code: no neighbour type is read unless a neighbour is Dirichlet.
+template <typename T>
+__device__ __forceinline__ void CodeStencil(const LevelView &v, int i, int j, int k, long long c, unsigned code,
+                                            T cq[6], T &diag)
+{
+    LevelCoefs<T>(v, i, j, k, cq);
+    const unsigned m = code & CODE_FLUID_MASK;
+    T d = 0;
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        if (m >> q & 1u) d += cq[q];
+    if (code & CODE_DIRICHLET)
+    {
+        const int nq = v.dim == 3 ? 6 : 4;
+        for (int q = 0; q < nq; q++)
+        {
+            const int t = v.types[c + NbrOffset(v, q)];
+            if (IsDirichlet(t))
+            {
+                const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3), nk = k + (q == 4) - (q == 5);
+                d += OnRing(v, ni, nj, nk) ? cq[q] * LevelRingFactor<T>(v, i, j, k, q) : cq[q];
+            }
+        }
+    }
+    diag = d;
+}
+
 // ---- reductions ----
 template <typename T>
 __device__ __forceinline__ T WarpSum(T x)
@@ -181,12 +267,19 @@ constexpr int kWarps = kBlock / 32;
 
 // Block-reduce NV values held by every thread, then the last block finishes; out[slot0 + s] = total s.
 // op 0 = sum, 1 = max.
+// bump: when not null, the last block adds 1 to *bump after storing the totals (the PCG iteration counter, which
+// every block of the launch has read before any block can be the last).
 template <int NV>
-__device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], int slot0, int op = 0)
+__device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], int slot0, int op = 0,
+                                           int *bump = nullptr)
 {
-    __shared__ double sh[NV][kWarps];
+    __shared__ double sh[NV][32];
     __shared__ bool amLast;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, warp = tid >> 5, nwarp = (nthr + 31) >> 5;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
 #pragma unroll
     for (int s = 0; s < NV; s++)
     {
@@ -194,18 +287,18 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
         if (lane == 0) sh[s][warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x == 0)
+    if (tid == 0)
     {
 #pragma unroll
         for (int s = 0; s < NV; s++)
         {
             double t = sh[s][0];
-            for (int w = 1; w < kWarps; w++) t = op == 0 ? t + sh[s][w] : fmax(t, sh[s][w]);
-            R.partials[(size_t)s * R.maxBlocks + blockIdx.x] = t;
+            for (int w = 1; w < nwarp; w++) t = op == 0 ? t + sh[s][w] : fmax(t, sh[s][w]);
+            R.partials[(size_t)s * R.maxBlocks + bid] = t;
         }
         __threadfence();
         const unsigned done = atomicAdd(R.counter, 1u);
-        amLast = (done == gridDim.x - 1);
+        amLast = (done == nblk - 1);
     }
     __syncthreads();
     if (!amLast) return;
@@ -213,8 +306,8 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
 #pragma unroll
     for (int s = 0; s < NV; s++)
     {
-        double t = op == 0 ? 0.0 : 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+        double t = 0.0;
+        for (unsigned b = tid; b < nblk; b += nthr)
         {
             const double pv = *((volatile double *)&R.partials[(size_t)s * R.maxBlocks + b]);
             t = op == 0 ? t + pv : fmax(t, pv);
@@ -223,15 +316,16 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
         if (lane == 0) sh[s][warp] = t;
     }
     __syncthreads();
-    if (threadIdx.x == 0)
+    if (tid == 0)
     {
 #pragma unroll
         for (int s = 0; s < NV; s++)
         {
             double t = sh[s][0];
-            for (int w = 1; w < kWarps; w++) t = op == 0 ? t + sh[s][w] : fmax(t, sh[s][w]);
+            for (int w = 1; w < nwarp; w++) t = op == 0 ? t + sh[s][w] : fmax(t, sh[s][w]);
             R.out[slot0 + s] = t;
         }
+        if (bump) *bump += 1;
         *R.counter = 0u;
     }
 }

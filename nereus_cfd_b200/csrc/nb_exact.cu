@@ -386,14 +386,13 @@ __device__ __forceinline__ double DivergenceAt(const LevelView &g, const Faces &
 
 __global__ void k_rhs(LevelView v, Faces F, const double *p, double rhoDt, double scale, double dh, double *b)
 {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int line = warp; line < v.nLines; line += nw)
-        for (int f = lane; f < v.lineLen; f += 32)
+    const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;
+    const int sBeg = blockIdx.z * v.slowChunk, sEnd = min(sBeg + v.slowChunk, v.slowLen);
+    for (int s = sBeg; s < sEnd; s++)
         {
             int i, j, k;
             long long c;
-            LineCell(v, line, f, i, j, k, c);
+            if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
             if (v.types[c] != FLUID) continue;
             double cq[6];
             CoefsExact(v, i, j, k, cq);
@@ -428,21 +427,20 @@ void LaunchRhs(const LevelView &v, const double *u, const double *vv, const doub
 {
     if (v.nLines <= 0) return;
     NB_COUNT_LAUNCH();
-    k_rhs<<<LineGrid(v.nLines, 148 * 8), kBlock, 0, st>>>(v, MakeFaces(v, u, vv, w), p, rhoDt, scale, dh, b);
+    k_rhs<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, MakeFaces(v, u, vv, w), p, rhoDt, scale, dh, b);
 }
 
 // max |div u| over FLUID cells (the post-projection check)
 __global__ void k_max_div(LevelView v, Faces F, double dh, Reducer R, int slot)
 {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;
+    const int sBeg = blockIdx.z * v.slowChunk, sEnd = min(sBeg + v.slowChunk, v.slowLen);
     double m[1] = {0.0};
-    for (int line = warp; line < v.nLines; line += nw)
-        for (int f = lane; f < v.lineLen; f += 32)
+    for (int s = sBeg; s < sEnd; s++)
         {
             int i, j, k;
             long long c;
-            LineCell(v, line, f, i, j, k, c);
+            if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
             if (v.types[c] != FLUID) continue;
             m[0] = fmax(m[0], fabs(DivergenceAt(v, F, i, j, k, dh)));
         }
@@ -454,7 +452,7 @@ void LaunchMaxDiv(const LevelView &v, const double *u, const double *vv, const d
 {
     const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_max_div<<<blocks, kBlock, 0, st>>>(v, MakeFaces(v, u, vv, w), dh, R, slot);
+    k_max_div<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, MakeFaces(v, u, vv, w), dh, R, slot);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -467,15 +465,14 @@ template <typename T, bool kAdd>
 __global__ void k_residual64(LevelView v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
                              double scale, double sfac, Reducer R, int slot)
 {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;
+    const int sBeg = blockIdx.z * v.slowChunk, sEnd = min(sBeg + v.slowChunk, v.slowLen);
     double acc[2] = {0.0, 0.0};
-    for (int line = warp; line < v.nLines; line += nw)
-        for (int f = lane; f < v.lineLen; f += 32)
+    for (int s = sBeg; s < sEnd; s++)
         {
             int i, j, k;
             long long c;
-            LineCell(v, line, f, i, j, k, c);
+            if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
             if (v.types[c] != FLUID) continue;
             double cq[6];
             int t[6];
@@ -507,7 +504,7 @@ void LaunchResidual64(const LevelView &v, const double *b, const double *x, T *r
 {
     const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_residual64<T, false><<<blocks, kBlock, 0, st>>>(v, b, x, (const T *)nullptr, nullptr, rOut, scale, sfac, R, slot);
+    k_residual64<T, false><<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, b, x, (const T *)nullptr, nullptr, rOut, scale, sfac, R, slot);
 }
 
 template <typename T>
@@ -516,7 +513,7 @@ void LaunchRefine64(const LevelView &v, const double *b, const double *xin, cons
 {
     const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_residual64<T, true><<<blocks, kBlock, 0, st>>>(v, b, xin, e, xout, rOut, scale, sfac, R, slot);
+    k_residual64<T, true><<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, b, xin, e, xout, rOut, scale, sfac, R, slot);
 }
 
 template void LaunchResidual64<float>(const LevelView &, const double *, const double *, float *, double, double,
@@ -536,37 +533,35 @@ template void LaunchRefine64<double>(const LevelView &, const double *, const do
 // sum of x over the unknowns, compensated (Neumaier) per thread, then the deterministic reduction of (sum, carry)
 __global__ void k_sum_unknowns(LevelView v, const double *x, Reducer R, int slot)
 {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    double s = 0.0, comp = 0.0;
-    for (int line = warp; line < v.nLines; line += nw)
-        for (int f = lane; f < v.lineLen; f += 32)
-        {
-            int i, j, k;
-            long long c;
-            LineCell(v, line, f, i, j, k, c);
-            if (v.types[c] != FLUID) continue;
-            const double a = x[c];
-            const double t = s + a;
-            comp += fabs(s) >= fabs(a) ? (s - t) + a : (a - t) + s;
-            s = t;
-        }
-    double acc[2] = {s, comp};
+    const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;
+    const int sBeg = blockIdx.z * v.slowChunk, sEnd = min(sBeg + v.slowChunk, v.slowLen);
+    double sum = 0.0, comp = 0.0;
+    for (int s = sBeg; s < sEnd; s++)
+    {
+        int i, j, k;
+        long long c;
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
+        if (v.types[c] != FLUID) continue;
+        const double a = x[c];
+        const double t = sum + a;
+        comp += fabs(sum) >= fabs(a) ? (sum - t) + a : (a - t) + sum;
+        sum = t;
+    }
+    double acc[2] = {sum, comp};
     GridReduce<2>(R, acc, slot);
 }
 
 // x -= (out[slot] + out[slot+1]) / n at the unknowns, then optionally scatter into p.
 __global__ void k_sub_mean_scatter(LevelView v, double *x, const double *sums, int n, int sub, double *p)
 {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;
+    const int sBeg = blockIdx.z * v.slowChunk, sEnd = min(sBeg + v.slowChunk, v.slowLen);
     const double mean = sub ? (sums[0] + sums[1]) / (double)n : 0.0;
-    for (int line = warp; line < v.nLines; line += nw)
-        for (int f = lane; f < v.lineLen; f += 32)
+    for (int s = sBeg; s < sEnd; s++)
         {
             int i, j, k;
             long long c;
-            LineCell(v, line, f, i, j, k, c);
+            if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
             if (v.types[c] != FLUID) continue;
             const double y = x[c] - mean;
             x[c] = y;
@@ -578,14 +573,14 @@ void LaunchSumUnknowns(const LevelView &v, const double *x, const Reducer &R, in
 {
     const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_sum_unknowns<<<blocks, kBlock, 0, st>>>(v, x, R, slot);
+    k_sum_unknowns<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, x, R, slot);
 }
 
 void LaunchSubMeanScatter(const LevelView &v, double *x, const double *sums, int n, int sub, double *p, cudaStream_t st)
 {
     if (v.nLines <= 0) return;
     NB_COUNT_LAUNCH();
-    k_sub_mean_scatter<<<LineGrid(v.nLines, 148 * 8), kBlock, 0, st>>>(v, x, sums, n, sub, p);
+    k_sub_mean_scatter<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, x, sums, n, sub, p);
 }
 
 __device__ __forceinline__ void RingEntry(const LevelView &v, double *p, long long d, long long s)

@@ -4,13 +4,18 @@
 // FP64 form. Every vector is zero off the unknowns (interior FLUID cells), which the kernels rely on: they never
 // write anywhere else.
 //
+// Iteration: blocks of 32 x 8 threads tile the (fast, mid) plane of the interior and march along the slow axis
+// (nb_device.cuh, TileCell); loads along the fast axis are coalesced 128-byte rows, the neighbours across the tile
+// come from L1/L2. A cell's stencil comes from its one-byte code (neighbour-FLUID mask, Dirichlet flag, unknown
+// flag), so the common cell reads no neighbour type.
+//
 // Multigrid (cell-centred, 2:1 coarsening, the hierarchy built in nb_solver.cu):
 //   - smoother: red-black Gauss-Seidel, colour (i+j+k)&1, red first before the coarse correction and in reverse
-//     order after it, so the V-cycle is a symmetric operator and can precondition CG;
-//   - restriction: the transpose of the prolongation (weights 1/4, 3/4, 3/4, 1/4 per axis over the 4-wide fine
-//     window), summed only from FLUID fine cells into FLUID coarse cells;
-//   - prolongation: trilinear (3/4 parent, 1/4 the neighbour on the child's side per axis), added only at FLUID
-//     fine cells; coarse cells that are not FLUID hold zero;
+//     order after it, so the V-cycle is a symmetric operator and can precondition CG; a half-sweep launches only
+//     the cells of its colour;
+//   - restriction: the transpose of the prolongation, summed only from FLUID fine cells into FLUID coarse cells;
+//   - prolongation: trilinear, except that a SOLID coarse contributor hands its weight to the child's parent
+//     (constant extrapolation across a Neumann wall) and a Dirichlet one keeps its zero; added only at FLUID cells;
 //   - coarsest level: symmetric red-black sweeps inside one CTA.
 #include "nb_kernels.h"
 
@@ -19,24 +24,31 @@ namespace nb
 
 std::atomic<long long> g_launches{0};
 
+static const dim3 kTile(kTileF, kTileM, 1);
+
+#define NB_TILE_LOOP(v)                                                                                            \
+    const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;                      \
+    const int sBeg = blockIdx.z * (v).slowChunk;                                                                   \
+    const int sEnd = min(sBeg + (v).slowChunk, (v).slowLen);                                                       \
+    for (int s = sBeg; s < sEnd; s++)
+
 // FP64 coefficients of level 0 exactly as the reference forms them (products and divisions only; FaceCoefs3D,
 // PressureSolver3D.cpp:47-63; 2D c[] PressureSolver2D.cpp:123-126).
 __device__ __forceinline__ void Coefs64(const LevelView &v, int i, int j, int k, double c[6])
 {
+    if (!v.stretched)
+    {
+#pragma unroll
+        for (int q = 0; q < 6; q++) c[q] = q < (v.dim == 3 ? 6 : 4) ? v.gamma : 0.0;
+        return;
+    }
     if (v.dim == 2)
     {
-        if (!v.stretched) { c[0] = c[1] = c[2] = c[3] = v.gamma; c[4] = c[5] = 0.0; return; }
         c[0] = Wd(v, 0, j) / Gp(v, 1, i);
         c[1] = Wd(v, 0, j) / Gp(v, 1, i - 1);
         c[2] = Wd(v, 1, i) / Gp(v, 0, j);
         c[3] = Wd(v, 1, i) / Gp(v, 0, j - 1);
         c[4] = c[5] = 0.0;
-        return;
-    }
-    if (!v.stretched)
-    {
-#pragma unroll
-        for (int q = 0; q < 6; q++) c[q] = v.gamma;
         return;
     }
     const double ax = Wd(v, 1, i) * Wd(v, 2, k);
@@ -59,55 +71,114 @@ __device__ __forceinline__ double RingFactor64(const LevelView &v, int i, int j,
     return Gp(v, a, s < 0 ? n - 1 : n) / (0.5 * Wd(v, a, n));
 }
 
-// Stencil of FLUID cell c: off-diagonal magnitudes cq, diagonal, and which neighbours are FLUID.
-// kExact: the FP64 tables and the reference's formula (level 0 of the FP64 solve); otherwise LevelStencil.
+// Stencil of an unknown cell. kExact: the FP64 tables and the reference's formula (the operator of the FP64 solve's
+// CG on level 0); otherwise the level's own (FP32-table) coefficients.
 template <typename T, bool kExact>
-__device__ __forceinline__ void Stencil(const LevelView &v, int i, int j, int k, long long c, T cq[6], T &diag,
-                                        unsigned &mask)
+__device__ __forceinline__ void Stencil(const LevelView &v, int i, int j, int k, long long c, unsigned code, T cq[6],
+                                        T &diag)
 {
     if (!kExact)
     {
-        LevelStencil<T>(v, i, j, k, c, cq, diag, mask);
+        CodeStencil<T>(v, i, j, k, c, code, cq, diag);
         return;
     }
     double c64[6];
     Coefs64(v, i, j, k, c64);
-    const int nq = v.dim == 3 ? 6 : 4;
     double d = 0.0;
-    unsigned m = 0;
-    for (int q = 0; q < nq; q++)
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        if (code >> q & 1u) d += c64[q];
+    if (code & CODE_DIRICHLET)
     {
-        const int t = v.types[c + NbrOffset(v, q)];
-        if (t == FLUID) { d += c64[q]; m |= 1u << q; }
-    }
-    for (int q = 0; q < nq; q++)
-    {
-        const int t = v.types[c + NbrOffset(v, q)];
-        if (IsDirichlet(t))
+        const int nq = v.dim == 3 ? 6 : 4;
+        for (int q = 0; q < nq; q++)
         {
-            const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3), nk = k + (q == 4) - (q == 5);
-            d += OnRing(v, ni, nj, nk) ? c64[q] * RingFactor64(v, i, j, k, q) : c64[q];
+            const int t = v.types[c + NbrOffset(v, q)];
+            if (IsDirichlet(t))
+            {
+                const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3), nk = k + (q == 4) - (q == 5);
+                d += OnRing(v, ni, nj, nk) ? c64[q] * RingFactor64(v, i, j, k, q) : c64[q];
+            }
         }
     }
 #pragma unroll
     for (int q = 0; q < 6; q++) cq[q] = (T)c64[q];
     diag = (T)d;
-    mask = m;
 }
 
-#define NB_LINE_LOOP(v)                                                                                            \
-    const int lane = threadIdx.x & 31, warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;                      \
-    const int nWarps = (gridDim.x * blockDim.x) >> 5;                                                              \
-    for (int line = warpId; line < (v).nLines; line += nWarps)                                                     \
-        for (int f = lane; f < (v).lineLen; f += 32)
+// sum over the FLUID neighbours of c_q x_q
+template <typename T>
+__device__ __forceinline__ T OffSum(const LevelView &v, long long c, unsigned code, const T cq[6], const T *x)
+{
+    T s = (T)0;
+    if (code & 1u) s += cq[0] * x[c + v.sI];
+    if (code & 2u) s += cq[1] * x[c - v.sI];
+    if (code & 4u) s += cq[2] * x[c + v.sJ];
+    if (code & 8u) s += cq[3] * x[c - v.sJ];
+    if (code & 16u) s += cq[4] * x[c + 1];
+    if (code & 32u) s += cq[5] * x[c - 1];
+    return s;
+}
 
-static inline int Blocks(const LevelView &v) { return LineGrid(v.nLines > 0 ? v.nLines : 1, 148 * 8); }
+// the six neighbours of an interior cell, loaded unconditionally (all in bounds; 2D reads its j neighbours twice)
+template <typename T>
+__device__ __forceinline__ void LoadNbrs(const LevelView &v, long long c, const T *x, T xn[6])
+{
+    xn[0] = x[c + v.sI];
+    xn[1] = x[c - v.sI];
+    xn[2] = x[c + v.sJ];
+    xn[3] = x[c - v.sJ];
+    xn[4] = x[c + 1];
+    xn[5] = x[c - 1];
+}
+
+// sum over the FLUID neighbours (code bits 0-5) of c_q x_q
+template <typename T> __device__ __forceinline__ T MaskedSum(unsigned code, const T cq[6], const T xn[6])
+{
+    T s = (T)0;
+#pragma unroll
+    for (int q = 0; q < 6; q++) s += ((code >> q) & 1u) ? cq[q] * xn[q] : (T)0;
+    return s;
+}
 
 // ---------------------------------------------------------------------------------------------------------------
-// coarse cell types: an interior coarse cell is Dirichlet (EMPTY) if any child is, else FLUID if any child is,
-// else SOLID (Neumann); a coarse ring cell on one face is Dirichlet if any of its ring children is Dirichlet or
-// FLUID, else SOLID; ring edges and corners are SOLID.
+// per-level cell codes and coarse cell types
 // ---------------------------------------------------------------------------------------------------------------
+__global__ void k_build_codes(LevelView v, uint8_t *code)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < v.cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int k = (int)(c % v.Nz);
+        const long long r = c / v.Nz;
+        const int j = (int)(r % v.Nx), i = (int)(r / v.Nx);
+        const bool interior = i > 0 && i < v.Ny - 1 && j > 0 && j < v.Nx - 1 &&
+                              (v.dim == 2 || (k > 0 && k < v.Nz - 1));
+        if (!interior || v.types[c] != FLUID) { code[c] = 0; continue; }
+        unsigned m = CODE_UNKNOWN;
+        const int nq = v.dim == 3 ? 6 : 4;
+        for (int q = 0; q < nq; q++)
+        {
+            const int t = v.types[c + NbrOffset(v, q)];
+            if (t == FLUID) m |= 1u << q;
+            else if (IsDirichlet(t)) m |= CODE_DIRICHLET;
+        }
+        code[c] = (uint8_t)m;
+    }
+}
+
+void LaunchBuildCodes(const LevelView &v, uint8_t *code, cudaStream_t st)
+{
+    int blocks = (int)((v.cells + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    NB_COUNT_LAUNCH();
+    k_build_codes<<<blocks, 256, 0, st>>>(v, code);
+}
+
+// An interior coarse cell is Dirichlet (EMPTY) if any child is, else FLUID if any child is, else SOLID (Neumann); a
+// coarse ring cell on one face is Dirichlet if any of its ring children is Dirichlet or FLUID, else SOLID; ring
+// edges and corners are SOLID.
 __global__ void k_coarsen_types(LevelView f, LevelView cv, uint8_t *ct)
 {
     const long long cells = cv.cells;
@@ -121,7 +192,6 @@ __global__ void k_coarsen_types(LevelView f, LevelView cv, uint8_t *ct)
         const bool rK = cv.dim == 3 && (K == 0 || K == cv.Nz - 1);
         const int codim = (int)rI + (int)rJ + (int)rK;
         if (codim >= 2) { ct[c] = SOLID; continue; }
-        // child index ranges along each axis (fine ring index when the coarse index is on the ring)
         int ia[2], ja[2], ka[2], ni = 0, nj = 0, nk = 0;
         auto kids = [](int C, int Nc, int Nf, int *out, int &cnt) {
             if (C == 0) { out[0] = 0; cnt = 1; return; }
@@ -158,92 +228,85 @@ void LaunchCoarsenTypes(const LevelView &fine, const LevelView &coarse, uint8_t 
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// smoother
+// smoother: one colour of a red-black sweep. kFirst: the red pass from a zero iterate (e = r / diag; the black
+// values that follow never read the old black ones, so nothing else needs clearing).
 // ---------------------------------------------------------------------------------------------------------------
 template <typename T, bool kFirst>
-__global__ void __launch_bounds__(kBlock) k_smooth(LevelView v, const T *__restrict__ r, T *e, int colour)
+__global__ void __launch_bounds__(256) k_smooth(LevelView v, const T *__restrict__ r, T *e, int colour)
 {
-    NB_LINE_LOOP(v)
+    NB_TILE_LOOP(v)
     {
         int i, j, k;
         long long c;
-        LineCell(v, line, f, i, j, k, c);
-        if (v.types[c] != FLUID) continue;
-        const int col = (i + j + k) & 1;
-        if (kFirst)
-        {
-            if (col == 0)
-            {
-                T cq[6], diag;
-                unsigned m;
-                LevelStencil<T>(v, i, j, k, c, cq, diag, m);
-                e[c] = diag != (T)0 ? r[c] / diag : (T)0;
-            }
-            else
-                e[c] = (T)0;
-            continue;
-        }
-        if (col != colour) continue;
+        if (!TileCellColour(v, fo, mo, s, colour, i, j, k, c)) continue;
+        // every load of the cell is issued before anything depends on one of them
+        const unsigned code = v.code[c];
+        const T rc = r[c];
+        T xn[6];
+        if (!kFirst) LoadNbrs<T>(v, c, e, xn);
+        if (!(code & CODE_UNKNOWN)) continue;
         T cq[6], diag;
-        unsigned m;
-        LevelStencil<T>(v, i, j, k, c, cq, diag, m);
-        T s = r[c];
-        const int nq = v.dim == 3 ? 6 : 4;
-#pragma unroll
-        for (int q = 0; q < 6; q++)
-            if (q < nq && (m >> q & 1u)) s += cq[q] * e[c + NbrOffset(v, q)];
-        e[c] = diag != (T)0 ? s / diag : (T)0;
+        CodeStencil<T>(v, i, j, k, c, code, cq, diag);
+        const T rhs = kFirst ? rc : rc + MaskedSum<T>(code, cq, xn);
+        e[c] = diag != (T)0 ? rhs / diag : (T)0;
     }
+}
+
+// Stencil launches with no reduction take one slow-axis step per block: many blocks, many warps per SM.
+static inline LevelView OnePlane(const LevelView &v)
+{
+    LevelView o = v;
+    o.slowChunk = 1;
+    return o;
 }
 
 template <typename T> void LaunchSmoothFirst(const LevelView &v, const T *r, T *e, cudaStream_t st)
 {
-    if (v.nLines <= 0) return;
+    if (v.fastLen <= 0 || v.midLen <= 0) return;
+    const LevelView o = OnePlane(v);
     NB_COUNT_LAUNCH();
-    k_smooth<T, true><<<Blocks(v), kBlock, 0, st>>>(v, r, e, 0);
+    k_smooth<T, true><<<TileGrid(o, true), kTile, 0, st>>>(o, r, e, 0);
 }
 
 template <typename T> void LaunchSmooth(const LevelView &v, const T *r, T *e, int colour, cudaStream_t st)
 {
-    if (v.nLines <= 0) return;
+    if (v.fastLen <= 0 || v.midLen <= 0) return;
+    const LevelView o = OnePlane(v);
     NB_COUNT_LAUNCH();
-    k_smooth<T, false><<<Blocks(v), kBlock, 0, st>>>(v, r, e, colour);
+    k_smooth<T, false><<<TileGrid(o, true), kTile, 0, st>>>(o, r, e, colour);
 }
 
 // res = r - M e
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_level_residual(LevelView v, const T *__restrict__ r,
-                                                           const T *__restrict__ e, T *__restrict__ res)
+__global__ void __launch_bounds__(256) k_level_residual(LevelView v, const T *__restrict__ r, const T *__restrict__ e,
+                                                        T *__restrict__ res)
 {
-    NB_LINE_LOOP(v)
+    NB_TILE_LOOP(v)
     {
         int i, j, k;
         long long c;
-        LineCell(v, line, f, i, j, k, c);
-        if (v.types[c] != FLUID) continue;
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
+        const unsigned code = v.code[c];
+        const T rc = r[c], ec = e[c];
+        T xn[6];
+        LoadNbrs<T>(v, c, e, xn);
+        if (!(code & CODE_UNKNOWN)) continue;
         T cq[6], diag;
-        unsigned m;
-        LevelStencil<T>(v, i, j, k, c, cq, diag, m);
-        T s = diag * e[c];
-        const int nq = v.dim == 3 ? 6 : 4;
-#pragma unroll
-        for (int q = 0; q < 6; q++)
-            if (q < nq && (m >> q & 1u)) s -= cq[q] * e[c + NbrOffset(v, q)];
-        res[c] = r[c] - s;
+        CodeStencil<T>(v, i, j, k, c, code, cq, diag);
+        res[c] = rc - (diag * ec - MaskedSum<T>(code, cq, xn));
     }
 }
 
 template <typename T> void LaunchLevelResidual(const LevelView &v, const T *r, const T *e, T *res, cudaStream_t st)
 {
-    if (v.nLines <= 0) return;
+    if (v.fastLen <= 0 || v.midLen <= 0) return;
+    const LevelView o = OnePlane(v);
     NB_COUNT_LAUNCH();
-    k_level_residual<T><<<Blocks(v), kBlock, 0, st>>>(v, r, e, res);
+    k_level_residual<T><<<TileGrid(o), kTile, 0, st>>>(o, r, e, res);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// transfers. The prolongation is trilinear except at Neumann boundaries: a coarse contributor that is SOLID hands
-// its weight to the child's parent (a constant extrapolation across the wall, the reflection a zero-gradient
-// boundary asks for), a Dirichlet contributor keeps its zero. The restriction is the exact transpose.
+// transfers
 // ---------------------------------------------------------------------------------------------------------------
 
 // Weight the prolongation moves onto coarse cell (I,J,K) from the SOLID contributors of its child on side
@@ -265,17 +328,18 @@ __device__ __forceinline__ T SolidWeight(const LevelView &cv, int I, int J, int 
             }
     return extra;
 }
+
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_restrict(LevelView fv, LevelView cv, const T *__restrict__ res,
-                                                     T *__restrict__ rc)
+__global__ void __launch_bounds__(256) k_restrict(LevelView fv, LevelView cv, const T *__restrict__ res,
+                                                  T *__restrict__ rc)
 {
-    NB_LINE_LOOP(cv)
+    NB_TILE_LOOP(cv)
     {
         int I, J, K;
         long long c;
-        LineCell(cv, line, f, I, J, K, c);
-        if (cv.types[c] != FLUID) continue;
-        T s = (T)0;
+        if (!TileCell(cv, fo, mo, s, I, J, K, c)) continue;
+        if (!(cv.code[c] & CODE_UNKNOWN)) continue;
+        T acc = (T)0;
         const T wt[4] = {(T)0.25, (T)0.75, (T)0.75, (T)0.25};
         for (int di = 0; di < 4; di++)
         {
@@ -296,10 +360,10 @@ __global__ void __launch_bounds__(kBlock) k_restrict(LevelView fv, LevelView cv,
                         const int d = 2 * K - 2 + dk;
                         if (d <= fv.Nz - 1) t += wt[dk] * res[rowBase + d];
                     }
-                    s += wij * t;
+                    acc += wij * t;
                 }
                 else
-                    s += wij * res[rowBase];
+                    acc += wij * res[rowBase];
             }
         }
         // the children of (I, J, K) also carry the weight the prolongation moved off their SOLID coarse contributors
@@ -310,37 +374,37 @@ __global__ void __launch_bounds__(kBlock) k_restrict(LevelView fv, LevelView cv,
                 {
                     const int a = 2 * I - 1 + ci, b = 2 * J - 1 + cj, d = fv.dim == 3 ? 2 * K - 1 + ck : 0;
                     if (a > fv.Ny - 2 || b > fv.Nx - 2 || (fv.dim == 3 && d > fv.Nz - 2)) continue;
-                    const int si = ci ? 1 : -1, sj = cj ? 1 : -1, sk = ck ? 1 : -1;
-                    const T extra = SolidWeight<T>(cv, I, J, K, si, sj, sk);
-                    if (extra != (T)0) s += extra * res[(long long)a * fv.sI + (long long)b * fv.sJ + d];
+                    const T extra = SolidWeight<T>(cv, I, J, K, ci ? 1 : -1, cj ? 1 : -1, ck ? 1 : -1);
+                    if (extra != (T)0) acc += extra * res[(long long)a * fv.sI + (long long)b * fv.sJ + d];
                 }
-        rc[c] = s;
+        rc[c] = acc;
     }
 }
 
 template <typename T>
 void LaunchRestrict(const LevelView &fine, const LevelView &coarse, const T *resFine, T *rCoarse, cudaStream_t st)
 {
-    if (coarse.nLines <= 0) return;
+    if (coarse.fastLen <= 0 || coarse.midLen <= 0) return;
+    const LevelView o = OnePlane(coarse);
     NB_COUNT_LAUNCH();
-    k_restrict<T><<<Blocks(coarse), kBlock, 0, st>>>(fine, coarse, resFine, rCoarse);
+    k_restrict<T><<<TileGrid(o), kTile, 0, st>>>(fine, o, resFine, rCoarse);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_prolong(LevelView fv, LevelView cv, const T *__restrict__ ec, T *ef)
+__global__ void __launch_bounds__(256) k_prolong(LevelView fv, LevelView cv, const T *__restrict__ ec, T *ef)
 {
-    NB_LINE_LOOP(fv)
+    NB_TILE_LOOP(fv)
     {
         int a, b, d;
         long long c;
-        LineCell(fv, line, f, a, b, d, c);
-        if (fv.types[c] != FLUID) continue;
+        if (!TileCell(fv, fo, mo, s, a, b, d, c)) continue;
+        if (!(fv.code[c] & CODE_UNKNOWN)) continue;
         const int A = (a + 1) >> 1, B = (b + 1) >> 1;
         const int D = fv.dim == 3 ? (d + 1) >> 1 : 0;
         const int si = (a & 1) ? -1 : 1, sj = (b & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
         const T wv[2] = {(T)0.75, (T)0.25};
         const long long parent = (long long)A * cv.sI + (long long)B * cv.sJ + D;
-        T s = (T)0, extra = (T)0;
+        T acc = (T)0, extra = (T)0;
         const int nk = fv.dim == 3 ? 2 : 1;
         for (int di = 0; di < 2; di++)
             for (int dj = 0; dj < 2; dj++)
@@ -349,18 +413,19 @@ __global__ void __launch_bounds__(kBlock) k_prolong(LevelView fv, LevelView cv, 
                     const long long cc = parent + (long long)(di * si) * cv.sI + (long long)(dj * sj) * cv.sJ + dk * sk;
                     const T w = wv[di] * wv[dj] * (fv.dim == 3 ? wv[dk] : (T)1);
                     if ((di | dj | dk) && cv.types[cc] == SOLID) extra += w; // Neumann: the parent's value
-                    else s += w * ec[cc];
+                    else acc += w * ec[cc];
                 }
-        ef[c] += s + extra * ec[parent];
+        ef[c] += acc + extra * ec[parent];
     }
 }
 
 template <typename T>
 void LaunchProlong(const LevelView &fine, const LevelView &coarse, const T *eCoarse, T *eFine, cudaStream_t st)
 {
-    if (fine.nLines <= 0) return;
+    if (fine.fastLen <= 0 || fine.midLen <= 0) return;
+    const LevelView o = OnePlane(fine);
     NB_COUNT_LAUNCH();
-    k_prolong<T><<<Blocks(fine), kBlock, 0, st>>>(fine, coarse, eCoarse, eFine);
+    k_prolong<T><<<TileGrid(o), kTile, 0, st>>>(o, coarse, eCoarse, eFine);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -371,26 +436,17 @@ __device__ void CoarseHalf(const LevelView &v, const T *r, T *e, int colour, int
 {
     for (long long c = threadIdx.x; c < v.cells; c += blockDim.x)
     {
+        const unsigned code = v.code[c];
+        if (!(code & CODE_UNKNOWN)) continue;
         const int k = (int)(c % v.Nz);
         const long long rr = c / v.Nz;
         const int j = (int)(rr % v.Nx), i = (int)(rr / v.Nx);
-        if (i == 0 || i == v.Ny - 1 || j == 0 || j == v.Nx - 1) continue;
-        if (v.dim == 3 && (k == 0 || k == v.Nz - 1)) continue;
-        if (v.types[c] != FLUID) continue;
         const int col = (i + j + k) & 1;
-        if (first && col != colour) { e[c] = (T)0; continue; }
         if (col != colour) continue;
         T cq[6], diag;
-        unsigned m;
-        LevelStencil<T>(v, i, j, k, c, cq, diag, m);
-        T s = r[c];
-        if (!first)
-        {
-            const int nq = v.dim == 3 ? 6 : 4;
-            for (int q = 0; q < nq; q++)
-                if (m >> q & 1u) s += cq[q] * e[c + NbrOffset(v, q)];
-        }
-        e[c] = diag != (T)0 ? s / diag : (T)0;
+        CodeStencil<T>(v, i, j, k, c, code, cq, diag);
+        const T rhs = first ? r[c] : r[c] + OffSum<T>(v, c, code, cq, e);
+        e[c] = diag != (T)0 ? rhs / diag : (T)0;
     }
     __syncthreads();
 }
@@ -422,15 +478,16 @@ template <typename T> void LaunchCoarseSolve(const LevelView &v, const T *r, T *
 // PCG
 // ---------------------------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_dot(LevelView v, const T *__restrict__ r, const T *__restrict__ z,
-                                                Reducer R, int base)
+__global__ void __launch_bounds__(256) k_dot(LevelView v, const T *__restrict__ r, const T *__restrict__ z, Reducer R,
+                                             const int *it, int baseEven, int baseOdd)
 {
+    const int base = (*it & 1) ? baseOdd : baseEven;
     double acc[3] = {0.0, 0.0, 0.0};
-    NB_LINE_LOOP(v)
+    NB_TILE_LOOP(v)
     {
         int i, j, k;
         long long c;
-        LineCell(v, line, f, i, j, k, c);
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
         const double rv = (double)r[c], zv = (double)z[c];
         acc[0] += rv * zv;
         acc[1] += zv;
@@ -440,10 +497,11 @@ __global__ void __launch_bounds__(kBlock) k_dot(LevelView v, const T *__restrict
 }
 
 template <typename T>
-void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, int base, cudaStream_t st)
+void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, const int *it, int baseEven, int baseOdd,
+               cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_dot<T><<<LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks), kBlock, 0, st>>>(v, r, z, R, base);
+    k_dot<T><<<TileGrid(v), kTile, 0, st>>>(v, r, z, R, it, baseEven, baseOdd);
 }
 
 __device__ __forceinline__ double RzEff(const double *S, int base, int n, int singular)
@@ -451,122 +509,129 @@ __device__ __forceinline__ double RzEff(const double *S, int base, int n, int si
     return singular ? S[base] - (S[base + 1] / (double)n) * S[base + 2] : S[base];
 }
 
+// p_new = (z - mean) + beta p_old, q = M p_new, sum p_new.q. The neighbours' p_new are formed from their z and
+// p_old, so p_old and p_new are different arrays. Every load of a cell is issued before any depends on another.
 template <typename T, bool kExact>
-__global__ void __launch_bounds__(kBlock) k_update_p_apply(LevelView v, const T *__restrict__ z,
-                                                           const T *__restrict__ pIn, T *__restrict__ pOut,
-                                                           T *__restrict__ q, Reducer R, const double *S, int first,
-                                                           int baseNew, int baseOld, int n, int singular, int slotPQ)
+__global__ void __launch_bounds__(256) k_update_p_apply(LevelView v, const T *__restrict__ z, T *p0, T *p1,
+                                                        T *__restrict__ q, Reducer R, const double *S, const int *it,
+                                                        int baseEven, int baseOdd, int n, int singular, int slotPQ)
 {
-    const double beta = first ? 0.0 : RzEff(S, baseNew, n, singular) / RzEff(S, baseOld, n, singular);
+    const int iter = *it, par = iter & 1;
+    const T *__restrict__ pIn = par ? p1 : p0;
+    T *__restrict__ pOut = par ? p0 : p1;
+    const int baseNew = par ? baseOdd : baseEven, baseOld = par ? baseEven : baseOdd;
+    const double beta = iter == 0 ? 0.0 : RzEff(S, baseNew, n, singular) / RzEff(S, baseOld, n, singular);
     const T b = (T)beta;
     const T mean = singular ? (T)(S[baseNew + 1] / (double)n) : (T)0;
     double acc[1] = {0.0};
-    NB_LINE_LOOP(v)
+    NB_TILE_LOOP(v)
     {
         int i, j, k;
         long long c;
-        LineCell(v, line, f, i, j, k, c);
-        if (v.types[c] != FLUID) continue;
-        T cq[6], diag;
-        unsigned m;
-        Stencil<T, kExact>(v, i, j, k, c, cq, diag, m);
-        const T pc = (z[c] - mean) + b * pIn[c];
-        T s = diag * pc;
-        const int nq = v.dim == 3 ? 6 : 4;
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
+        const unsigned code = v.code[c];
+        const long long o[6] = {v.sI, -v.sI, v.sJ, -v.sJ, 1, -1};
+        T zn[6], pn[6];
 #pragma unroll
         for (int qq = 0; qq < 6; qq++)
         {
-            if (qq >= nq || !(m >> qq & 1u)) continue;
-            const long long nb = c + NbrOffset(v, qq);
-            T pn;
+            zn[qq] = z[c + o[qq]];
+            pn[qq] = pIn[c + o[qq]];
+        }
+        const T zc = z[c], pcOld = pIn[c];
+        if (!(code & CODE_UNKNOWN)) continue;
+        T cq[6], diag;
+        Stencil<T, kExact>(v, i, j, k, c, code, cq, diag);
+        const T pc = (zc - mean) + b * pcOld;
+        T sum = diag * pc;
+#pragma unroll
+        for (int qq = 0; qq < 6; qq++)
+        {
+            T pnew = (zn[qq] - mean) + b * pn[qq];
             if (singular)
             {
                 const int ni = i + (qq == 0) - (qq == 1), nj = j + (qq == 2) - (qq == 3), nk = k + (qq == 4) - (qq == 5);
-                pn = OnRing(v, ni, nj, nk) ? (T)0 : (z[nb] - mean) + b * pIn[nb];
+                if (OnRing(v, ni, nj, nk)) pnew = (T)0;
             }
-            else
-                pn = z[nb] + b * pIn[nb];
-            s -= cq[qq] * pn;
+            sum -= ((code >> qq) & 1u) ? cq[qq] * pnew : (T)0;
         }
         pOut[c] = pc;
-        q[c] = s;
-        acc[0] += (double)pc * (double)s;
+        q[c] = sum;
+        acc[0] += (double)pc * (double)sum;
     }
     GridReduce<1>(R, acc, slotPQ);
 }
 
 template <typename T>
-void LaunchUpdatePApply(const LevelView &v, const T *z, const T *pIn, T *pOut, T *q, const Reducer &R,
-                        const double *S, int first, int baseNew, int baseOld, int n, int singular, int slotPQ,
-                        int exact, cudaStream_t st)
+void LaunchUpdatePApply(const LevelView &v, const T *z, T *p0, T *p1, T *q, const Reducer &R, const double *S,
+                        const int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int exact,
+                        cudaStream_t st)
 {
-    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
+    NB_COUNT_LAUNCH();
     if (exact)
-        {
-            NB_COUNT_LAUNCH();
-            k_update_p_apply<T, true><<<blocks, kBlock, 0, st>>>(v, z, pIn, pOut, q, R, S, first, baseNew, baseOld, n,
+        k_update_p_apply<T, true><<<TileGrid(v), kTile, 0, st>>>(v, z, p0, p1, q, R, S, it, baseEven, baseOdd, n,
                                                                  singular, slotPQ);
-        }
     else
-        {
-            NB_COUNT_LAUNCH();
-            k_update_p_apply<T, false><<<blocks, kBlock, 0, st>>>(v, z, pIn, pOut, q, R, S, first, baseNew, baseOld, n,
+        k_update_p_apply<T, false><<<TileGrid(v), kTile, 0, st>>>(v, z, p0, p1, q, R, S, it, baseEven, baseOdd, n,
                                                                   singular, slotPQ);
-        }
 }
 
+// alpha = rz/pq; x += alpha p_new; r -= alpha q; sum r.r. The last block advances the iteration counter.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_update_xr(LevelView v, T *__restrict__ x, T *__restrict__ r,
-                                                      const T *__restrict__ p, const T *__restrict__ q, Reducer R,
-                                                      const double *S, int baseRZ, int n, int singular, int slotPQ,
-                                                      int slotRR)
+__global__ void __launch_bounds__(256) k_update_xr(LevelView v, T *__restrict__ x, T *__restrict__ r, const T *p0,
+                                                   const T *p1, const T *__restrict__ q, Reducer R, const double *S,
+                                                   int *it, int baseEven, int baseOdd, int n, int singular,
+                                                   int slotPQ, int slotRR)
 {
-    const double alpha = RzEff(S, baseRZ, n, singular) / S[slotPQ];
+    const int par = *it & 1;
+    const T *__restrict__ p = par ? p0 : p1;
+    const int base = par ? baseOdd : baseEven;
+    const double alpha = RzEff(S, base, n, singular) / S[slotPQ];
     const T a = (T)alpha;
     double acc[1] = {0.0};
-    NB_LINE_LOOP(v)
+    NB_TILE_LOOP(v)
     {
         int i, j, k;
         long long c;
-        LineCell(v, line, f, i, j, k, c);
-        const T pv = p[c];
-        if (pv == (T)0 && q[c] == (T)0) { const double rv = (double)r[c]; acc[0] += rv * rv; continue; }
-        x[c] += a * pv;
-        const T rn = r[c] - a * q[c];
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
+        const T pv = p[c], qv = q[c], xv = x[c], rv = r[c];
+        x[c] = xv + a * pv;
+        const T rn = rv - a * qv;
         r[c] = rn;
         acc[0] += (double)rn * (double)rn;
     }
-    GridReduce<1>(R, acc, slotRR);
+    GridReduce<1>(R, acc, slotRR, 0, it);
 }
 
 template <typename T>
-void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p, const T *q, const Reducer &R, const double *S,
-                    int baseRZ, int n, int singular, int slotPQ, int slotRR, cudaStream_t st)
+void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p0, const T *p1, const T *q, const Reducer &R,
+                    const double *S, int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int slotRR,
+                    cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_update_xr<T><<<LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks), kBlock, 0, st>>>(
-        v, x, r, p, q, R, S, baseRZ, n, singular, slotPQ, slotRR);
+    k_update_xr<T><<<TileGrid(v), kTile, 0, st>>>(v, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, n, singular,
+                                                  slotPQ, slotRR);
 }
 
 template <typename Tin, typename Tout>
-__global__ void __launch_bounds__(kBlock) k_scale_copy(LevelView v, const Tin *x, Tout *y, double s)
+__global__ void __launch_bounds__(256) k_scale_copy(LevelView v, const Tin *x, Tout *y, double sc)
 {
-    NB_LINE_LOOP(v)
+    NB_TILE_LOOP(v)
     {
         int i, j, k;
         long long c;
-        LineCell(v, line, f, i, j, k, c);
-        if (v.types[c] != FLUID) continue;
-        y[c] = (Tout)((double)x[c] * s);
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
+        if (!(v.code[c] & CODE_UNKNOWN)) continue;
+        y[c] = (Tout)((double)x[c] * sc);
     }
 }
 
 template <typename Tin, typename Tout>
 void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaStream_t st)
 {
-    if (v.nLines <= 0) return;
+    if (v.fastLen <= 0 || v.midLen <= 0) return;
     NB_COUNT_LAUNCH();
-    k_scale_copy<Tin, Tout><<<Blocks(v), kBlock, 0, st>>>(v, x, y, s);
+    k_scale_copy<Tin, Tout><<<TileGrid(v), kTile, 0, st>>>(v, x, y, s);
 }
 
 // ---- instantiations ----
@@ -577,11 +642,12 @@ void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaSt
     template void LaunchRestrict<T>(const LevelView &, const LevelView &, const T *, T *, cudaStream_t);           \
     template void LaunchProlong<T>(const LevelView &, const LevelView &, const T *, T *, cudaStream_t);            \
     template void LaunchCoarseSolve<T>(const LevelView &, const T *, T *, int, cudaStream_t);                      \
-    template void LaunchDot<T>(const LevelView &, const T *, const T *, const Reducer &, int, cudaStream_t);       \
-    template void LaunchUpdatePApply<T>(const LevelView &, const T *, const T *, T *, T *, const Reducer &,        \
-                                        const double *, int, int, int, int, int, int, int, cudaStream_t);          \
-    template void LaunchUpdateXR<T>(const LevelView &, T *, T *, const T *, const T *, const Reducer &,            \
-                                    const double *, int, int, int, int, int, cudaStream_t);
+    template void LaunchDot<T>(const LevelView &, const T *, const T *, const Reducer &, const int *, int, int,     \
+                               cudaStream_t);                                                                      \
+    template void LaunchUpdatePApply<T>(const LevelView &, const T *, T *, T *, T *, const Reducer &,              \
+                                        const double *, const int *, int, int, int, int, int, int, cudaStream_t);  \
+    template void LaunchUpdateXR<T>(const LevelView &, T *, T *, const T *, const T *, const T *, const Reducer &, \
+                                    const double *, int *, int, int, int, int, int, int, cudaStream_t);
 NB_INST(float)
 NB_INST(double)
 template void LaunchScaleCopy<double, float>(const LevelView &, const double *, float *, double, cudaStream_t);

@@ -15,6 +15,7 @@ namespace nb
 // Kernel launches made by this library in this process (nereus_b200_kernel_launches).
 extern std::atomic<long long> g_launches;
 #define NB_COUNT_LAUNCH() ::nb::g_launches.fetch_add(1, std::memory_order_relaxed)
+#define NB_COUNT_LAUNCHES(n) ::nb::g_launches.fetch_add((n), std::memory_order_relaxed)
 
 // ---- nb_exact.cu: reference-exact kernels ----
 void LaunchLabelCells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
@@ -45,7 +46,24 @@ void LaunchGather(const LevelView &v, const int32_t *idp, const double *grid, do
 void LaunchScatterVolume(const LevelView &v, const int32_t *idp, const double *compact, double *grid, int volume,
                          cudaStream_t st);
 
+// ---- nb_fused.cu: one red-black sweep per launch on 3D levels (shared-memory tiles, slow-axis marching) ----
+template <typename T> void PrepareSweeps();
+template <typename T>
+void LaunchRBSweep(const LevelView &v, const LevelView &cv, const T *r, const T *eIn, const T *ec, T *eOut,
+                   int firstColour, bool first, bool prolong, bool dot, const Reducer &R, const int *it, int baseEven,
+                   int baseOdd, cudaStream_t st);
+
+// ---- nb_tail.cu: the coarse end of the V-cycle in one thread block, in shared memory ----
+constexpr int kMaxTailLevels = 8;
+constexpr size_t kTailMaxSmem = 200 * 1024;
+template <typename T> size_t TailSmemBytes(const LevelView *levels, int nlev);
+template <typename T> bool PrepareTail(size_t bytes);
+template <typename T>
+void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pre, int post, int coarseSweeps,
+                cudaStream_t st);
+
 // ---- nb_kernels.cu: multigrid and PCG kernels, T = float (inner solve) or double (plain FP64) ----
+void LaunchBuildCodes(const LevelView &v, uint8_t *code, cudaStream_t st);
 void LaunchCoarsenTypes(const LevelView &fine, const LevelView &coarse, uint8_t *coarseTypes, cudaStream_t st);
 
 template <typename T> void LaunchSmoothFirst(const LevelView &v, const T *r, T *e, cudaStream_t st);
@@ -64,15 +82,20 @@ template <typename T> void LaunchCoarseSolve(const LevelView &v, const T *r, T *
 //   pupd:  beta = first ? 0 : rz_eff(new)/rz_eff(old); pOut = (z - mean) + beta pIn; q = M pOut;
 //          out[slotPQ] = sum pOut.q
 //   xr:    alpha = rz_eff/S[pq]; x += alpha p; r -= alpha q; out[slotRR] = sum r.r
+// The iteration number lives on the device (*it, advanced by the x,r update's last block), so one captured graph
+// serves every iteration: even iterations read p0 and write p1 and use the scalar block baseEven, odd ones the
+// other way round; iteration 0 takes beta = 0.
 template <typename T>
-void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, int base, cudaStream_t st);
+void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, const int *it, int baseEven, int baseOdd,
+               cudaStream_t st);
 template <typename T>
-void LaunchUpdatePApply(const LevelView &v, const T *z, const T *pIn, T *pOut, T *q, const Reducer &R,
-                        const double *S, int first, int baseNew, int baseOld, int n, int singular, int slotPQ,
-                        int exact, cudaStream_t st);
+void LaunchUpdatePApply(const LevelView &v, const T *z, T *p0, T *p1, T *q, const Reducer &R, const double *S,
+                        const int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int exact,
+                        cudaStream_t st);
 template <typename T>
-void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p, const T *q, const Reducer &R, const double *S,
-                    int baseRZ, int n, int singular, int slotPQ, int slotRR, cudaStream_t st);
+void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p0, const T *p1, const T *q, const Reducer &R,
+                    const double *S, int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int slotRR,
+                    cudaStream_t st);
 // y = s * x over the level's unknowns (x and y may alias)
 template <typename Tin, typename Tout>
 void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaStream_t st);

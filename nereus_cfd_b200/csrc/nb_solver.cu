@@ -40,6 +40,18 @@ LevelView LevelData::view() const
     }
     if (v.nLines < 0 || v.lineLen <= 0) v.nLines = 0;
     if (v.lineDiv <= 0) v.lineDiv = 1;
+    v.fastLen = std::max(0, dim == 3 ? Nz - 2 : Nx - 2);
+    v.midLen = std::max(0, dim == 3 ? Nx - 2 : Ny - 2);
+    v.slowLen = dim == 3 ? std::max(0, Ny - 2) : 1;
+    {
+        // reduction launches march far enough along the slow axis to be about two waves of 8 blocks per SM (their
+        // partial sums stay few); the other stencil launches take one step per block
+        const long long perPlane = (long long)((v.fastLen + kTileF - 1) / kTileF) * ((v.midLen + kTileM - 1) / kTileM);
+        const long long target = 148 * 16;
+        long long chunk = perPlane > 0 ? (v.slowLen * perPlane + target - 1) / target : 1;
+        v.slowChunk = (int)std::max(1LL, std::min<long long>(chunk, std::max(1, v.slowLen)));
+    }
+    v.code = code.p;
     v.types = types.p;
     v.stretched = stretched ? 1 : 0;
     v.gamma = gamma;
@@ -59,6 +71,8 @@ template <> float *LevelData::e<float>() { return e32.p; }
 template <> double *LevelData::e<double>() { return e64.p; }
 template <> float *LevelData::res<float>() { return res32.p; }
 template <> double *LevelData::res<double>() { return res64.p; }
+template <> float *LevelData::f<float>() { return f32.p; }
+template <> double *LevelData::f<double>() { return f64.p; }
 
 static void UploadTables(LevelData &Lv, cudaStream_t st)
 {
@@ -115,7 +129,9 @@ void Context::BuildHierarchy()
         L0.gamma = 1.0;
         for (int a = 0; a < 3; a++) { L0.w[a] = wt[a]; L0.g[a] = gt[a]; }
         L0.types.upload(layout.data(), layout.size(), st);
+        L0.code.alloc(layout.size());
         UploadTables(L0, st);
+        LaunchBuildCodes(L0.view(), L0.code.p, st);
         L.push_back(std::move(L0));
     }
     const int maxLevels = std::max(1, opt.max_levels);
@@ -125,7 +141,7 @@ void Context::BuildHierarchy()
         const int nx = F.Nx - 2, ny = F.Ny - 2, nz = dim == 3 ? F.Nz - 2 : 1;
         const int mn = dim == 3 ? std::min(nx, std::min(ny, nz)) : std::min(nx, ny);
         const long long interior = (long long)nx * ny * nz;
-        if (mn < 8 || interior <= 512) break;
+        if (mn < 4 || interior <= 8) break; // down to about 2 cells a side: the coarse end runs in shared memory
         LevelData C;
         C.dim = dim;
         C.Nx = (nx + 1) / 2 + 2;
@@ -139,11 +155,35 @@ void Context::BuildHierarchy()
         if (dim == 3) CoarseAxis(F.w[2], F.Nz, C.Nz, C.w[2], C.g[2]);
         else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }
         C.types.alloc((size_t)C.cells);
+        C.code.alloc((size_t)C.cells);
         UploadTables(C, st);
         LaunchCoarsenTypes(F.view(), C.view(), C.types.p, st);
+        LaunchBuildCodes(C.view(), C.code.p, st);
         L.push_back(std::move(C));
     }
     NB_CK(cudaGetLastError());
+    // The tail: the first level from which every coarser level has at most kTailCellCap cells and all of them fit
+    // in one block's shared memory in the solver's precision.
+    const bool mixed = opt.precision == NB_PRECISION_MIXED;
+    tailStart = (int)L.size();
+    std::vector<LevelView> views;
+    for (auto &Lv : L) views.push_back(Lv.view());
+    for (int l = (int)L.size() - 1; l >= 0; l--)
+    {
+        const int nl = (int)L.size() - l;
+        if (nl > kMaxTailLevels || L[l].cells > kTailCellCap) break;
+        const size_t bytes = mixed ? TailSmemBytes<float>(&views[l], nl) : TailSmemBytes<double>(&views[l], nl);
+        if (bytes > kTailMaxSmem) break;
+        tailStart = l;
+    }
+    if (tailStart < (int)L.size())
+    {
+        const bool ok = mixed ? PrepareTail<float>(kTailMaxSmem) : PrepareTail<double>(kTailMaxSmem);
+        if (!ok) tailStart = (int)L.size();
+    }
+    if (mixed) PrepareSweeps<float>();
+    else PrepareSweeps<double>();
+    cudaGetLastError(); // an attribute the device refuses leaves the per-colour path, checked at launch
 }
 
 void Context::AllocVectors()
@@ -154,19 +194,22 @@ void Context::AllocVectors()
         LevelData &Lv = L[l];
         const size_t c = (size_t)Lv.cells;
         const bool last = l + 1 == L.size();
+        const bool fused = FusedLevel((int)l);
         if (mixed)
         {
             Lv.r32.alloc(c); Lv.r32.zero(st);
             Lv.e32.alloc(c); Lv.e32.zero(st);
             if (!last) { Lv.res32.alloc(c); Lv.res32.zero(st); }
-            Lv.r64.release(); Lv.e64.release(); Lv.res64.release();
+            if (fused) { Lv.f32.alloc(c); Lv.f32.zero(st); } else Lv.f32.release();
+            Lv.r64.release(); Lv.e64.release(); Lv.res64.release(); Lv.f64.release();
         }
         else
         {
             Lv.r64.alloc(c); Lv.r64.zero(st);
             Lv.e64.alloc(c); Lv.e64.zero(st);
             if (!last) { Lv.res64.alloc(c); Lv.res64.zero(st); }
-            Lv.r32.release(); Lv.e32.release(); Lv.res32.release();
+            if (fused) { Lv.f64.alloc(c); Lv.f64.zero(st); } else Lv.f64.release();
+            Lv.r32.release(); Lv.e32.release(); Lv.res32.release(); Lv.f32.release();
         }
     }
     const size_t c = Cells();
@@ -205,12 +248,14 @@ Context::Context(const nb_options &o) : opt(o)
         NB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         ownStream = true;
     }
-    red.maxBlocks = 148 * 8;
+    red.maxBlocks = 1 << 16; // partial sums per reduction launch (the tile grids stay well below)
     partials.alloc((size_t)red.maxBlocks * 4);
     slots.alloc(S_COUNT);
     slots.zero(st);
     counter.alloc(1);
     counter.zero(st);
+    iter.alloc(1);
+    iter.zero(st);
     red.partials = partials.p;
     red.out = slots.p;
     red.counter = counter.p;
@@ -222,6 +267,7 @@ Context::Context(const nb_options &o) : opt(o)
 Context::~Context()
 {
     if (st) cudaStreamSynchronize(st);
+    for (auto &g : graphs) g.Release();
     for (cudaEvent_t e : evPool) cudaEventDestroy(e);
     if (hostSlots) cudaFreeHost(hostSlots);
     if (ev0) cudaEventDestroy(ev0);
@@ -234,15 +280,26 @@ Context::~Context()
 void Context::ProfBegin(int id, double bytes)
 {
     if (!(profMask >> id & 1u)) return;
-    if (evUsed + 2 > evPool.size())
-        for (int q = 0; q < 256; q++)
-        {
-            cudaEvent_t e;
-            NB_CK(cudaEventCreate(&e));
-            evPool.push_back(e);
-        }
-    profA = evPool[evUsed++];
-    NB_CK(cudaEventRecord(profA, st));
+    cudaEvent_t a;
+    if (capturing)
+    {
+        NB_CK(cudaEventCreate(&a));
+        capturing->events.push_back(a);
+    }
+    else
+    {
+        if (evUsed + 2 > evPool.size())
+            for (int q = 0; q < 256; q++)
+            {
+                cudaEvent_t e;
+                NB_CK(cudaEventCreate(&e));
+                evPool.push_back(e);
+            }
+        a = evPool[evUsed++];
+    }
+    profA = a;
+    // inside a capture, an external record becomes an event-record node that every replay executes
+    NB_CK(capturing ? cudaEventRecordWithFlags(profA, st, cudaEventRecordExternal) : cudaEventRecord(profA, st));
     profOpen = id;
     profBytes = bytes;
 }
@@ -250,10 +307,39 @@ void Context::ProfBegin(int id, double bytes)
 void Context::ProfEnd()
 {
     if (profOpen < 0) return;
-    cudaEvent_t b = evPool[evUsed++];
-    NB_CK(cudaEventRecord(b, st));
-    prof.push_back({profOpen, profA, b, profBytes});
+    cudaEvent_t b;
+    if (capturing)
+    {
+        NB_CK(cudaEventCreate(&b));
+        capturing->events.push_back(b);
+    }
+    else
+        b = evPool[evUsed++];
+    NB_CK(capturing ? cudaEventRecordWithFlags(b, st, cudaEventRecordExternal) : cudaEventRecord(b, st));
+    (capturing ? capturing->prof : prof).push_back({profOpen, profA, b, profBytes});
     profOpen = -1;
+}
+
+static void Accumulate(const std::vector<Context::ProfRecord> &recs, Context::ProfTotal *tot)
+{
+    for (const Context::ProfRecord &r : recs)
+    {
+        float m = 0.0f;
+        NB_CK(cudaEventElapsedTime(&m, r.a, r.b));
+        tot[r.id].launches += 1;
+        tot[r.id].ms += m;
+        tot[r.id].bytes += r.bytes;
+    }
+}
+
+// Resolve the stream-launch records into the totals and recycle their events (the stream must be idle).
+void Context::ProfFlush()
+{
+    if (prof.empty()) return;
+    NB_CK(cudaStreamSynchronize(st));
+    Accumulate(prof, profTot);
+    prof.clear();
+    evUsed = 0;
 }
 
 void Context::ProfClear()
@@ -261,25 +347,28 @@ void Context::ProfClear()
     prof.clear();
     evUsed = 0;
     profOpen = -1;
+    for (auto &t : profTot) t = ProfTotal();
 }
 
 void Context::ProfRead(int id, int *launches, double *ms, double *bytesPerLaunch)
 {
-    NB_CK(cudaStreamSynchronize(st));
-    int cnt = 0;
-    double t = 0.0, by = 0.0;
-    for (const ProfRecord &r : prof)
-        if (r.id == id)
-        {
-            float m = 0.0f;
-            NB_CK(cudaEventElapsedTime(&m, r.a, r.b));
-            t += m;
-            by += r.bytes;
-            cnt++;
-        }
-    *launches = cnt;
-    *ms = t;
-    *bytesPerLaunch = cnt ? by / cnt : 0.0;
+    ProfFlush();
+    const ProfTotal &t = profTot[id];
+    *launches = (int)t.launches;
+    *ms = t.ms;
+    *bytesPerLaunch = t.launches ? t.bytes / (double)t.launches : 0.0;
+}
+
+void Context::IterGraph::Release()
+{
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g) cudaGraphDestroy(g);
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+    exec = nullptr;
+    g = nullptr;
+    events.clear();
+    prof.clear();
+    mask = 0;
 }
 
 double Context::ReadSlot(int s)
@@ -319,6 +408,8 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
                std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
     }
     if (same) return; // PressureLayoutChanged: nothing moved
+    NB_CK(cudaStreamSynchronize(st));
+    for (auto &g : graphs) g.Release(); // they hold the old hierarchy's pointers
     dim = dim_;
     Nx = Nx_;
     Ny = Ny_;
@@ -406,11 +497,25 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
     auto prof = [&](int id, double bytesPerCell) {
         ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
     };
+    if (l == tailStart)
+    {
+        std::vector<LevelView> views;
+        for (size_t q = (size_t)l; q < L.size(); q++) views.push_back(L[q].view());
+        prof(NB_K_COARSE, 0.0);
+        LaunchTail<T>(views.data(), (int)views.size(), r, e, opt.pre_sweeps, opt.post_sweeps, opt.coarse_sweeps, st);
+        ProfEnd();
+        return;
+    }
     if (l + 1 == (int)L.size())
     {
         prof(NB_K_COARSE, 0.0);
         LaunchCoarseSolve<T>(v, r, e, opt.coarse_sweeps, st);
         ProfEnd();
+        return;
+    }
+    if (FusedLevel(l))
+    {
+        VCycleFused<T>(l, r, e);
         return;
     }
     const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
@@ -454,32 +559,134 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
     }
 }
 
+// The V-cycle on a 3D level with one launch per red-black sweep (nb_fused.cu): the pre-smoothing from zero into f,
+// the residual and its restriction, the coarser levels, then the post-smoothing that reads f + P(e_coarse) and
+// writes e. On level 0 the last sweep also sums r.z for CG (IterBody then skips its own r.z launch).
+template <typename T> void Context::VCycleFused(int l, T *r, T *e)
+{
+    LevelData &Lv = L[l];
+    const LevelView v = Lv.view();
+    LevelData &Lc = L[l + 1];
+    const LevelView vc = Lc.view();
+    const double s = sizeof(T), cells = (double)Lv.cells;
+    auto prof = [&](int id, double bytesPerCell) {
+        ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
+    };
+    const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
+    T *f = Lv.f<T>(), *res = Lv.res<T>();
+    // pre-smoothing: the first sweep from zero (reads r, codes; writes the iterate), the rest in turn, ending in f
+    T *dst = (pre % 2 == 1) ? f : e;
+    prof(NB_K_SMOOTH0, s + 1.0 + s);
+    LaunchRBSweep<T>(v, vc, r, nullptr, nullptr, dst, 0, true, false, false, red, iter.p, S_RZ0, S_RZ1, st);
+    ProfEnd();
+    for (int q = 1; q < pre; q++)
+    {
+        T *src = dst;
+        dst = (src == f) ? e : f;
+        prof(NB_K_SMOOTH0, 3.0 * s + 1.0);
+        LaunchRBSweep<T>(v, vc, r, src, nullptr, dst, 0, false, false, false, red, iter.p, S_RZ0, S_RZ1, st);
+        ProfEnd();
+    }
+    prof(NB_K_RESIDUAL0, 3.0 * s + 1.0);
+    LaunchLevelResidual<T>(v, r, f, res, st);
+    ProfEnd();
+    prof(NB_K_RESTRICT0, s + s / 8.0);
+    LaunchRestrict<T>(v, vc, res, Lc.r<T>(), st);
+    ProfEnd();
+    VCycle<T>(l + 1, Lc.r<T>(), Lc.e<T>());
+    // post-smoothing, black first: the first sweep adds the prolonged coarse correction, the last ends in e
+    const bool dotHere = l == 0;
+    T *src = f;
+    dst = (post % 2 == 1) ? e : res;
+    for (int q = 0; q < post; q++)
+    {
+        const bool lastSweep = q + 1 == post;
+        prof(q == 0 ? NB_K_PROLONG0 : NB_K_SMOOTH0, 3.0 * s + 1.0 + (q == 0 ? s / 8.0 : 0.0));
+        LaunchRBSweep<T>(v, vc, r, src, Lc.e<T>(), dst, 1, false, q == 0, dotHere && lastSweep, red, iter.p, S_RZ0,
+                         S_RZ1, st);
+        ProfEnd();
+        src = dst;
+        dst = (src == e) ? res : e;
+    }
+}
+
+// One CG iteration on level 0: z = V-cycle(r), r.z, p = z + beta p (and q = M p, p.q), x += alpha p, r -= alpha q,
+// r.r copied to the host. The iteration number and the parity of the p buffers live on the device.
+template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact)
+{
+    const LevelView v0 = L[0].view();
+    const double s = sizeof(T), cells = (double)Cells();
+    const int sing = singular ? 1 : 0;
+    VCycle<T>(0, r, z);
+    if (!FusedLevel(0)) // else the V-cycle's last sweep summed r.z already
+    {
+        ProfBegin(NB_K_DOT, 2.0 * s * cells);
+        LaunchDot<T>(v0, r, z, red, iter.p, S_RZ0, S_RZ1, st);
+        ProfEnd();
+    }
+    ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
+    LaunchUpdatePApply<T>(v0, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, exact ? 1 : 0, st);
+    ProfEnd();
+    ProfBegin(NB_K_XR, 6.0 * s * cells);
+    LaunchUpdateXR<T>(v0, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, S_RR, st);
+    ProfEnd();
+    NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+}
+
 template <typename T>
 int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
                     double *rrEnd)
 {
-    const LevelView v0 = L[0].view();
-    T *p[2] = {p0, p1};
     NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * Cells(), st));
+    NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
+    IterGraph *G = nullptr;
+    if (opt.use_graphs)
+    {
+        G = &graphs[sizeof(T) == 8 ? 1 : 0];
+        if (G->exec && G->mask != profMask) G->Release();
+        if (!G->exec)
+        {
+            ProfFlush();
+            const long long before = g_launches.load();
+            NB_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            capturing = G;
+            try
+            {
+                IterBody<T>(x, r, z, p0, p1, q, exact);
+            }
+            catch (...)
+            {
+                capturing = nullptr;
+                cudaGraph_t dead = nullptr;
+                cudaStreamEndCapture(st, &dead);
+                if (dead) cudaGraphDestroy(dead);
+                throw;
+            }
+            capturing = nullptr;
+            NB_CK(cudaStreamEndCapture(st, &G->g));
+            NB_CK(cudaGraphInstantiate(&G->exec, G->g, 0));
+            G->mask = profMask;
+            G->launches = g_launches.load() - before; // counted when replayed, not when recorded
+            NB_COUNT_LAUNCHES(-G->launches);
+        }
+    }
     double rr = rrStart;
     int it = 0;
     while (it < maxIt && rr > rrTarget)
     {
-        VCycle<T>(0, r, z);
-        const int baseNew = (it & 1) ? S_RZ1 : S_RZ0, baseOld = (it & 1) ? S_RZ0 : S_RZ1;
-        const double s = sizeof(T), cells = (double)Cells();
-        ProfBegin(NB_K_DOT, 2.0 * s * cells);
-        LaunchDot<T>(v0, r, z, red, baseNew, st);
-        ProfEnd();
-        T *pin = p[it & 1], *pout = p[(it + 1) & 1];
-        ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
-        LaunchUpdatePApply<T>(v0, z, pin, pout, q, red, slots.p, it == 0, baseNew, baseOld, n, singular ? 1 : 0,
-                              S_PQ, exact ? 1 : 0, st);
-        ProfEnd();
-        ProfBegin(NB_K_XR, 6.0 * s * cells);
-        LaunchUpdateXR<T>(v0, x, r, pout, q, red, slots.p, baseNew, n, singular ? 1 : 0, S_PQ, S_RR, st);
-        ProfEnd();
-        rr = ReadSlot(S_RR);
+        if (G)
+        {
+            NB_COUNT_LAUNCHES(G->launches);
+            NB_CK(cudaGraphLaunch(G->exec, st));
+            NB_CK(cudaStreamSynchronize(st));
+            if (!G->prof.empty()) Accumulate(G->prof, profTot);
+        }
+        else
+        {
+            IterBody<T>(x, r, z, p0, p1, q, exact);
+            NB_CK(cudaStreamSynchronize(st));
+        }
+        rr = hostSlots[S_RR];
         it++;
         if (!std::isfinite(rr)) break;
     }
@@ -734,5 +941,7 @@ void Context::GetIdp(int32_t *out)
 
 template void Context::VCycle<float>(int, float *, float *);
 template void Context::VCycle<double>(int, double *, double *);
+template void Context::VCycleFused<float>(int, float *, float *);
+template void Context::VCycleFused<double>(int, double *, double *);
 
 } // namespace nb

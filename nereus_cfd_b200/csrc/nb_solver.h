@@ -94,13 +94,14 @@ struct LevelData
     std::vector<double> w[3], g[3];
     DevArray<double> dw[3], dg[3];
     DevArray<float> dw32[3], dig32[3];
-    DevArray<uint8_t> types;
-    DevArray<float> r32, e32, res32;
-    DevArray<double> r64, e64, res64;
+    DevArray<uint8_t> types, code;
+    DevArray<float> r32, e32, res32, f32; // f: the pre-smoothed iterate of a fused V-cycle
+    DevArray<double> r64, e64, res64, f64;
     LevelView view() const;
     template <typename T> T *r();
     template <typename T> T *e();
     template <typename T> T *res();
+    template <typename T> T *f();
 };
 
 struct Context
@@ -118,6 +119,8 @@ struct Context
     std::vector<uint8_t> layout;
     std::vector<double> wt[3], gt[3];
     std::vector<LevelData> L;
+    int tailStart = 0;                       // levels from here down run in one shared-memory block (nb_tail.cu)
+    static constexpr long long kTailCellCap = 8192;
     DevArray<int32_t> idp;
     int n = 0;
     bool singular = false;
@@ -142,24 +145,47 @@ struct Context
 
     int lastIterations = 0;
 
-    // per-kernel device timing (nereus_b200_profile_*)
+    // per-kernel device timing (nereus_b200_profile_*): CUDA events around the selected launches, on the context's
+    // stream, or as event nodes inside a captured iteration graph, summed per kernel id
     struct ProfRecord
     {
         int id;
         cudaEvent_t a, b;
         double bytes;
     };
+    struct ProfTotal
+    {
+        long long launches = 0;
+        double ms = 0.0, bytes = 0.0;
+    };
     unsigned profMask = 0;
     std::vector<cudaEvent_t> evPool;
     size_t evUsed = 0;
-    std::vector<ProfRecord> prof;
+    std::vector<ProfRecord> prof;    // stream launches not yet read
+    ProfTotal profTot[NB_K_COUNT];
     int profOpen = -1;
     cudaEvent_t profA = nullptr;
     double profBytes = 0.0;
     void ProfBegin(int id, double bytes);
     void ProfEnd();
     void ProfClear();
+    void ProfFlush();
     void ProfRead(int id, int *launches, double *ms, double *bytesPerLaunch);
+
+    // one captured CG iteration (V-cycle, r.z, direction update + apply, x/r update, rr to the host) per precision
+    struct IterGraph
+    {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<ProfRecord> prof;
+        std::vector<cudaEvent_t> events;
+        unsigned mask = 0;
+        long long launches = 0; // kernels one replay runs
+        void Release();
+    };
+    IterGraph graphs[2]; // [0] float, [1] double
+    IterGraph *capturing = nullptr;
+    DevArray<int> iter;  // the CG iteration number, advanced on the device
 
     Context(const nb_options &o);
     ~Context();
@@ -192,6 +218,9 @@ struct Context
     int SolveMixed(double tol, double **xOut, nb_result *out);
     int SolveFP64(double tol, double **xOut, nb_result *out);
     template <typename T> void VCycle(int l, T *r, T *e);
+    template <typename T> void VCycleFused(int l, T *r, T *e);
+    bool FusedLevel(int l) const { return opt.fused_sweeps && dim == 3 && l < tailStart && l + 1 < (int)L.size(); }
+    template <typename T> void IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact);
     template <typename T>
     int RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
                double *rrEnd);
