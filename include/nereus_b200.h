@@ -187,6 +187,19 @@ typedef struct nb_scene
 int nereus_b200_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
                             const nb_scene *scene, uint8_t *cellTypes);
 
+/* ---- IDP numbering without allocation. No counterpart in the reference: its IDP loop runs inside
+ *      AssembleSystem (PressureSolver3D.cpp:133-139); this is the same numbering as nereus_b200_get_idp gives after
+ *      nereus_b200_set_layout, for callers that must not allocate device memory at the point they renumber. ----
+ * cellTypes (Nx*Ny*Nz bytes), idp (Nx*Ny*Nz int32) and n (one int32) are DEVICE pointers on `device`; the call is
+ * asynchronous on `stream` (a cudaStream_t, NULL = the default stream). idp gets -1 off the system, *n the count.
+ * Makes no cudaMalloc/cudaFree: its scratch is one fixed 2 MiB array per device, enough for grids of at most
+ * NB_NOALLOC_MAX_LINES interior lines ((Ny-2)*(Nx-2) in 3D, Ny-2 in 2D); larger grids get NB_BAD_INPUT.
+ * The first call on a device looks up that array's address (and may load the library's device code), so make it
+ * before any stream capture begins. Calls that overlap in time on one device share the scratch and race. */
+#define NB_NOALLOC_MAX_LINES 262144
+int nereus_b200_number_unknowns_noalloc(int device, int dim, int Nx, int Ny, int Nz, const uint8_t *cellTypes,
+                                        int32_t *idp, int32_t *n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ SOURCES = {
     "nb_fused.cu": [],
     "nb_solver.cu": [],
     "nb_capi.cu": [],
+    "nb_noalloc.cu": [],
 }
 HEADERS = ["nb_device.cuh", "nb_kernels.h", "nb_solver.h"]
 

@@ -86,6 +86,9 @@ SIGNATURES = {
     "nereus_b200_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "nereus_b200_kernel_launches": (ctypes.c_longlong, []),
+    "nereus_b200_number_unknowns_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                           ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                           ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 # kernel ids of nereus_b200_profile_* (include/nereus_b200.h)

@@ -247,6 +247,31 @@ int nereus_b200_get_idp(nb_ctx *ctx, int32_t *idp)
     });
 }
 
+int nereus_b200_number_unknowns_noalloc(int device, int dim, int Nx, int Ny, int Nz, const uint8_t *cellTypes,
+                                        int32_t *idp, int32_t *n, void *stream)
+{
+    static_assert(NB_NOALLOC_MAX_LINES == nb::kNoAllocMaxLines, "header and library disagree on the limit");
+    return Guard([&] {
+        int count = 0;
+        NB_CK(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) throw nb::InputError("no such device");
+        int prev = 0;
+        NB_CK(cudaGetDevice(&prev));
+        NB_CK(cudaSetDevice(device));
+        try
+        {
+            nb::NumberUnknownsNoAlloc(device, dim, Nx, Ny, Nz, cellTypes, idp, n, (cudaStream_t)stream);
+        }
+        catch (...)
+        {
+            cudaSetDevice(prev);
+            throw;
+        }
+        NB_CK(cudaSetDevice(prev));
+        return (int)NB_OK;
+    });
+}
+
 int nereus_b200_export_matrix(nb_ctx *ctx, int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singular)
 {
     if (!ctx || !ctx->c || !rowptr || !col || !val || !nnz || !singular) return Fail(NB_BAD_INPUT, "null argument");

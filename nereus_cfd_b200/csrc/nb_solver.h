@@ -226,4 +226,10 @@ struct Context
                double *rrEnd);
 };
 
+// nb_noalloc.cu: the IDP numbering of device-resident cell types with scratch in a fixed per-device array (no
+// allocation); at most kNoAllocMaxLines interior lines. idp and *n are device memory; asynchronous on st.
+constexpr int kNoAllocMaxLines = 1 << 18;
+void NumberUnknownsNoAlloc(int device, int dim, int Nx, int Ny, int Nz, const uint8_t *types, int32_t *idp,
+                           int32_t *n, cudaStream_t st);
+
 } // namespace nb
