@@ -64,6 +64,8 @@ typedef struct nb_options
     int use_graphs;      /* 1: each CG iteration (V-cycle included) replays one captured CUDA graph; 0: launches */
     int fused_sweeps;    /* 1: 3D levels smooth with one shared-memory tiled launch per red-black sweep, the
                             prolongation and r.z fused in; 0 (default): one launch per colour */
+    int pair_kernels;    /* 1 (default): FP32 kernels on cell pairs for 3D uniform levels with Nz even; 0: the
+                            general per-cell kernels */
 } nb_options;
 
 typedef struct nb_result

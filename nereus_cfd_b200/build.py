@@ -25,6 +25,7 @@ SOURCES = {
     "nb_kernels.cu": [],
     "nb_tail.cu": [],
     "nb_fused.cu": [],
+    "nb_pairs.cu": [],
     "nb_solver.cu": [],
     "nb_capi.cu": [],
     "nb_noalloc.cu": [],

@@ -62,6 +62,22 @@ template <typename T>
 void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pre, int post, int coarseSweeps,
                 cudaStream_t st);
 
+// ---- nb_pairs.cu: FP32 kernels for 3D levels of a uniform grid with Nz even (cell pairs, unmasked stencil) ----
+bool PairLevelShape(const LevelView &v);
+void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st);
+void LaunchPairFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st);
+void LaunchPairHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st);
+void LaunchPairResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
+                        cudaStream_t st);
+void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
+                      const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int n,
+                      int singular, int slotPQ, cudaStream_t st);
+void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
+                  int baseOdd, cudaStream_t st);
+void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,
+                 const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int n, int singular,
+                 int slotPQ, int slotRR, cudaStream_t st);
+
 // ---- nb_kernels.cu: multigrid and PCG kernels, T = float (inner solve) or double (plain FP64) ----
 void LaunchBuildCodes(const LevelView &v, uint8_t *code, cudaStream_t st);
 void LaunchCoarsenTypes(const LevelView &fine, const LevelView &coarse, uint8_t *coarseTypes, cudaStream_t st);

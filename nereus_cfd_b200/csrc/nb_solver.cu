@@ -7,6 +7,7 @@
 #include "nb_solver.h"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace nb
 {
@@ -160,6 +161,17 @@ void Context::BuildHierarchy()
         LaunchCoarsenTypes(F.view(), C.view(), C.types.p, st);
         LaunchBuildCodes(C.view(), C.code.p, st);
         L.push_back(std::move(C));
+    }
+    // the FP32 cell-pair kernels' diagonal units (mixed precision: the inner solve runs in FP32)
+    for (auto &Lv : L)
+    {
+        const LevelView v = Lv.view();
+        if (opt.precision == NB_PRECISION_MIXED && opt.pair_kernels && PairLevelShape(v))
+        {
+            Lv.du.alloc((size_t)Lv.cells);
+            LaunchBuildDu(v, Lv.du.p, st);
+        }
+        else Lv.du.release();
     }
     NB_CK(cudaGetLastError());
     // The tail: the first level from which every coarser level has at most kTailCellCap cells and all of them fit
@@ -518,6 +530,14 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
         VCycleFused<T>(l, r, e);
         return;
     }
+    if constexpr (std::is_same<T, float>::value)
+    {
+        if (PairLevel(l))
+        {
+            VCyclePairs(l, r, e);
+            return;
+        }
+    }
     const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
     const double half = (3.0 * s + 1.0) / 2.0; // one red-black sweep reads e, r, types and writes e: 3s + 1
     prof(NB_K_SMOOTH0, 2.0 * s + 1.0);
@@ -557,6 +577,50 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
         LaunchSmooth<T>(v, r, e, 0, st);
         ProfEnd();
     }
+}
+
+// The V-cycle on a 3D uniform FP32 level with the cell-pair kernels (nb_pairs.cu): the first red-black sweep from
+// zero in one launch, further sweeps one colour per launch, the residual, then the transfers of nb_kernels.cu.
+void Context::VCyclePairs(int l, float *r, float *e)
+{
+    LevelData &Lv = L[l];
+    const LevelView v = Lv.view();
+    const double s = sizeof(float), cells = (double)Lv.cells;
+    auto prof = [&](int id, double bytesPerCell) {
+        ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
+    };
+    const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
+    const double half = (3.0 * s + 1.0) / 2.0;
+    prof(NB_K_SMOOTH0, s + 1.0 + s); // reads r and du, writes e
+    LaunchPairFirst(v, Lv.du.p, r, e, st);
+    ProfEnd();
+    for (int q = 1; q < pre; q++)
+        for (int c = 0; c < 2; c++)
+        {
+            prof(NB_K_SMOOTH0, half);
+            LaunchPairHalf(v, Lv.du.p, r, e, c, st);
+            ProfEnd();
+        }
+    float *res = Lv.res<float>();
+    prof(NB_K_RESIDUAL0, 3.0 * s + 1.0);
+    LaunchPairResidual(v, Lv.du.p, r, e, res, st);
+    ProfEnd();
+    LevelData &Lc = L[l + 1];
+    const LevelView vc = Lc.view();
+    prof(NB_K_RESTRICT0, s + s / 8.0);
+    LaunchRestrict<float>(v, vc, res, Lc.r<float>(), st);
+    ProfEnd();
+    VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
+    prof(NB_K_PROLONG0, 2.0 * s + s / 8.0 + 1.0);
+    LaunchProlong<float>(v, vc, Lc.e<float>(), e, st);
+    ProfEnd();
+    for (int q = 0; q < post; q++)
+        for (int c = 1; c >= 0; c--)
+        {
+            prof(NB_K_SMOOTH0, half);
+            LaunchPairHalf(v, Lv.du.p, r, e, c, st);
+            ProfEnd();
+        }
 }
 
 // The V-cycle on a 3D level with one launch per red-black sweep (nb_fused.cu): the pre-smoothing from zero into f,
@@ -618,6 +682,23 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
     const double s = sizeof(T), cells = (double)Cells();
     const int sing = singular ? 1 : 0;
     VCycle<T>(0, r, z);
+    if constexpr (std::is_same<T, float>::value)
+    {
+        if (PairLevel(0))
+        {
+            ProfBegin(NB_K_DOT, 2.0 * s * cells);
+            LaunchLinDot(L[0].cells, r, z, red, iter.p, S_RZ0, S_RZ1, st);
+            ProfEnd();
+            ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
+            LaunchPairPApply(v0, L[0].du.p, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, st);
+            ProfEnd();
+            ProfBegin(NB_K_XR, 6.0 * s * cells);
+            LaunchLinXR(L[0].cells, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, S_RR, st);
+            ProfEnd();
+            NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+            return;
+        }
+    }
     if (!FusedLevel(0)) // else the V-cycle's last sweep summed r.z already
     {
         ProfBegin(NB_K_DOT, 2.0 * s * cells);

@@ -95,6 +95,7 @@ struct LevelData
     DevArray<double> dw[3], dg[3];
     DevArray<float> dw32[3], dig32[3];
     DevArray<uint8_t> types, code;
+    DevArray<uint8_t> du;                 // diagonal units for the pair kernels (nb_pairs.cu); empty elsewhere
     DevArray<float> r32, e32, res32, f32; // f: the pre-smoothed iterate of a fused V-cycle
     DevArray<double> r64, e64, res64, f64;
     LevelView view() const;
@@ -220,6 +221,9 @@ struct Context
     template <typename T> void VCycle(int l, T *r, T *e);
     template <typename T> void VCycleFused(int l, T *r, T *e);
     bool FusedLevel(int l) const { return opt.fused_sweeps && dim == 3 && l < tailStart && l + 1 < (int)L.size(); }
+    // the FP32 cell-pair kernels serve this level (its du is built)
+    bool PairLevel(int l) const { return opt.pair_kernels && L[l].du.p != nullptr; }
+    void VCyclePairs(int l, float *r, float *e);
     template <typename T> void IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact);
     template <typename T>
     int RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
