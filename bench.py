@@ -210,16 +210,22 @@ def run_b200(args, rank, world, dist):
     # ---- the chosen form: FP32 MG-PCG inside FP64 refinement ----
     mixed = PressureSolver("mixed", device=dev, stream=stream.cuda_stream, **args.solver_opts)
     mixed.InitializePressureSolver(mac)
-    total_ms, lat, res, launches, clk, prof = timed(mixed, args.steps, args.warmup,
-                                                   profile_mask=(1 << 11) - 1, clocks=True)
+    # the headline: no timing events inside the solve
+    total_ms, lat, res, launches, clk, _ = timed(mixed, args.steps, args.warmup, clocks=True)
     total_ms = max_over_ranks(total_ms)
     value = world * args.steps / (total_ms / 1e3)
+    # the breakdown: events around every kernel of the solve (they cost some time of their own, so the shares come
+    # from this pass and the headline from the one above)
+    _, _, _, _, _, prof = timed(mixed, args.steps, args.warmup, profile_mask=(1 << len(capi.KERNEL_NAMES)) - 1)
 
-    # ---- roofline of the dominant kernel (largest summed device time over the timed region) ----
+    # ---- roofline of the dominant kernel (largest summed device time), timed alone: events around its launches only
     peak, peak_kind = measured_peaks()
     roof = None
     if prof:
-        name, (cnt, ms, bpl) = max(((k, v) for k, v in prof.items() if v[2] > 0), key=lambda kv: kv[1][1])
+        name, _ = max(((k, v) for k, v in prof.items() if v[2] > 0), key=lambda kv: kv[1][1])
+        kid = capi.KERNEL_NAMES.index(name)
+        _, _, _, _, _, prof1 = timed(mixed, args.steps, args.warmup, profile_mask=1 << kid)
+        cnt, ms, bpl = prof1[name]
         per_launch_s = ms / cnt / 1e3
         achieved = bpl / per_launch_s / 1e9
         tr = ncu_traffic(name)

@@ -66,7 +66,7 @@ void nereus_b200_default_options(nb_options *o)
     o->inner_tol = 1e-4;
     o->pre_sweeps = 1;
     o->post_sweeps = 1;
-    o->coarse_sweeps = 8;
+    o->coarse_sweeps = 4;
     o->max_levels = 16;
     o->stream = nullptr;
     o->use_graphs = 1;

@@ -306,10 +306,14 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
 #pragma unroll
     for (int s = 0; s < NV; s++)
     {
+        // L2 loads (the partials were written and fenced by the other blocks; nothing of them sits in this SM's
+        // L1), unrolled so that many are in flight at once
         double t = 0.0;
+        const double *part = R.partials + (size_t)s * R.maxBlocks;
+#pragma unroll 8
         for (unsigned b = tid; b < nblk; b += nthr)
         {
-            const double pv = *((volatile double *)&R.partials[(size_t)s * R.maxBlocks + b]);
+            const double pv = __ldcg(part + b);
             t = op == 0 ? t + pv : fmax(t, pv);
         }
         t = op == 0 ? WarpSum(t) : WarpMax(t);

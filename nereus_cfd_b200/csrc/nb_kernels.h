@@ -67,11 +67,19 @@ bool PairLevelShape(const LevelView &v);
 void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st);
 void LaunchPairFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st);
 void LaunchPairHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st);
+// the same sweep, also summing (r.z, z, r) into the scalar block of the iteration's parity (k_dot's output)
+void LaunchPairHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, const Reducer &R,
+                       const int *it, int baseEven, int baseOdd, cudaStream_t st);
 void LaunchPairResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
                         cudaStream_t st);
 void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
                       const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int n,
                       int singular, int slotPQ, cudaStream_t st);
+void LaunchBuildPext(const LevelView &fine, const LevelView &coarse, uint8_t *pext, cudaStream_t st);
+void LaunchPairProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
+                       float *eFine, cudaStream_t st);
+void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
+                        float *rCoarse, cudaStream_t st);
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
                   int baseOdd, cudaStream_t st);
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,

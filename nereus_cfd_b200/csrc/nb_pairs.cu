@@ -188,10 +188,14 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_first(LevelView v, const 
 }
 
 // One colour of a red-black sweep, in place: e_c = (r_c + gamma * sum of the six neighbours) / diag_c. Every value
-// read has the other colour, so nothing read changes during the sweep.
+// read has the other colour, so nothing read changes during the sweep. kDot (the last sweep of the level-0 V-cycle,
+// whose result is the CG's z): also (sum r.z, sum z, sum r) into the scalar block of the iteration's parity.
+template <bool kDot>
 __global__ void __launch_bounds__(kPairThreads) k_pair_half(LevelView v, const uint8_t *__restrict__ du,
-                                                            const float *__restrict__ r, float *e, int colour)
+                                                            const float *__restrict__ r, float *e, int colour,
+                                                            Reducer R, const int *it, int baseEven, int baseOdd)
 {
+    float facc[3] = {0.f, 0.f, 0.f}; // a thread's 2 x kPairS terms in FP32, the block and grid sums in FP64
     __shared__ float inv[32];
     FillInverse(inv, v.gamma);
     const PairPos P = PairStart(v);
@@ -226,9 +230,25 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_half(LevelView v, const u
             rv = rc.x;
             units = d & 0x7Fu;
         }
-        if (P.valid) ep[off + (second ? 1 : 0)] = (rv + g * s) * inv[units];
+        const float nv = (rv + g * s) * inv[units];
+        if (P.valid)
+        {
+            ep[off + (second ? 1 : 0)] = nv;
+            if (kDot)
+            {
+                const float z0 = second ? eC.x : nv, z1 = second ? nv : eC.y;
+                facc[0] += rc.x * z0 + rc.y * z1;
+                facc[1] += z0 + z1;
+                facc[2] += rc.x + rc.y;
+            }
+        }
         eM = eC;
         eC = eP;
+    }
+    if (kDot)
+    {
+        double acc[3] = {facc[0], facc[1], facc[2]};
+        GridReduce<3>(R, acc, (*it & 1) ? baseOdd : baseEven);
     }
 }
 
@@ -278,7 +298,14 @@ void LaunchPairFirst(const LevelView &v, const uint8_t *du, const float *r, floa
 void LaunchPairHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_pair_half<<<PairGrid(v), kPairThreads, 0, st>>>(v, du, r, e, colour);
+    k_pair_half<false><<<PairGrid(v), kPairThreads, 0, st>>>(v, du, r, e, colour, Reducer{}, nullptr, 0, 0);
+}
+
+void LaunchPairHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, const Reducer &R,
+                       const int *it, int baseEven, int baseOdd, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_pair_half<true><<<PairGrid(v), kPairThreads, 0, st>>>(v, du, r, e, colour, R, it, baseEven, baseOdd);
 }
 
 void LaunchPairResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
@@ -286,6 +313,146 @@ void LaunchPairResidual(const LevelView &v, const uint8_t *du, const float *r, c
 {
     NB_COUNT_LAUNCH();
     k_pair_residual<<<PairGrid(v), kPairThreads, 0, st>>>(v, du, r, e, res);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// transfers between a pair level and the next coarser level (the operators of k_prolong / k_restrict)
+// ---------------------------------------------------------------------------------------------------------------
+// Per fine cell: 0x80 for an unknown, plus in the low six bits the weight (in 1/64) that the Neumann-aware
+// prolongation moves from the cell's SOLID coarse contributors onto its parent. Coarse vectors are zero at SOLID
+// cells, so P e_c at a fine unknown = the plain trilinear sum + extra/64 * e_c[parent], and R = P^T.
+__global__ void k_build_pext(LevelView fv, LevelView cv, uint8_t *pext)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < fv.cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int d = (int)(c % fv.Nz);
+        const long long rr = c / fv.Nz;
+        const int b = (int)(rr % fv.Nx), a = (int)(rr / fv.Nx);
+        const bool interior = a > 0 && a < fv.Ny - 1 && b > 0 && b < fv.Nx - 1 && d > 0 && d < fv.Nz - 1;
+        if (!interior || fv.types[c] != FLUID) { pext[c] = 0; continue; }
+        const int A = (a + 1) >> 1, B = (b + 1) >> 1, D = (d + 1) >> 1;
+        const int si = (a & 1) ? -1 : 1, sj = (b & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
+        const int w[2] = {3, 1};
+        unsigned extra = 0;
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < 2; dj++)
+                for (int dk = 0; dk < 2; dk++)
+                {
+                    if (!(di | dj | dk)) continue;
+                    const long long cc = (long long)(A + di * si) * cv.sI + (long long)(B + dj * sj) * cv.sJ +
+                                         (D + dk * sk);
+                    if (cv.types[cc] == SOLID) extra += (unsigned)(w[di] * w[dj] * w[dk]);
+                }
+        pext[c] = (uint8_t)(0x80u | extra);
+    }
+}
+
+void LaunchBuildPext(const LevelView &fine, const LevelView &coarse, uint8_t *pext, cudaStream_t st)
+{
+    int blocks = (int)((fine.cells + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    NB_COUNT_LAUNCH();
+    k_build_pext<<<blocks, 256, 0, st>>>(fine, coarse, pext);
+}
+
+// e_f += P e_c on the fine unknowns; one thread per fine pair (k0 even: parents k0/2 and k0/2 + 1 along k).
+__global__ void __launch_bounds__(kPairThreads) k_pair_prolong(LevelView fv, LevelView cv,
+                                                               const uint8_t *__restrict__ pext,
+                                                               const float *__restrict__ ec, float *ef)
+{
+    const PairPos P = PairStart(fv);
+    const int m = P.k0 >> 1;
+    int off = 0;
+    for (int a = P.i0; a < P.i1; a++, off += P.sI)
+    {
+        const unsigned x = LdDu(pext + P.base + off);
+        if (!P.valid || !(x & 0x8080u)) continue;
+        const int b = P.j;
+        const int A = (a + 1) >> 1, A2 = A + ((a & 1) ? -1 : 1);
+        const int B = (b + 1) >> 1, B2 = B + ((b & 1) ? -1 : 1);
+        const float *r00 = ec + (long long)A * cv.sI + (long long)B * cv.sJ + m;
+        const float *r01 = ec + (long long)A * cv.sI + (long long)B2 * cv.sJ + m;
+        const float *r10 = ec + (long long)A2 * cv.sI + (long long)B * cv.sJ + m;
+        const float *r11 = ec + (long long)A2 * cv.sI + (long long)B2 * cv.sJ + m;
+        // rows weighted 3/4 (parent's row and plane) and 1/4 across i and j, then along k
+        const float lo = 0.5625f * r00[0] + 0.1875f * (r01[0] + r10[0]) + 0.0625f * r11[0];
+        const float hi = 0.5625f * r00[1] + 0.1875f * (r01[1] + r10[1]) + 0.0625f * r11[1];
+        float2 v = *reinterpret_cast<float2 *>(ef + P.base + off);
+        if (x & 0x80u) v.x += (0.75f * lo + 0.25f * hi) + (float)(x & 0x3Fu) * (1.0f / 64.0f) * r00[0];
+        if (x & 0x8000u) v.y += (0.75f * hi + 0.25f * lo) + (float)((x >> 8) & 0x3Fu) * (1.0f / 64.0f) * r00[1];
+        *reinterpret_cast<float2 *>(ef + P.base + off) = v;
+    }
+}
+
+void LaunchPairProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
+                       float *eFine, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_pair_prolong<<<PairGrid(fine), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+}
+
+// r_c = R res_f = P^T res_f at the coarse unknowns. A thread owns one coarse cell (K along the 32 lanes, J across
+// the 8 warps) and marches along I: fine planes 2I-2 .. 2I+1 enter as their (j, k)-weighted 4x4 sums T(a), each
+// fine plane summed once and kept for the next coarse plane; the children's moved weights enter as X(a).
+constexpr int kRestrictS = 8;
+
+__device__ __forceinline__ void RestrictPlane(const LevelView &fv, const uint8_t *pext, const float *res, int a,
+                                              int J, int K, float &T, float &X)
+{
+    T = 0.f;
+    X = 0.f;
+    if (a > fv.Ny - 1) return;
+    const float wt[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+#pragma unroll
+    for (int dj = 0; dj < 4; dj++)
+    {
+        const int b = 2 * J - 2 + dj;
+        if (b > fv.Nx - 1) continue;
+        const long long row = (long long)a * fv.sI + (long long)b * fv.sJ + 2 * K - 2;
+        const float2 u = *reinterpret_cast<const float2 *>(res + row);
+        const float2 w = *reinterpret_cast<const float2 *>(res + row + 2);
+        T += wt[dj] * ((0.25f * u.x + 0.75f * u.y) + (0.75f * w.x + 0.25f * w.y));
+        if (dj == 1 || dj == 2)
+        {
+            // children 2K-1 (u.y) and 2K (w.x) of this row
+            X += (float)(pext[row + 1] & 0x3Fu) * u.y + (float)(pext[row + 2] & 0x3Fu) * w.x;
+        }
+    }
+    X *= 1.0f / 64.0f;
+}
+
+__global__ void __launch_bounds__(256) k_pair_restrict(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
+                                                       const float *__restrict__ res, float *__restrict__ rc)
+{
+    const int K = 1 + blockIdx.x * 32 + threadIdx.x, J = 1 + blockIdx.y * 8 + threadIdx.y;
+    if (K > cv.Nz - 2 || J > cv.Nx - 2) return;
+    const int I0 = 1 + blockIdx.z * kRestrictS, I1 = min(I0 + kRestrictS, cv.Ny - 1);
+    float Tm2, Tm1, Xm1, Xdummy;
+    RestrictPlane(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
+    RestrictPlane(fv, pext, res, 2 * I0 - 1, J, K, Tm1, Xm1);
+    for (int I = I0; I < I1; I++)
+    {
+        float T0, X0, T1, X1;
+        RestrictPlane(fv, pext, res, 2 * I, J, K, T0, X0);
+        RestrictPlane(fv, pext, res, 2 * I + 1, J, K, T1, X1);
+        const long long c = (long long)I * cv.sI + (long long)J * cv.sJ + K;
+        if (cv.code[c] & CODE_UNKNOWN)
+            rc[c] = ((0.25f * Tm2 + 0.75f * Tm1) + (0.75f * T0 + 0.25f * T1)) + (Xm1 + X0);
+        Tm2 = T0;
+        Tm1 = T1;
+        Xm1 = X1;
+    }
+}
+
+void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
+                        float *rCoarse, cudaStream_t st)
+{
+    const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
+                    (unsigned)((coarse.Ny - 2 + kRestrictS - 1) / kRestrictS));
+    NB_COUNT_LAUNCH();
+    k_pair_restrict<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -333,7 +500,7 @@ __global__ void __launch_bounds__(kPairThreads)
         return x;
     };
     float2 NM = pnew(-P.sI), NC = pnew(0);
-    double acc[1] = {0.0};
+    float facc = 0.f;
     int off = 0;
     for (int i = P.i0; i < P.i1; i++, off += P.sI)
     {
@@ -353,11 +520,12 @@ __global__ void __launch_bounds__(kPairThreads)
         {
             *reinterpret_cast<float2 *>(pOut + P.base + off) = NC;
             *reinterpret_cast<float2 *>(q + P.base + off) = qq;
-            acc[0] += (double)NC.x * (double)qq.x + (double)NC.y * (double)qq.y;
+            facc += NC.x * qq.x + NC.y * qq.y;
         }
         NM = NC;
         NC = NP;
     }
+    double acc[1] = {facc};
     GridReduce<1>(R, acc, slotPQ);
 }
 

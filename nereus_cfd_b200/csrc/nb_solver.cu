@@ -173,6 +173,15 @@ void Context::BuildHierarchy()
         }
         else Lv.du.release();
     }
+    for (size_t l = 0; l < L.size(); l++)
+    {
+        if (L[l].du.p && l + 1 < L.size())
+        {
+            L[l].pext.alloc((size_t)L[l].cells);
+            LaunchBuildPext(L[l].view(), L[l + 1].view(), L[l].pext.p, st);
+        }
+        else L[l].pext.release();
+    }
     NB_CK(cudaGetLastError());
     // The tail: the first level from which every coarser level has at most kTailCellCap cells and all of them fit
     // in one block's shared memory in the solver's precision.
@@ -608,17 +617,20 @@ void Context::VCyclePairs(int l, float *r, float *e)
     LevelData &Lc = L[l + 1];
     const LevelView vc = Lc.view();
     prof(NB_K_RESTRICT0, s + s / 8.0);
-    LaunchRestrict<float>(v, vc, res, Lc.r<float>(), st);
+    LaunchPairRestrict(v, vc, Lv.pext.p, res, Lc.r<float>(), st);
     ProfEnd();
     VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
     prof(NB_K_PROLONG0, 2.0 * s + s / 8.0 + 1.0);
-    LaunchProlong<float>(v, vc, Lc.e<float>(), e, st);
+    LaunchPairProlong(v, vc, Lv.pext.p, Lc.e<float>(), e, st);
     ProfEnd();
     for (int q = 0; q < post; q++)
         for (int c = 1; c >= 0; c--)
         {
             prof(NB_K_SMOOTH0, half);
-            LaunchPairHalf(v, Lv.du.p, r, e, c, st);
+            if (l == 0 && q + 1 == post && c == 0) // z is final: r.z for CG here (IterBody skips its own)
+                LaunchPairHalfDot(v, Lv.du.p, r, e, c, red, iter.p, S_RZ0, S_RZ1, st);
+            else
+                LaunchPairHalf(v, Lv.du.p, r, e, c, st);
             ProfEnd();
         }
 }
@@ -686,9 +698,13 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
     {
         if (PairLevel(0))
         {
-            ProfBegin(NB_K_DOT, 2.0 * s * cells);
-            LaunchLinDot(L[0].cells, r, z, red, iter.p, S_RZ0, S_RZ1, st);
-            ProfEnd();
+            // r.z came with the V-cycle's last sweep unless level 0 is itself the coarse end (tail or single level)
+            if (!(tailStart > 0 && L.size() > 1))
+            {
+                ProfBegin(NB_K_DOT, 2.0 * s * cells);
+                LaunchLinDot(L[0].cells, r, z, red, iter.p, S_RZ0, S_RZ1, st);
+                ProfEnd();
+            }
             ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
             LaunchPairPApply(v0, L[0].du.p, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, st);
             ProfEnd();

@@ -96,6 +96,7 @@ struct LevelData
     DevArray<float> dw32[3], dig32[3];
     DevArray<uint8_t> types, code;
     DevArray<uint8_t> du;                 // diagonal units for the pair kernels (nb_pairs.cu); empty elsewhere
+    DevArray<uint8_t> pext;               // unknown flag + moved prolongation weight toward the next coarser level
     DevArray<float> r32, e32, res32, f32; // f: the pre-smoothed iterate of a fused V-cycle
     DevArray<double> r64, e64, res64, f64;
     LevelView view() const;
