@@ -122,6 +122,21 @@ int nereus_b200_project_velocity(nb_ctx *ctx, double *u, double *v, double *w, c
 int nereus_b200_project_device(nb_ctx *ctx, double *d_u, double *d_v, double *d_w, double *d_p, double rho,
                                double dt, int needsCompat, double tol, nb_result *out);
 
+/* The pressure step with the previous step's pressure p_prev (the reference's gridAnt->p, ring included), then the
+ * projection. Replaces SolveIncremental + Project (PressureSolver3D.h:58,71; PressureSolver3D.cpp:262-401) for
+ * scheme = NB_SCHEME_INCREMENTAL: the solve is for phi = p^{n+1} - p^n with the prescribed-pressure increments
+ * p_b(t^{n+1}) - p_b(t^n) on the ring, to ||r|| < tol max(||b||, ||b + A p^n||); the velocity is corrected with
+ * grad phi; p returns as p^n + phi on the unknowns, levelled like LevelPressure, with p's prescribed ring values (as
+ * given on entry) put back. For NB_SCHEME_CHORIN, warm_start = 1 starts the solve from p_prev on the unknowns
+ * (BuildWarmStartGuess, PressureSolver3D.cpp:222-244; uniform grids only, as WarmStartEnabled); otherwise it is
+ * nereus_b200_project. p_prev may be NULL for a cold Chorin step. Host buffers; the _device form takes device
+ * pointers on the context's device and stream. */
+int nereus_b200_project_ex(nb_ctx *ctx, double *u, double *v, double *w, double *p, const double *p_prev, double rho,
+                           double dt, int scheme, int needs_compat, int warm_start, double tol, nb_result *out);
+int nereus_b200_project_device_ex(nb_ctx *ctx, double *d_u, double *d_v, double *d_w, double *d_p,
+                                  const double *d_p_prev, double rho, double dt, int scheme, int needs_compat,
+                                  int warm_start, double tol, nb_result *out);
+
 /* SolveLaplacian (PressureSolver3D.h:64, PressureSolver3D.cpp:355-371): L x = f on the unknowns, f and x indexed
  * like the matrix (IDP order, n = SystemSize entries); x = 0 at air and pressure cells, no flux at solids. */
 int nereus_b200_solve_laplacian(nb_ctx *ctx, const double *f, double *x, double tol, nb_result *out);

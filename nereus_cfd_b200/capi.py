@@ -63,6 +63,13 @@ SIGNATURES = {
                                               ctypes.c_int, _u8, _dp * 3, _dp * 3, ctypes.c_int, ctypes.c_double]),
     "nereus_b200_project": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Result)]),
+    "nereus_b200_project_ex": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.POINTER(Result)]),
+    "nereus_b200_project_device_ex": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                                     ctypes.c_int, ctypes.c_double, ctypes.POINTER(Result)]),
     "nereus_b200_solve_pressure": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_double,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                   ctypes.POINTER(Result)]),

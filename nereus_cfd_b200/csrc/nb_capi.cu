@@ -164,6 +164,48 @@ int nereus_b200_project(nb_ctx *ctx, double *u, double *v, double *w, double *p,
     });
 }
 
+int nereus_b200_project_ex(nb_ctx *ctx, double *u, double *v, double *w, double *p, const double *pPrev, double rho,
+                           double dt, int scheme, int needsCompat, int warmStart, double tol, nb_result *out)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        if (!C.built) throw nb::InputError("set_layout has not been called");
+        if (!u || !v || !p || (C.dim == 3 && !w)) throw nb::InputError("null field pointer");
+        nb_result local{};
+        nb_result *r = out ? out : &local;
+        C.du.upload(u, C.FieldSizeU(), C.st);
+        C.dv.upload(v, C.FieldSizeV(), C.st);
+        if (C.dim == 3) C.dw.upload(w, C.FieldSizeW(), C.st);
+        C.dp.upload(p, C.Cells(), C.st);
+        if (pPrev) C.dpPrev.upload(pPrev, C.Cells(), C.st);
+        const int status = C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, rho, dt,
+                                           needsCompat, tol, r, true, true, pPrev ? C.dpPrev.p : nullptr, scheme,
+                                           warmStart != 0);
+        NB_CK(cudaMemcpyAsync(u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaMemcpyAsync(v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
+        if (C.dim == 3) NB_CK(cudaMemcpyAsync(w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaMemcpyAsync(p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+        NB_CK(cudaStreamSynchronize(C.st));
+        return status;
+    });
+}
+
+int nereus_b200_project_device_ex(nb_ctx *ctx, double *d_u, double *d_v, double *d_w, double *d_p,
+                                  const double *d_pPrev, double rho, double dt, int scheme, int needsCompat,
+                                  int warmStart, double tol, nb_result *out)
+{
+    if (!ctx || !ctx->c) return Fail(NB_BAD_INPUT, "ctx is null");
+    return Guard([&] {
+        nb::Context &C = *ctx->c;
+        NB_CK(cudaSetDevice(C.device));
+        nb_result local{};
+        return C.ProjectDevice(d_u, d_v, C.dim == 3 ? d_w : d_u, d_p, rho, dt, needsCompat, tol, out ? out : &local,
+                               true, true, d_pPrev, scheme, warmStart != 0);
+    });
+}
+
 int nereus_b200_solve_pressure(nb_ctx *ctx, const double *u, const double *v, const double *w, double *p, double rho,
                                double dt, int scheme, int needsCompat, double tol, nb_result *out)
 {

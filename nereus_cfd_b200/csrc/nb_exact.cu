@@ -456,6 +456,53 @@ void LaunchMaxDiv(const LevelView &v, const double *u, const double *vv, const d
 }
 
 // ---------------------------------------------------------------------------------------------------------------
+// The incremental scheme's cell-by-cell steps and the warm start's guess, each the reference's expression:
+//   CELL_DELTA      out = a - b on PRESSURE cells, 0 elsewhere: DirichletSum's known value p_b(t^{n+1}) - p_b(t^n)
+//                   (PressureSolver3D.cpp:248-260, `old` non-null)
+//   CELL_RING_DELTA a -= b on PRESSURE cells: the increment's ring after EnforcePressureBC (:321-328)
+//   CELL_NEG        out = -a on the unknowns, 0 elsewhere: b + A p^n = b - A(-p^n) (IncrementReferenceNorm :262-276)
+//   CELL_TAKE       out = a on the unknowns, 0 elsewhere: BuildWarmStartGuess's x0 (:222-244)
+//   CELL_SUM        out = a + b on the unknowns, 0 elsewhere: p^n + phi (AccumulatePressureIncrement :374-393)
+//   CELL_RESTORE    a = b on PRESSURE cells: the prescribed ring p_b(t^{n+1}) put back (EnforcePressureBC)
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_cellwise(LevelView v, int op, double *a, const double *b, double *out)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < v.cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int t = v.types[c];
+        bool unknown = false;
+        if (op == CELL_NEG || op == CELL_TAKE || op == CELL_SUM)
+        {
+            const int k = v.dim == 3 ? (int)(c % v.Nz) : 1;
+            const long long rr = v.dim == 3 ? c / v.Nz : c;
+            const int j = (int)(rr % v.Nx), i = (int)(rr / v.Nx);
+            unknown = t == FLUID && i > 0 && i < v.Ny - 1 && j > 0 && j < v.Nx - 1 &&
+                      (v.dim == 2 || (k > 0 && k < v.Nz - 1));
+        }
+        switch (op)
+        {
+        case CELL_DELTA: out[c] = t == PRESSURE ? a[c] - b[c] : 0.0; break;
+        case CELL_RING_DELTA: if (t == PRESSURE) a[c] = a[c] - b[c]; break;
+        case CELL_NEG: out[c] = unknown ? -a[c] : 0.0; break;
+        case CELL_TAKE: out[c] = unknown ? a[c] : 0.0; break;
+        case CELL_SUM: out[c] = unknown ? a[c] + b[c] : 0.0; break;
+        case CELL_RESTORE: if (t == PRESSURE) a[c] = b[c]; break;
+        default: break;
+        }
+    }
+}
+
+void LaunchCellwise(const LevelView &v, int op, double *a, const double *b, double *out, cudaStream_t st)
+{
+    int blocks = (int)((v.cells + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    NB_COUNT_LAUNCH();
+    k_cellwise<<<blocks, 256, 0, st>>>(v, op, a, b, out);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
 // FP64 residual of the reference's matrix: r = b - A x, A = scale * (off-diagonals c_q, diagonal DiagExact).
 // Writes the unit-form residual -r/scale in T for the solver, sums ||r||^2 (and r for a singular system).
 // The refinement form also adds a correction e first: x_out = x_in + e, r = b - A x_out, read from the

@@ -36,6 +36,8 @@ void LaunchResidual64(const LevelView &v, const double *b, const double *x, T *r
 template <typename T>
 void LaunchRefine64(const LevelView &v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
                     double scale, double sfac, const Reducer &R, int slot, cudaStream_t st);
+enum : int { CELL_DELTA = 0, CELL_RING_DELTA, CELL_NEG, CELL_TAKE, CELL_SUM, CELL_RESTORE };
+void LaunchCellwise(const LevelView &v, int op, double *a, const double *b, double *out, cudaStream_t st);
 void LaunchSumUnknowns(const LevelView &v, const double *x, const Reducer &R, int slot, cudaStream_t st);
 void LaunchSubMeanScatter(const LevelView &v, double *x, const double *sums, int n, int sub, double *p,
                           cudaStream_t st);

@@ -792,7 +792,22 @@ int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double
     return it;
 }
 
-int Context::SolveMixed(double tol, double **xOut, nb_result *out)
+bool Context::StartFrom(const double *guess, double refNorm, double tol, double bn2, double *tolEff)
+{
+    *tolEff = tol;
+    bool go = true;
+    if (refNorm > 0.0)
+    {
+        const double bn = std::sqrt(bn2);
+        if (bn <= tol * refNorm) go = false; // nothing to solve: the answer is the guess (the increment is zero)
+        else *tolEff = std::min(0.5, tol * refNorm / bn);
+    }
+    if (guess && guess != xa.p)
+        NB_CK(cudaMemcpyAsync(xa.p, guess, sizeof(double) * Cells(), cudaMemcpyDeviceToDevice, st));
+    return go;
+}
+
+int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double *guess, double refNorm)
 {
     const LevelView v0 = L[0].view();
     const double sfac = -1.0 / scale;
@@ -805,13 +820,23 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out)
     const double bn2 = ReadSlot(S_RES);
     out->b_norm = std::sqrt(bn2);
     int outer = 0, inner = 0, status = NB_OK;
-    double rr64 = bn2;
-    if (bn2 > 0.0)
+    double rr64 = bn2, tolEff = tol;
+    bool go = bn2 > 0.0;
+    if (go)
+    {
+        go = StartFrom(guess, refNorm, tol, bn2, &tolEff);
+        if (guess)
+        {
+            LaunchResidual64<float>(v0, b.p, x, r32, scale, sfac, red, S_RES, st);
+            rr64 = ReadSlot(S_RES);
+        }
+    }
+    if (go)
     {
         const int maxOuter = std::max(1, opt.max_outer);
         while (true)
         {
-            if (std::sqrt(rr64 / bn2) <= tol) break;
+            if (std::sqrt(rr64 / bn2) <= tolEff) break;
             if (outer >= maxOuter || !std::isfinite(rr64)) { status = NB_NOT_CONVERGED; break; }
             x32.zero(st);
             double rrEnd = 0.0;
@@ -833,7 +858,7 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out)
     return status;
 }
 
-int Context::SolveFP64(double tol, double **xOut, nb_result *out)
+int Context::SolveFP64(double tol, double **xOut, nb_result *out, const double *guess, double refNorm)
 {
     const LevelView v0 = L[0].view();
     const double sfac = -1.0 / scale;
@@ -846,17 +871,27 @@ int Context::SolveFP64(double tol, double **xOut, nb_result *out)
     const double bn2 = ReadSlot(S_RES);
     out->b_norm = std::sqrt(bn2);
     int its = 0, status = NB_OK, restarts = 0;
-    double rr = bn2;
-    if (bn2 > 0.0)
+    double rr = bn2, tolEff = tol;
+    bool go = bn2 > 0.0;
+    if (go)
+    {
+        go = StartFrom(guess, refNorm, tol, bn2, &tolEff);
+        if (guess)
+        {
+            LaunchResidual64<double>(v0, b.p, x, r, scale, sfac, red, S_RES, st);
+            rr = ReadSlot(S_RES);
+        }
+    }
+    if (go)
     {
         const int maxIt = std::max(1, opt.max_iters) * std::max(1, opt.max_outer);
         while (true)
         {
-            if (std::sqrt(rr / bn2) <= tol) break;
+            if (std::sqrt(rr / bn2) <= tolEff) break;
             if (its >= maxIt || restarts > 4 || !std::isfinite(rr)) { status = NB_NOT_CONVERGED; break; }
             double rrEnd = 0.0;
             // the recursive residual is driven a little below the target, then checked against the true one
-            const double target = 0.25 * tol * tol * bn2 * sfac * sfac;
+            const double target = 0.25 * tolEff * tolEff * bn2 * sfac * sfac;
             its += RunPCG<double>(x, r, z, p64[0].p, p64[1].p, q64.p, rr * sfac * sfac, target, maxIt - its, true,
                                   &rrEnd);
             ProfBegin(NB_K_REFINE, (8.0 + 8.0 + 1.0 + 8.0) * (double)Cells());
@@ -873,7 +908,7 @@ int Context::SolveFP64(double tol, double **xOut, nb_result *out)
     return status;
 }
 
-int Context::Solve(double tol, double **xOut, nb_result *out)
+int Context::Solve(double tol, double **xOut, nb_result *out, const double *guess, double refNorm)
 {
     if (!(tol > 0.0)) throw InputError("tolerance must be positive");
     if (n == 0)
@@ -885,18 +920,23 @@ int Context::Solve(double tol, double **xOut, nb_result *out)
         out->iters_inner = out->iters_outer = 0;
         return NB_OK;
     }
-    return opt.precision == NB_PRECISION_MIXED ? SolveMixed(tol, xOut, out) : SolveFP64(tol, xOut, out);
+    return opt.precision == NB_PRECISION_MIXED ? SolveMixed(tol, xOut, out, guess, refNorm)
+                                               : SolveFP64(tol, xOut, out, guess, refNorm);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
 // the pressure step and projection
 // ---------------------------------------------------------------------------------------------------------------
 int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rho, double dt, int compat, double tol,
-                           nb_result *out, bool solve, bool correct)
+                           nb_result *out, bool solve, bool correct, const double *pPrev, int scheme, bool warm)
 {
     if (!built) throw InputError("set_layout has not been called");
     if (!u || !v || !p || (dim == 3 && !w)) throw InputError("null field pointer");
     if (!(rho > 0.0) || !(dt > 0.0)) throw InputError("rho and dt must be positive");
+    if (scheme != NB_SCHEME_CHORIN && scheme != NB_SCHEME_INCREMENTAL) throw InputError("unknown scheme");
+    const bool incr = scheme == NB_SCHEME_INCREMENTAL;
+    if ((incr || warm) && !pPrev) throw InputError("the previous pressure is required");
+    if (incr && !(solve && correct)) throw InputError("the incremental scheme runs the whole step");
     std::memset(out, 0, sizeof(*out));
     out->n = n;
     out->singular = singular ? 1 : 0;
@@ -919,8 +959,18 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
         return NB_OK;
     }
     LaunchRing(v0, p, st); // EnforcePressureBC at the start of SolveScheme
+    const double *pKnown = p; // the values DirichletSum reads on PRESSURE cells
+    if (incr)
+    {
+        // SolveIncremental: the known Dirichlet values are p_b(t^{n+1}) - p_b(t^n); p_b(t^{n+1}) is kept for the end
+        pSave.alloc(Cells());
+        dq.alloc(Cells());
+        NB_CK(cudaMemcpyAsync(pSave.p, p, pSave.bytes(), cudaMemcpyDeviceToDevice, st));
+        LaunchCellwise(v0, CELL_DELTA, const_cast<double *>(p), pPrev, dq.p, st);
+        pKnown = dq.p;
+    }
     ProfBegin(NB_K_RHS, (3.0 * 8.0 + 1.0 + 8.0) * (double)Cells());
-    LaunchRhs(v0, u, v, w, p, rho / dt, scale, dh, b.p, st);
+    LaunchRhs(v0, u, v, w, pKnown, rho / dt, scale, dh, b.p, st);
     ProfEnd();
     const bool compatOn = compat && singular && n > 0;
     if (compatOn)
@@ -929,18 +979,55 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
             LaunchSumUnknowns(v0, b.p, red, S_SUM, st);
             LaunchSubMeanScatter(v0, b.p, slots.p + S_SUM, n, 1, nullptr, st);
         }
+    const double *guess = nullptr;
+    double refNorm = 0.0;
+    if (incr && n > 0)
+    {
+        // IncrementReferenceNorm: ||b + A p^n|| over the unknowns, the stopping floor of the increment's solve
+        LaunchCellwise(v0, CELL_NEG, const_cast<double *>(pPrev), nullptr, xb.p, st);
+        if (opt.precision == NB_PRECISION_MIXED)
+            LaunchResidual64<float>(v0, b.p, xb.p, L[0].r32.p, scale, 1.0, red, S_RES, st);
+        else
+            LaunchResidual64<double>(v0, b.p, xb.p, L[0].r64.p, scale, 1.0, red, S_RES, st);
+        refNorm = std::sqrt(ReadSlot(S_RES));
+    }
+    else if (warm && !nonuniform && n > 0)
+    {
+        // BuildWarmStartGuess: x0 = p^n on the unknowns, mean-free for a singular system with compatibility on
+        LaunchCellwise(v0, CELL_TAKE, const_cast<double *>(pPrev), nullptr, xb.p, st);
+        if (compatOn)
+        {
+            LaunchSumUnknowns(v0, xb.p, red, S_SUM, st);
+            LaunchSubMeanScatter(v0, xb.p, slots.p + S_SUM, n, 1, nullptr, st);
+        }
+        guess = xb.p;
+    }
     double *x = nullptr;
-    const int status = Solve(tol, &x, out);
-    // LevelPressure's mean removal (PressureSolver3D.cpp:181-187), then the scatter into p
-    if (compatOn) LaunchSumUnknowns(v0, x, red, S_SUM, st);
-    LaunchSubMeanScatter(v0, x, slots.p + S_SUM, n, compatOn ? 1 : 0, p, st);
+    const int status = Solve(tol, &x, out, guess, refNorm);
+    // LevelPressure's mean removal (PressureSolver3D.cpp:181-187), then the scatter into p; the increment is not
+    // levelled (its constant does not enter the gradient)
+    const bool level = compatOn && !incr;
+    if (level) LaunchSumUnknowns(v0, x, red, S_SUM, st);
+    LaunchSubMeanScatter(v0, x, slots.p + S_SUM, n, level ? 1 : 0, p, st);
     LaunchRing(v0, p, st);
+    if (incr) LaunchCellwise(v0, CELL_RING_DELTA, p, pPrev, nullptr, st); // the ring carries phi (:321-328)
     if (correct)
     {
         ProfBegin(NB_K_PROJECT, (8.0 + 1.0 + 6.0 * 8.0) * (double)Cells());
         LaunchProject(v0, u, v, w, p, dt / rho, st);
         ProfEnd();
         LaunchMaxDiv(v0, u, v, w, dh, red, S_DIV, st);
+    }
+    if (incr)
+    {
+        // AccumulatePressureIncrement (:374-393): p = p^n + phi on the unknowns, levelled, scattered, then
+        // EnforcePressureBC with the prescribed values kept from the start
+        double *acc = (x == xa.p) ? xb.p : xa.p;
+        LaunchCellwise(v0, CELL_SUM, const_cast<double *>(pPrev), p, acc, st);
+        if (compatOn) LaunchSumUnknowns(v0, acc, red, S_SUM, st);
+        LaunchSubMeanScatter(v0, acc, slots.p + S_SUM, n, compatOn ? 1 : 0, p, st);
+        LaunchCellwise(v0, CELL_RESTORE, p, pSave.p, nullptr, st);
+        LaunchRing(v0, p, st);
     }
     NB_CK(cudaEventRecord(ev1, st));
     NB_CK(cudaGetLastError());

@@ -136,7 +136,8 @@ struct Context
     DevArray<double> p64[2], q64;
 
     // fields for the host-buffer entry points
-    DevArray<double> du, dv, dw, dp;
+    DevArray<double> du, dv, dw, dp, dpPrev;
+    DevArray<double> pSave, dq; // the incremental scheme's prescribed ring values and known Dirichlet increments
 
     // reductions
     DevArray<double> partials, slots;
@@ -197,8 +198,11 @@ struct Context
     // The pressure step and projection on device fields; returns the nb_status.
     // solve: the pressure step (ring, RHS, compatibility, solve, level, scatter, ring); correct: the velocity
     // correction with the p that results.
+    // pPrev: p^n with its ring (the reference's gridAnt->p), used by the incremental scheme (required) and by the
+    // Chorin warm start (warm = true; uniform grids only, as WarmStartEnabled, PressureSolver3D.cpp:215-220).
     int ProjectDevice(double *u, double *v, double *w, double *p, double rho, double dt, int compat, double tol,
-                      nb_result *out, bool solve = true, bool correct = true);
+                      nb_result *out, bool solve = true, bool correct = true, const double *pPrev = nullptr,
+                      int scheme = NB_SCHEME_CHORIN, bool warm = false);
     int SolveLaplacian(const double *f, double *x, double tol, nb_result *out);
     void Rhs(const double *u, const double *v, const double *w, const double *p, double rho, double dt, double *bOut);
     void ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singularOut);
@@ -216,9 +220,14 @@ struct Context
     double ReadSlot(int s);
     void ReadSlots(int s, int count);
     // Solve A x = b (b in this->b, grid layout); the solution ends in *xOut (xa or xb). Fills out->iters/rel_res.
-    int Solve(double tol, double **xOut, nb_result *out);
-    int SolveMixed(double tol, double **xOut, nb_result *out);
-    int SolveFP64(double tol, double **xOut, nb_result *out);
+    // guess: the initial iterate (grid layout, zero off the unknowns; may be xb), else zero. refNorm > 0: stop at
+    // ||r|| < tol max(||b||, refNorm), and when ||b|| <= tol refNorm already the answer is the guess (or zero)
+    // (SolveEigenPressure, PressureSettings.h:411-427).
+    int Solve(double tol, double **xOut, nb_result *out, const double *guess = nullptr, double refNorm = 0.0);
+    int SolveMixed(double tol, double **xOut, nb_result *out, const double *guess, double refNorm);
+    int SolveFP64(double tol, double **xOut, nb_result *out, const double *guess, double refNorm);
+    // the initial residual of the guess, and the tolerance the refNorm floor turns `tol` into; false: nothing to do
+    bool StartFrom(const double *guess, double refNorm, double tol, double bn2, double *tolEff);
     template <typename T> void VCycle(int l, T *r, T *e);
     template <typename T> void VCycleFused(int l, T *r, T *e);
     bool FusedLevel(int l) const { return opt.fused_sweeps && dim == 3 && l < tailStart && l + 1 < (int)L.size(); }

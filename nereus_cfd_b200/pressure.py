@@ -60,11 +60,17 @@ class PressureSolver:
         self.grid: Optional[MACGrid] = None
         self.last: Optional[capi.Result] = None
         self.projected = False
+        self.scheme = capi.SCHEME_CHORIN
+        self.warm_start = False
 
     # ---- life cycle (PressureSolver3D.h:52-54) ----
-    def InitializePressureSolver(self, grid: MACGrid, scheme: int = capi.SCHEME_CHORIN):
-        if scheme != capi.SCHEME_CHORIN:
-            raise capi.NBError(capi.NB_BAD_INPUT, "only the Chorin scheme is served")
+    def InitializePressureSolver(self, grid: MACGrid, scheme: int = capi.SCHEME_CHORIN, warm_start: bool = False):
+        """scheme: SCHEME_CHORIN or SCHEME_INCREMENTAL (SYSTEM.scheme); warm_start: Chorin solves start from the
+        previous pressure (PRESSURE_SETTINGS.warmStart, honoured on uniform grids as WarmStartEnabled)."""
+        if scheme not in (capi.SCHEME_CHORIN, capi.SCHEME_INCREMENTAL):
+            raise capi.NBError(capi.NB_BAD_INPUT, "unknown scheme %r" % (scheme,))
+        self.scheme = scheme
+        self.warm_start = bool(warm_start)
         if not self.ctx:
             capi.check(self.lib.nereus_b200_create(ctypes.byref(self.ctx), ctypes.byref(self.opts)))
         self.EnsureSystem(grid)
@@ -99,23 +105,54 @@ class PressureSolver:
             pass
 
     # ---- the pressure step (SolveChorin / SolvePressure, PressureSolver3D.h:57-60) ----
-    def SolvePressure(self, grid: MACGrid, tol: float = 1e-8, needs_compat: bool = False) -> capi.Result:
-        """Pressure step + projection of ``grid`` in place. Returns the solve's report; raises on bad input or a
+    def SolvePressure(self, grid: MACGrid, tol: float = 1e-8, needs_compat: bool = False,
+                      grid_ant: Optional[MACGrid] = None) -> capi.Result:
+        """Pressure step + projection of ``grid`` in place, in the scheme chosen at initialisation. ``grid_ant``
+        is the previous step's state (the reference's gridAnt): its pressure is p^n of the incremental scheme
+        (required there) and the Chorin warm start's guess. Returns the solve's report; raises on bad input or a
         device error; a solve that hits its caps returns with status NOT_CONVERGED (the reference warns once)."""
         if self.grid is None or grid.grid is not self.grid.grid or not np.array_equal(grid.types, self._tables[2]):
-            self.InitializePressureSolver(grid) if not self.ctx else self.EnsureSystem(grid)
+            self.InitializePressureSolver(grid, self.scheme, self.warm_start) if not self.ctx else \
+                self.EnsureSystem(grid)
         r = capi.Result()
         g = grid.grid
         w = grid.w if g.dim == 3 else np.zeros(1)
-        st = self.lib.nereus_b200_project(self.ctx, capi.ptr(grid.u), capi.ptr(grid.v), capi.ptr(w),
-                                          capi.ptr(grid.p), grid.rho, grid.dt, capi.SCHEME_CHORIN,
-                                          int(needs_compat), tol, ctypes.byref(r))
+        incremental = self.scheme == capi.SCHEME_INCREMENTAL
+        if incremental and grid_ant is None:
+            raise capi.NBError(capi.NB_BAD_INPUT, "the incremental scheme needs the previous step's grid")
+        if incremental or (self.warm_start and grid_ant is not None):
+            p_prev = np.ascontiguousarray(grid_ant.p, dtype=np.float64)
+            st = self.lib.nereus_b200_project_ex(self.ctx, capi.ptr(grid.u), capi.ptr(grid.v), capi.ptr(w),
+                                                 capi.ptr(grid.p), capi.ptr(p_prev), grid.rho, grid.dt,
+                                                 self.scheme, int(needs_compat), int(self.warm_start), tol,
+                                                 ctypes.byref(r))
+        else:
+            st = self.lib.nereus_b200_project(self.ctx, capi.ptr(grid.u), capi.ptr(grid.v), capi.ptr(w),
+                                              capi.ptr(grid.p), grid.rho, grid.dt, capi.SCHEME_CHORIN,
+                                              int(needs_compat), tol, ctypes.byref(r))
         capi.check(st, allow=(capi.NB_OK, capi.NB_NOT_CONVERGED))
         self.last = r
         self.projected = True
         return r
 
-    SolveChorin = SolvePressure
+    def SolveChorin(self, grid: MACGrid, tol: float = 1e-8, needs_compat: bool = False,
+                    grid_ant: Optional[MACGrid] = None) -> capi.Result:
+        """SolveChorin (PressureSolver3D.h:57): the Chorin step whatever the initialised scheme."""
+        keep, self.scheme = self.scheme, capi.SCHEME_CHORIN
+        try:
+            return self.SolvePressure(grid, tol, needs_compat, grid_ant)
+        finally:
+            self.scheme = keep
+
+    def SolveIncremental(self, grid_ant: MACGrid, grid: MACGrid, tol: float = 1e-8,
+                         needs_compat: bool = False) -> capi.Result:
+        """SolveIncremental + Project (PressureSolver3D.h:58,71): phi = p^{n+1} - p^n, the velocity corrected with
+        grad phi, p = p^n + phi levelled."""
+        keep, self.scheme = self.scheme, capi.SCHEME_INCREMENTAL
+        try:
+            return self.SolvePressure(grid, tol, needs_compat, grid_ant)
+        finally:
+            self.scheme = keep
 
     def ProjectPressure(self, grid: MACGrid) -> bool:
         """The velocity correction already ran inside SolvePressure; True when it did for this grid."""

@@ -466,6 +466,43 @@ def dirichlet_linear_3d(n: int = 20) -> Case:
                 velocity_rule="zero")
 
 
+def pressure_outlet_3d(n: int = 12, seed: int = 8) -> Case:
+    """3D unit cube, uniform n^3, a solid sphere at (0.5, 0.5, 0.5) radius 0.2, no-slip walls and a pressure outlet
+    on x = 1 that prescribes a time-dependent p = 0.2 + 0.5 t + 0.3 y (PRESSURE ring cells: the incremental
+    scheme's Dirichlet increments p_b(t^{n+1}) - p_b(t^n) are non-zero)."""
+    g = uniform_grid(3, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    sph = Region(REGION_SOLID, PRIM_SPHERE, (0.5, 0.5, 0.5), radius=0.2)
+    faces = [(f, BC_NOSLIP, 0) for f in (0, 2, 3, 4, 5)] + [(1, BC_PRESSURE_OUTLET, 1)]
+    return Case("pressure_outlet_3d_%d" % n, g, Scene(faces, [sph], True, PRESSURE_OUTLET_EXPR), seed)
+
+
+PRESSURE_OUTLET_EXPR = "0.2 + 0.5*t + 0.3*y"
+
+
+def outlet_pressure(t):
+    """p_b of pressure_outlet_3d at time t, as a function of the ring face position."""
+    return lambda x, y, z=0.0: 0.2 + 0.5 * t + 0.3 * y
+
+
+def previous_pressure(grid: Grid, types: np.ndarray, seed: int, ring_fn=None) -> np.ndarray:
+    """A previous step's pressure p^n for the incremental scheme and the warm start: seeded N(0,1) values on the
+    interior FLUID cells (stream 7 of the case seed), the prescribed values ring_fn(x, y, z) on PRESSURE ring cells,
+    0 elsewhere."""
+    t = np.asarray(types).reshape(-1)
+    p = ring_prescribed_pressure(grid, t, ring_fn) if ring_fn is not None else np.zeros(grid.cells)
+    tv = t.reshape(grid.shape)
+    interior = np.zeros(grid.shape, dtype=bool)
+    if grid.dim == 3:
+        interior[1:-1, 1:-1, 1:-1] = True
+    else:
+        interior[1:-1, 1:-1, :] = True
+    fluid = (tv == FLUID) & interior
+    vals = normals(stream_seed(seed, 7), int(fluid.sum()))
+    pv = p.reshape(grid.shape)
+    pv[fluid] = vals
+    return p
+
+
 def linear_pressure(x, y, z=0.0):
     """p_b of the known-answer case, evaluated where MAC::PrescribedPressure evaluates it."""
     return 0.3 + 1.1 * x - 0.7 * y

@@ -213,6 +213,89 @@ def solve_projection(grid, types, u, v, w, p_in, rho, dt, needs_compat, tol, max
     return Projection(gv.types.copy(), asm, b_raw, b, x, it, rr, p, uu, vv, ww if w.size else w, md)
 
 
+PRESSURE = 4
+
+
+def solve_scheme(grid, types, u, v, w, p_in, p_prev, rho, dt, needs_compat, tol, incremental, warm=False,
+                 max_iters=1000000) -> Projection:
+    """The step with a previous pressure p_prev, restated from the reference:
+    incremental (SolveScheme with `old`, PressureSolver3D.cpp:262-328, then Project :396-401 =
+    ProjectPressure + AccumulatePressureIncrement :374-393): DirichletSum reads p_b(t^{n+1}) - p_b(t^n) on PRESSURE
+    cells; the Eigen CG stops at ||r|| < tol max(||b||, ||b + A p^n||) (SolveEigenPressure, PressureSettings.h:
+    411-427); phi is not levelled; the ring carries phi; the velocity takes grad phi; p = p^n + phi on the unknowns,
+    levelled, and EnforcePressureBC puts the prescribed ring back.
+    warm (Chorin, BuildWarmStartGuess :222-244): the CG starts from p_prev on the unknowns, mean-free when the
+    compatibility condition applies. Returns the Projection with p = the final pressure; .x is the solve's result."""
+    gv = GridView(grid, types)
+    asm = assemble(gv)
+    sing = needs_compat and asm.singular and asm.n > 0
+    p = np.ascontiguousarray(p_in, dtype=np.float64).copy()
+    lib().or_ring_replay(gv.ref, _p(p, _dp))
+    ring_entry = p.copy()
+    prev = np.ascontiguousarray(p_prev, dtype=np.float64)
+    t = gv.types
+    known = np.where(t == PRESSURE, p - prev, 0.0) if incremental else p
+    b_raw = rhs(gv, asm, u, v, w, np.ascontiguousarray(known), rho, dt)
+    b = compat(b_raw) if sing else b_raw.copy()
+    idp = asm.idp
+    on = idp >= 0
+    pn = np.zeros(max(asm.n, 1))
+    pn[idp[on]] = prev[on]
+    pn = pn[: asm.n]
+    x = np.zeros(max(asm.n, 1))
+    it, tol_eff, solve = 0, tol, asm.n > 0
+    if incremental and asm.n > 0:
+        ref = float(np.linalg.norm(b + spmv(asm, pn)))
+        bn = float(np.linalg.norm(b))
+        if ref > 0.0:
+            if bn <= tol * ref:
+                solve = False
+            else:
+                tol_eff = min(0.5, tol * ref / bn)
+    if warm and asm.n > 0 and not grid.nonuniform:
+        x[: asm.n] = pn
+        if sing:
+            x[: asm.n] -= x[: asm.n].mean()
+    if solve:
+        err = ctypes.c_double(0.0)
+        it = lib().or_cg(_p(asm.rowptr, _ip), _p(asm.col, _ip), _p(asm.val, _dp), asm.n,
+                         _p(np.ascontiguousarray(b), _dp), _p(x, _dp), tol_eff, max_iters, ctypes.byref(err))
+    x = x[: asm.n].copy()
+    if sing and not incremental:
+        lib().or_level_mean(_p(x, _dp), asm.n)
+    xs = x if x.size else np.zeros(1)
+    lib().or_scatter(gv.ref, _p(idp, _ip), _p(xs, _dp), _p(p, _dp))
+    lib().or_ring_replay(gv.ref, _p(p, _dp))
+    if incremental:
+        p = np.where(t == PRESSURE, p - prev, p)
+    uu, vv = u.copy(), v.copy()
+    ww = w.copy() if w.size else np.zeros(1)
+    lib().or_project(gv.ref, _p(uu, _dp), _p(vv, _dp), _p(ww, _dp), _p(p, _dp), rho, dt)
+    md = lib().or_max_divergence(gv.ref, _p(uu, _dp), _p(vv, _dp), _p(ww, _dp))
+    if incremental:
+        acc = np.zeros(max(asm.n, 1))
+        acc[idp[on]] = prev[on] + p[on]
+        acc = acc[: asm.n].copy()
+        if sing:
+            lib().or_level_mean(_p(acc, _dp), asm.n)
+        accs = acc if acc.size else np.zeros(1)
+        lib().or_scatter(gv.ref, _p(idp, _ip), _p(accs, _dp), _p(p, _dp))
+        p = np.where(t == PRESSURE, ring_entry, p)
+        lib().or_ring_replay(gv.ref, _p(p, _dp))
+    bn = float(np.linalg.norm(b))
+    rr = residual_norm(asm, b, x) / bn if bn > 0 else 0.0
+    return Projection(t.copy(), asm, b_raw, b, x, it, rr, p, uu, vv, ww if w.size else w, md)
+
+
+def spmv(asm: Assembly, x: np.ndarray) -> np.ndarray:
+    """A x with the assembled CSR (rows in order, each row's entries in column order)."""
+    y = np.zeros(asm.n)
+    for r in range(asm.n):
+        a, b = asm.rowptr[r], asm.rowptr[r + 1]
+        y[r] = np.dot(asm.val[a:b], x[asm.col[a:b]])
+    return y
+
+
 def ring_replay(grid, types, p):
     gv = GridView(grid, types)
     p = np.ascontiguousarray(p, dtype=np.float64).copy()

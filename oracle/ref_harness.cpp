@@ -16,9 +16,14 @@
 //   "NBCASE01", int32 hdr[16], double dom[6], double rho, dt, tol, time,
 //   [grid_mode 1] double wx[nxi], wy[nyi], wz[nzi] (interior widths),
 //   [label_mode 0] int32 len + scene text; [label_mode 1] uint8 labels[cells],
-//   double u[], v[], (w[] in 3D), in the MAC layouts (MAC.h:235-242, 369-374).
+//   double u[], v[], (w[] in 3D), in the MAC layouts (MAC.h:235-242, 369-374),
+//   [scheme 1 or 2] double p_prev[cells]: the previous step's pressure (gridAnt->p, ring included).
 // hdr: dim, grid_mode, grid_size, nxi, nyi, nzi, label_mode, needs_compat, scheme, solver, max_iters, threads,
 //      method_kind (0 Eulerian/ADI-like, 1 hybrid/FLIP-like), repeats, Nx, Ny (expected, ring included).
+// scheme: 0 Chorin; 1 incremental (SolvePressure with SYSTEM.scheme = PRESSURE_INCREMENTAL from gridAnt, then
+// ProjectPressure + AccumulatePressureIncrement as Project does); 2 Chorin with the warm start from gridAnt.
+// The result file then ends with double ref_norm (IncrementReferenceNorm, 0 for Chorin) and double p_final[cells]
+// (the pressure after Project).
 #include <algorithm>
 #include <array>
 #include <cctype>
@@ -193,7 +198,7 @@ int main(int argc, char **argv)
     if (std::memcmp(magic, "NBCASE01", 8) != 0) { std::fprintf(stderr, "bad magic\n"); return 2; }
     int32_t h[16];
     ReadN(f, h, 16);
-    const int dim = h[0], gridMode = h[1], gridSize = h[2], labelMode = h[6];
+    const int dim = h[0], gridMode = h[1], gridSize = h[2], labelMode = h[6], scheme = h[8];
     double dom[6], rho, dt, tol, time;
     ReadN(f, dom, 6); ReadN(f, &rho, 1); ReadN(f, &dt, 1); ReadN(f, &tol, 1); ReadN(f, &time, 1);
     std::vector<double> wx, wy, wz;
@@ -219,7 +224,7 @@ int main(int argc, char **argv)
     SIMULATION.f = Vec3{0.0, 0.0, 0.0};
     SIMULATION.grid.nonUniform = (gridMode == 1);
     PRESSURE_SETTINGS.needsCompatibilityCondition = h[7] != 0;
-    PRESSURE_SETTINGS.warmStart = false;
+    PRESSURE_SETTINGS.warmStart = scheme == 2;
     // The PRESSURE block the oracle runs with: eigen_* keys only (PressureSettings.h:212-255).
     {
         const char *solver = h[9] == 1 ? "AMG" : (h[9] == 2 ? "BICGSTAB" : "CG");
@@ -273,15 +278,26 @@ int main(int argc, char **argv)
     ReadN(f, grid.u.data(), grid.u.size());
     ReadN(f, grid.v.data(), grid.v.size());
     if (dim == 3) ReadN(f, grid.w.data(), grid.w.size());
+    // the previous step: the same geometry and labels, its own pressure
+    static MAC gridAnt;
+    MAC *ant = nullptr;
+    if (scheme == 1 || scheme == 2)
+    {
+        gridAnt = grid;
+        ReadN(f, gridAnt.p.data(), gridAnt.p.size());
+        ant = &gridAnt;
+    }
     std::fclose(f);
 
     // The pressure ring as the step sees it (SolveScheme's first call, PressureSolver3D.cpp:281).
     grid.EnforcePressureBC(time);
 
     const double t0 = Now();
-    if (dim == 3) PressureSolver3D::InitializePressureSolver(&grid, PRESSURE_CHORIN);
-    else PressureSolver2D::InitializePressureSolver(&grid, PRESSURE_CHORIN);
+    const PressureScheme ps = scheme == 1 ? PRESSURE_INCREMENTAL : PRESSURE_CHORIN;
+    if (dim == 3) PressureSolver3D::InitializePressureSolver(&grid, ps);
+    else PressureSolver2D::InitializePressureSolver(&grid, ps);
     const double tAssemble = Now() - t0;
+    MAC *old = scheme == 1 ? ant : nullptr; // DirichletSum's `old` under the incremental scheme
 
     PressureSystem &S = dim == 3 ? PressureSolver3D::SYSTEM : PressureSolver2D::SYSTEM;
     const std::vector<int> &IDP = dim == 3 ? PressureSolver3D::IDP : PressureSolver2D::IDP;
@@ -301,10 +317,10 @@ int main(int argc, char **argv)
                     if (id < 0) continue;
                     if (dim == 3)
                         braw[id] = rhoDt * grid.GetDivergencyAt(i, j, k) * (grid.nonUniform ? grid.CellVolume(i, j, k) : 1.0)
-                                   - scale * PressureSolver3D::DirichletSum(&grid, nullptr, i, j, k);
+                                   - scale * PressureSolver3D::DirichletSum(&grid, old, i, j, k);
                     else
                         braw[id] = rhoDt * grid.GetDivergencyAt(i, j) * (grid.nonUniform ? grid.CellVolume(i, j) : 1.0)
-                                   - scale * PressureSolver2D::DirichletSum(&grid, nullptr, i, j);
+                                   - scale * PressureSolver2D::DirichletSum(&grid, old, i, j);
                 }
         b = braw;
         if (PRESSURE_SETTINGS.needsCompatibilityCondition && S.singular && n > 0)
@@ -317,13 +333,21 @@ int main(int argc, char **argv)
         }
     }
 
-    // Cold solve (AMGCL builds its hierarchy here), then warm repeats of the same solve.
+    double refNorm = 0.0;
+    if (scheme == 1 && n > 0)
+    {
+        Eigen::Map<const Eigen::VectorXd> bv(b.data(), n);
+        refNorm = dim == 3 ? PressureSolver3D::IncrementReferenceNorm(ant, bv)
+                           : PressureSolver2D::IncrementReferenceNorm(ant, bv);
+    }
+
+    // Cold solve (AMGCL builds its hierarchy here), then warm repeats of the same solve (Chorin only).
     double t1 = Now();
-    if (dim == 3) PressureSolver3D::SolvePressure(nullptr, &grid, nullptr, time);
-    else PressureSolver2D::SolvePressure(nullptr, &grid, nullptr, time);
+    if (dim == 3) PressureSolver3D::SolvePressure(ant, &grid, nullptr, time);
+    else PressureSolver2D::SolvePressure(ant, &grid, nullptr, time);
     const double tCold = Now() - t1;
     int iters = PRESSURE_TELEMETRY.lastIterations;
-    const int repeats = h[13];
+    const int repeats = scheme == 0 ? h[13] : 0;
     double tWarm = 0.0;
     std::vector<double> tEach(repeats > 0 ? repeats : 0);
     for (int r = 0; r < repeats; r++)
@@ -353,6 +377,11 @@ int main(int argc, char **argv)
     if (dim == 3) PressureSolver3D::ProjectPressure(&grid);
     else PressureSolver2D::ProjectPressure(&grid);
     const double tProject = Now() - t1;
+    if (scheme == 1) // the rest of Project under the incremental scheme
+    {
+        if (dim == 3) PressureSolver3D::AccumulatePressureIncrement(ant, &grid);
+        else PressureSolver2D::AccumulatePressureIncrement(ant, &grid);
+    }
 
     // Post-projection divergence over FLUID cells (MAC::GetDivergencyAt).
     double maxDiv = 0.0;
@@ -399,6 +428,11 @@ int main(int argc, char **argv)
     const int32_t nr = (int32_t)tEach.size();
     WriteN(o, &nr, 1);
     WriteN(o, tEach.data(), tEach.size());
+    if (scheme == 1 || scheme == 2)
+    {
+        WriteN(o, &refNorm, 1);
+        WriteN(o, grid.p.data(), grid.p.size());
+    }
     std::fclose(o);
     return 0;
 }

@@ -61,21 +61,26 @@ class RefResult:
     gap: list
     centre: list
     t_each: np.ndarray  # wall time of each warm repeat
+    ref_norm: float = 0.0  # IncrementReferenceNorm (incremental scheme)
+    p_final: np.ndarray = None  # the pressure after Project (schemes 1 and 2)
+
+
+SCHEME_CHORIN, SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM = 0, 1, 2
 
 
 def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000,
-               threads=1, repeats=0):
+               threads=1, repeats=0, scheme=SCHEME_CHORIN, p_prev=None, time=0.0):
     g = case.grid
     grid_mode = 0 if not g.nonuniform else 1
     nxi, nyi = g.Nx - 2, g.Ny - 2
     nzi = g.Nz - 2 if g.dim == 3 else 0
-    hdr = [g.dim, grid_mode, g.grid_size, nxi, nyi, nzi, label_mode, int(case.needs_compat), 0, solver, max_iters,
-           threads, case.method, repeats, g.Nx, g.Ny]
+    hdr = [g.dim, grid_mode, g.grid_size, nxi, nyi, nzi, label_mode, int(case.needs_compat), scheme, solver,
+           max_iters, threads, case.method, repeats, g.Nx, g.Ny]
     with open(path, "wb") as f:
         f.write(b"NBCASE01")
         f.write(struct.pack("<16i", *hdr))
         f.write(struct.pack("<6d", *g.domain))
-        f.write(struct.pack("<4d", case.rho, case.dt, case.tol if tol is None else tol, 0.0))
+        f.write(struct.pack("<4d", case.rho, case.dt, case.tol if tol is None else tol, time))
         if grid_mode == 1:
             for a in range(g.dim):
                 f.write(np.ascontiguousarray(g.interior_widths[a], dtype="<f8").tobytes())
@@ -89,9 +94,11 @@ def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, 
         f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
         if g.dim == 3:
             f.write(np.ascontiguousarray(w, dtype="<f8").tobytes())
+        if scheme != SCHEME_CHORIN:
+            f.write(np.ascontiguousarray(p_prev, dtype="<f8").reshape(-1).tobytes())
 
 
-def read_result(path, dim) -> RefResult:
+def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
     with open(path, "rb") as f:
         data = f.read()
     assert data[:8] == b"NBRES001", "bad result file"
@@ -132,21 +139,26 @@ def read_result(path, dim) -> RefResult:
     if off + 4 <= len(data):
         (nr,) = struct.unpack_from("<i", data, off); off += 4
         t_each = take("<f8", nr)
+    ref_norm, p_final = 0.0, None
+    if scheme != SCHEME_CHORIN:
+        (ref_norm,) = struct.unpack_from("<d", data, off); off += 8
+        p_final = take("<f8", cells)
     return RefResult(Nx, Ny, Nz, n, iters, bool(sing), thr, tA, tC, tW, tP, rr, md, dh, types, idp, rowptr, col, val,
-                     b_raw, b, x, p, u, v, w, width, gap, centre, t_each)
+                     b_raw, b, x, p, u, v, w, width, gap, centre, t_each, ref_norm, p_final)
 
 
 def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000, threads=1,
-        repeats=0, timeout=3600) -> RefResult:
+        repeats=0, timeout=3600, scheme=SCHEME_CHORIN, p_prev=None, time=0.0) -> RefResult:
     """Runs the reference on ``case`` with face velocities u, v, w; labels from the scene text (label_mode 0) or
     the given ``types`` (label_mode 1)."""
     if not available():
         raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle ref)")
     with tempfile.TemporaryDirectory() as td:
         cp, rp = os.path.join(td, "case.bin"), os.path.join(td, "res.bin")
-        write_case(cp, case, u, v, w, label_mode, types, solver, tol, max_iters, threads, repeats)
+        write_case(cp, case, u, v, w, label_mode, types, solver, tol, max_iters, threads, repeats, scheme, p_prev,
+                   time)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         r = subprocess.run([HARNESS, cp, rp], capture_output=True, text=True, timeout=timeout, env=env, cwd=td)
         if r.returncode != 0:
             raise RuntimeError("ref_harness failed (%d): %s %s" % (r.returncode, r.stdout[-2000:], r.stderr[-2000:]))
-        return read_result(rp, case.grid.dim)
+        return read_result(rp, case.grid.dim, scheme)

@@ -17,8 +17,19 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (runs the CUDA path through the C ABI)")
 
 
+SCHEME_PREFIXES = ("incremental_", "warm_")
+
+
 def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    """The Chorin fixtures (one solve from zero)."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    return [n for n in names if not n.startswith(SCHEME_PREFIXES)]
+
+
+def scheme_golden_names():
+    """The fixtures with a previous step: the incremental scheme and the Chorin warm start."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    return [n for n in names if n.startswith(SCHEME_PREFIXES)]
 
 
 def load_golden(name):

@@ -38,8 +38,53 @@ CASES = [
 ]
 
 
+# the schemes with a previous step: (fixture name, builder, kwargs, tol, scheme, time of the new step)
+SCHEME_CASES = [
+    ("incremental_pressure_outlet_3d_12", "pressure_outlet_3d", {"n": 12, "seed": 18}, 1e-12,
+     refcase.SCHEME_INCREMENTAL, 0.3),
+    ("incremental_closed_box_2d_16", "closed_box_2d", {"n": 16, "seed": 19}, 1e-12, refcase.SCHEME_INCREMENTAL, 0.0),
+    ("warm_sphere_outlet_3d_12", "sphere_outlet_3d", {"n": 12, "seed": 20}, 1e-12, refcase.SCHEME_CHORIN_WARM, 0.0),
+]
+
+
 def build_case(builder: str, kwargs: dict) -> W.Case:
     return getattr(W, builder)(**kwargs)
+
+
+def previous_step(case, types, u, v, w, scheme, time):
+    """p^n for a scheme case: seeded interior values with the outlet's p_b at t - dt (incremental), or the cold
+    Chorin solution plus a 1e-3 N(0,1) perturbation on the unknowns (warm start: a guess close to the answer)."""
+    g = case.grid
+    if scheme == refcase.SCHEME_INCREMENTAL:
+        ring = W.outlet_pressure(time - case.dt) if case.scene.pressure_expr == W.PRESSURE_OUTLET_EXPR else None
+        return W.previous_pressure(g, types, case.seed, ring)
+    cold = refcase.run(case, u, v, w, tol=1e-12)
+    noise = W.previous_pressure(g, types, case.seed)
+    return cold.p + 1e-3 * noise
+
+
+def write_scheme_case(name, builder, kwargs, tol, scheme, time):
+    case = build_case(builder, kwargs)
+    g = case.grid
+    probe = refcase.run(case, *[np.zeros(int(np.prod(s))) if s != (0,) else np.zeros(0)
+                                for s in (g.u_shape(), g.v_shape(), g.w_shape())], tol=1e-6)
+    types = probe.types
+    u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
+    p_prev = previous_step(case, types, u, v, w, scheme, time)
+    ref = refcase.run(case, u, v, w, tol=tol, scheme=scheme, p_prev=p_prev, time=time)
+    cold = refcase.run(case, u, v, w, tol=tol, time=time)
+    p_in = np.where(ref.types == W.PRESSURE, ref.p_final, 0.0)
+    meta = dict(name=name, builder=builder, kwargs=kwargs, tol=tol, needs_compat=case.needs_compat, rho=case.rho,
+                dt=case.dt, n=ref.n, iters=ref.iters, cold_iters=cold.iters, singular=ref.singular,
+                rel_res=ref.rel_res, max_div=ref.max_div, dh=ref.dh, scheme=scheme, time=time,
+                ref_norm=ref.ref_norm)
+    out = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(
+        out, meta=np.array(json.dumps(meta)), u=u.ravel(), v=v.ravel(), w=w.ravel(), p_in=p_in, p_prev=p_prev,
+        types=ref.types, idp=ref.idp, b_raw=ref.b_raw, b=ref.b, x=ref.x, p=ref.p, p_final=ref.p_final,
+        u_out=ref.u, v_out=ref.v, w_out=ref.w)
+    print("%-36s n=%-6d iters=%-4d (cold %d) rel_res=%.2e max_div=%.2e ref_norm=%.3g  %d KB" % (
+        name, ref.n, ref.iters, cold.iters, ref.rel_res, ref.max_div, ref.ref_norm, os.path.getsize(out) // 1024))
 
 
 def main(ref_root: str = "/root/reference") -> None:
@@ -67,6 +112,8 @@ def main(ref_root: str = "/root/reference") -> None:
             **{"centre%d" % a: ref.centre[a] for a in range(3)})
         print("%-36s n=%-6d iters=%-4d rel_res=%.2e max_div=%.2e  %d KB" % (
             name, ref.n, ref.iters, ref.rel_res, ref.max_div, os.path.getsize(out) // 1024))
+    for args in SCHEME_CASES:
+        write_scheme_case(*args)
 
 
 if __name__ == "__main__":
