@@ -204,6 +204,68 @@ typedef struct nb_scene
 int nereus_b200_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
                             const nb_scene *scene, uint8_t *cellTypes);
 
+/* ---- batched and served solves. The reference has one solve per call from the manager thread
+ *      (SimulationManager.h:345-353 -> PressureSolver3D::SolvePressure + Project); a server runs many independent
+ *      pressure steps (tanks of a batch, requests of a stream) concurrently on one or more devices. Each device
+ *      runs `slots_per_device` solves at once (a host thread, a solver context and a CUDA stream each; a context
+ *      keeps its hierarchy while the layout bytes are unchanged, PressureLayoutChanged). A free slot takes the
+ *      oldest queued request whose estimated device memory fits its device's budget: the device that frees a slot
+ *      first takes the next request (least-loaded), and a finished request's slot is refilled at once. ---- */
+typedef struct nb_server nb_server;
+
+typedef struct nb_server_options
+{
+    int n_devices;         /* devices served (>= 1) */
+    const int *devices;    /* their ordinals; NULL: 0 .. n_devices-1 */
+    int slots_per_device;  /* concurrent solves per device (>= 1) */
+    double hbm_budget_gb;  /* admission budget per device, GB of estimated solver memory */
+    nb_options solver;     /* options of every solve; its device and stream fields are ignored */
+} nb_server_options;
+
+typedef struct nb_request
+{
+    int dim, Nx, Ny, Nz;            /* ring included; Nz = 1 in 2D */
+    const uint8_t *cell_types;      /* copied at submission */
+    const double *width[3];         /* padded Width tables (copied at submission) */
+    const double *gap[3];           /* padded FaceGap tables (copied at submission) */
+    int non_uniform;
+    double dh;
+    double *u, *v, *w, *p;          /* host fields, read when the request starts and rewritten when it completes:
+                                       they must stay valid and untouched until then */
+    const double *p_prev;           /* the previous pressure (incremental scheme, warm start), else NULL; read at
+                                       the start */
+    int scheme, needs_compat, warm_start;
+    double rho, dt, tol;
+} nb_request;
+
+typedef struct nb_server_stats
+{
+    long long submitted, completed, failed, queued, running;
+    double seconds;          /* since the first submission */
+    double solves_per_s;     /* completed / seconds */
+    double p50_ms, p99_ms;   /* submission-to-completion latency of the completed requests */
+    double mean_ms;
+    double admitted_gb;      /* estimated device memory of the running requests */
+    long long device_completed[8]; /* completions per served device (the first 8) */
+} nb_server_stats;
+
+void nereus_b200_default_server_options(nb_server_options *o);
+int nereus_b200_server_create(nb_server **srv, const nb_server_options *opt);
+/* Waits for the requests in flight to finish; queued requests that have not started are dropped. */
+void nereus_b200_server_destroy(nb_server *srv);
+/* Queues one request; *ticket identifies it. NB_BAD_INPUT: malformed, or larger than a device's budget. */
+int nereus_b200_submit(nb_server *srv, const nb_request *req, uint64_t *ticket);
+/* NB_BUSY while queued or running; then the request's nb_status, with *out its report. */
+int nereus_b200_poll(nb_server *srv, uint64_t ticket, nb_result *out);
+/* As poll, blocking up to timeout_s seconds (< 0: no limit) for completion. */
+int nereus_b200_wait(nb_server *srv, uint64_t ticket, double timeout_s, nb_result *out);
+int nereus_b200_server_stats(nb_server *srv, nb_server_stats *stats);
+/* Estimated device bytes of one solve (the admission cost): fields, right-hand side and solution, level vectors. */
+double nereus_b200_request_bytes(int dim, int Nx, int Ny, int Nz, int precision);
+/* Host only: a deterministic least-loaded assignment of n requests with the given costs to k devices (or processes):
+ * in submission order, each goes to the device with the smallest assigned total (lowest index on ties). */
+int nereus_b200_plan(const double *costs, int n, int k, int *device_of);
+
 /* ---- IDP numbering without allocation. No counterpart in the reference: its IDP loop runs inside
  *      AssembleSystem (PressureSolver3D.cpp:133-139); this is the same numbering as nereus_b200_get_idp gives after
  *      nereus_b200_set_layout, for callers that must not allocate device memory at the point they renumber. ----

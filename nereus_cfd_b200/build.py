@@ -29,8 +29,9 @@ SOURCES = {
     "nb_solver.cu": [],
     "nb_capi.cu": [],
     "nb_noalloc.cu": [],
+    "nb_server.cu": [],
 }
-HEADERS = ["nb_device.cuh", "nb_kernels.h", "nb_solver.h"]
+HEADERS = ["nb_device.cuh", "nb_kernels.h", "nb_solver.h", "nb_guard.h"]
 
 
 def _newest_input() -> float:

@@ -42,6 +42,35 @@ class Result(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("n_devices", ctypes.c_int), ("devices", ctypes.POINTER(ctypes.c_int)),
+                ("slots_per_device", ctypes.c_int), ("hbm_budget_gb", ctypes.c_double), ("solver", Options)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+                ("cell_types", ctypes.POINTER(ctypes.c_uint8)), ("width", ctypes.POINTER(ctypes.c_double) * 3),
+                ("gap", ctypes.POINTER(ctypes.c_double) * 3), ("non_uniform", ctypes.c_int), ("dh", ctypes.c_double),
+                ("u", ctypes.POINTER(ctypes.c_double)), ("v", ctypes.POINTER(ctypes.c_double)),
+                ("w", ctypes.POINTER(ctypes.c_double)), ("p", ctypes.POINTER(ctypes.c_double)),
+                ("p_prev", ctypes.POINTER(ctypes.c_double)), ("scheme", ctypes.c_int), ("needs_compat", ctypes.c_int),
+                ("warm_start", ctypes.c_int), ("rho", ctypes.c_double), ("dt", ctypes.c_double),
+                ("tol", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("queued", ctypes.c_longlong), ("running", ctypes.c_longlong), ("seconds", ctypes.c_double),
+                ("solves_per_s", ctypes.c_double), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("admitted_gb", ctypes.c_double),
+                ("device_completed", ctypes.c_longlong * 8)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "device_completed"}
+        d["device_completed"] = list(self.device_completed)
+        return d
+
+
 class Region(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("region", ctypes.c_int), ("axis", ctypes.c_int), ("invert", ctypes.c_int),
                 ("p0", ctypes.c_double * 3), ("p1", ctypes.c_double * 3), ("radius", ctypes.c_double)]
@@ -94,6 +123,18 @@ SIGNATURES = {
     "nereus_b200_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "nereus_b200_kernel_launches": (ctypes.c_longlong, []),
+    "nereus_b200_default_server_options": (None, [ctypes.POINTER(ServerOptions)]),
+    "nereus_b200_server_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ServerOptions)]),
+    "nereus_b200_server_destroy": (None, [ctypes.c_void_p]),
+    "nereus_b200_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request),
+                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "nereus_b200_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result)]),
+    "nereus_b200_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
+                                        ctypes.POINTER(Result)]),
+    "nereus_b200_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "nereus_b200_request_bytes": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int]),
+    "nereus_b200_plan": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "nereus_b200_number_unknowns_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                            ctypes.c_void_p, ctypes.c_void_p]),

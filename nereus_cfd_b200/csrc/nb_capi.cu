@@ -1,6 +1,6 @@
 // The extern "C" entry points of include/nereus_b200.h. Every call catches its own exceptions and turns them into an
 // nb_status; the message of the last failure on this host thread is kept for nereus_b200_last_error().
-#include "nb_solver.h"
+#include "nb_guard.h"
 
 #include <memory>
 #include <new>
@@ -11,48 +11,16 @@ struct nb_ctx
     std::unique_ptr<nb::Context> c;
 };
 
-namespace
+namespace nb
+{
+namespace capi
 {
 thread_local std::string g_error;
-
-int Fail(int code, const std::string &msg)
-{
-    g_error = msg;
-    return code;
 }
-
-template <typename F> int Guard(F &&f)
-{
-    try
-    {
-        return f();
-    }
-    catch (const nb::InputError &e)
-    {
-        return Fail(NB_BAD_INPUT, e.what());
-    }
-    catch (const nb::CudaError &e)
-    {
-        if (e.code == cudaErrorMemoryAllocation) return Fail(NB_OUT_OF_MEMORY, e.what());
-        if (e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver ||
-            e.code == cudaErrorNoKernelImageForDevice)
-            return Fail(NB_NO_DEVICE, e.what());
-        return Fail(NB_DEVICE_ERROR, e.what());
-    }
-    catch (const std::bad_alloc &)
-    {
-        return Fail(NB_OUT_OF_MEMORY, "host allocation failed");
-    }
-    catch (const std::exception &e)
-    {
-        return Fail(NB_DEVICE_ERROR, e.what());
-    }
-    catch (...)
-    {
-        return Fail(NB_DEVICE_ERROR, "unknown failure");
-    }
-}
-} // namespace
+} // namespace nb
+using nb::capi::Fail;
+using nb::capi::Guard;
+using nb::capi::g_error;
 
 extern "C" {
 

@@ -1,0 +1,202 @@
+"""Batched and served pressure steps through the library's server (include/nereus_b200.h, nereus_b200_server_*):
+many independent projections (the tanks of a batch, the requests of a stream) run concurrently on one or more
+devices, admitted by a per-device memory budget, each returning like one nereus_b200_project_ex call.
+
+Across processes (torchrun, one process per GPU) the requests are split by the library's deterministic least-loaded
+plan (nereus_b200_plan), each rank serves its share on its own device, and the per-rank results are gathered with
+torch.distributed (NCCL on GPUs, gloo elsewhere). The solve path itself has no collective.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+
+from . import capi
+from .pressure import MACGrid
+
+
+@dataclass
+class Job:
+    """One pressure step: a grid state (fields rewritten in place on completion) and how to solve it."""
+    grid: MACGrid
+    tol: float = 1e-8
+    needs_compat: bool = False
+    scheme: int = capi.SCHEME_CHORIN
+    p_prev: Optional[np.ndarray] = None
+    warm_start: bool = False
+    result: Optional[dict] = None
+    status: Optional[int] = None
+    latency_ms: Optional[float] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def cells(self) -> int:
+        return self.grid.grid.cells
+
+
+def job_from_case(case, tol: Optional[float] = None, types: Optional[np.ndarray] = None) -> Job:
+    """A job for one synthetic case: cell labels (on the device unless given), the case's seeded face velocities,
+    p = 0 with no prescribed ring values."""
+    from . import workloads as W
+
+    g = case.grid
+    if types is None:
+        types = capi.label_cells(g, case.scene)
+    u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
+    m = MACGrid.from_case(case, types, u, v, w)
+    return Job(m, tol=case.tol if tol is None else tol, needs_compat=case.needs_compat)
+
+
+def tank_batch(count: int = 64, n: int = 128, seed: int = 4) -> list:
+    """The batch of FLIP-style tanks: ``count`` unit-cube n^3 tanks, liquid where x < a and z < b with a, b ~
+    U(0.3, 0.7) drawn per tank from the seed, FP32-rounded liquid-face velocities."""
+    from . import workloads as W
+
+    return [W.flip_tank_3d(n, seed=seed + 1000 * t) for t in range(count)]
+
+
+def request_bytes(job: Job, precision: int = capi.PRECISION_MIXED) -> float:
+    g = job.grid.grid
+    return capi.load().nereus_b200_request_bytes(g.dim, g.Nx, g.Ny, g.Nz, precision)
+
+
+def plan(costs: Sequence[float], k: int) -> List[int]:
+    """The least-loaded assignment of requests (in order) to k devices or ranks (nereus_b200_plan)."""
+    n = len(costs)
+    c = np.ascontiguousarray(costs, dtype=np.float64)
+    out = (ctypes.c_int * max(n, 1))()
+    capi.check(capi.load().nereus_b200_plan(capi.ptr(c), n, k, out))
+    return [out[i] for i in range(n)]
+
+
+class Server:
+    """nereus_b200_server_*: submit jobs, poll or wait for them, read the server's statistics."""
+
+    def __init__(self, devices: Sequence[int] = (0,), slots_per_device: int = 4, hbm_budget_gb: float = 150.0,
+                 precision: str = "mixed", **solver_options):
+        self.lib = capi.load()
+        o = capi.ServerOptions()
+        self.lib.nereus_b200_default_server_options(ctypes.byref(o))
+        self._devs = (ctypes.c_int * len(devices))(*devices)
+        o.n_devices = len(devices)
+        o.devices = ctypes.cast(self._devs, ctypes.POINTER(ctypes.c_int))
+        o.slots_per_device = slots_per_device
+        o.hbm_budget_gb = hbm_budget_gb
+        o.solver.precision = {"mixed": capi.PRECISION_MIXED, "fp64": capi.PRECISION_FP64}[precision]
+        for k, v in solver_options.items():
+            setattr(o.solver, k, v)
+        self.precision = o.solver.precision
+        self.srv = ctypes.c_void_p()
+        capi.check(self.lib.nereus_b200_server_create(ctypes.byref(self.srv), ctypes.byref(o)))
+        self.jobs = {}
+
+    def submit(self, job: Job) -> int:
+        m, g = job.grid, job.grid.grid
+        widths = [np.ascontiguousarray(a) for a in g.width_tables()]
+        gaps = [np.ascontiguousarray(a) for a in g.gap_tables()]
+        types = np.ascontiguousarray(m.types, dtype=np.uint8)
+        w = m.w if g.dim == 3 else np.zeros(1)
+        r = capi.Request()
+        r.dim, r.Nx, r.Ny, r.Nz = g.dim, g.Nx, g.Ny, g.Nz
+        r.cell_types = capi.ptr(types, capi._u8)
+        for a in range(3):
+            r.width[a] = capi.ptr(widths[a])
+            r.gap[a] = capi.ptr(gaps[a])
+        r.non_uniform, r.dh = int(g.nonuniform), g.dh
+        r.u, r.v, r.w, r.p = capi.ptr(m.u), capi.ptr(m.v), capi.ptr(w), capi.ptr(m.p)
+        prev = None
+        if job.p_prev is not None:
+            prev = np.ascontiguousarray(job.p_prev, dtype=np.float64)
+            r.p_prev = capi.ptr(prev)
+        r.scheme, r.needs_compat, r.warm_start = job.scheme, int(job.needs_compat), int(job.warm_start)
+        r.rho, r.dt, r.tol = m.rho, m.dt, job.tol
+        ticket = ctypes.c_uint64(0)
+        capi.check(self.lib.nereus_b200_submit(self.srv, ctypes.byref(r), ctypes.byref(ticket)))
+        job._keep = [w, prev]  # the fields must outlive the request
+        self.jobs[ticket.value] = (job, time.perf_counter())
+        return ticket.value
+
+    def _finish(self, ticket: int, st: int, res: capi.Result):
+        job, t0 = self.jobs[ticket]
+        job.status = st
+        job.result = res.as_dict()
+        if job.latency_ms is None:
+            job.latency_ms = 1e3 * (time.perf_counter() - t0)
+        return st
+
+    def poll(self, ticket: int) -> int:
+        res = capi.Result()
+        st = self.lib.nereus_b200_poll(self.srv, ticket, ctypes.byref(res))
+        return st if st == capi.NB_BUSY else self._finish(ticket, st, res)
+
+    def wait(self, ticket: int, timeout_s: float = -1.0) -> int:
+        res = capi.Result()
+        st = self.lib.nereus_b200_wait(self.srv, ticket, timeout_s, ctypes.byref(res))
+        return st if st == capi.NB_BUSY else self._finish(ticket, st, res)
+
+    def stats(self) -> dict:
+        s = capi.ServerStats()
+        capi.check(self.lib.nereus_b200_server_stats(self.srv, ctypes.byref(s)))
+        return s.as_dict()
+
+    def close(self):
+        if self.srv:
+            self.lib.nereus_b200_server_destroy(self.srv)
+            self.srv = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve(jobs: Sequence[Job], server: Server) -> dict:
+    """Submits every job, waits for all, and returns the server's statistics (solves/s, p50/p99 latency)."""
+    tickets = [server.submit(j) for j in jobs]
+    for t in tickets:
+        server.wait(t)
+    return server.stats()
+
+
+def run_sharded(jobs: Sequence[Job], execute: Callable[[List[Job]], dict], dist=None) -> dict:
+    """Splits ``jobs`` over the ranks of the default process group by the least-loaded plan on their cell counts,
+    runs this rank's share with ``execute`` (a list of jobs -> {"seconds": wall seconds, ...}; the B200 form wraps
+    ``serve``), and gathers (completed, seconds, latencies) from every rank. ``seconds`` is the max over ranks, so
+    solves/s = all completions / that time. With no process group it runs everything here."""
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None else (0, 1)
+    owner = plan([j.cells for j in jobs], world)
+    mine = [j for j, o in zip(jobs, owner) if o == rank]
+    out = execute(mine)
+    lat = [j.latency_ms for j in mine if j.latency_ms is not None]
+    local = {"rank": rank, "jobs": len(mine), "completed": sum(1 for j in mine if j.status in (0, 1)),
+             "seconds": float(out.get("seconds", 0.0)), "latencies": lat}
+    if dist is None:
+        gathered = [local]
+    else:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local)
+    seconds = max(g["seconds"] for g in gathered)
+    lats = sorted(x for g in gathered for x in g["latencies"])
+    completed = sum(g["completed"] for g in gathered)
+
+    def pct(q):
+        if not lats:
+            return None
+        k = (len(lats) - 1) * q
+        lo, hi = int(k), min(int(k) + 1, len(lats) - 1)
+        return lats[lo] + (lats[hi] - lats[lo]) * (k - lo)
+
+    return {"world": world, "completed": completed, "seconds": seconds,
+            "solves_per_s": completed / seconds if seconds > 0 else None, "p50_ms": pct(0.5), "p99_ms": pct(0.99),
+            "per_rank": [{k: g[k] for k in ("rank", "jobs", "completed", "seconds")} for g in gathered]}
