@@ -287,6 +287,8 @@ def run_b200(args, rank, world, dist):
                "p99_ms": round(1e3 * percentile(ts, 0.99), 3), "api": "nereus_b200_project (host buffers)"}
         s.DestroyPressureSolver()
 
+    tanks = run_tanks(args, rank, world, dist, dev) if args.tanks > 0 else None
+
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
@@ -299,8 +301,64 @@ def run_b200(args, rank, world, dist):
         "latency_ms": {"p50": round(percentile(lat, 0.5), 3), "p99": round(percentile(lat, 0.99), 3)},
         "solve": {k: mixed_res[k] for k in ("iters_outer", "iters_inner", "rel_res", "max_div", "status")},
         "fp64_plain": fp64, "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": int(launches),
+        "batched_tanks": tanks,
     }
     return out
+
+
+def run_tanks(args, rank, world, dist, dev):
+    """The batched form: `tanks` FLIP-style n^3 tanks (liquid where x < a, z < b; a, b ~ U(0.3, 0.7) per tank),
+    each one pressure step to 1e-8 through the server (`slots` concurrent solves on this rank's device; every solve's
+    layout and host fields uploaded, projected and read back), split over the ranks by the least-loaded plan; against
+    the same tanks solved one at a time in plain FP64. Wall clock from the first submission to the last completion,
+    max over ranks."""
+    import copy
+
+    from nereus_cfd_b200 import serving
+    from nereus_cfd_b200.pressure import PressureSolver
+
+    cases = serving.tank_batch(args.tanks, args.tank_size)
+    summary = {}
+
+    def execute(mine):
+        jobs = [serving.job_from_case(c, tol=TOL) for c in mine]
+        if not jobs:
+            return {"seconds": 0.0, "completed": 0, "latencies": []}
+        with serving.Server(devices=(dev,), slots_per_device=args.slots, **args.solver_opts) as srv:
+            warm = [copy.deepcopy(j) for j in jobs[: args.slots]]
+            serving.serve_jobs(warm, srv)  # each slot's context, graphs and buffers
+            out = serving.serve_jobs(jobs, srv)
+        out["iters_inner"] = [j.result["iters_inner"] for j in jobs if j.result]
+        # one at a time in plain FP64 on a sample of the same tanks
+        sample = [serving.job_from_case(c, tol=TOL) for c in mine[: args.fp64_tanks]]
+        s = PressureSolver("fp64", device=dev, **args.solver_opts)
+        s.InitializePressureSolver(sample[0].grid)
+        s.SolvePressure(copy.deepcopy(sample[0].grid), tol=TOL)  # warm-up
+        t0 = time.perf_counter()
+        for j in sample:
+            s.SolvePressure(j.grid, tol=TOL)
+        out["fp64_seconds_each"] = (time.perf_counter() - t0) / len(sample)
+        s.DestroyPressureSolver()
+        summary.update(out)
+        return out
+
+    res = serving.run_sharded(cases, lambda c: c.grid.cells, execute, dist)
+    fp64_each = summary.get("fp64_seconds_each")
+    if dist:
+        vals = [None] * world
+        dist.all_gather_object(vals, fp64_each)
+        fp64_each = max(v for v in vals if v is not None)
+    fp64_rate = world / fp64_each if fp64_each else None
+    its = summary.get("iters_inner", [])
+    return {"workload": "flip_tanks_%dx%d^3" % (args.tanks, args.tank_size), "tanks": args.tanks,
+            "slots_per_device": args.slots, "value": round(res["solves_per_s"], 3), "unit": "solves/s",
+            "p50_ms": round(res["p50_ms"], 3), "p99_ms": round(res["p99_ms"], 3), "seconds": round(res["seconds"], 4),
+            "scaling": "strong", "iters_inner_rank0": [int(min(its)), int(max(its))] if its else None,
+            "fp64_one_at_a_time": {"value": round(fp64_rate, 3) if fp64_rate else None, "unit": "solves/s",
+                                   "sample_tanks": args.fp64_tanks},
+            "speedup_over_fp64_one_at_a_time": round(res["solves_per_s"] / fp64_rate, 3) if fp64_rate else None,
+            "timing": "host wall clock, first submission to last completion, max over ranks",
+            "per_rank": res["per_rank"]}
 
 
 # ---------------------------------------------------------------------------------------------------------------------
@@ -379,6 +437,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--opt", action="append", default=[], help="solver option key=value (nb_options field)")
+    ap.add_argument("--tanks", type=int, default=64, help="batched tanks (0: skip the batched form)")
+    ap.add_argument("--tank-size", type=int, default=128)
+    ap.add_argument("--slots", type=int, default=4, help="concurrent solves per device in the batched form")
+    ap.add_argument("--fp64-tanks", type=int, default=4, help="tanks solved one at a time in plain FP64")
     args = ap.parse_args()
     args.solver_opts = {k: int(v) if v.lstrip("-").isdigit() else float(v)
                         for k, v in (o.split("=", 1) for o in args.opt)}

@@ -169,18 +169,18 @@ def serve(jobs: Sequence[Job], server: Server) -> dict:
     return server.stats()
 
 
-def run_sharded(jobs: Sequence[Job], execute: Callable[[List[Job]], dict], dist=None) -> dict:
-    """Splits ``jobs`` over the ranks of the default process group by the least-loaded plan on their cell counts,
-    runs this rank's share with ``execute`` (a list of jobs -> {"seconds": wall seconds, ...}; the B200 form wraps
-    ``serve``), and gathers (completed, seconds, latencies) from every rank. ``seconds`` is the max over ranks, so
-    solves/s = all completions / that time. With no process group it runs everything here."""
+def run_sharded(items: Sequence, cost: Callable, execute: Callable[[list], dict], dist=None) -> dict:
+    """Splits ``items`` (jobs, or cases that ``execute`` turns into jobs) over the ranks of the default process
+    group by the least-loaded plan on ``cost(item)``, runs this rank's share with ``execute`` (a list of items ->
+    {"seconds": wall seconds, "completed": count, "latencies": [ms, ...]}), and gathers every rank's figures.
+    ``seconds`` is the max over ranks, so solves/s = all completions / that time. With no process group it runs
+    everything here."""
     rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None else (0, 1)
-    owner = plan([j.cells for j in jobs], world)
-    mine = [j for j, o in zip(jobs, owner) if o == rank]
+    owner = plan([cost(x) for x in items], world)
+    mine = [x for x, o in zip(items, owner) if o == rank]
     out = execute(mine)
-    lat = [j.latency_ms for j in mine if j.latency_ms is not None]
-    local = {"rank": rank, "jobs": len(mine), "completed": sum(1 for j in mine if j.status in (0, 1)),
-             "seconds": float(out.get("seconds", 0.0)), "latencies": lat}
+    local = {"rank": rank, "items": len(mine), "completed": int(out.get("completed", 0)),
+             "seconds": float(out.get("seconds", 0.0)), "latencies": list(out.get("latencies", []))}
     if dist is None:
         gathered = [local]
     else:
@@ -199,4 +199,16 @@ def run_sharded(jobs: Sequence[Job], execute: Callable[[List[Job]], dict], dist=
 
     return {"world": world, "completed": completed, "seconds": seconds,
             "solves_per_s": completed / seconds if seconds > 0 else None, "p50_ms": pct(0.5), "p99_ms": pct(0.99),
-            "per_rank": [{k: g[k] for k in ("rank", "jobs", "completed", "seconds")} for g in gathered]}
+            "per_rank": [{k: g[k] for k in ("rank", "items", "completed", "seconds")} for g in gathered]}
+
+
+def serve_jobs(jobs: Sequence[Job], server: Server) -> dict:
+    """``execute`` for run_sharded on this rank's device: serve the jobs, report wall seconds from the first
+    submission to the last completion, completions and latencies."""
+    t0 = time.perf_counter()
+    tickets = [server.submit(j) for j in jobs]
+    for t in tickets:
+        server.wait(t)
+    seconds = time.perf_counter() - t0
+    done = [j for j in jobs if j.status in (capi.NB_OK, capi.NB_NOT_CONVERGED)]
+    return {"seconds": seconds, "completed": len(done), "latencies": [j.latency_ms for j in done]}

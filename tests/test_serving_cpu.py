@@ -78,7 +78,7 @@ def _oracle_execute(jobs):
         if m.w.size:
             m.w[:] = r.w
         j.status, j.latency_ms, j.result = 0, 1e3 * (time.perf_counter() - t1), {"rel_res": r.rel_res}
-    return {"seconds": time.perf_counter() - t0}
+    return {"seconds": time.perf_counter() - t0, "completed": len(jobs), "latencies": [j.latency_ms for j in jobs]}
 
 
 def _rank_main(rank, world, port, out_dir):
@@ -86,7 +86,7 @@ def _rank_main(rank, world, port, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         jobs = _jobs()
-        summary = serving.run_sharded(jobs, _oracle_execute, dist)
+        summary = serving.run_sharded(jobs, lambda j: j.cells, _oracle_execute, dist)
         owner = serving.plan([j.cells for j in jobs], world)
         mine = [i for i, o in enumerate(owner) if o == rank]
         np.savez(os.path.join(out_dir, "rank%d.npz" % rank), mine=np.array(mine, dtype=np.int64),
