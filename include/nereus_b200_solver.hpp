@@ -58,10 +58,13 @@ class PressureSolver
 
     nb_options &Options() { return opt_; }
 
-    // InitializePressureSolver (PressureSolver3D.cpp:89-102): backend up, system assembled for this layout.
-    void InitializePressureSolver(const GridView &g, int scheme = NB_SCHEME_CHORIN)
+    // InitializePressureSolver (PressureSolver3D.cpp:89-102): backend up, system assembled for this layout, the
+    // scheme (SYSTEM.scheme) kept for SolvePressure. warmStart: PRESSURE_SETTINGS.warmStart for the Chorin scheme.
+    void InitializePressureSolver(const GridView &g, int scheme = NB_SCHEME_CHORIN, bool warmStart = false)
     {
-        if (scheme != NB_SCHEME_CHORIN) throw Error(NB_BAD_INPUT, "only the Chorin scheme is served");
+        if (scheme != NB_SCHEME_CHORIN && scheme != NB_SCHEME_INCREMENTAL) throw Error(NB_BAD_INPUT, "unknown scheme");
+        scheme_ = scheme;
+        warmStart_ = warmStart;
         if (!ctx_) Check(nereus_b200_create(&ctx_, &opt_));
         EnsureSystem(g);
     }
@@ -80,13 +83,34 @@ class PressureSolver
     }
     void ReleasePressureSolver() { DestroyPressureSolver(); }
 
-    // SolveChorin / SolvePressure (PressureSolver3D.cpp:279-345) fused with ProjectPressure (:417-438): p must carry
-    // the ring values EnforcePressureBC(time) wrote. Returns the report; NOT_CONVERGED is reported, not thrown.
-    nb_result SolvePressure(const GridView &g, double rho, double dt, bool needsCompat, double tol)
+    // SolvePressure (PressureSolver3D.cpp:279-345) fused with Project (:396-438) in the initialised scheme: p must
+    // carry the ring values EnforcePressureBC(time) wrote; pPrev is gridAnt's pressure (required by the incremental
+    // scheme, the guess of the Chorin warm start, else may be null). Returns the report; NOT_CONVERGED is reported,
+    // not thrown.
+    nb_result SolvePressure(const GridView &g, double rho, double dt, bool needsCompat, double tol,
+                            const double *pPrev = nullptr)
     {
         EnsureSystem(g);
         nb_result r{};
-        Check(nereus_b200_project(ctx_, g.u, g.v, g.w, g.p, rho, dt, NB_SCHEME_CHORIN, needsCompat ? 1 : 0, tol, &r));
+        if (scheme_ == NB_SCHEME_INCREMENTAL || (warmStart_ && pPrev))
+            Check(nereus_b200_project_ex(ctx_, g.u, g.v, g.w, g.p, pPrev, rho, dt, scheme_, needsCompat ? 1 : 0,
+                                         warmStart_ ? 1 : 0, tol, &r));
+        else
+            Check(nereus_b200_project(ctx_, g.u, g.v, g.w, g.p, rho, dt, NB_SCHEME_CHORIN, needsCompat ? 1 : 0, tol,
+                                      &r));
+        lastIterations_ = r.iters_inner;
+        return r;
+    }
+
+    // SolveIncremental + Project (PressureSolver3D.h:58,71) from the previous step's pressure, whatever the
+    // initialised scheme.
+    nb_result SolveIncremental(const double *pPrev, const GridView &g, double rho, double dt, bool needsCompat,
+                               double tol)
+    {
+        EnsureSystem(g);
+        nb_result r{};
+        Check(nereus_b200_project_ex(ctx_, g.u, g.v, g.w, g.p, pPrev, rho, dt, NB_SCHEME_INCREMENTAL,
+                                     needsCompat ? 1 : 0, 0, tol, &r));
         lastIterations_ = r.iters_inner;
         return r;
     }
@@ -128,6 +152,8 @@ class PressureSolver
     nb_options opt_{};
     nb_ctx *ctx_ = nullptr;
     int lastIterations_ = 0;
+    int scheme_ = NB_SCHEME_CHORIN;
+    bool warmStart_ = false;
 };
 
 } // namespace nereus_b200
