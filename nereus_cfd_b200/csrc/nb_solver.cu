@@ -193,6 +193,7 @@ void Context::BuildHierarchy()
     {
         const int nl = (int)L.size() - l;
         if (nl > kMaxTailLevels || L[l].cells > kTailCellCap) break;
+        if (std::max(L[l].Nx, std::max(L[l].Ny, L[l].Nz)) > 1023) break; // the tail packs i, j, k in 10 bits each
         const size_t bytes = mixed ? TailSmemBytes<float>(&views[l], nl) : TailSmemBytes<double>(&views[l], nl);
         if (bytes > kTailMaxSmem) break;
         tailStart = l;

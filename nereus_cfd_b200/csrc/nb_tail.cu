@@ -24,19 +24,33 @@ template <typename T> struct TailArgs
     int pre, post, coarseSweeps;
 };
 
-// The level's arrays in shared memory: r, e, res (T), then code and types (bytes), each padded to 16 bytes.
+// The level's arrays in shared memory: r, e, res (T), then code and types (bytes), then the list of its unknowns
+// (4 bytes each: red ones from the front, black ones from the back), each padded to 16 bytes.
 template <typename T> __host__ __device__ inline unsigned LevelBytes(long long cells)
 {
     const unsigned a = (unsigned)((cells * sizeof(T) + 15) / 16 * 16);
     const unsigned b = (unsigned)((cells + 15) / 16 * 16);
-    return 3 * a + 2 * b;
+    const unsigned l = (unsigned)((cells * 4 + 15) / 16 * 16);
+    return 3 * a + 2 * b + l;
 }
 
 template <typename T> struct SmemLevel
 {
     LevelView v; // types/code point into shared memory
     T *r, *e, *res;
+    unsigned *list; // packed (i << 20 | j << 10 | k) of the unknowns; red [0, nRed), black [cells - nBlack, cells)
+    int nRed, nBlack;
 };
+
+// unknowns per colour of each tail level, counted while the lists are built
+__shared__ int g_tailCount[kMaxTailLevels][2];
+
+__device__ __forceinline__ void Unpack(unsigned x, int &i, int &j, int &k)
+{
+    i = (int)(x >> 20);
+    j = (int)((x >> 10) & 1023u);
+    k = (int)(x & 1023u);
+}
 
 template <typename T> __device__ __forceinline__ SmemLevel<T> Bind(const TailLevel<T> &tl, unsigned char *smem)
 {
@@ -51,7 +65,31 @@ template <typename T> __device__ __forceinline__ SmemLevel<T> Bind(const TailLev
     s.res = (T *)(base + 2 * a);
     s.v.code = base + 3 * a;
     s.v.types = base + 3 * a + b;
+    s.list = (unsigned *)(base + 3 * a + 2 * b);
     return s;
+}
+
+// the level bound with its unknown counts (valid once the lists are built)
+template <typename T> __device__ __forceinline__ SmemLevel<T> BindL(const TailLevel<T> &tl, unsigned char *smem, int l)
+{
+    SmemLevel<T> s = Bind<T>(tl, smem);
+    s.nRed = g_tailCount[l][0];
+    s.nBlack = g_tailCount[l][1];
+    return s;
+}
+
+// the t-th unknown of the given colour (0 red, 1 black, 2 both: red then black)
+template <typename T> __device__ __forceinline__ unsigned ListAt(const SmemLevel<T> &L, int colour, int t)
+{
+    const long long cells = L.v.cells;
+    if (colour == 0) return L.list[t];
+    if (colour == 1) return L.list[cells - 1 - t];
+    return t < L.nRed ? L.list[t] : L.list[cells - 1 - (t - L.nRed)];
+}
+
+template <typename T> __device__ __forceinline__ int ListLen(const SmemLevel<T> &L, int colour)
+{
+    return colour == 0 ? L.nRed : (colour == 1 ? L.nBlack : L.nRed + L.nBlack);
 }
 
 __device__ __forceinline__ void Decode(const LevelView &v, long long c, int &i, int &j, int &k)
@@ -65,13 +103,13 @@ __device__ __forceinline__ void Decode(const LevelView &v, long long c, int &i, 
 template <typename T> __device__ void TSmooth(const SmemLevel<T> &L, int colour, bool first)
 {
     const LevelView &v = L.v;
-    for (long long c = threadIdx.x; c < v.cells; c += blockDim.x)
+    const int n = ListLen(L, colour);
+    for (int t = threadIdx.x; t < n; t += blockDim.x)
     {
-        const unsigned code = v.code[c];
-        if (!(code & CODE_UNKNOWN)) continue;
         int i, j, k;
-        Decode(v, c, i, j, k);
-        if (((i + j + k) & 1) != colour) continue;
+        Unpack(ListAt(L, colour, t), i, j, k);
+        const long long c = (long long)i * v.sI + (long long)j * v.sJ + k;
+        const unsigned code = v.code[c];
         T cq[6], diag;
         CodeStencil<T>(v, i, j, k, c, code, cq, diag);
         T rhs = L.r[c];
@@ -92,12 +130,13 @@ template <typename T> __device__ void TSmooth(const SmemLevel<T> &L, int colour,
 template <typename T> __device__ void TResidual(const SmemLevel<T> &L)
 {
     const LevelView &v = L.v;
-    for (long long c = threadIdx.x; c < v.cells; c += blockDim.x)
+    const int n = ListLen(L, 2);
+    for (int t = threadIdx.x; t < n; t += blockDim.x)
     {
-        const unsigned code = v.code[c];
-        if (!(code & CODE_UNKNOWN)) continue;
         int i, j, k;
-        Decode(v, c, i, j, k);
+        Unpack(ListAt(L, 2, t), i, j, k);
+        const long long c = (long long)i * v.sI + (long long)j * v.sJ + k;
+        const unsigned code = v.code[c];
         T cq[6], diag;
         CodeStencil<T>(v, i, j, k, c, code, cq, diag);
         T s = diag * L.e[c];
@@ -133,11 +172,12 @@ __device__ __forceinline__ T TSolidWeight(const LevelView &cv, int I, int J, int
 template <typename T> __device__ void TRestrict(const SmemLevel<T> &F, const SmemLevel<T> &C)
 {
     const LevelView &fv = F.v, &cv = C.v;
-    for (long long c = threadIdx.x; c < cv.cells; c += blockDim.x)
+    const int n = ListLen(C, 2);
+    for (int t = threadIdx.x; t < n; t += blockDim.x)
     {
-        if (!(cv.code[c] & CODE_UNKNOWN)) continue;
         int I, J, K;
-        Decode(cv, c, I, J, K);
+        Unpack(ListAt(C, 2, t), I, J, K);
+        const long long c = (long long)I * cv.sI + (long long)J * cv.sJ + K;
         T acc = (T)0;
         const T wt[4] = {(T)0.25, (T)0.75, (T)0.75, (T)0.25};
         for (int di = 0; di < 4; di++)
@@ -182,11 +222,12 @@ template <typename T> __device__ void TRestrict(const SmemLevel<T> &F, const Sme
 template <typename T> __device__ void TProlong(const SmemLevel<T> &F, const SmemLevel<T> &C)
 {
     const LevelView &fv = F.v, &cv = C.v;
-    for (long long c = threadIdx.x; c < fv.cells; c += blockDim.x)
+    const int n = ListLen(F, 2);
+    for (int t = threadIdx.x; t < n; t += blockDim.x)
     {
-        if (!(fv.code[c] & CODE_UNKNOWN)) continue;
         int a, b, d;
-        Decode(fv, c, a, b, d);
+        Unpack(ListAt(F, 2, t), a, b, d);
+        const long long c = (long long)a * fv.sI + (long long)b * fv.sJ + d;
         const int A = (a + 1) >> 1, B = (b + 1) >> 1;
         const int D = fv.dim == 3 ? (d + 1) >> 1 : 0;
         const int si = (a & 1) ? -1 : 1, sj = (b & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
@@ -225,11 +266,31 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tail(TailArgs<T>
             S.r[c] = l == 0 ? A.rIn[c] : (T)0;
         }
     }
+    if (threadIdx.x < 2 * kMaxTailLevels) g_tailCount[threadIdx.x >> 1][threadIdx.x & 1] = 0;
+    __syncthreads();
+    // the unknowns of every level by colour (i + j + k) & 1; their order within a colour does not matter (the
+    // cells of one colour are updated independently)
+    for (int l = 0; l < A.nlev; l++)
+    {
+        const LevelView &g = A.lv[l].v;
+        const SmemLevel<T> S = Bind<T>(A.lv[l], smem);
+        for (long long c = threadIdx.x; c < g.cells; c += blockDim.x)
+        {
+            if (!(S.v.code[c] & CODE_UNKNOWN)) continue;
+            int i, j, k;
+            Decode(g, c, i, j, k);
+            const int col = (i + j + k) & 1;
+            const int pos = atomicAdd(&g_tailCount[l][col], 1);
+            const unsigned packed = ((unsigned)i << 20) | ((unsigned)j << 10) | (unsigned)k;
+            if (col == 0) S.list[pos] = packed;
+            else S.list[g.cells - 1 - pos] = packed;
+        }
+    }
     __syncthreads();
     const int last = A.nlev - 1;
     for (int l = 0; l < last; l++)
     {
-        const SmemLevel<T> F = Bind<T>(A.lv[l], smem);
+        const SmemLevel<T> F = BindL<T>(A.lv[l], smem, l);
         TSmooth<T>(F, 0, true);
         TSmooth<T>(F, 1, false);
         for (int s = 1; s < A.pre; s++)
@@ -238,10 +299,10 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tail(TailArgs<T>
             TSmooth<T>(F, 1, false);
         }
         TResidual<T>(F);
-        TRestrict<T>(F, Bind<T>(A.lv[l + 1], smem));
+        TRestrict<T>(F, BindL<T>(A.lv[l + 1], smem, l + 1));
     }
     {
-        const SmemLevel<T> C = Bind<T>(A.lv[last], smem);
+        const SmemLevel<T> C = BindL<T>(A.lv[last], smem, last);
         TSmooth<T>(C, 0, true);
         TSmooth<T>(C, 1, false);
         for (int s = 1; s < A.coarseSweeps; s++)
@@ -257,8 +318,8 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tail(TailArgs<T>
     }
     for (int l = last - 1; l >= 0; l--)
     {
-        const SmemLevel<T> F = Bind<T>(A.lv[l], smem);
-        TProlong<T>(F, Bind<T>(A.lv[l + 1], smem));
+        const SmemLevel<T> F = BindL<T>(A.lv[l], smem, l);
+        TProlong<T>(F, BindL<T>(A.lv[l + 1], smem, l + 1));
         for (int s = 0; s < A.post; s++)
         {
             TSmooth<T>(F, 1, false);
