@@ -3,7 +3,8 @@
 //
 // Cell pairs. With Nz even, the two cells (i, j, 2m) and (i, j, 2m+1) form an 8-byte aligned pair, and a plane of
 // Nx*Nz cells is Nx*Nz/2 consecutive pairs. Thread t of the launch takes pair t of the plane (crossing row ends
-// freely: a row's ring cells ride along, their vector entries are zero) and marches along i over kPairS planes,
+// freely: a row's ring cells ride along, their vector entries are zero) and marches along i over up to kPairS
+// planes (fewer on small levels, so that a launch still has about 148 x 8 blocks and no long serial chains),
 // keeping the pairs of planes i-1, i, i+1 in registers. A warp's load of one plane is 256 contiguous bytes; the j
 // neighbours are the pairs Nz/2 away; the k neighbours are the other cell of the pair and, across the pair
 // boundary, the neighbouring lane's pair (a shuffle; lanes 0 and 31 load that one cell).
@@ -17,6 +18,8 @@
 // isolated cells at zero like the reference's zero diagonal guard).
 #include "nb_kernels.h"
 
+#include <algorithm>
+
 namespace nb
 {
 
@@ -24,7 +27,15 @@ namespace
 {
 
 constexpr int kPairThreads = 256;
-constexpr int kPairS = 8; // planes a thread marches
+constexpr int kPairS = 8;             // planes a thread marches at most
+constexpr long long kPairBlocks = 148 * 8; // blocks a launch aims for
+
+// Planes per thread for `planes` planes of `perPlane` blocks each: about kPairBlocks blocks, 1 .. kPairS planes.
+inline int MarchPlanes(long long planes, long long perPlane)
+{
+    long long s = (planes * perPlane + kPairBlocks - 1) / kPairBlocks;
+    return (int)std::max(1LL, std::min<long long>(kPairS, s));
+}
 
 // Per-thread position of a pair kernel.
 struct PairPos
@@ -45,8 +56,11 @@ __device__ __forceinline__ PairPos PairStart(const LevelView &v)
     int q = blockIdx.x * kPairThreads + threadIdx.x;
     p.valid = q < P;
     if (!p.valid) q = P - 1;
-    p.i0 = 1 + blockIdx.y * kPairS;
-    p.i1 = min(p.i0 + kPairS, v.Ny - 1);
+    // the launch's grid.y splits the Ny-2 interior planes into chunks of S (the host sized it); a block past the
+    // last plane starts at the ring plane and marches none
+    const int S = (v.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
+    p.i0 = min(1 + (int)blockIdx.y * S, v.Ny - 1);
+    p.i1 = min(p.i0 + S, v.Ny - 1);
     p.sI = (int)v.sI;
     p.sJ = (int)v.sJ;
     const int cin = 2 * q;
@@ -111,8 +125,9 @@ void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st)
 
 static inline dim3 PairGrid(const LevelView &v)
 {
-    const long long P = v.sI / 2;
-    return dim3((unsigned)((P + kPairThreads - 1) / kPairThreads), (unsigned)((v.Ny - 2 + kPairS - 1) / kPairS));
+    const long long P = v.sI / 2, perPlane = (P + kPairThreads - 1) / kPairThreads, planes = v.Ny - 2;
+    const int S = MarchPlanes(planes, perPlane);
+    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_half(LevelView v, const u
                                                             const float *__restrict__ r, float *e, int colour,
                                                             Reducer R, const int *it, int baseEven, int baseOdd)
 {
-    float facc[3] = {0.f, 0.f, 0.f}; // a thread's 2 x kPairS terms in FP32, the block and grid sums in FP64
+    float facc[3] = {0.f, 0.f, 0.f}; // a thread's (at most 2 x kPairS) terms in FP32, the block and grid sums in FP64
     __shared__ float inv[32];
     FillInverse(inv, v.gamma);
     const PairPos P = PairStart(v);
@@ -396,7 +411,6 @@ void LaunchPairProlong(const LevelView &fine, const LevelView &coarse, const uin
 // r_c = R res_f = P^T res_f at the coarse unknowns. A thread owns one coarse cell (K along the 32 lanes, J across
 // the 8 warps) and marches along I: fine planes 2I-2 .. 2I+1 enter as their (j, k)-weighted 4x4 sums T(a), each
 // fine plane summed once and kept for the next coarse plane; the children's moved weights enter as X(a).
-constexpr int kRestrictS = 8;
 
 __device__ __forceinline__ void RestrictPlane(const LevelView &fv, const uint8_t *pext, const float *res, int a,
                                               int J, int K, float &T, float &X)
@@ -428,7 +442,10 @@ __global__ void __launch_bounds__(256) k_pair_restrict(LevelView fv, LevelView c
 {
     const int K = 1 + blockIdx.x * 32 + threadIdx.x, J = 1 + blockIdx.y * 8 + threadIdx.y;
     if (K > cv.Nz - 2 || J > cv.Nx - 2) return;
-    const int I0 = 1 + blockIdx.z * kRestrictS, I1 = min(I0 + kRestrictS, cv.Ny - 1);
+    // coarse planes in chunks of S (grid.z as the host sized it, MarchPlanes)
+    const int S = (cv.Ny - 2 + (int)gridDim.z - 1) / (int)gridDim.z;
+    const int I0 = 1 + (int)blockIdx.z * S, I1 = min(I0 + S, cv.Ny - 1);
+    if (I0 >= I1) return;
     float Tm2, Tm1, Xm1, Xdummy;
     RestrictPlane(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
     RestrictPlane(fv, pext, res, 2 * I0 - 1, J, K, Tm1, Xm1);
@@ -449,8 +466,10 @@ __global__ void __launch_bounds__(256) k_pair_restrict(LevelView fv, LevelView c
 void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
                         float *rCoarse, cudaStream_t st)
 {
+    const long long perPlane = (long long)((coarse.Nz - 2 + 31) / 32) * ((coarse.Nx - 2 + 7) / 8);
+    const int S = MarchPlanes(coarse.Ny - 2, perPlane);
     const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
-                    (unsigned)((coarse.Ny - 2 + kRestrictS - 1) / kRestrictS));
+                    (unsigned)((coarse.Ny - 2 + S - 1) / S));
     NB_COUNT_LAUNCH();
     k_pair_restrict<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
 }
