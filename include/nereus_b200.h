@@ -66,6 +66,8 @@ typedef struct nb_options
                             prolongation and r.z fused in; 0 (default): one launch per colour */
     int pair_kernels;    /* 1 (default): FP32 kernels on cell pairs for 3D uniform levels with Nz even; 0: the
                             general per-cell kernels */
+    int tail_cells;      /* the coarse end runs in one thread block from the first level with at most this many
+                            cells (and shared memory for all of them); 0: no such block */
 } nb_options;
 
 typedef struct nb_result

@@ -40,6 +40,7 @@ void nereus_b200_default_options(nb_options *o)
     o->use_graphs = 1;
     o->fused_sweeps = 0;
     o->pair_kernels = 1;
+    o->tail_cells = 2048;
 }
 
 const char *nereus_b200_last_error(void) { return g_error.c_str(); }

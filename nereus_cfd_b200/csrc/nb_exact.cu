@@ -393,16 +393,20 @@ __global__ void k_rhs(LevelView v, Faces F, const double *p, double rhoDt, doubl
             int i, j, k;
             long long c;
             if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
-            if (v.types[c] != FLUID) continue;
-            double cq[6];
-            CoefsExact(v, i, j, k, cq);
+            const unsigned code = v.code[c];
+            if (!(code & CODE_UNKNOWN)) continue; // an interior FLUID cell
             double ds = 0.0;
-            const int nq = v.dim == 3 ? 6 : 4;
-            for (int q = 0; q < nq; q++)
+            if (code & CODE_DIRICHLET) // a PRESSURE neighbour is a Dirichlet one: the others skip the scan
             {
-                const long long n = c + NbrOffset(v, q);
-                const int t = v.types[n];
-                if (t == PRESSURE) ds += cq[q] * RingFactorExact(v, i, j, k, q, t) * p[n];
+                double cq[6];
+                CoefsExact(v, i, j, k, cq);
+                const int nq = v.dim == 3 ? 6 : 4;
+                for (int q = 0; q < nq; q++)
+                {
+                    const long long n = c + NbrOffset(v, q);
+                    const int t = v.types[n];
+                    if (t == PRESSURE) ds += cq[q] * RingFactorExact(v, i, j, k, q, t) * p[n];
+                }
             }
             double vol = 1.0;
             if (v.stretched) vol = v.dim == 3 ? Wd(v, 0, j) * Wd(v, 1, i) * Wd(v, 2, k) : Wd(v, 0, j) * Wd(v, 1, i);

@@ -634,6 +634,41 @@ void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaSt
     k_scale_copy<Tin, Tout><<<TileGrid(v), kTile, 0, st>>>(v, x, y, s);
 }
 
+// r = sfac * b over the whole level and (sum b^2, sum b): the FP64 residual b - A x of a zero iterate. b is zero off
+// the unknowns, so the sums over all cells are the sums over the unknowns.
+template <typename T>
+__global__ void __launch_bounds__(256) k_scale_sum(long long cells, const double *__restrict__ b, T *__restrict__ r,
+                                                   double sfac, Reducer R, int slot)
+{
+    double acc[2] = {0.0, 0.0};
+    const long long n2 = cells >> 1, stride = (long long)gridDim.x * blockDim.x;
+    const double2 *b2 = reinterpret_cast<const double2 *>(b);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n2; t += stride)
+    {
+        const double2 x = b2[t];
+        r[2 * t] = (T)(x.x * sfac);
+        r[2 * t + 1] = (T)(x.y * sfac);
+        acc[0] += x.x * x.x + x.y * x.y;
+        acc[1] += x.x + x.y;
+    }
+    for (long long t = 2 * n2 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells; t += stride)
+    {
+        r[t] = (T)(b[t] * sfac);
+        acc[0] += b[t] * b[t];
+        acc[1] += b[t];
+    }
+    GridReduce<2>(R, acc, slot);
+}
+
+template <typename T>
+void LaunchScaleSum(long long cells, const double *b, T *r, double sfac, const Reducer &R, int slot, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_scale_sum<T><<<148 * 8, 256, 0, st>>>(cells, b, r, sfac, R, slot);
+}
+template void LaunchScaleSum<float>(long long, const double *, float *, double, const Reducer &, int, cudaStream_t);
+template void LaunchScaleSum<double>(long long, const double *, double *, double, const Reducer &, int, cudaStream_t);
+
 // ---- instantiations ----
 #define NB_INST(T)                                                                                                 \
     template void LaunchSmoothFirst<T>(const LevelView &, const T *, T *, cudaStream_t);                           \

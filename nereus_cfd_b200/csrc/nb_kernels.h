@@ -122,6 +122,9 @@ template <typename T>
 void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p0, const T *p1, const T *q, const Reducer &R,
                     const double *S, int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int slotRR,
                     cudaStream_t st);
+// r = sfac * b over all `cells` and out[slot..slot+1] = (sum b^2, sum b): the residual of a zero iterate
+template <typename T>
+void LaunchScaleSum(long long cells, const double *b, T *r, double sfac, const Reducer &R, int slot, cudaStream_t st);
 // y = s * x over the level's unknowns (x and y may alias)
 template <typename Tin, typename Tout>
 void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaStream_t st);

@@ -183,7 +183,7 @@ void Context::BuildHierarchy()
         else L[l].pext.release();
     }
     NB_CK(cudaGetLastError());
-    // The tail: the first level from which every coarser level has at most kTailCellCap cells and all of them fit
+    // The tail: the first level from which every coarser level has at most opt.tail_cells cells and all of them fit
     // in one block's shared memory in the solver's precision.
     const bool mixed = opt.precision == NB_PRECISION_MIXED;
     tailStart = (int)L.size();
@@ -192,7 +192,7 @@ void Context::BuildHierarchy()
     for (int l = (int)L.size() - 1; l >= 0; l--)
     {
         const int nl = (int)L.size() - l;
-        if (nl > kMaxTailLevels || L[l].cells > kTailCellCap) break;
+        if (nl > kMaxTailLevels || L[l].cells > (long long)opt.tail_cells) break;
         if (std::max(L[l].Nx, std::max(L[l].Ny, L[l].Nz)) > 1023) break; // the tail packs i, j, k in 10 bits each
         const size_t bytes = mixed ? TailSmemBytes<float>(&views[l], nl) : TailSmemBytes<double>(&views[l], nl);
         if (bytes > kTailMaxSmem) break;
@@ -815,8 +815,8 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
     double *x = xa.p, *xo = xb.p;
     xa.zero(st);
     float *r32 = L[0].r32.p, *z32 = L[0].e32.p;
-    ProfBegin(NB_K_REFINE, (8.0 + 8.0 + 1.0 + 4.0) * (double)Cells());
-    LaunchResidual64<float>(v0, b.p, x, r32, scale, sfac, red, S_RES, st);
+    ProfBegin(NB_K_REFINE, (8.0 + 4.0) * (double)Cells());
+    LaunchScaleSum<float>(L[0].cells, b.p, r32, sfac, red, S_RES, st); // the residual of x = 0
     ProfEnd();
     const double bn2 = ReadSlot(S_RES);
     out->b_norm = std::sqrt(bn2);
@@ -866,8 +866,8 @@ int Context::SolveFP64(double tol, double **xOut, nb_result *out, const double *
     double *x = xa.p;
     xa.zero(st);
     double *r = L[0].r64.p, *z = L[0].e64.p;
-    ProfBegin(NB_K_REFINE, (8.0 + 8.0 + 1.0 + 8.0) * (double)Cells());
-    LaunchResidual64<double>(v0, b.p, x, r, scale, sfac, red, S_RES, st);
+    ProfBegin(NB_K_REFINE, (8.0 + 8.0) * (double)Cells());
+    LaunchScaleSum<double>(L[0].cells, b.p, r, sfac, red, S_RES, st); // the residual of x = 0
     ProfEnd();
     const double bn2 = ReadSlot(S_RES);
     out->b_norm = std::sqrt(bn2);

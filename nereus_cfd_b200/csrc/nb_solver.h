@@ -122,7 +122,6 @@ struct Context
     std::vector<double> wt[3], gt[3];
     std::vector<LevelData> L;
     int tailStart = 0;                       // levels from here down run in one shared-memory block (nb_tail.cu)
-    static constexpr long long kTailCellCap = 8192;
     DevArray<int32_t> idp;
     int n = 0;
     bool singular = false;
