@@ -235,6 +235,64 @@ __device__ __forceinline__ void CodeStencil(const LevelView &v, int i, int j, in
     diag = d;
 }
 
+// ---- cell pairs (3D levels with Nz even): cells (i, j, 2m) and (i, j, 2m+1) form an aligned pair; a plane is
+//      Nx*Nz/2 consecutive pairs; thread t of a launch takes pair t of the plane and marches along i ----
+constexpr int kPairThreads = 256;
+constexpr int kPairS = 8;                  // planes a thread marches at most
+constexpr long long kPairBlocks = 148 * 8; // blocks a launch aims for
+
+// Planes per thread for `planes` planes of `perPlane` blocks each: about kPairBlocks blocks, 1 .. kPairS planes.
+inline int MarchPlanes(long long planes, long long perPlane)
+{
+    const long long s = (planes * perPlane + kPairBlocks - 1) / kPairBlocks;
+    return (int)(s < 1 ? 1 : (s > kPairS ? kPairS : s));
+}
+
+// The launch grid of a pair kernel; minS: at least this many planes per thread (the launches that end in a
+// grid-wide sum keep their partial sums few).
+inline dim3 PairGrid(const LevelView &v, int minS = 1)
+{
+    const long long P = v.sI / 2, perPlane = (P + kPairThreads - 1) / kPairThreads, planes = v.Ny - 2;
+    int S = MarchPlanes(planes, perPlane);
+    const int cap = (int)(planes > 1 ? planes : 1);
+    const int m = minS < cap ? minS : cap;
+    if (m > S) S = m;
+    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
+}
+
+// Per-thread position of a pair kernel.
+struct PairPos
+{
+    int lane;
+    bool valid;     // false for the clamped threads past the plane's last pair (they still load and shuffle)
+    int i0, i1;     // planes [i0, i1)
+    int sI, sJ;
+    int j, k0;      // row and first cell of the pair (k0 even)
+    long long base; // cell index of the pair's first cell on plane i0
+};
+
+__device__ __forceinline__ PairPos PairStart(const LevelView &v)
+{
+    PairPos p;
+    const int P = (int)(v.sI >> 1);
+    p.lane = threadIdx.x & 31;
+    int q = blockIdx.x * kPairThreads + threadIdx.x;
+    p.valid = q < P;
+    if (!p.valid) q = P - 1;
+    // the launch's grid.y splits the Ny-2 interior planes into chunks of S (the host sized it); a block past the
+    // last plane starts at the ring plane and marches none
+    const int S = (v.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
+    p.i0 = min(1 + (int)blockIdx.y * S, v.Ny - 1);
+    p.i1 = min(p.i0 + S, v.Ny - 1);
+    p.sI = (int)v.sI;
+    p.sJ = (int)v.sJ;
+    const int cin = 2 * q;
+    p.j = cin / v.Nz;
+    p.k0 = cin - p.j * v.Nz;
+    p.base = (long long)p.i0 * v.sI + cin;
+    return p;
+}
+
 // ---- reductions ----
 template <typename T>
 __device__ __forceinline__ T WarpSum(T x)

@@ -414,6 +414,63 @@ __global__ void k_rhs(LevelView v, Faces F, const double *p, double rhoDt, doubl
         }
 }
 
+// The same right-hand side on a uniform 3D grid with Nz even, two cells along k per thread (nb_device.cuh, PairPos):
+// the u faces of a pair are one aligned 16-byte load per row (u rows have Nz entries), the v faces one per plane (the
+// v plane of i+1 is kept for the next step of the march), the w faces three scalars (w rows have Nz+1 entries). Each
+// cell's expression is k_rhs's, operation for operation.
+__global__ void __launch_bounds__(kPairThreads, 4) k_pair_rhs(LevelView v, Faces F, const double *p, double rhoDt,
+                                                           double scale, double dh, double *b)
+{
+    const PairPos P = PairStart(v);
+    const long long uPlane = F.uI, wPlane = F.wI;
+    const int Nz = v.Nz;
+    // plane i's v faces (i, j, k) are the pair at the cell index; (i+1, j, k) one plane on
+    double2 vC = *reinterpret_cast<const double2 *>(F.v + P.base);
+    int off = 0;
+    for (int i = P.i0; i < P.i1; i++, off += P.sI)
+    {
+        const long long c = P.base + off;
+        const long long cu = (long long)i * uPlane + (long long)P.j * Nz + P.k0;
+        const long long cw = (long long)i * wPlane + (long long)P.j * (Nz + 1) + P.k0;
+        const double2 u0 = *reinterpret_cast<const double2 *>(F.u + cu);
+        const double2 u1 = *reinterpret_cast<const double2 *>(F.u + cu + Nz);
+        const double2 vP = *reinterpret_cast<const double2 *>(F.v + c + P.sI);
+        const double w0 = F.w[cw], w1 = F.w[cw + 1], w2 = F.w[cw + 2];
+        const unsigned code2 = *reinterpret_cast<const unsigned short *>(v.code + c);
+        if (P.valid && (code2 & ((unsigned)CODE_UNKNOWN | ((unsigned)CODE_UNKNOWN << 8))))
+        {
+            double out[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                const unsigned code = (code2 >> (8 * h)) & 0xFFu;
+                out[h] = 0.0;
+                if (!(code & CODE_UNKNOWN)) continue;
+                const int k = P.k0 + h;
+                double ds = 0.0;
+                if (code & CODE_DIRICHLET)
+                {
+                    double cq[6];
+                    CoefsExact(v, i, P.j, k, cq);
+                    for (int q = 0; q < 6; q++)
+                    {
+                        const long long n = c + h + NbrOffset(v, q);
+                        const int t = v.types[n];
+                        if (t == PRESSURE) ds += cq[q] * RingFactorExact(v, i, P.j, k, q, t) * p[n];
+                    }
+                }
+                const double divU = ((h ? u1.y : u1.x) - (h ? u0.y : u0.x)) / dh;
+                const double divV = ((h ? vP.y : vP.x) - (h ? vC.y : vC.x)) / dh;
+                const double divW = ((h ? w2 : w1) - (h ? w1 : w0)) / dh;
+                const double vol = 1.0;
+                out[h] = rhoDt * (divU + divV + divW) * vol - scale * ds;
+            }
+            *reinterpret_cast<double2 *>(b + c) = make_double2(out[0], out[1]);
+        }
+        vC = vP;
+    }
+}
+
 Faces MakeFaces(const LevelView &v, const double *u, const double *vv, const double *w)
 {
     Faces F;
@@ -431,7 +488,10 @@ void LaunchRhs(const LevelView &v, const double *u, const double *vv, const doub
 {
     if (v.nLines <= 0) return;
     NB_COUNT_LAUNCH();
-    k_rhs<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, MakeFaces(v, u, vv, w), p, rhoDt, scale, dh, b);
+    if (v.dim == 3 && !v.stretched && v.Nz % 2 == 0 && v.code)
+        k_pair_rhs<<<PairGrid(v), kPairThreads, 0, st>>>(v, MakeFaces(v, u, vv, w), p, rhoDt, scale, dh, b);
+    else
+        k_rhs<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, MakeFaces(v, u, vv, w), p, rhoDt, scale, dh, b);
 }
 
 // max |div u| over FLUID cells (the post-projection check)

@@ -82,6 +82,10 @@ void LaunchPairProlong(const LevelView &fine, const LevelView &coarse, const uin
                        float *eFine, cudaStream_t st);
 void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
                         float *rCoarse, cudaStream_t st);
+// the FP64 refinement step x_out = x_in + e, r = sfac (b - A x_out) on a uniform 3D level 0 (k_residual64's)
+void LaunchPairRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
+                        double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
+                        cudaStream_t st);
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
                   int baseOdd, cudaStream_t st);
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,

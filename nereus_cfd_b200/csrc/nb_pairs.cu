@@ -26,50 +26,6 @@ namespace nb
 namespace
 {
 
-constexpr int kPairThreads = 256;
-constexpr int kPairS = 8;             // planes a thread marches at most
-constexpr long long kPairBlocks = 148 * 8; // blocks a launch aims for
-
-// Planes per thread for `planes` planes of `perPlane` blocks each: about kPairBlocks blocks, 1 .. kPairS planes.
-inline int MarchPlanes(long long planes, long long perPlane)
-{
-    long long s = (planes * perPlane + kPairBlocks - 1) / kPairBlocks;
-    return (int)std::max(1LL, std::min<long long>(kPairS, s));
-}
-
-// Per-thread position of a pair kernel.
-struct PairPos
-{
-    int lane;
-    bool valid;  // false for the clamped threads past the plane's last pair (they still load and shuffle)
-    int i0, i1;  // planes [i0, i1)
-    int sI, sJ;
-    int j, k0;   // row and first cell of the pair (k0 even)
-    long long base; // cell index of the pair's first cell on plane i0
-};
-
-__device__ __forceinline__ PairPos PairStart(const LevelView &v)
-{
-    PairPos p;
-    const int P = (int)(v.sI >> 1);
-    p.lane = threadIdx.x & 31;
-    int q = blockIdx.x * kPairThreads + threadIdx.x;
-    p.valid = q < P;
-    if (!p.valid) q = P - 1;
-    // the launch's grid.y splits the Ny-2 interior planes into chunks of S (the host sized it); a block past the
-    // last plane starts at the ring plane and marches none
-    const int S = (v.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
-    p.i0 = min(1 + (int)blockIdx.y * S, v.Ny - 1);
-    p.i1 = min(p.i0 + S, v.Ny - 1);
-    p.sI = (int)v.sI;
-    p.sJ = (int)v.sJ;
-    const int cin = 2 * q;
-    p.j = cin / v.Nz;
-    p.k0 = cin - p.j * v.Nz;
-    p.base = (long long)p.i0 * v.sI + cin;
-    return p;
-}
-
 __device__ __forceinline__ float2 Ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ unsigned LdDu(const uint8_t *p) { return *reinterpret_cast<const unsigned short *>(p); }
 
@@ -121,14 +77,6 @@ void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st)
     if (blocks < 1) blocks = 1;
     NB_COUNT_LAUNCH();
     k_build_du<<<blocks, 256, 0, st>>>(v, du);
-}
-
-// minS: at least this many planes per thread (the launches that end in a grid-wide sum keep their partial sums few)
-static inline dim3 PairGrid(const LevelView &v, int minS = 1)
-{
-    const long long P = v.sI / 2, perPlane = (P + kPairThreads - 1) / kPairThreads, planes = v.Ny - 2;
-    const int S = std::max(MarchPlanes(planes, perPlane), std::min<int>(minS, (int)std::max(1LL, planes)));
-    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
 }
 
 // planes per thread at least in the launches that end in a grid-wide sum: fewer blocks, fewer partial sums for the
@@ -564,6 +512,65 @@ void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, flo
     else
         k_pair_papply<false><<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd,
                                                                     n, slotPQ);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// FP64 refinement step on level 0 (the semantics of k_residual64<float, true> in nb_exact.cu for a uniform 3D grid)
+// ---------------------------------------------------------------------------------------------------------------
+// x_out = x_in + e; r = sfac (b - A x_out) in FP32; (sum (b - A x_out)^2, sum (b - A x_out)) in FP64. A is the
+// reference's matrix on a uniform grid: scale (sum of the FLUID neighbours - diag units / 2 x), c_q = 1 and scale =
+// 1/dh^2 (FaceCoefs3D, MatrixScale3D, PressureSolver3D.cpp:34-63). x_in and e are zero off the unknowns, so the
+// neighbour sum runs over all six; the sum's order differs from the per-cell kernel's, within FP64 rounding.
+__device__ __forceinline__ double2 Ld2d(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+
+__global__ void __launch_bounds__(kPairThreads)
+    k_pair_refine64(LevelView v, const uint8_t *__restrict__ du, const double *__restrict__ b,
+                    const double *__restrict__ xin, const float *__restrict__ e, double *__restrict__ xout,
+                    float *__restrict__ r, double scale, double sfac, Reducer R, int slot)
+{
+    const PairPos P = PairStart(v);
+    auto X = [&](int o) {
+        const double2 a = Ld2d(xin + P.base + o);
+        const float2 f = Ld2(e + P.base + o);
+        return make_double2(a.x + (double)f.x, a.y + (double)f.y);
+    };
+    auto X1 = [&](long long c) { return xin[c] + (double)e[c]; };
+    double2 XM = X(-P.sI), XC = X(0);
+    double acc[2] = {0.0, 0.0};
+    int off = 0;
+    for (int i = P.i0; i < P.i1; i++, off += P.sI)
+    {
+        const double2 XP = X(off + P.sI), XJp = X(off + P.sJ), XJm = X(off - P.sJ);
+        const double2 bb = Ld2d(b + P.base + off);
+        const unsigned d = LdDu(du + P.base + off);
+        double left = __shfl_up_sync(0xffffffffu, XC.y, 1);
+        double right = __shfl_down_sync(0xffffffffu, XC.x, 1);
+        if (P.lane == 0) left = X1(P.base + off - 1);
+        if (P.lane == 31) right = X1(P.base + off + 2);
+        const double s0 = ((XP.x + XM.x) + (XJp.x + XJm.x)) + (left + XC.y);
+        const double s1 = ((XP.y + XM.y) + (XJp.y + XJm.y)) + (XC.x + right);
+        const double r0 = (d & 0x80u) ? bb.x - scale * (s0 - 0.5 * (double)(d & 0x7Fu) * XC.x) : 0.0;
+        const double r1 = (d & 0x8000u) ? bb.y - scale * (s1 - 0.5 * (double)((d >> 8) & 0x7Fu) * XC.y) : 0.0;
+        if (P.valid)
+        {
+            *reinterpret_cast<double2 *>(xout + P.base + off) = XC;
+            *reinterpret_cast<float2 *>(r + P.base + off) = make_float2((float)(r0 * sfac), (float)(r1 * sfac));
+            acc[0] += r0 * r0 + r1 * r1;
+            acc[1] += r0 + r1;
+        }
+        XM = XC;
+        XC = XP;
+    }
+    GridReduce<2>(R, acc, slot);
+}
+
+void LaunchPairRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
+                        double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
+                        cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_pair_refine64<<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, b, xin, e, xout, r, scale, sfac, R,
+                                                                      slot);
 }
 
 // Whole-array kernels (every entry off the unknowns is zero): 16-byte loads over the level's cells.

@@ -845,7 +845,10 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
             inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0,
                                    rr0 * opt.inner_tol * opt.inner_tol, std::max(1, opt.max_iters), false, &rrEnd);
             ProfBegin(NB_K_REFINE, (8.0 + 4.0 + 8.0 + 1.0 + 8.0 + 4.0) * (double)Cells());
-            LaunchRefine64<float>(v0, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);
+            if (PairLevel(0) && !nonuniform && dim == 3)
+                LaunchPairRefine64(v0, L[0].du.p, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);
+            else
+                LaunchRefine64<float>(v0, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);
             ProfEnd();
             std::swap(x, xo);
             rr64 = ReadSlot(S_RES);
