@@ -511,12 +511,50 @@ __global__ void k_max_div(LevelView v, Faces F, double dh, Reducer R, int slot)
     GridReduce<1>(R, m, slot, 1);
 }
 
+// The same check on a uniform 3D grid with Nz even, two cells per thread (the face loads of k_pair_rhs).
+__global__ void __launch_bounds__(kPairThreads) k_pair_max_div(LevelView v, Faces F, double dh, Reducer R, int slot)
+{
+    const PairPos P = PairStart(v);
+    const int Nz = v.Nz;
+    double m[1] = {0.0};
+    double2 vC = *reinterpret_cast<const double2 *>(F.v + P.base);
+    int off = 0;
+    for (int i = P.i0; i < P.i1; i++, off += P.sI)
+    {
+        const long long c = P.base + off;
+        const long long cu = (long long)i * F.uI + (long long)P.j * Nz + P.k0;
+        const long long cw = (long long)i * F.wI + (long long)P.j * (Nz + 1) + P.k0;
+        const double2 u0 = *reinterpret_cast<const double2 *>(F.u + cu);
+        const double2 u1 = *reinterpret_cast<const double2 *>(F.u + cu + Nz);
+        const double2 vP = *reinterpret_cast<const double2 *>(F.v + c + P.sI);
+        const double w0 = F.w[cw], w1 = F.w[cw + 1], w2 = F.w[cw + 2];
+        const unsigned code2 = *reinterpret_cast<const unsigned short *>(v.code + c);
+        if (P.valid)
+        {
+            if (code2 & CODE_UNKNOWN)
+            {
+                const double d = (u1.x - u0.x) / dh + (vP.x - vC.x) / dh + (w1 - w0) / dh;
+                m[0] = fmax(m[0], fabs(d));
+            }
+            if ((code2 >> 8) & CODE_UNKNOWN)
+            {
+                const double d = (u1.y - u0.y) / dh + (vP.y - vC.y) / dh + (w2 - w1) / dh;
+                m[0] = fmax(m[0], fabs(d));
+            }
+        }
+        vC = vP;
+    }
+    GridReduce<1>(R, m, slot, 1);
+}
+
 void LaunchMaxDiv(const LevelView &v, const double *u, const double *vv, const double *w, double dh,
                   const Reducer &R, int slot, cudaStream_t st)
 {
-    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_max_div<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, MakeFaces(v, u, vv, w), dh, R, slot);
+    if (v.dim == 3 && !v.stretched && v.Nz % 2 == 0 && v.code && v.Ny >= 3)
+        k_pair_max_div<<<PairGrid(v, 16), kPairThreads, 0, st>>>(v, MakeFaces(v, u, vv, w), dh, R, slot);
+    else
+        k_max_div<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, MakeFaces(v, u, vv, w), dh, R, slot);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -687,11 +725,30 @@ void LaunchSumUnknowns(const LevelView &v, const double *x, const Reducer &R, in
     k_sum_unknowns<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, x, R, slot);
 }
 
+// The same over the whole array in order, the unknowns told by their code byte (interior FLUID cells).
+__global__ void __launch_bounds__(256) k_lin_sub_mean_scatter(long long cells, const uint8_t *__restrict__ code,
+                                                              double *x, const double *sums, int n, int sub,
+                                                              double *p)
+{
+    const double mean = sub ? (sums[0] + sums[1]) / (double)n : 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        if (!(code[t] & CODE_UNKNOWN)) continue;
+        const double y = x[t] - mean;
+        if (sub) x[t] = y;
+        if (p) p[t] = y;
+    }
+}
+
 void LaunchSubMeanScatter(const LevelView &v, double *x, const double *sums, int n, int sub, double *p, cudaStream_t st)
 {
     if (v.nLines <= 0) return;
     NB_COUNT_LAUNCH();
-    k_sub_mean_scatter<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, x, sums, n, sub, p);
+    if (v.code)
+        k_lin_sub_mean_scatter<<<148 * 8, 256, 0, st>>>(v.cells, v.code, x, sums, n, sub, p);
+    else
+        k_sub_mean_scatter<<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, x, sums, n, sub, p);
 }
 
 __device__ __forceinline__ void RingEntry(const LevelView &v, double *p, long long d, long long s)
@@ -819,9 +876,117 @@ __global__ void k_project(LevelView g, double *u, double *v, double *w, const do
     }
 }
 
+// ProjectionGradient3D from the two cell pressures (pc at the face's high cell, pn at its low cell), as ProjGrad.
+__device__ __forceinline__ double ProjGradV(const LevelView &g, int a, int i, int j, int k, double pc, double pn)
+{
+    const int n = a == 0 ? j : (a == 1 ? i : k);
+    const double grad = (pc - pn) / Gp(g, a, n - 1);
+    const int N = a == 0 ? g.Nx : (a == 1 ? g.Ny : g.Nz);
+    if (n != 1 && n != N - 1) return grad;
+    const int r = n == 1 ? 0 : N - 1;
+    const long long rc = a == 0 ? (long long)i * g.sI + (long long)r * g.sJ + k
+                       : (a == 1 ? (long long)r * g.sI + (long long)j * g.sJ + k
+                                 : (long long)i * g.sI + (long long)j * g.sJ + r);
+    if (!IsDirichlet(g.types[rc])) return grad;
+    return n == 1 ? grad * DRF(g, a, 1, -1) : grad * DRF(g, a, N - 2, +1);
+}
+
+// The same projection on a 3D grid with Nz even, one thread per cell pair (nb_device.cuh, PairPos) marching along
+// i: the pair's u faces and v faces are one aligned 16-byte load and store each (a face outside its loop range or
+// behind a wall is stored back unchanged), its two w faces scalars; the pressures of the low neighbours come from
+// the pair loads of the previous plane and row and, along k, from the neighbouring lane. The block whose planes end
+// at Ny-2 also does the v faces of plane Ny-1 (v's loop runs to Ny-1).
+__global__ void __launch_bounds__(kPairThreads) k_pair_project(LevelView g, double *u, double *v, double *w,
+                                                               const double *p, double f)
+{
+    const PairPos P = PairStart(g);
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz, j = P.j;
+    const int iEnd = (P.i0 < P.i1 && P.i1 == Ny - 1) ? Ny : P.i1;
+    double2 pM = *reinterpret_cast<const double2 *>(p + P.base - P.sI);
+    unsigned tM = *reinterpret_cast<const unsigned short *>(g.types + P.base - P.sI);
+    int off = 0;
+    for (int i = P.i0; i < iEnd; i++, off += P.sI)
+    {
+        const long long c = P.base + off;
+        const double2 pC = *reinterpret_cast<const double2 *>(p + c);
+        const unsigned tC = *reinterpret_cast<const unsigned short *>(g.types + c);
+        double pKm = __shfl_up_sync(0xffffffffu, pC.y, 1);
+        unsigned tKm = __shfl_up_sync(0xffffffffu, tC >> 8, 1);
+        if (P.lane == 0)
+        {
+            pKm = p[c - 1];
+            tKm = g.types[c - 1];
+        }
+        if (P.valid)
+        {
+            const bool inner = i <= Ny - 2;
+            const double pc[2] = {pC.x, pC.y}, pm[2] = {pM.x, pM.y};
+            const int tc[2] = {(int)(tC & 0xFFu), (int)(tC >> 8)}, tm[2] = {(int)(tM & 0xFFu), (int)(tM >> 8)};
+            // u faces (i, j, k): i in [1, Ny-2], j in [1, Nx-1], k in [1, Nz-2]
+            if (inner && j >= 1)
+            {
+                const long long fu = ((long long)i * (Nx + 1) + j) * Nz + P.k0;
+                double2 uu = *reinterpret_cast<double2 *>(u + fu);
+                const double2 pJ = *reinterpret_cast<const double2 *>(p + c - P.sJ);
+                const unsigned tJ = *reinterpret_cast<const unsigned short *>(g.types + c - P.sJ);
+                double ux[2] = {uu.x, uu.y};
+                const double pj[2] = {pJ.x, pJ.y};
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const int k = P.k0 + h;
+                    if (k < 1 || k > Nz - 2) continue;
+                    if (tc[h] == SOLID || (int)((tJ >> (8 * h)) & 0xFFu) == SOLID) continue;
+                    ux[h] = ux[h] - f * ProjGradV(g, 0, i, j, k, pc[h], pj[h]);
+                }
+                *reinterpret_cast<double2 *>(u + fu) = make_double2(ux[0], ux[1]);
+            }
+            // v faces: i in [1, Ny-1], j in [1, Nx-2], k in [1, Nz-2]
+            if (j >= 1 && j <= Nx - 2)
+            {
+                const long long fv = c; // ((i * Nx + j) * Nz + k): the cell index
+                double2 vv = *reinterpret_cast<double2 *>(v + fv);
+                double vx[2] = {vv.x, vv.y};
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const int k = P.k0 + h;
+                    if (k < 1 || k > Nz - 2) continue;
+                    if (tc[h] == SOLID || tm[h] == SOLID) continue;
+                    vx[h] = vx[h] - f * ProjGradV(g, 1, i, j, k, pc[h], pm[h]);
+                }
+                *reinterpret_cast<double2 *>(v + fv) = make_double2(vx[0], vx[1]);
+            }
+            // w faces: i in [1, Ny-2], j in [1, Nx-2], k in [1, Nz-1]
+            if (inner && j >= 1 && j <= Nx - 2)
+            {
+                const long long fw = ((long long)i * Nx + j) * (Nz + 1) + P.k0;
+                const double plow[2] = {pKm, pC.x};
+                const int tlow[2] = {(int)tKm, tc[0]};
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const int k = P.k0 + h;
+                    if (k < 1 || k > Nz - 1) continue;
+                    if (tc[h] == SOLID || tlow[h] == SOLID) continue;
+                    w[fw + h] = w[fw + h] - f * ProjGradV(g, 2, i, j, k, pc[h], plow[h]);
+                }
+            }
+        }
+        pM = pC;
+        tM = tC;
+    }
+}
+
 void LaunchProject(const LevelView &g, double *u, double *v, double *w, const double *p, double dtOverRho,
                    cudaStream_t st)
 {
+    if (g.dim == 3 && g.Nz % 2 == 0 && g.Ny >= 3)
+    {
+        NB_COUNT_LAUNCH();
+        k_pair_project<<<PairGrid(g), kPairThreads, 0, st>>>(g, u, v, w, p, dtOverRho);
+        return;
+    }
     const int kCount = g.dim == 3 ? g.Nz - 1 : 1;
     const int jCount = g.Nx - 1, iCount = g.Ny - 1;
     if (kCount <= 0 || jCount <= 0 || iCount <= 0) return;
