@@ -504,9 +504,11 @@ void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, con
     k_dot<T><<<TileGrid(v), kTile, 0, st>>>(v, r, z, R, it, baseEven, baseOdd);
 }
 
-__device__ __forceinline__ double RzEff(const double *S, int base, int n, int singular)
+// n (the unknowns) is read from S[slotN] on the device, so a captured iteration outlives a change of the layout
+// that keeps the hierarchy's shape
+__device__ __forceinline__ double RzEff(const double *S, int base, double n, int singular)
 {
-    return singular ? S[base] - (S[base + 1] / (double)n) * S[base + 2] : S[base];
+    return singular ? S[base] - (S[base + 1] / n) * S[base + 2] : S[base];
 }
 
 // p_new = (z - mean) + beta p_old, q = M p_new, sum p_new.q. The neighbours' p_new are formed from their z and
@@ -514,15 +516,16 @@ __device__ __forceinline__ double RzEff(const double *S, int base, int n, int si
 template <typename T, bool kExact>
 __global__ void __launch_bounds__(256) k_update_p_apply(LevelView v, const T *__restrict__ z, T *p0, T *p1,
                                                         T *__restrict__ q, Reducer R, const double *S, const int *it,
-                                                        int baseEven, int baseOdd, int n, int singular, int slotPQ)
+                                                        int baseEven, int baseOdd, int slotN, int singular, int slotPQ)
 {
     const int iter = *it, par = iter & 1;
     const T *__restrict__ pIn = par ? p1 : p0;
     T *__restrict__ pOut = par ? p0 : p1;
     const int baseNew = par ? baseOdd : baseEven, baseOld = par ? baseEven : baseOdd;
+    const double n = S[slotN];
     const double beta = iter == 0 ? 0.0 : RzEff(S, baseNew, n, singular) / RzEff(S, baseOld, n, singular);
     const T b = (T)beta;
-    const T mean = singular ? (T)(S[baseNew + 1] / (double)n) : (T)0;
+    const T mean = singular ? (T)(S[baseNew + 1] / n) : (T)0;
     double acc[1] = {0.0};
     NB_TILE_LOOP(v)
     {
@@ -564,15 +567,15 @@ __global__ void __launch_bounds__(256) k_update_p_apply(LevelView v, const T *__
 
 template <typename T>
 void LaunchUpdatePApply(const LevelView &v, const T *z, T *p0, T *p1, T *q, const Reducer &R, const double *S,
-                        const int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int exact,
+                        const int *it, int baseEven, int baseOdd, int slotN, int singular, int slotPQ, int exact,
                         cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
     if (exact)
-        k_update_p_apply<T, true><<<TileGrid(v), kTile, 0, st>>>(v, z, p0, p1, q, R, S, it, baseEven, baseOdd, n,
+        k_update_p_apply<T, true><<<TileGrid(v), kTile, 0, st>>>(v, z, p0, p1, q, R, S, it, baseEven, baseOdd, slotN,
                                                                  singular, slotPQ);
     else
-        k_update_p_apply<T, false><<<TileGrid(v), kTile, 0, st>>>(v, z, p0, p1, q, R, S, it, baseEven, baseOdd, n,
+        k_update_p_apply<T, false><<<TileGrid(v), kTile, 0, st>>>(v, z, p0, p1, q, R, S, it, baseEven, baseOdd, slotN,
                                                                   singular, slotPQ);
 }
 
@@ -580,13 +583,13 @@ void LaunchUpdatePApply(const LevelView &v, const T *z, T *p0, T *p1, T *q, cons
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_xr(LevelView v, T *__restrict__ x, T *__restrict__ r, const T *p0,
                                                    const T *p1, const T *__restrict__ q, Reducer R, const double *S,
-                                                   int *it, int baseEven, int baseOdd, int n, int singular,
+                                                   int *it, int baseEven, int baseOdd, int slotN, int singular,
                                                    int slotPQ, int slotRR)
 {
     const int par = *it & 1;
     const T *__restrict__ p = par ? p0 : p1;
     const int base = par ? baseOdd : baseEven;
-    const double alpha = RzEff(S, base, n, singular) / S[slotPQ];
+    const double alpha = RzEff(S, base, S[slotN], singular) / S[slotPQ];
     const T a = (T)alpha;
     double acc[1] = {0.0};
     NB_TILE_LOOP(v)
@@ -605,11 +608,11 @@ __global__ void __launch_bounds__(256) k_update_xr(LevelView v, T *__restrict__ 
 
 template <typename T>
 void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p0, const T *p1, const T *q, const Reducer &R,
-                    const double *S, int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int slotRR,
+                    const double *S, int *it, int baseEven, int baseOdd, int slotN, int singular, int slotPQ, int slotRR,
                     cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_update_xr<T><<<TileGrid(v), kTile, 0, st>>>(v, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, n, singular,
+    k_update_xr<T><<<TileGrid(v), kTile, 0, st>>>(v, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, singular,
                                                   slotPQ, slotRR);
 }
 
@@ -632,6 +635,36 @@ void LaunchScaleCopy(const LevelView &v, const Tin *x, Tout *y, double s, cudaSt
     if (v.fastLen <= 0 || v.midLen <= 0) return;
     NB_COUNT_LAUNCH();
     k_scale_copy<Tin, Tout><<<TileGrid(v), kTile, 0, st>>>(v, x, y, s);
+}
+
+// (count of unknowns, count of unknowns whose row reaches a Dirichlet neighbour or a FLUID ring cell): the system
+// size and, when the second is 0, the singular (all-Neumann) case (AssembleSystem's `dirichlet`,
+// PressureSolver3D.cpp:128-178).
+__global__ void __launch_bounds__(256) k_count_unknowns(LevelView v, Reducer R, int slot)
+{
+    double acc[2] = {0.0, 0.0};
+    NB_TILE_LOOP(v)
+    {
+        int i, j, k;
+        long long c;
+        if (!TileCell(v, fo, mo, s, i, j, k, c)) continue;
+        const unsigned code = v.code[c];
+        if (!(code & CODE_UNKNOWN)) continue;
+        acc[0] += 1.0;
+        bool dir = (code & CODE_DIRICHLET) != 0;
+        const int nq = v.dim == 3 ? 6 : 4;
+        for (int q = 0; q < nq && !dir; q++)
+            if ((code >> q) & 1u)
+                dir = OnRing(v, i + (q == 0) - (q == 1), j + (q == 2) - (q == 3), k + (q == 4) - (q == 5));
+        if (dir) acc[1] += 1.0;
+    }
+    GridReduce<2>(R, acc, slot);
+}
+
+void LaunchCountUnknowns(const LevelView &v, const Reducer &R, int slot, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_count_unknowns<<<TileGrid(v), kTile, 0, st>>>(v, R, slot);
 }
 
 // r = sfac * b over the whole level and (sum b^2, sum b): the FP64 residual b - A x of a zero iterate. b is zero off

@@ -75,7 +75,7 @@ void LaunchPairHalfDot(const LevelView &v, const uint8_t *du, const float *r, fl
 void LaunchPairResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
                         cudaStream_t st);
 void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
-                      const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int n,
+                      const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
                       int singular, int slotPQ, cudaStream_t st);
 void LaunchBuildPext(const LevelView &fine, const LevelView &coarse, uint8_t *pext, cudaStream_t st);
 void LaunchPairProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
@@ -89,11 +89,13 @@ void LaunchPairRefine64(const LevelView &v, const uint8_t *du, const double *b, 
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
                   int baseOdd, cudaStream_t st);
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,
-                 const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int n, int singular,
+                 const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int slotN, int singular,
                  int slotPQ, int slotRR, cudaStream_t st);
 
 // ---- nb_kernels.cu: multigrid and PCG kernels, T = float (inner solve) or double (plain FP64) ----
 void LaunchBuildCodes(const LevelView &v, uint8_t *code, cudaStream_t st);
+// out[slot] = unknowns, out[slot + 1] = unknowns whose row reaches a Dirichlet value (0: the system is singular)
+void LaunchCountUnknowns(const LevelView &v, const Reducer &R, int slot, cudaStream_t st);
 void LaunchCoarsenTypes(const LevelView &fine, const LevelView &coarse, uint8_t *coarseTypes, cudaStream_t st);
 
 template <typename T> void LaunchSmoothFirst(const LevelView &v, const T *r, T *e, cudaStream_t st);
@@ -107,7 +109,8 @@ template <typename T> void LaunchCoarseSolve(const LevelView &v, const T *r, T *
 
 // PCG on the unit-form operator M = -A/scale of level 0. A singular (all-Neumann) system removes the mean of the
 // preconditioned residual z over the unknowns; its effect on r.z is carried in the scalars, so z itself is not
-// rewritten: with S[b..b+2] = (sum r.z, sum z, sum r), rz_eff = S[b] - (S[b+1]/n) S[b+2].
+// rewritten: with S[b..b+2] = (sum r.z, sum z, sum r), rz_eff = S[b] - (S[b+1]/n) S[b+2], n = S[slotN] (the count of
+// unknowns, kept on the device).
 //   dot:   out[base..base+2] = (sum r.z, sum z, sum r)
 //   pupd:  beta = first ? 0 : rz_eff(new)/rz_eff(old); pOut = (z - mean) + beta pIn; q = M pOut;
 //          out[slotPQ] = sum pOut.q
@@ -120,11 +123,11 @@ void LaunchDot(const LevelView &v, const T *r, const T *z, const Reducer &R, con
                cudaStream_t st);
 template <typename T>
 void LaunchUpdatePApply(const LevelView &v, const T *z, T *p0, T *p1, T *q, const Reducer &R, const double *S,
-                        const int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int exact,
+                        const int *it, int baseEven, int baseOdd, int slotN, int singular, int slotPQ, int exact,
                         cudaStream_t st);
 template <typename T>
 void LaunchUpdateXR(const LevelView &v, T *x, T *r, const T *p0, const T *p1, const T *q, const Reducer &R,
-                    const double *S, int *it, int baseEven, int baseOdd, int n, int singular, int slotPQ, int slotRR,
+                    const double *S, int *it, int baseEven, int baseOdd, int slotN, int singular, int slotPQ, int slotRR,
                     cudaStream_t st);
 // r = sfac * b over all `cells` and out[slot..slot+1] = (sum b^2, sum b): the residual of a zero iterate
 template <typename T>

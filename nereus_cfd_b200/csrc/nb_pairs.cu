@@ -430,9 +430,10 @@ void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const ui
 // ---------------------------------------------------------------------------------------------------------------
 // PCG on level 0 (the semantics of k_update_p_apply / k_dot / k_update_xr in nb_kernels.cu)
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ double RzEffP(const double *S, int base, int n, int singular)
+// n (the unknowns) comes from S[slotN] on the device (a captured iteration outlives a same-shape layout change)
+__device__ __forceinline__ double RzEffP(const double *S, int base, double n, int singular)
 {
-    return singular ? S[base] - (S[base + 1] / (double)n) * S[base + 2] : S[base];
+    return singular ? S[base] - (S[base + 1] / n) * S[base + 2] : S[base];
 }
 
 // p_new = U (z - mean + beta p_old), q = M p_new, sum p_new.q; U = 1 on unknowns (needed only when the mean of z is
@@ -440,16 +441,17 @@ __device__ __forceinline__ double RzEffP(const double *S, int base, int n, int s
 template <bool kSingular>
 __global__ void __launch_bounds__(kPairThreads)
     k_pair_papply(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ z, float *p0, float *p1,
-                  float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd, int n,
+                  float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
                   int slotPQ)
 {
     const int iter = *it, par = iter & 1;
     const float *__restrict__ pIn = par ? p1 : p0;
     float *__restrict__ pOut = par ? p0 : p1;
     const int baseNew = par ? baseOdd : baseEven, baseOld = par ? baseEven : baseOdd;
+    const double n = S[slotN];
     const double beta = iter == 0 ? 0.0 : RzEffP(S, baseNew, n, kSingular) / RzEffP(S, baseOld, n, kSingular);
     const float b = (float)beta;
-    const float mean = kSingular ? (float)(S[baseNew + 1] / (double)n) : 0.f;
+    const float mean = kSingular ? (float)(S[baseNew + 1] / n) : 0.f;
     const PairPos P = PairStart(v);
     const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
     const float *zp = z + P.base;
@@ -502,16 +504,16 @@ __global__ void __launch_bounds__(kPairThreads)
 }
 
 void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
-                      const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int n,
+                      const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
                       int singular, int slotPQ, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
     if (singular)
         k_pair_papply<true><<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd,
-                                                                   n, slotPQ);
+                                                                   slotN, slotPQ);
     else
         k_pair_papply<false><<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd,
-                                                                    n, slotPQ);
+                                                                    slotN, slotPQ);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -604,13 +606,13 @@ __global__ void __launch_bounds__(256) k_lin_dot(long long cells, const float *_
 // alpha = rz / pq; x += alpha p; r -= alpha q; sum r.r; the last block advances the iteration counter
 __global__ void __launch_bounds__(256) k_lin_xr(long long cells, float *__restrict__ x, float *__restrict__ r,
                                                 const float *p0, const float *p1, const float *__restrict__ q,
-                                                Reducer R, const double *S, int *it, int baseEven, int baseOdd, int n,
+                                                Reducer R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
                                                 int singular, int slotPQ, int slotRR)
 {
     const int par = *it & 1;
     const float *__restrict__ p = par ? p0 : p1;
     const int base = par ? baseOdd : baseEven;
-    const float a = (float)(RzEffP(S, base, n, singular) / S[slotPQ]);
+    const float a = (float)(RzEffP(S, base, S[slotN], singular) / S[slotPQ]);
     double acc[1] = {0.0};
     const long long n4 = cells >> 2, stride = (long long)gridDim.x * blockDim.x;
     float4 *x4 = reinterpret_cast<float4 *>(x), *r4 = reinterpret_cast<float4 *>(r);
@@ -643,11 +645,11 @@ void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer
 }
 
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,
-                 const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int n, int singular,
+                 const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int slotN, int singular,
                  int slotPQ, int slotRR, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_lin_xr<<<kLinBlocks, 256, 0, st>>>(cells, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, n, singular, slotPQ,
+    k_lin_xr<<<kLinBlocks, 256, 0, st>>>(cells, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, singular, slotPQ,
                                          slotRR);
 }
 

@@ -162,26 +162,7 @@ void Context::BuildHierarchy()
         LaunchBuildCodes(C.view(), C.code.p, st);
         L.push_back(std::move(C));
     }
-    // the FP32 cell-pair kernels' diagonal units (mixed precision: the inner solve runs in FP32)
-    for (auto &Lv : L)
-    {
-        const LevelView v = Lv.view();
-        if (opt.precision == NB_PRECISION_MIXED && opt.pair_kernels && PairLevelShape(v))
-        {
-            Lv.du.alloc((size_t)Lv.cells);
-            LaunchBuildDu(v, Lv.du.p, st);
-        }
-        else Lv.du.release();
-    }
-    for (size_t l = 0; l < L.size(); l++)
-    {
-        if (L[l].du.p && l + 1 < L.size())
-        {
-            L[l].pext.alloc((size_t)L[l].cells);
-            LaunchBuildPext(L[l].view(), L[l + 1].view(), L[l].pext.p, st);
-        }
-        else L[l].pext.release();
-    }
+    BuildPairData();
     NB_CK(cudaGetLastError());
     // The tail: the first level from which every coarser level has at most opt.tail_cells cells and all of them fit
     // in one block's shared memory in the solver's precision.
@@ -206,6 +187,46 @@ void Context::BuildHierarchy()
     if (mixed) PrepareSweeps<float>();
     else PrepareSweeps<double>();
     cudaGetLastError(); // an attribute the device refuses leaves the per-colour path, checked at launch
+}
+
+// The per-level bytes of the cell-pair kernels: diagonal units and the prolongation's moved weights.
+void Context::BuildPairData()
+{
+    // the FP32 cell-pair kernels' diagonal units (mixed precision: the inner solve runs in FP32)
+    for (auto &Lv : L)
+    {
+        const LevelView v = Lv.view();
+        if (opt.precision == NB_PRECISION_MIXED && opt.pair_kernels && PairLevelShape(v))
+        {
+            Lv.du.alloc((size_t)Lv.cells);
+            LaunchBuildDu(v, Lv.du.p, st);
+        }
+        else Lv.du.release();
+    }
+    for (size_t l = 0; l < L.size(); l++)
+    {
+        if (L[l].du.p && l + 1 < L.size())
+        {
+            L[l].pext.alloc((size_t)L[l].cells);
+            LaunchBuildPext(L[l].view(), L[l + 1].view(), L[l].pext.p, st);
+        }
+        else L[l].pext.release();
+    }
+}
+
+// A new layout with the hierarchy's shape (sizes and spacing tables) unchanged: the cell types, codes and pair bytes of
+// every level are rebuilt in the arrays they have; pointers, tail and captured iterations stay as they are.
+void Context::RefillHierarchy()
+{
+    L[0].types.upload(layout.data(), layout.size(), st);
+    LaunchBuildCodes(L[0].view(), L[0].code.p, st);
+    for (size_t l = 1; l < L.size(); l++)
+    {
+        LaunchCoarsenTypes(L[l - 1].view(), L[l].view(), L[l].types.p, st);
+        LaunchBuildCodes(L[l].view(), L[l].code.p, st);
+    }
+    BuildPairData();
+    NB_CK(cudaGetLastError());
 }
 
 void Context::AllocVectors()
@@ -430,78 +451,60 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
                std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
     }
     if (same) return; // PressureLayoutChanged: nothing moved
+    // the same shape (sizes, spacing tables, dh): only the cell types moved, the hierarchy is refilled in place
+    bool shapeSame = built && dim_ == dim && Nx_ == Nx && Ny_ == Ny && Nz_ == Nz &&
+                     (nonUniform != 0) == nonuniform && dh_ == dh && layout.size() == cells;
+    for (int a = 0; a < 3 && shapeSame; a++)
+    {
+        const size_t nw = (size_t)N[a] + 2, ng = (size_t)N[a] + 1;
+        if (a == 2 && dim_ == 2) continue;
+        shapeSame = wt[a].size() == nw && gt[a].size() == ng && std::memcmp(wt[a].data(), width[a], nw * 8) == 0 &&
+                    std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
+    }
     NB_CK(cudaStreamSynchronize(st));
-    for (auto &g : graphs) g.Release(); // they hold the old hierarchy's pointers
-    dim = dim_;
-    Nx = Nx_;
-    Ny = Ny_;
-    Nz = Nz_;
-    nonuniform = nonUniform != 0;
-    dh = dh_;
-    scale = nonuniform ? 1.0 : 1.0 / (dh * dh); // MatrixScale3D (PressureSolver3D.cpp:34-37)
-    layout.assign(types, types + cells);
-    for (int a = 0; a < 3; a++)
-    {
-        if (a == 2 && dim == 2)
-        {
-            const double w0 = width[2] ? width[2][1] : (width[0] ? width[0][1] : 1.0);
-            wt[2].assign(3, w0);
-            gt[2].assign(2, w0);
-            continue;
-        }
-        wt[a].assign(width[a], width[a] + N[a] + 2);
-        gt[a].assign(gap[a], gap[a] + N[a] + 1);
-        for (double x : wt[a])
-            if (!(x > 0.0) || !std::isfinite(x)) throw InputError("width table entries must be positive");
-        for (double x : gt[a])
-            if (!(x > 0.0) || !std::isfinite(x)) throw InputError("gap table entries must be positive");
-    }
+    const bool wasSingular = singular;
     built = false;
-    BuildHierarchy();
-    // IDP numbering and the singular flag
-    const LevelView v0 = L[0].view();
-    idp.alloc(cells);
-    lineCounts.alloc((size_t)std::max(v0.nLines, 0) + 1);
-    lineOffsets.alloc((size_t)std::max(v0.nLines, 0) + 1);
-    lineCounts.zero(st);
-    size_t need = std::max(ScanTempBytes(std::max(v0.nLines, 0) + 1), ScanTempBytes(1 << 20));
-    if (need > scanTmpBytes)
+    idpValid = false;
+    layout.assign(types, types + cells);
+    if (shapeSame)
+        RefillHierarchy();
+    else
     {
-        scanTmp.alloc(need);
-        scanTmpBytes = need;
+        for (auto &g : graphs) g.Release(); // they hold the old hierarchy's pointers
+        dim = dim_;
+        Nx = Nx_;
+        Ny = Ny_;
+        Nz = Nz_;
+        nonuniform = nonUniform != 0;
+        dh = dh_;
+        scale = nonuniform ? 1.0 : 1.0 / (dh * dh); // MatrixScale3D (PressureSolver3D.cpp:34-37)
+        for (int a = 0; a < 3; a++)
+        {
+            if (a == 2 && dim == 2)
+            {
+                const double w0 = width[2] ? width[2][1] : (width[0] ? width[0][1] : 1.0);
+                wt[2].assign(3, w0);
+                gt[2].assign(2, w0);
+                continue;
+            }
+            wt[a].assign(width[a], width[a] + N[a] + 2);
+            gt[a].assign(gap[a], gap[a] + N[a] + 1);
+            for (double x : wt[a])
+                if (!(x > 0.0) || !std::isfinite(x)) throw InputError("width table entries must be positive");
+            for (double x : gt[a])
+                if (!(x > 0.0) || !std::isfinite(x)) throw InputError("gap table entries must be positive");
+        }
+        BuildHierarchy();
     }
-    int total = 0;
-    NumberUnknowns(v0, idp.p, lineCounts.p, lineOffsets.p, scanTmp.p, scanTmpBytes, &total, st);
-    n = total;
-    // singular: no FLUID row touches a Dirichlet neighbour or a FLUID ring cell (AssembleSystem's `dirichlet`)
-    {
-        bool dir = false;
-        const int nq = dim == 3 ? 6 : 4;
-        const long long sI = dim == 3 ? (long long)Nx * Nz : Nx, sJ = dim == 3 ? Nz : 1;
-        const long long off[6] = {sI, -sI, sJ, -sJ, 1, -1};
-        for (int i = 1; i < Ny - 1 && !dir; i++)
-            for (int j = 1; j < Nx - 1 && !dir; j++)
-                for (int k = dim == 3 ? 1 : 0; k < (dim == 3 ? Nz - 1 : 1) && !dir; k++)
-                {
-                    const long long c = (long long)i * sI + (long long)j * sJ + k;
-                    if (layout[c] != FLUID) continue;
-                    for (int q = 0; q < nq; q++)
-                    {
-                        const long long nb = c + off[q];
-                        const int t = layout[nb];
-                        if (IsDirichlet(t)) { dir = true; break; }
-                        if (t == FLUID)
-                        {
-                            const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3);
-                            const int nk = k + (q == 4) - (q == 5);
-                            const bool ring = ni == 0 || ni == Ny - 1 || nj == 0 || nj == Nx - 1 ||
-                                              (dim == 3 && (nk == 0 || nk == Nz - 1));
-                            if (ring) { dir = true; break; }
-                        }
-                    }
-                }
-        singular = !dir;
-    }
+    // the system size and the singular flag, counted on the device (the IDP numbering waits until it is asked for)
+    LaunchCountUnknowns(L[0].view(), red, S_RES, st);
+    ReadSlots(S_RES, 2);
+    n = (int)hostSlots[S_RES];
+    singular = hostSlots[S_RES + 1] == 0.0;
+    if (shapeSame && singular != wasSingular)
+        for (auto &g : graphs) g.Release(); // the iteration's kernels depend on the flag
+    hostSlots[S_NUNK] = (double)n;
+    NB_CK(cudaMemcpyAsync(slots.p + S_NUNK, hostSlots + S_NUNK, sizeof(double), cudaMemcpyHostToDevice, st));
     AllocVectors();
     NB_CK(cudaStreamSynchronize(st));
     built = true;
@@ -707,10 +710,10 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
                 ProfEnd();
             }
             ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
-            LaunchPairPApply(v0, L[0].du.p, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, st);
+            LaunchPairPApply(v0, L[0].du.p, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, st);
             ProfEnd();
             ProfBegin(NB_K_XR, 6.0 * s * cells);
-            LaunchLinXR(L[0].cells, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, S_RR, st);
+            LaunchLinXR(L[0].cells, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, S_RR, st);
             ProfEnd();
             NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
             return;
@@ -723,10 +726,10 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
         ProfEnd();
     }
     ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
-    LaunchUpdatePApply<T>(v0, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, exact ? 1 : 0, st);
+    LaunchUpdatePApply<T>(v0, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, exact ? 1 : 0, st);
     ProfEnd();
     ProfBegin(NB_K_XR, 6.0 * s * cells);
-    LaunchUpdateXR<T>(v0, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, n, sing, S_PQ, S_RR, st);
+    LaunchUpdateXR<T>(v0, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, S_RR, st);
     ProfEnd();
     NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
 }
@@ -1048,6 +1051,7 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
 int Context::SolveLaplacian(const double *f, double *xh, double tol, nb_result *out)
 {
     if (!built) throw InputError("set_layout has not been called");
+    EnsureIdp();
     std::memset(out, 0, sizeof(*out));
     out->n = n;
     out->singular = singular ? 1 : 0;
@@ -1078,6 +1082,7 @@ void Context::Rhs(const double *u, const double *v, const double *w, const doubl
                   double *bOut)
 {
     if (!built) throw InputError("set_layout has not been called");
+    EnsureIdp();
     const LevelView v0 = L[0].view();
     DevArray<double> U, V, W, P, bc;
     U.upload(u, FieldSizeU(), st);
@@ -1096,6 +1101,7 @@ void Context::Rhs(const double *u, const double *v, const double *w, const doubl
 void Context::ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnzOut, int *singularOut)
 {
     if (!built) throw InputError("set_layout has not been called");
+    EnsureIdp();
     const LevelView v0 = L[0].view();
     const size_t cap = (size_t)std::max(n, 1) * (dim == 3 ? 7 : 5);
     DevArray<int> rowLen, rowPtr, flag;
@@ -1120,9 +1126,30 @@ void Context::ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnzO
     *singularOut = sing;
 }
 
+void Context::EnsureIdp()
+{
+    if (idpValid) return;
+    const LevelView v0 = L[0].view();
+    idp.alloc(Cells());
+    lineCounts.alloc((size_t)std::max(v0.nLines, 0) + 1);
+    lineOffsets.alloc((size_t)std::max(v0.nLines, 0) + 1);
+    lineCounts.zero(st);
+    size_t need = std::max(ScanTempBytes(std::max(v0.nLines, 0) + 1), ScanTempBytes(1 << 20));
+    if (need > scanTmpBytes)
+    {
+        scanTmp.alloc(need);
+        scanTmpBytes = need;
+    }
+    int total = 0;
+    NumberUnknowns(v0, idp.p, lineCounts.p, lineOffsets.p, scanTmp.p, scanTmpBytes, &total, st);
+    if (total != n) throw CudaError("IDP numbering disagrees with the unknown count", cudaErrorUnknown);
+    idpValid = true;
+}
+
 void Context::GetIdp(int32_t *out)
 {
     if (!built) throw InputError("set_layout has not been called");
+    EnsureIdp();
     NB_CK(cudaMemcpyAsync(out, idp.p, sizeof(int32_t) * Cells(), cudaMemcpyDeviceToHost, st));
     NB_CK(cudaStreamSynchronize(st));
 }

@@ -82,6 +82,7 @@ enum : int
     S_RES = 8,   // ||b - A x||^2, sum (b - A x)
     S_SUM = 10,  // compensated sum (sum, carry)
     S_DIV = 12,
+    S_NUNK = 14, // the count of unknowns, read by the CG kernels on the device
     S_COUNT = 16
 };
 
@@ -123,6 +124,7 @@ struct Context
     std::vector<LevelData> L;
     int tailStart = 0;                       // levels from here down run in one shared-memory block (nb_tail.cu)
     DevArray<int32_t> idp;
+    bool idpValid = false; // the numbering is made when first asked for (GetIdp, ExportMatrix, SolveLaplacian, Rhs)
     int n = 0;
     bool singular = false;
     DevArray<int> lineCounts, lineOffsets;
@@ -215,6 +217,9 @@ struct Context
 
   private:
     void BuildHierarchy();
+    void RefillHierarchy();
+    void BuildPairData();
+    void EnsureIdp();
     void AllocVectors();
     double ReadSlot(int s);
     void ReadSlots(int s, int count);
