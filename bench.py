@@ -308,20 +308,22 @@ def run_b200(args, rank, world, dist):
 
 def run_tanks(args, rank, world, dist, dev):
     """The batched form: `tanks` FLIP-style n^3 tanks (liquid where x < a, z < b; a, b ~ U(0.3, 0.7) per tank),
-    each one pressure step to 1e-8 through the server (`slots` concurrent solves on this rank's device; every solve's
-    layout and host fields uploaded, projected and read back), split over the ranks by the least-loaded plan; against
-    the same tanks solved one at a time in plain FP64. Wall clock from the first submission to the last completion,
-    max over ranks."""
+    each one pressure step to 1e-8 through the server (`slots` concurrent solves on this rank's device; the tanks'
+    fields resident on the device as in a simulation step, each request bringing its own cell labels), split over the
+    ranks by the least-loaded plan; against the same tanks solved one at a time in plain FP64 on the device. Wall
+    clock from the first submission to the last completion, max over ranks."""
     import copy
 
-    from nereus_cfd_b200 import serving
+    from nereus_cfd_b200 import capi, serving
     from nereus_cfd_b200.pressure import PressureSolver
 
     cases = serving.tank_batch(args.tanks, args.tank_size)
     summary = {}
 
+    import torch
+
     def execute(mine):
-        jobs = [serving.job_from_case(c, tol=TOL) for c in mine]
+        jobs = [serving.to_device(serving.job_from_case(c, tol=TOL), dev) for c in mine]
         if not jobs:
             return {"seconds": 0.0, "completed": 0, "latencies": []}
         with serving.Server(devices=(dev,), slots_per_device=args.slots, **args.solver_opts) as srv:
@@ -329,14 +331,25 @@ def run_tanks(args, rank, world, dist, dev):
             serving.serve_jobs(warm, srv)  # each slot's context, graphs and buffers
             out = serving.serve_jobs(jobs, srv)
         out["iters_inner"] = [j.result["iters_inner"] for j in jobs if j.result]
-        # one at a time in plain FP64 on a sample of the same tanks
-        sample = [serving.job_from_case(c, tol=TOL) for c in mine[: args.fp64_tanks]]
+        # one at a time in plain FP64 on a sample of the same tanks, fields on the device likewise
+        sample = [serving.to_device(serving.job_from_case(c, tol=TOL), dev) for c in mine[: args.fp64_tanks]]
         s = PressureSolver("fp64", device=dev, **args.solver_opts)
+        lib = capi.load()
+
+        def one(j):
+            s.EnsureSystem(j.grid)
+            f, res = j.device_fields, capi.Result()
+            capi.check(lib.nereus_b200_project_device(s.ctx, f["u"].data_ptr(), f["v"].data_ptr(), f["w"].data_ptr(),
+                                                      f["p"].data_ptr(), j.grid.rho, j.grid.dt, 0, TOL,
+                                                      ctypes.byref(res)), allow=(0, 1))
+
         s.InitializePressureSolver(sample[0].grid)
-        s.SolvePressure(copy.deepcopy(sample[0].grid), tol=TOL)  # warm-up
+        one(copy.deepcopy(sample[0]))  # warm-up
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         for j in sample:
-            s.SolvePressure(j.grid, tol=TOL)
+            one(j)
+        torch.cuda.synchronize()
         out["fp64_seconds_each"] = (time.perf_counter() - t0) / len(sample)
         s.DestroyPressureSolver()
         summary.update(out)
@@ -439,7 +452,7 @@ def main():
     ap.add_argument("--opt", action="append", default=[], help="solver option key=value (nb_options field)")
     ap.add_argument("--tanks", type=int, default=64, help="batched tanks (0: skip the batched form)")
     ap.add_argument("--tank-size", type=int, default=128)
-    ap.add_argument("--slots", type=int, default=4, help="concurrent solves per device in the batched form")
+    ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device in the batched form")
     ap.add_argument("--fp64-tanks", type=int, default=4, help="tanks solved one at a time in plain FP64")
     args = ap.parse_args()
     args.solver_opts = {k: int(v) if v.lstrip("-").isdigit() else float(v)

@@ -238,6 +238,9 @@ typedef struct nb_request
                                        the start */
     int scheme, needs_compat, warm_start;
     double rho, dt, tol;
+    int fields_on_device;           /* 1: u, v, w, p (and p_prev) are device memory on the server's only device, their
+                                       writers finished before the submission; the step runs on them in place, with
+                                       no host copies */
 } nb_request;
 
 typedef struct nb_server_stats

@@ -55,7 +55,7 @@ class Request(ctypes.Structure):
                 ("w", ctypes.POINTER(ctypes.c_double)), ("p", ctypes.POINTER(ctypes.c_double)),
                 ("p_prev", ctypes.POINTER(ctypes.c_double)), ("scheme", ctypes.c_int), ("needs_compat", ctypes.c_int),
                 ("warm_start", ctypes.c_int), ("rho", ctypes.c_double), ("dt", ctypes.c_double),
-                ("tol", ctypes.c_double)]
+                ("tol", ctypes.c_double), ("fields_on_device", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):

@@ -133,18 +133,27 @@ void nb_server::Slot(int dev)
             const double *W[3] = {q->tables[0].data(), q->tables[1].data(), q->tables[2].data()};
             const double *G[3] = {q->tables[3].data(), q->tables[4].data(), q->tables[5].data()};
             C.SetLayout(r.dim, r.Nx, r.Ny, r.Nz, q->types.data(), W, G, r.non_uniform, r.dh);
-            C.du.upload(r.u, C.FieldSizeU(), C.st);
-            C.dv.upload(r.v, C.FieldSizeV(), C.st);
-            if (C.dim == 3) C.dw.upload(r.w, C.FieldSizeW(), C.st);
-            C.dp.upload(r.p, C.Cells(), C.st);
-            if (r.p_prev) C.dpPrev.upload(r.p_prev, C.Cells(), C.st);
-            status = C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, r.rho, r.dt,
-                                     r.needs_compat, r.tol, &res, true, true, r.p_prev ? C.dpPrev.p : nullptr,
-                                     r.scheme, r.warm_start != 0);
-            NB_CK(cudaMemcpyAsync(r.u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
-            NB_CK(cudaMemcpyAsync(r.v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
-            if (C.dim == 3) NB_CK(cudaMemcpyAsync(r.w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
-            NB_CK(cudaMemcpyAsync(r.p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+            if (r.fields_on_device)
+            {
+                // the caller's device fields, in place
+                status = C.ProjectDevice(r.u, r.v, C.dim == 3 ? r.w : r.u, r.p, r.rho, r.dt, r.needs_compat, r.tol,
+                                         &res, true, true, r.p_prev, r.scheme, r.warm_start != 0);
+            }
+            else
+            {
+                C.du.upload(r.u, C.FieldSizeU(), C.st);
+                C.dv.upload(r.v, C.FieldSizeV(), C.st);
+                if (C.dim == 3) C.dw.upload(r.w, C.FieldSizeW(), C.st);
+                C.dp.upload(r.p, C.Cells(), C.st);
+                if (r.p_prev) C.dpPrev.upload(r.p_prev, C.Cells(), C.st);
+                status = C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, r.rho, r.dt,
+                                         r.needs_compat, r.tol, &res, true, true, r.p_prev ? C.dpPrev.p : nullptr,
+                                         r.scheme, r.warm_start != 0);
+                NB_CK(cudaMemcpyAsync(r.u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
+                NB_CK(cudaMemcpyAsync(r.v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
+                if (C.dim == 3) NB_CK(cudaMemcpyAsync(r.w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
+                NB_CK(cudaMemcpyAsync(r.p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+            }
             NB_CK(cudaStreamSynchronize(C.st));
         }
         catch (...)
@@ -253,6 +262,8 @@ int nereus_b200_submit(nb_server *srv, const nb_request *req, uint64_t *ticket)
             if (!r.width[a] || !r.gap[a]) throw nb::InputError("null spacing table");
         if ((r.scheme == NB_SCHEME_INCREMENTAL || r.warm_start) && !r.p_prev)
             throw nb::InputError("the previous pressure is required");
+        if (r.fields_on_device && srv->devices.size() != 1)
+            throw nb::InputError("device-resident fields need a server of one device");
         auto q = std::make_unique<nb::Request>();
         q->r = r;
         q->r.Nz = Nz;

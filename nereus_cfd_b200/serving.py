@@ -31,11 +31,34 @@ class Job:
     result: Optional[dict] = None
     status: Optional[int] = None
     latency_ms: Optional[float] = None
+    device_fields: Optional[dict] = None  # torch CUDA tensors u, v, w, p (, p_prev) when the fields live on the device
     _keep: list = field(default_factory=list, repr=False)
 
     @property
     def cells(self) -> int:
         return self.grid.grid.cells
+
+
+def to_device(job: Job, device: int = 0) -> Job:
+    """Puts the job's fields on the device (torch tensors): the server then solves them in place, with no host
+    copies."""
+    import torch
+
+    d = "cuda:%d" % device
+    f = {k: torch.from_numpy(np.ascontiguousarray(getattr(job.grid, k), dtype=np.float64)).to(d)
+         for k in ("u", "v", "w", "p")}
+    if job.p_prev is not None:
+        f["p_prev"] = torch.from_numpy(np.ascontiguousarray(job.p_prev, dtype=np.float64)).to(d)
+    torch.cuda.synchronize(d)
+    job.device_fields = f
+    return job
+
+
+def fetch(job: Job) -> Job:
+    """Copies a device job's fields back into its grid arrays."""
+    for k in ("u", "v", "w", "p"):
+        getattr(job.grid, k)[:] = job.device_fields[k].cpu().numpy()
+    return job
 
 
 def job_from_case(case, tol: Optional[float] = None, types: Optional[np.ndarray] = None) -> Job:
@@ -107,11 +130,19 @@ class Server:
             r.width[a] = capi.ptr(widths[a])
             r.gap[a] = capi.ptr(gaps[a])
         r.non_uniform, r.dh = int(g.nonuniform), g.dh
-        r.u, r.v, r.w, r.p = capi.ptr(m.u), capi.ptr(m.v), capi.ptr(w), capi.ptr(m.p)
         prev = None
-        if job.p_prev is not None:
-            prev = np.ascontiguousarray(job.p_prev, dtype=np.float64)
-            r.p_prev = capi.ptr(prev)
+        if job.device_fields is not None:
+            dp = lambda t: ctypes.cast(t.data_ptr(), capi._dp)
+            f = job.device_fields
+            r.u, r.v, r.w, r.p = dp(f["u"]), dp(f["v"]), dp(f["w"] if g.dim == 3 else f["u"]), dp(f["p"])
+            if "p_prev" in f:
+                r.p_prev = dp(f["p_prev"])
+            r.fields_on_device = 1
+        else:
+            r.u, r.v, r.w, r.p = capi.ptr(m.u), capi.ptr(m.v), capi.ptr(w), capi.ptr(m.p)
+            if job.p_prev is not None:
+                prev = np.ascontiguousarray(job.p_prev, dtype=np.float64)
+                r.p_prev = capi.ptr(prev)
         r.scheme, r.needs_compat, r.warm_start = job.scheme, int(job.needs_compat), int(job.warm_start)
         r.rho, r.dt, r.tol = m.rho, m.dt, job.tol
         ticket = ctypes.c_uint64(0)

@@ -55,6 +55,21 @@ def test_mix_equals_alone(nb, precision):
             assert np.array_equal(getattr(a.grid, f), getattr(b.grid, f)), f
 
 
+def test_device_fields_equal_host_fields(nb):
+    host = mix()
+    dev = [serving.to_device(j) for j in mix()]
+    with serving.Server(slots_per_device=4) as srv:
+        serving.serve(host, srv)
+    with serving.Server(slots_per_device=4) as srv:
+        serving.serve(dev, srv)
+    for a, b in zip(host, dev):
+        serving.fetch(b)
+        assert a.status == b.status == capi.NB_OK
+        assert a.result["iters_inner"] == b.result["iters_inner"]
+        for f in ("p", "u", "v", "w"):
+            assert np.array_equal(getattr(a.grid, f), getattr(b.grid, f)), f
+
+
 def test_admission_budget(nb):
     job = mix()[0]
     with serving.Server(hbm_budget_gb=0.01) as srv:
