@@ -288,6 +288,7 @@ def run_b200(args, rank, world, dist):
         s.DestroyPressureSolver()
 
     tanks = run_tanks(args, rank, world, dist, dev) if args.tanks > 0 else None
+    trace = run_trace(args, dev) if args.trace > 0 and world == 1 else None
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -301,8 +302,60 @@ def run_b200(args, rank, world, dist):
         "latency_ms": {"p50": round(percentile(lat, 0.5), 3), "p99": round(percentile(lat, 0.99), 3)},
         "solve": {k: mixed_res[k] for k in ("iters_outer", "iters_inner", "rel_res", "max_div", "status")},
         "fp64_plain": fp64, "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": int(launches),
-        "batched_tanks": tanks,
+        "batched_tanks": tanks, "serving_trace": trace,
     }
+    return out
+
+
+def run_trace(args, dev):
+    """The served form: `trace` requests of mixed dimension (3D side log-U[32, 256], 2D side log-U[64, 1024]), mask
+    (closed, obstacle + outlet, free surface) and spacing (uniform, 1.04-stretched), fields drawn on the device, each
+    to 1e-8. A closed loop (all submitted at once) gives the capacity; Poisson arrivals at 0.5x and 0.9x of it give
+    p50/p99 latency from arrival to completion; the first `trace_fp64` requests are also solved one at a time in plain
+    FP64 on the device (the one-at-a-time path)."""
+    import torch
+
+    from nereus_cfd_b200 import capi, serving
+    from nereus_cfd_b200.pressure import PressureSolver
+
+    rng = np.random.default_rng(5)
+    cases = [serving.trace_case(rng, i) for i in range(args.trace)]
+    fresh = lambda cs: [serving.device_job(c, dev, TOL) for c in cs]
+    out = {"requests": len(cases), "slots_per_device": args.slots, "hbm_budget_gb": 150.0,
+           "mix": {"3d": sum(c.grid.dim == 3 for c in cases), "2d": sum(c.grid.dim == 2 for c in cases),
+                   "stretched": sum(c.grid.nonuniform for c in cases)}}
+    with serving.Server(devices=(dev,), slots_per_device=args.slots, hbm_budget_gb=150.0, **args.solver_opts) as srv:
+        serving.serve_jobs(fresh(cases[: args.slots]), srv)  # warm-up
+        closed = serving.serve_jobs(fresh(cases), srv)
+        cap = closed["completed"] / closed["seconds"]
+        out["closed_loop"] = {"solves_per_s": round(cap, 3), "seconds": round(closed["seconds"], 4),
+                              "p50_ms": round(closed["p50_ms"], 3), "p99_ms": round(closed["p99_ms"], 3)}
+        out["poisson"] = [serving.run_trace(srv, fresh(cases), f * cap, seed=11 + k)
+                          for k, f in enumerate((0.5, 0.9))]
+    k = min(args.trace_fp64, len(cases))
+    sample = fresh(cases[:k])
+    s = PressureSolver("fp64", device=dev, **args.solver_opts)
+    lib = capi.load()
+    s.InitializePressureSolver(sample[0].grid)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for j in sample:
+        s.EnsureSystem(j.grid)
+        f, res = j.device_fields, capi.Result()
+        capi.check(lib.nereus_b200_project_device(s.ctx, f["u"].data_ptr(), f["v"].data_ptr(), f["w"].data_ptr(),
+                                                  f["p"].data_ptr(), j.grid.rho, j.grid.dt, int(j.needs_compat), TOL,
+                                                  ctypes.byref(res)), allow=(0, 1))
+    torch.cuda.synchronize()
+    fp64_rate = k / (time.perf_counter() - t0)
+    s.DestroyPressureSolver()
+    mixed_k = serving.Server(devices=(dev,), slots_per_device=args.slots, **args.solver_opts)
+    with mixed_k as srv:
+        same = serving.serve_jobs(fresh(cases[:k]), srv)
+    out["fp64_one_at_a_time"] = {"value": round(fp64_rate, 3), "unit": "solves/s", "requests": k}
+    out["served_same_requests"] = {"value": round(same["completed"] / same["seconds"], 3), "unit": "solves/s",
+                                   "requests": k}
+    out["speedup_over_fp64_one_at_a_time"] = round(same["completed"] / same["seconds"] / fp64_rate, 3)
+    out["timing"] = "host wall clock; latency from submission (arrival) to completion"
     return out
 
 
@@ -454,6 +507,8 @@ def main():
     ap.add_argument("--tank-size", type=int, default=128)
     ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device in the batched form")
     ap.add_argument("--fp64-tanks", type=int, default=4, help="tanks solved one at a time in plain FP64")
+    ap.add_argument("--trace", type=int, default=200, help="requests of the serving trace (0: skip)")
+    ap.add_argument("--trace-fp64", type=int, default=40, help="trace requests solved one at a time in plain FP64")
     args = ap.parse_args()
     args.solver_opts = {k: int(v) if v.lstrip("-").isdigit() else float(v)
                         for k, v in (o.split("=", 1) for o in args.opt)}

@@ -82,6 +82,7 @@ typedef struct nb_result
     double rel_res;      /* ||b - A x||_2 / ||b||_2 in FP64, A the reference's matrix */
     double max_div;      /* max |div u| over FLUID cells after the projection (-1 when not computed) */
     double seconds;      /* device time of the call's solve + projection (CUDA events) */
+    double latency_ms;   /* served requests: submission to completion on the host clock; 0 elsewhere */
 } nb_result;
 
 typedef struct nb_ctx nb_ctx;
@@ -265,6 +266,8 @@ int nereus_b200_poll(nb_server *srv, uint64_t ticket, nb_result *out);
 /* As poll, blocking up to timeout_s seconds (< 0: no limit) for completion. */
 int nereus_b200_wait(nb_server *srv, uint64_t ticket, double timeout_s, nb_result *out);
 int nereus_b200_server_stats(nb_server *srv, nb_server_stats *stats);
+/* Starts the statistics afresh (counts, latencies, the clock) from now; queued and running requests are kept. */
+int nereus_b200_server_reset_stats(nb_server *srv);
 /* Estimated device bytes of one solve (the admission cost): fields, right-hand side and solution, level vectors. */
 double nereus_b200_request_bytes(int dim, int Nx, int Ny, int Nz, int precision);
 /* Host only: a deterministic least-loaded assignment of n requests with the given costs to k devices (or processes):

@@ -36,7 +36,7 @@ class Result(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("n", ctypes.c_int), ("singular", ctypes.c_int),
                 ("iters_outer", ctypes.c_int), ("iters_inner", ctypes.c_int), ("levels", ctypes.c_int),
                 ("b_norm", ctypes.c_double), ("rel_res", ctypes.c_double), ("max_div", ctypes.c_double),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("latency_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -132,6 +132,7 @@ SIGNATURES = {
     "nereus_b200_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
                                         ctypes.POINTER(Result)]),
     "nereus_b200_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "nereus_b200_server_reset_stats": (ctypes.c_int, [ctypes.c_void_p]),
     "nereus_b200_request_bytes": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_int]),
     "nereus_b200_plan": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),

@@ -174,6 +174,7 @@ void nb_server::Slot(int dev)
             rec.state = 2;
             rec.status = status;
             rec.result = res;
+            rec.result.latency_ms = ms;
             rec.error = err;
             if (status == NB_OK || status == NB_NOT_CONVERGED)
             {
@@ -364,6 +365,18 @@ int nereus_b200_server_stats(nb_server *srv, nb_server_stats *st)
     for (double u : srv->used) adm += u;
     st->admitted_gb = adm / 1e9;
     for (size_t d = 0; d < srv->doneOn.size() && d < 8; d++) st->device_completed[d] = srv->doneOn[d];
+    return (int)NB_OK;
+}
+
+int nereus_b200_server_reset_stats(nb_server *srv)
+{
+    if (!srv) return Fail(NB_BAD_INPUT, "srv is null");
+    std::lock_guard<std::mutex> lock(srv->mu);
+    srv->submitted = (long long)srv->queue.size() + srv->running;
+    srv->completed = srv->failed = 0;
+    srv->latencies.clear();
+    std::fill(srv->doneOn.begin(), srv->doneOn.end(), 0LL);
+    srv->started = false;
     return (int)NB_OK;
 }
 

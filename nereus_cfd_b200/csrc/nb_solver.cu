@@ -117,10 +117,18 @@ static void CoarseAxis(const std::vector<double> &wFine, int Nf, int Nc, std::ve
 
 void Context::BuildHierarchy()
 {
+    // the previous levels lend their device arrays to the new ones of the same index (a DevArray keeps its
+    // allocation when the new size fits), so a new shape allocates only where it outgrows the old
+    std::vector<LevelData> old = std::move(L);
     L.clear();
     L.reserve(32);
+    auto take = [&](size_t l) {
+        LevelData X = l < old.size() ? std::move(old[l]) : LevelData();
+        for (int a = 0; a < 3; a++) { X.w[a].clear(); X.g[a].clear(); }
+        return X;
+    };
     {
-        LevelData L0;
+        LevelData L0 = take(0);
         L0.dim = dim;
         L0.Nx = Nx;
         L0.Ny = Ny;
@@ -143,7 +151,7 @@ void Context::BuildHierarchy()
         const int mn = dim == 3 ? std::min(nx, std::min(ny, nz)) : std::min(nx, ny);
         const long long interior = (long long)nx * ny * nz;
         if (mn < 4 || interior <= 8) break; // down to about 2 cells a side: the coarse end runs in shared memory
-        LevelData C;
+        LevelData C = take(L.size());
         C.dim = dim;
         C.Nx = (nx + 1) / 2 + 2;
         C.Ny = (ny + 1) / 2 + 2;

@@ -32,30 +32,30 @@ struct InputError : std::runtime_error
         if (e_ != cudaSuccess) throw ::nb::CudaError(#x, e_);                                                      \
     } while (0)
 
+// A device array that keeps its allocation: a smaller or equal size reuses it (no cudaFree, which would synchronize
+// the device, and no cudaMalloc), a larger one replaces it.
 template <typename T> struct DevArray
 {
     T *p = nullptr;
-    size_t n = 0;
+    size_t n = 0, cap = 0;
     DevArray() = default;
     DevArray(const DevArray &) = delete;
     DevArray &operator=(const DevArray &) = delete;
-    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n), cap(o.cap) { o.p = nullptr; o.n = o.cap = 0; }
     DevArray &operator=(DevArray &&o) noexcept
     {
-        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        if (this != &o) { release(); p = o.p; n = o.n; cap = o.cap; o.p = nullptr; o.n = o.cap = 0; }
         return *this;
     }
     ~DevArray() { release(); }
     void alloc(size_t count)
     {
-        if (count == n && p) return;
+        if (count == 0) { n = 0; return; }
+        if (p && count <= cap) { n = count; return; }
         release();
-        if (count)
-        {
-            cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
-            if (e != cudaSuccess) { p = nullptr; throw CudaError("cudaMalloc", e); }
-        }
-        n = count;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e != cudaSuccess) { p = nullptr; throw CudaError("cudaMalloc", e); }
+        n = cap = count;
     }
     void zero(cudaStream_t st) { if (p && n) NB_CK(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
     void upload(const T *h, size_t count, cudaStream_t st)
@@ -67,7 +67,7 @@ template <typename T> struct DevArray
     {
         if (p) cudaFree(p);
         p = nullptr;
-        n = 0;
+        n = cap = 0;
     }
     size_t bytes() const { return n * sizeof(T); }
 };

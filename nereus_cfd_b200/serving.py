@@ -155,8 +155,7 @@ class Server:
         job, t0 = self.jobs[ticket]
         job.status = st
         job.result = res.as_dict()
-        if job.latency_ms is None:
-            job.latency_ms = 1e3 * (time.perf_counter() - t0)
+        job.latency_ms = res.latency_ms  # the server's own submission-to-completion time
         return st
 
     def poll(self, ticket: int) -> int:
@@ -173,6 +172,9 @@ class Server:
         s = capi.ServerStats()
         capi.check(self.lib.nereus_b200_server_stats(self.srv, ctypes.byref(s)))
         return s.as_dict()
+
+    def reset_stats(self):
+        capi.check(self.lib.nereus_b200_server_reset_stats(self.srv))
 
     def close(self):
         if self.srv:
@@ -235,11 +237,113 @@ def run_sharded(items: Sequence, cost: Callable, execute: Callable[[list], dict]
 
 def serve_jobs(jobs: Sequence[Job], server: Server) -> dict:
     """``execute`` for run_sharded on this rank's device: serve the jobs, report wall seconds from the first
-    submission to the last completion, completions and latencies."""
+    submission to the last completion, completions, and the server's p50/p99 submission-to-completion latency."""
+    server.reset_stats()
     t0 = time.perf_counter()
     tickets = [server.submit(j) for j in jobs]
     for t in tickets:
         server.wait(t)
     seconds = time.perf_counter() - t0
+    st = server.stats()
     done = [j for j in jobs if j.status in (capi.NB_OK, capi.NB_NOT_CONVERGED)]
-    return {"seconds": seconds, "completed": len(done), "latencies": [j.latency_ms for j in done]}
+    return {"seconds": seconds, "completed": len(done), "latencies": [j.latency_ms for j in done],
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"]}
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# a serving trace: requests of mixed dimension, size, mask and spacing arriving as a Poisson process
+# ---------------------------------------------------------------------------------------------------------------------
+def trace_case(rng, index: int):
+    """One request of the trace: 3D with side ~ log-U[32, 256] or 2D with side ~ log-U[64, 1024] (even); mask
+    closed box (singular, compatibility on), sphere/disc obstacle with a p = 0 outlet on x = 1, or a free-surface
+    tank (liquid where x < a and y or z < b, air elsewhere); uniform, or stretched in x by 1.04 per cell over the
+    outer 64 cells of each side."""
+    from . import workloads as W
+
+    dim = 3 if rng.random() < 0.5 else 2
+    lo, hi = (32, 256) if dim == 3 else (64, 1024)
+    n = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))) / 2.0)) * 2
+    mask = ("closed", "obstacle", "free")[int(rng.integers(3))]
+    stretched = rng.random() < 0.5
+    dom = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    if stretched:
+        # a uniform band in the middle, 1.04 growth over the outer 64 cells of each side (width ratio 1.04^64 ~ 12)
+        wx = W.band_stretched_widths(n, 1.0, max(2, (n - 128) // 2 * 2), 0.5, 1.04)
+        ws = [wx, np.full(n, 1.0 / n)] + ([np.full(n, 1.0 / n)] if dim == 3 else [])
+        g = W.stretched_grid(dim, dom, ws)
+    else:
+        g = W.uniform_grid(dim, dom, n)
+    compat, rule = False, "solid"
+    if mask == "closed":
+        sc, compat = W.walls_scene(dim), True
+    elif mask == "obstacle":
+        sph = W.Region(W.REGION_SOLID, W.PRIM_SPHERE, (0.5, 0.5, 0.5), radius=0.15)
+        sc = W.walls_scene(dim, outlet_face=1, regions=[sph])
+    else:
+        a, b = rng.uniform(0.3, 0.7, 2)
+        air = W.Region(W.REGION_EMPTY, W.PRIM_BOX, (-1.0, -1.0, -1.0), (2.0, 2.0, 2.0))
+        top = (a, 2.0, b) if dim == 3 else (a, b, 2.0)
+        liquid = W.Region(W.REGION_FLUID, W.PRIM_BOX, (-1.0, -1.0, -1.0), top)
+        sc, rule = W.walls_scene(dim, regions=[air, liquid]), "liquid"
+    name = "trace%d_%dd_%d_%s_%s" % (index, dim, n, mask, "stretched" if stretched else "uniform")
+    return W.Case(name, g, sc, int(rng.integers(1 << 31)), needs_compat=compat, velocity_rule=rule)
+
+
+def device_job(case, device: int = 0, tol: float = 1e-8) -> Job:
+    """A job whose fields are drawn on the device: labels by the library, N(0,1) face velocities from a torch
+    generator seeded by the case, zeroed by the case's rule (face_velocities' rules), p = 0."""
+    import torch
+
+    from . import workloads as W
+
+    g = case.grid
+    types = capi.label_cells(g, case.scene)
+    d = "cuda:%d" % device
+    t = torch.from_numpy(types.reshape(g.shape)).to(d)
+    gen = torch.Generator(device=d)
+    gen.manual_seed(case.seed)
+    fields = {}
+    comps = 3 if g.dim == 3 else 2
+    for c in range(comps):
+        shape = [g.u_shape(), g.v_shape(), g.w_shape()][c]
+        vals = torch.randn(shape, generator=gen, device=d, dtype=torch.float64)
+        ax = [1, 0, 2][c]
+        pad = [0, 0, 0, 0, 0, 0]  # last dim first
+        pad[2 * (2 - ax)] = pad[2 * (2 - ax) + 1] = 1
+        tp = torch.nn.functional.pad(t, pad, value=W.SOLID)
+        a, b = tp.narrow(ax, 0, tp.shape[ax] - 1), tp.narrow(ax, 1, tp.shape[ax] - 1)
+        keep = (a != W.SOLID) & (b != W.SOLID)
+        if case.velocity_rule == "liquid":
+            keep &= (a == W.FLUID) | (b == W.FLUID)
+        fields["uvw"[c]] = torch.where(keep, vals, torch.zeros_like(vals)).reshape(-1).contiguous()
+    if comps == 2:
+        fields["w"] = torch.zeros(1, dtype=torch.float64, device=d)
+    fields["p"] = torch.zeros(g.cells, dtype=torch.float64, device=d)
+    m = MACGrid(g, types, np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), case.rho, case.dt)
+    job = Job(m, tol=tol, needs_compat=case.needs_compat)
+    job.device_fields = fields
+    return job
+
+
+def run_trace(server: Server, jobs: Sequence[Job], rate: float, seed: int = 0) -> dict:
+    """Submits the jobs at Poisson arrival times of the given rate (per second) and waits for all. Latency is the
+    server's own, from a request's submission (its arrival) to its completion."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, len(jobs))
+    server.reset_stats()
+    t0 = time.perf_counter()
+    due = t0
+    tickets = []
+    for j, gap in zip(jobs, gaps):
+        due += gap
+        while time.perf_counter() < due:
+            time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
+        j.latency_ms = None
+        tickets.append(server.submit(j))
+    for t in tickets:
+        server.wait(t)
+    seconds = time.perf_counter() - t0
+    st = server.stats()
+    return {"rate_per_s": round(rate, 3), "requests": len(jobs), "completed": st["completed"],
+            "failed": st["failed"], "seconds": round(seconds, 4), "solves_per_s": round(st["completed"] / seconds, 3),
+            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3)}
