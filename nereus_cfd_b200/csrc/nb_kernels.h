@@ -69,6 +69,11 @@ bool PairLevelShape(const LevelView &v);
 void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st);
 void LaunchPairFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st);
 void LaunchPairHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st);
+// stretched levels: the coefficients from the level's tables, the diagonal from its code (first: red from zero)
+void LaunchPairHalfSt(const LevelView &v, const float *r, float *e, int colour, bool first, cudaStream_t st);
+void LaunchPairHalfStDot(const LevelView &v, const float *r, float *e, int colour, const Reducer &R, const int *it,
+                         int baseEven, int baseOdd, cudaStream_t st);
+void LaunchPairResidualSt(const LevelView &v, const float *r, const float *e, float *res, cudaStream_t st);
 // the same sweep, also summing (r.z, z, r) into the scalar block of the iteration's parity (k_dot's output)
 void LaunchPairHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, const Reducer &R,
                        const int *it, int baseEven, int baseOdd, cudaStream_t st);

@@ -68,7 +68,7 @@ __global__ void k_build_du(LevelView v, uint8_t *du)
     }
 }
 
-bool PairLevelShape(const LevelView &v) { return v.dim == 3 && !v.stretched && (v.Nz % 2) == 0 && v.Ny >= 3; }
+bool PairLevelShape(const LevelView &v) { return v.dim == 3 && (v.Nz % 2) == 0 && v.Ny >= 3; }
 
 void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st)
 {
@@ -257,6 +257,162 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_residual(LevelView v, con
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// the same on a stretched level: the six coefficients of a cell come from the level's FP32 width and gap tables and
+// the diagonal from its code byte (CodeStencil, nb_device.cuh); the neighbour sum stays unmasked (vectors are zero
+// off the unknowns), weighted per direction. The first sweep from zero is a red pass writing r/diag (and zero on
+// black) followed by a black pass.
+// ---------------------------------------------------------------------------------------------------------------
+// sum_q c_q x_q over the six neighbours of unknown cell (i, j, k) and its diagonal; neighbours in NbrOffset order
+__device__ __forceinline__ float StSum(const LevelView &v, int i, int j, int k, long long c, unsigned code, float nP,
+                                       float nM, float nJp, float nJm, float nKp, float nKm, float &diag)
+{
+    float cq[6];
+    CodeStencil<float>(v, i, j, k, c, code, cq, diag);
+    return ((cq[0] * nP + cq[1] * nM) + (cq[2] * nJp + cq[3] * nJm)) + (cq[4] * nKp + cq[5] * nKm);
+}
+
+template <bool kDot, bool kFirst>
+__global__ void __launch_bounds__(kPairThreads) k_pair_half_st(LevelView v, const float *__restrict__ r, float *e,
+                                                               int colour, Reducer R, const int *it, int baseEven,
+                                                               int baseOdd)
+{
+    float facc[3] = {0.f, 0.f, 0.f};
+    const PairPos P = PairStart(v);
+    const float *rp = r + P.base;
+    const uint8_t *cp = v.code + P.base;
+    float *ep = e + P.base;
+    float2 eM = kFirst ? make_float2(0.f, 0.f) : Ld2(ep - P.sI), eC = kFirst ? make_float2(0.f, 0.f) : Ld2(ep);
+    int off = 0;
+    for (int i = P.i0; i < P.i1; i++, off += P.sI)
+    {
+        float2 eP = make_float2(0.f, 0.f), eJp = eP, eJm = eP;
+        if (!kFirst)
+        {
+            eP = Ld2(ep + off + P.sI);
+            eJp = Ld2(ep + off + P.sJ);
+            eJm = Ld2(ep + off - P.sJ);
+        }
+        const float2 rc = Ld2(rp + off);
+        const unsigned d = LdDu(cp + off);
+        float left = 0.f, right = 0.f;
+        if (!kFirst)
+        {
+            left = __shfl_up_sync(0xffffffffu, eC.y, 1);
+            right = __shfl_down_sync(0xffffffffu, eC.x, 1);
+            if (P.lane == 0) left = ep[off - 1];
+            if (P.lane == 31) right = ep[off + 2];
+        }
+        const bool second = ((i + P.j + P.k0) & 1) != colour; // the cell of this colour is the pair's second
+        const int h = second ? 1 : 0, k = P.k0 + h;
+        const unsigned code = (d >> (8 * h)) & 0xFFu;
+        float nv = 0.f;
+        if (code & CODE_UNKNOWN)
+        {
+            float diag, s = 0.f;
+            const long long c = P.base + off + h;
+            if (kFirst)
+            {
+                float cq[6];
+                CodeStencil<float>(v, i, P.j, k, c, code, cq, diag);
+            }
+            else if (second)
+                s = StSum(v, i, P.j, k, c, code, eP.y, eM.y, eJp.y, eJm.y, right, eC.x, diag);
+            else
+                s = StSum(v, i, P.j, k, c, code, eP.x, eM.x, eJp.x, eJm.x, eC.y, left, diag);
+            nv = diag != 0.f ? ((second ? rc.y : rc.x) + s) / diag : 0.f;
+        }
+        if (P.valid)
+        {
+            if (kFirst) // red from zero: the black cells start at zero
+                *reinterpret_cast<float2 *>(ep + off) = second ? make_float2(0.f, nv) : make_float2(nv, 0.f);
+            else
+                ep[off + h] = nv;
+            if (kDot)
+            {
+                const float z0 = second ? eC.x : nv, z1 = second ? nv : eC.y;
+                facc[0] += rc.x * z0 + rc.y * z1;
+                facc[1] += z0 + z1;
+                facc[2] += rc.x + rc.y;
+            }
+        }
+        eM = eC;
+        eC = eP;
+    }
+    if (kDot)
+    {
+        double acc[3] = {facc[0], facc[1], facc[2]};
+        GridReduce<3>(R, acc, (*it & 1) ? baseOdd : baseEven);
+    }
+}
+
+__global__ void __launch_bounds__(kPairThreads) k_pair_residual_st(LevelView v, const float *__restrict__ r,
+                                                                   const float *__restrict__ e,
+                                                                   float *__restrict__ res)
+{
+    const PairPos P = PairStart(v);
+    const float *ep = e + P.base;
+    const float *rp = r + P.base;
+    const uint8_t *cp = v.code + P.base;
+    float *op = res + P.base;
+    float2 eM = Ld2(ep - P.sI), eC = Ld2(ep);
+    int off = 0;
+    for (int i = P.i0; i < P.i1; i++, off += P.sI)
+    {
+        const float2 eP = Ld2(ep + off + P.sI);
+        const float2 eJp = Ld2(ep + off + P.sJ), eJm = Ld2(ep + off - P.sJ);
+        const float2 rc = Ld2(rp + off);
+        const unsigned d = LdDu(cp + off);
+        float left = __shfl_up_sync(0xffffffffu, eC.y, 1);
+        float right = __shfl_down_sync(0xffffffffu, eC.x, 1);
+        if (P.lane == 0) left = ep[off - 1];
+        if (P.lane == 31) right = ep[off + 2];
+        if (P.valid && (d & 0x8080u))
+        {
+            float2 o = make_float2(0.f, 0.f);
+            const long long c = P.base + off;
+            float diag;
+            if (d & 0x80u)
+            {
+                const float s = StSum(v, i, P.j, P.k0, c, d & 0xFFu, eP.x, eM.x, eJp.x, eJm.x, eC.y, left, diag);
+                o.x = rc.x - (diag * eC.x - s);
+            }
+            if (d & 0x8000u)
+            {
+                const float s = StSum(v, i, P.j, P.k0 + 1, c + 1, (d >> 8) & 0xFFu, eP.y, eM.y, eJp.y, eJm.y, right,
+                                      eC.x, diag);
+                o.y = rc.y - (diag * eC.y - s);
+            }
+            *reinterpret_cast<float2 *>(op + off) = o;
+        }
+        eM = eC;
+        eC = eP;
+    }
+}
+
+void LaunchPairHalfSt(const LevelView &v, const float *r, float *e, int colour, bool first, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    if (first)
+        k_pair_half_st<false, true><<<PairGrid(v), kPairThreads, 0, st>>>(v, r, e, colour, Reducer{}, nullptr, 0, 0);
+    else
+        k_pair_half_st<false, false><<<PairGrid(v), kPairThreads, 0, st>>>(v, r, e, colour, Reducer{}, nullptr, 0, 0);
+}
+
+void LaunchPairHalfStDot(const LevelView &v, const float *r, float *e, int colour, const Reducer &R, const int *it,
+                         int baseEven, int baseOdd, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_pair_half_st<true, false><<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, r, e, colour, R, it, baseEven,
+                                                                               baseOdd);
+}
+
+void LaunchPairResidualSt(const LevelView &v, const float *r, const float *e, float *res, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_pair_residual_st<<<PairGrid(v), kPairThreads, 0, st>>>(v, r, e, res);
+}
+
 void LaunchPairFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
@@ -438,7 +594,8 @@ __device__ __forceinline__ double RzEffP(const double *S, int base, double n, in
 
 // p_new = U (z - mean + beta p_old), q = M p_new, sum p_new.q; U = 1 on unknowns (needed only when the mean of z is
 // removed: elsewhere z and p_old are zero already).
-template <bool kSingular>
+// kSt: a stretched level, `du` is then the level's code array (its unknown flag is the same bit)
+template <bool kSingular, bool kSt>
 __global__ void __launch_bounds__(kPairThreads)
     k_pair_papply(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ z, float *p0, float *p1,
                   float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
@@ -488,8 +645,28 @@ __global__ void __launch_bounds__(kPairThreads)
         const float s0 = ((NP.x + NM.x) + (NJp.x + NJm.x)) + (left + NC.y);
         const float s1 = ((NP.y + NM.y) + (NJp.y + NJm.y)) + (NC.x + right);
         float2 qq;
-        qq.x = Unk(d) * (hg * (float)(d & 0x7Fu) * NC.x - g * s0);
-        qq.y = Unk(d >> 8) * (hg * (float)((d >> 8) & 0x7Fu) * NC.y - g * s1);
+        if (kSt)
+        {
+            qq = make_float2(0.f, 0.f);
+            float diag;
+            if (d & 0x80u)
+            {
+                const float s = StSum(v, i, P.j, P.k0, P.base + off, d & 0xFFu, NP.x, NM.x, NJp.x, NJm.x, NC.y, left,
+                                      diag);
+                qq.x = diag * NC.x - s;
+            }
+            if (d & 0x8000u)
+            {
+                const float s = StSum(v, i, P.j, P.k0 + 1, P.base + off + 1, (d >> 8) & 0xFFu, NP.y, NM.y, NJp.y,
+                                      NJm.y, right, NC.x, diag);
+                qq.y = diag * NC.y - s;
+            }
+        }
+        else
+        {
+            qq.x = Unk(d) * (hg * (float)(d & 0x7Fu) * NC.x - g * s0);
+            qq.y = Unk(d >> 8) * (hg * (float)((d >> 8) & 0x7Fu) * NC.y - g * s1);
+        }
         if (P.valid)
         {
             *reinterpret_cast<float2 *>(pOut + P.base + off) = NC;
@@ -508,12 +685,22 @@ void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, flo
                       int singular, int slotPQ, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
+    const dim3 grid = PairGrid(v, kReduceS);
+    const uint8_t *bytes = v.stretched ? v.code : du;
+#define NB_PAPPLY(SING, ST)                                                                                        \
+    k_pair_papply<SING, ST><<<grid, kPairThreads, 0, st>>>(v, bytes, z, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, \
+                                                           slotPQ)
     if (singular)
-        k_pair_papply<true><<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd,
-                                                                   slotN, slotPQ);
+    {
+        if (v.stretched) NB_PAPPLY(true, true);
+        else NB_PAPPLY(true, false);
+    }
     else
-        k_pair_papply<false><<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd,
-                                                                    slotN, slotPQ);
+    {
+        if (v.stretched) NB_PAPPLY(false, true);
+        else NB_PAPPLY(false, false);
+    }
+#undef NB_PAPPLY
 }
 
 // ---------------------------------------------------------------------------------------------------------------

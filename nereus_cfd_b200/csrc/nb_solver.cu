@@ -600,31 +600,47 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
     }
 }
 
-// The V-cycle on a 3D uniform FP32 level with the cell-pair kernels (nb_pairs.cu): the first red-black sweep from
-// zero in one launch, further sweeps one colour per launch, the residual, then the transfers of nb_kernels.cu.
+// The V-cycle on a 3D FP32 level with the cell-pair kernels (nb_pairs.cu): the first red-black sweep from zero (one
+// launch on a uniform level, a red and a black one on a stretched level), further sweeps one colour per launch, the
+// residual, and the pair transfers.
 void Context::VCyclePairs(int l, float *r, float *e)
 {
     LevelData &Lv = L[l];
     const LevelView v = Lv.view();
+    const bool stretched = v.stretched != 0;
     const double s = sizeof(float), cells = (double)Lv.cells;
     auto prof = [&](int id, double bytesPerCell) {
         ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
     };
     const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
     const double half = (3.0 * s + 1.0) / 2.0;
-    prof(NB_K_SMOOTH0, s + 1.0 + s); // reads r and du, writes e
-    LaunchPairFirst(v, Lv.du.p, r, e, st);
-    ProfEnd();
+    if (stretched)
+    {
+        prof(NB_K_SMOOTH0, s + 1.0 + s / 2.0); // red from zero: reads r and codes, writes e
+        LaunchPairHalfSt(v, r, e, 0, true, st);
+        ProfEnd();
+        prof(NB_K_SMOOTH0, half);
+        LaunchPairHalfSt(v, r, e, 1, false, st);
+        ProfEnd();
+    }
+    else
+    {
+        prof(NB_K_SMOOTH0, s + 1.0 + s); // reads r and du, writes e
+        LaunchPairFirst(v, Lv.du.p, r, e, st);
+        ProfEnd();
+    }
     for (int q = 1; q < pre; q++)
         for (int c = 0; c < 2; c++)
         {
             prof(NB_K_SMOOTH0, half);
-            LaunchPairHalf(v, Lv.du.p, r, e, c, st);
+            if (stretched) LaunchPairHalfSt(v, r, e, c, false, st);
+            else LaunchPairHalf(v, Lv.du.p, r, e, c, st);
             ProfEnd();
         }
     float *res = Lv.res<float>();
     prof(NB_K_RESIDUAL0, 3.0 * s + 1.0);
-    LaunchPairResidual(v, Lv.du.p, r, e, res, st);
+    if (stretched) LaunchPairResidualSt(v, r, e, res, st);
+    else LaunchPairResidual(v, Lv.du.p, r, e, res, st);
     ProfEnd();
     LevelData &Lc = L[l + 1];
     const LevelView vc = Lc.view();
@@ -639,10 +655,17 @@ void Context::VCyclePairs(int l, float *r, float *e)
         for (int c = 1; c >= 0; c--)
         {
             prof(NB_K_SMOOTH0, half);
-            if (l == 0 && q + 1 == post && c == 0) // z is final: r.z for CG here (IterBody skips its own)
-                LaunchPairHalfDot(v, Lv.du.p, r, e, c, red, iter.p, S_RZ0, S_RZ1, st);
+            const bool dot = l == 0 && q + 1 == post && c == 0; // z is final: r.z for CG here (IterBody skips its own)
+            if (stretched)
+            {
+                if (dot) LaunchPairHalfStDot(v, r, e, c, red, iter.p, S_RZ0, S_RZ1, st);
+                else LaunchPairHalfSt(v, r, e, c, false, st);
+            }
             else
-                LaunchPairHalf(v, Lv.du.p, r, e, c, st);
+            {
+                if (dot) LaunchPairHalfDot(v, Lv.du.p, r, e, c, red, iter.p, S_RZ0, S_RZ1, st);
+                else LaunchPairHalf(v, Lv.du.p, r, e, c, st);
+            }
             ProfEnd();
         }
 }
