@@ -287,6 +287,7 @@ def run_b200(args, rank, world, dist):
                "p99_ms": round(1e3 * percentile(ts, 0.99), 3), "api": "nereus_b200_project (host buffers)"}
         s.DestroyPressureSolver()
 
+    stretched = run_stretched(args, dev) if args.stretched_steps > 0 and world == 1 else None
     tanks = run_tanks(args, rank, world, dist, dev) if args.tanks > 0 else None
     trace = run_trace(args, dev) if args.trace > 0 and world == 1 else None
 
@@ -302,7 +303,7 @@ def run_b200(args, rank, world, dist):
         "latency_ms": {"p50": round(percentile(lat, 0.5), 3), "p99": round(percentile(lat, 0.99), 3)},
         "solve": {k: mixed_res[k] for k in ("iters_outer", "iters_inner", "rel_res", "max_div", "status")},
         "fp64_plain": fp64, "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": int(launches),
-        "batched_tanks": tanks, "serving_trace": trace,
+        "stretched_cylinder": stretched, "batched_tanks": tanks, "serving_trace": trace,
     }
     return out
 
@@ -358,6 +359,49 @@ def run_trace(args, dev):
                                    "requests": k}
     out["speedup_over_fp64_one_at_a_time"] = round(same["completed"] / same["seconds"] / fp64_rate, 3)
     out["timing"] = "host wall clock; latency from submission (arrival) to completion"
+    return out
+
+
+def run_stretched(args, dev):
+    """The stretched workload: 192x128x128 on [0,2.2]x[0,0.41]^2, widths x 1.04 per cell away from a 24-cell band
+    at x = 0.5, a solid cylinder along z, inflow at x = 0, p = 0 outlet at x = 2.2, seeded N(0,1) faces; mixed and
+    plain FP64 to 1e-8, fields device-resident and restored each step, CUDA events."""
+    import torch
+
+    from nereus_cfd_b200 import capi, workloads as W
+    from nereus_cfd_b200.pressure import MACGrid, PressureSolver
+
+    lib = capi.load()
+    case = W.stretched_cylinder_3d(192, 128, 128, seed=3)
+    types = capi.label_cells(case.grid, case.scene)
+    u, v, w = W.face_velocities(case.grid, types, case.seed)
+    td = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to("cuda")
+    orig = [td(u), td(v), td(w), torch.zeros(case.grid.cells, dtype=torch.float64, device="cuda")]
+    work = [t.clone() for t in orig]
+    out = {"workload": "stretched_cylinder_192x128x128", "unknowns": None}
+    for prec in ("mixed", "fp64"):
+        s = PressureSolver(prec, device=dev, **args.solver_opts)
+        s.InitializePressureSolver(MACGrid.from_case(case, types, u, v, w))
+        res = capi.Result()
+        evs = []
+        for k in range(3 + args.stretched_steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for x, y in zip(work, orig):
+                x.copy_(y)
+            capi.check(lib.nereus_b200_project_device(s.ctx, *[t.data_ptr() for t in work], case.rho, case.dt, 0,
+                                                      TOL, ctypes.byref(res)), allow=(0, 1))
+            b.record()
+            if k >= 3:
+                evs.append((a, b))
+        torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        out[prec] = {"value": round(1e3 / statistics.mean(ms), 3), "unit": "solves/s",
+                     "p50_ms": round(percentile(ms, 0.5), 3), "iters_inner": res.iters_inner,
+                     "iters_outer": res.iters_outer, "rel_res": res.rel_res, "steps": len(ms)}
+        out["unknowns"] = res.n
+        s.DestroyPressureSolver()
+    out["speedup_mixed_over_fp64"] = round(out["mixed"]["value"] / out["fp64"]["value"], 3)
     return out
 
 
@@ -510,6 +554,7 @@ def main():
     ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device in the batched form")
     ap.add_argument("--fp64-tanks", type=int, default=4, help="tanks solved one at a time in plain FP64")
     ap.add_argument("--trace", type=int, default=200, help="requests of the serving trace (0: skip)")
+    ap.add_argument("--stretched-steps", type=int, default=5, help="steps of the stretched workload (0: skip)")
     ap.add_argument("--trace-fp64", type=int, default=40, help="trace requests solved one at a time in plain FP64")
     args = ap.parse_args()
     args.solver_opts = {k: int(v) if v.lstrip("-").isdigit() else float(v)

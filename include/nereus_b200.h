@@ -68,6 +68,8 @@ typedef struct nb_options
                             general per-cell kernels */
     int tail_cells;      /* the coarse end runs in one thread block from the first level with at most this many
                             cells (and shared memory for all of them); 0: no such block */
+    int stretched_sweeps; /* red-black sweeps before and after the coarse correction on a stretched grid's levels
+                             (their anisotropy asks for more smoothing); pre_sweeps/post_sweeps apply to uniform ones */
 } nb_options;
 
 typedef struct nb_result

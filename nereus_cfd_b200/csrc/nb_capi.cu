@@ -41,6 +41,7 @@ void nereus_b200_default_options(nb_options *o)
     o->fused_sweeps = 0;
     o->pair_kernels = 1;
     o->tail_cells = 2048;
+    o->stretched_sweeps = 2;
 }
 
 const char *nereus_b200_last_error(void) { return g_error.c_str(); }

@@ -535,7 +535,7 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
         std::vector<LevelView> views;
         for (size_t q = (size_t)l; q < L.size(); q++) views.push_back(L[q].view());
         prof(NB_K_COARSE, 0.0);
-        LaunchTail<T>(views.data(), (int)views.size(), r, e, opt.pre_sweeps, opt.post_sweeps, opt.coarse_sweeps, st);
+        LaunchTail<T>(views.data(), (int)views.size(), r, e, PreSweeps(l), PostSweeps(l), opt.coarse_sweeps, st);
         ProfEnd();
         return;
     }
@@ -559,7 +559,7 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
             return;
         }
     }
-    const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
+    const int pre = PreSweeps(l), post = PostSweeps(l);
     const double half = (3.0 * s + 1.0) / 2.0; // one red-black sweep reads e, r, types and writes e: 3s + 1
     prof(NB_K_SMOOTH0, 2.0 * s + 1.0);
     LaunchSmoothFirst<T>(v, r, e, st);
@@ -612,7 +612,7 @@ void Context::VCyclePairs(int l, float *r, float *e)
     auto prof = [&](int id, double bytesPerCell) {
         ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
     };
-    const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
+    const int pre = PreSweeps(l), post = PostSweeps(l);
     const double half = (3.0 * s + 1.0) / 2.0;
     if (stretched)
     {
@@ -683,7 +683,7 @@ template <typename T> void Context::VCycleFused(int l, T *r, T *e)
     auto prof = [&](int id, double bytesPerCell) {
         ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
     };
-    const int pre = std::max(1, opt.pre_sweeps), post = std::max(1, opt.post_sweeps);
+    const int pre = PreSweeps(l), post = PostSweeps(l);
     T *f = Lv.f<T>(), *res = Lv.res<T>();
     // pre-smoothing: the first sweep from zero (reads r, codes; writes the iterate), the rest in turn, ending in f
     T *dst = (pre % 2 == 1) ? f : e;

@@ -234,6 +234,9 @@ struct Context
     bool StartFrom(const double *guess, double refNorm, double tol, double bn2, double *tolEff);
     template <typename T> void VCycle(int l, T *r, T *e);
     template <typename T> void VCycleFused(int l, T *r, T *e);
+    // red-black sweeps before / after the coarse correction on level l (stretched levels take stretched_sweeps)
+    int PreSweeps(int l) const { return std::max(1, L[l].stretched ? opt.stretched_sweeps : opt.pre_sweeps); }
+    int PostSweeps(int l) const { return std::max(1, L[l].stretched ? opt.stretched_sweeps : opt.post_sweeps); }
     bool FusedLevel(int l) const { return opt.fused_sweeps && dim == 3 && l < tailStart && l + 1 < (int)L.size(); }
     // the FP32 cell-pair kernels serve this level (its du is built)
     bool PairLevel(int l) const { return opt.pair_kernels && L[l].du.p != nullptr; }
