@@ -64,8 +64,10 @@ typedef struct nb_options
     int use_graphs;      /* 1: each CG iteration (V-cycle included) replays one captured CUDA graph; 0: launches */
     int fused_sweeps;    /* 1: 3D levels smooth with one shared-memory tiled launch per red-black sweep, the
                             prolongation and r.z fused in; 0 (default): one launch per colour */
-    int pair_kernels;    /* 1 (default): kernels on cell pairs for 3D levels with Nz even (uniform or stretched),
-                            and the FP64 refinement on uniform 3D grids; 0: the general per-cell kernels */
+    int pair_kernels;    /* FP32 kernels of the mixed form on 3D levels with Nz even (uniform or stretched):
+                            2 (default): the colour-split layout, red and black cells in separate arrays, so that
+                            one colour's sweep moves half the bytes; 1: cell pairs in the grid layout; 0: the
+                            general per-cell kernels */
     int tail_cells;      /* the coarse end runs in one thread block from the first level with at most this many
                             cells (and shared memory for all of them); 0: no such block */
     int stretched_sweeps; /* red-black sweeps before and after the coarse correction on a stretched grid's levels

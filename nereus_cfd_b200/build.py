@@ -26,6 +26,7 @@ SOURCES = {
     "nb_tail.cu": [],
     "nb_fused.cu": [],
     "nb_pairs.cu": [],
+    "nb_split.cu": [],
     "nb_solver.cu": [],
     "nb_capi.cu": [],
     "nb_noalloc.cu": [],

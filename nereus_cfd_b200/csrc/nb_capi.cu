@@ -39,7 +39,7 @@ void nereus_b200_default_options(nb_options *o)
     o->stream = nullptr;
     o->use_graphs = 1;
     o->fused_sweeps = 0;
-    o->pair_kernels = 1;
+    o->pair_kernels = 2;
     o->tail_cells = 2048;
     o->stretched_sweeps = 2;
 }

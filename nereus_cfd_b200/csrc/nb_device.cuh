@@ -41,7 +41,20 @@ struct LevelView
     // the mid axis and marches `slowChunk` steps along the slow axis. 3D: (fast, mid, slow) = (k, j, i);
     // 2D: (j, i, -) with slowLen = 1.
     int fastLen, midLen, slowLen, slowChunk;
+    // Colour-split layout of the level's FP32 vectors (sRS = 0: the grid layout). Cell (i, j, k) of colour
+    // c = (i+j+k) & 1 sits at c*sHalf + i*sPS + j*sRS + (k >> 1): each colour is an Ny x Nx x sRS array whose rows
+    // hold the Nz/2 cells of that colour, padded with zeros to a multiple of 4.
+    int sRS, sPS;
+    long long sHalf;
 };
+
+// Index of cell (i, j, k) in a level vector of the level's layout.
+__device__ __forceinline__ long long VecIdx(const LevelView &v, int i, int j, int k)
+{
+    if (v.sRS)
+        return (long long)((i + j + k) & 1) * v.sHalf + (long long)i * v.sPS + (long long)j * v.sRS + (k >> 1);
+    return (long long)i * v.sI + (long long)j * v.sJ + k;
+}
 
 enum : unsigned { CODE_FLUID_MASK = 0x3Fu, CODE_DIRICHLET = 0x40u, CODE_UNKNOWN = 0x80u };
 
@@ -327,9 +340,10 @@ constexpr int kWarps = kBlock / 32;
 // op 0 = sum, 1 = max.
 // bump: when not null, the last block adds 1 to *bump after storing the totals (the PCG iteration counter, which
 // every block of the launch has read before any block can be the last).
+// addSlot0 >= 0 (sums only): each total also adds out[addSlot0 + s], the totals an earlier launch left there.
 template <int NV>
 __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], int slot0, int op = 0,
-                                           int *bump = nullptr)
+                                           int *bump = nullptr, int addSlot0 = -1)
 {
     __shared__ double sh[NV][32];
     __shared__ bool amLast;
@@ -385,6 +399,7 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
         {
             double t = sh[s][0];
             for (int w = 1; w < nwarp; w++) t = op == 0 ? t + sh[s][w] : fmax(t, sh[s][w]);
+            if (addSlot0 >= 0) t += __ldcg(R.out + addSlot0 + s);
             R.out[slot0 + s] = t;
         }
         if (bump) *bump += 1;

@@ -627,20 +627,22 @@ __global__ void k_residual64(LevelView v, const double *b, const double *xin, co
             int t[6];
             CoefsExact(v, i, j, k, cq);
             const double diag = DiagExact(v, i, j, k, c, cq, t);
-            const double xc = kAdd ? xin[c] + (double)e[c] : xin[c];
+            // e and rOut are level vectors: the grid layout, or the colour-split one of a split level 0
+            const double xc = kAdd ? xin[c] + (double)e[VecIdx(v, i, j, k)] : xin[c];
             double off = 0.0;
             const int nq = v.dim == 3 ? 6 : 4;
             for (int q = 0; q < nq; q++)
                 if (t[q] == FLUID)
                 {
                     const long long n = c + NbrOffset(v, q);
-                    const double xn = kAdd ? xin[n] + (double)e[n] : xin[n];
+                    const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3), nk = k + (q == 4) - (q == 5);
+                    const double xn = kAdd ? xin[n] + (double)e[VecIdx(v, ni, nj, nk)] : xin[n];
                     off += cq[q] * xn;
                 }
             const double ax = scale * (off + diag * xc);
             const double r = b[c] - ax;
             if (kAdd) xout[c] = xc;
-            rOut[c] = (T)(r * sfac);
+            rOut[VecIdx(v, i, j, k)] = (T)(r * sfac);
             acc[0] += r * r;
             acc[1] += r;
         }

@@ -60,9 +60,12 @@ constexpr int kMaxTailLevels = 8;
 constexpr size_t kTailMaxSmem = 200 * 1024;
 template <typename T> size_t TailSmemBytes(const LevelView *levels, int nlev);
 template <typename T> bool PrepareTail(size_t bytes);
+// the per-colour lists of the tail levels' unknowns (once per layout): TailListEntries entries, 2 * nlev counts
+long long TailListEntries(const LevelView *levels, int nlev);
+void LaunchTailLists(const LevelView *levels, int nlev, unsigned *lists, int *counts, cudaStream_t st);
 template <typename T>
 void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pre, int post, int coarseSweeps,
-                cudaStream_t st);
+                const unsigned *lists, const int *counts, cudaStream_t st);
 
 // ---- nb_pairs.cu: FP32 kernels for 3D levels of a uniform grid with Nz even (cell pairs, unmasked stencil) ----
 bool PairLevelShape(const LevelView &v);
@@ -96,6 +99,32 @@ void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,
                  const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int slotN, int singular,
                  int slotPQ, int slotRR, cudaStream_t st);
+
+// ---- nb_split.cu: FP32 kernels for 3D levels with Nz even in the colour-split layout (LevelView::sRS) ----
+// du: the level's bytes in that layout (diagonal units; the codes on a stretched level); pext: the red cells' bytes
+void LaunchSplitBytes(const LevelView &v, const uint8_t *in, uint8_t *out, cudaStream_t st);
+// the first red-black sweep from a zero iterate (a stretched level: its red half; the black half follows)
+void LaunchSplitFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st);
+void LaunchSplitHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st);
+// the post-smoothing's last sweep on level 0: the black half (last = false) sums its (r.z, z, r) into
+// out[partSlot..], the red half (last = true) adds its own into the scalar block of the iteration's parity
+void LaunchSplitHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, bool last,
+                        const Reducer &R, const int *it, int baseEven, int baseOdd, int partSlot, cudaStream_t st);
+// the red residual after a sweep that ended black (into the first half of res)
+void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
+                         cudaStream_t st);
+void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
+                        float *eFine, cudaStream_t st);
+void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
+                         float *rCoarse, cudaStream_t st);
+void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
+                       const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
+                       int singular, int slotPQ, cudaStream_t st);
+void LaunchSplitScaleSum(const LevelView &v, const double *b, float *r, double sfac, const Reducer &R, int slot,
+                         cudaStream_t st);
+void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
+                         double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
+                         cudaStream_t st);
 
 // ---- nb_kernels.cu: multigrid and PCG kernels, T = float (inner solve) or double (plain FP64) ----
 void LaunchBuildCodes(const LevelView &v, uint8_t *code, cudaStream_t st);

@@ -52,7 +52,8 @@ __global__ void k_build_du(LevelView v, uint8_t *du)
         const long long rr = c / v.Nz;
         const int j = (int)(rr % v.Nx), i = (int)(rr / v.Nx);
         const bool interior = i > 0 && i < v.Ny - 1 && j > 0 && j < v.Nx - 1 && k > 0 && k < v.Nz - 1;
-        if (!interior || v.types[c] != FLUID) { du[c] = 0; continue; }
+        const long long o = VecIdx(v, i, j, k); // the grid layout, or the colour-split one of a split level
+        if (!interior || v.types[c] != FLUID) { du[o] = 0; continue; }
         unsigned units = 0;
         for (int q = 0; q < 6; q++)
         {
@@ -64,7 +65,7 @@ __global__ void k_build_du(LevelView v, uint8_t *du)
                 units += OnRing(v, ni, nj, nk) ? 4 : 2;
             }
         }
-        du[c] = (uint8_t)(0x80u | units);
+        du[o] = (uint8_t)(0x80u | units);
     }
 }
 
@@ -445,6 +446,7 @@ void LaunchPairResidual(const LevelView &v, const uint8_t *du, const float *r, c
 // Per fine cell: 0x80 for an unknown, plus in the low six bits the weight (in 1/64) that the Neumann-aware
 // prolongation moves from the cell's SOLID coarse contributors onto its parent. Coarse vectors are zero at SOLID
 // cells, so P e_c at a fine unknown = the plain trilinear sum + extra/64 * e_c[parent], and R = P^T.
+// A colour-split fine level keeps the red cells' bytes only (its transfers run over the red cells).
 __global__ void k_build_pext(LevelView fv, LevelView cv, uint8_t *pext)
 {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < fv.cells;
@@ -453,8 +455,10 @@ __global__ void k_build_pext(LevelView fv, LevelView cv, uint8_t *pext)
         const int d = (int)(c % fv.Nz);
         const long long rr = c / fv.Nz;
         const int b = (int)(rr % fv.Nx), a = (int)(rr / fv.Nx);
+        if (fv.sRS && ((a + b + d) & 1)) continue;
+        const long long o = VecIdx(fv, a, b, d);
         const bool interior = a > 0 && a < fv.Ny - 1 && b > 0 && b < fv.Nx - 1 && d > 0 && d < fv.Nz - 1;
-        if (!interior || fv.types[c] != FLUID) { pext[c] = 0; continue; }
+        if (!interior || fv.types[c] != FLUID) { pext[o] = 0; continue; }
         const int A = (a + 1) >> 1, B = (b + 1) >> 1, D = (d + 1) >> 1;
         const int si = (a & 1) ? -1 : 1, sj = (b & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
         const int w[2] = {3, 1};
@@ -468,7 +472,7 @@ __global__ void k_build_pext(LevelView fv, LevelView cv, uint8_t *pext)
                                          (D + dk * sk);
                     if (cv.types[cc] == SOLID) extra += (unsigned)(w[di] * w[dj] * w[dk]);
                 }
-        pext[c] = (uint8_t)(0x80u | extra);
+        pext[o] = (uint8_t)(0x80u | extra);
     }
 }
 

@@ -54,6 +54,9 @@ LevelView LevelData::view() const
     }
     v.code = code.p;
     v.types = types.p;
+    v.sRS = sRS;
+    v.sPS = sPS;
+    v.sHalf = sHalf;
     v.stretched = stretched ? 1 : 0;
     v.gamma = gamma;
     for (int a = 0; a < 3; a++)
@@ -170,7 +173,6 @@ void Context::BuildHierarchy()
         LaunchBuildCodes(C.view(), C.code.p, st);
         L.push_back(std::move(C));
     }
-    BuildPairData();
     NB_CK(cudaGetLastError());
     // The tail: the first level from which every coarser level has at most opt.tail_cells cells and all of them fit
     // in one block's shared memory in the solver's precision.
@@ -192,22 +194,60 @@ void Context::BuildHierarchy()
         const bool ok = mixed ? PrepareTail<float>(kTailMaxSmem) : PrepareTail<double>(kTailMaxSmem);
         if (!ok) tailStart = (int)L.size();
     }
+    AssignSplit();
+    BuildPairData();
+    BuildTailLists();
+    NB_CK(cudaGetLastError());
     if (mixed) PrepareSweeps<float>();
     else PrepareSweeps<double>();
     cudaGetLastError(); // an attribute the device refuses leaves the per-colour path, checked at launch
 }
 
-// The per-level bytes of the cell-pair kernels: diagonal units and the prolongation's moved weights.
+// The colour-split levels (pair_kernels = 2, mixed precision): the 3D levels with Nz even above the coarse end, as
+// long as every finer level is one too (a level's transfers read and write the next coarser level in either layout,
+// the grid-layout kernels only the grid layout).
+void Context::AssignSplit()
+{
+    const bool on = opt.precision == NB_PRECISION_MIXED && opt.pair_kernels == 2 && !opt.fused_sweeps;
+    bool finer = true;
+    for (size_t l = 0; l < L.size(); l++)
+    {
+        LevelData &Lv = L[l];
+        Lv.sRS = Lv.sPS = 0;
+        Lv.sHalf = 0;
+        const bool s = on && finer && (int)l < tailStart && l + 1 < L.size() && PairLevelShape(Lv.view());
+        if (s)
+        {
+            Lv.sRS = ((Lv.Nz / 2) + 3) & ~3;
+            Lv.sPS = Lv.Nx * Lv.sRS;
+            Lv.sHalf = ((long long)Lv.Ny * Lv.sPS + 63) & ~63LL; // each colour starts 256-byte aligned
+        }
+        finer = s;
+    }
+}
+
+// The per-level bytes of the cell-pair and colour-split kernels: diagonal units (codes on a stretched split level)
+// and the prolongation's moved weights.
 void Context::BuildPairData()
 {
-    // the FP32 cell-pair kernels' diagonal units (mixed precision: the inner solve runs in FP32)
+    // the FP32 kernels' diagonal units (mixed precision: the inner solve runs in FP32)
     for (auto &Lv : L)
     {
         const LevelView v = Lv.view();
         if (opt.precision == NB_PRECISION_MIXED && opt.pair_kernels && PairLevelShape(v))
         {
-            Lv.du.alloc((size_t)Lv.cells);
-            LaunchBuildDu(v, Lv.du.p, st);
+            if (Lv.sRS)
+            {
+                Lv.du.alloc((size_t)(2 * Lv.sHalf));
+                Lv.du.zero(st); // the padding
+                if (v.stretched) LaunchSplitBytes(v, Lv.code.p, Lv.du.p, st);
+                else LaunchBuildDu(v, Lv.du.p, st);
+            }
+            else
+            {
+                Lv.du.alloc((size_t)Lv.cells);
+                LaunchBuildDu(v, Lv.du.p, st);
+            }
         }
         else Lv.du.release();
     }
@@ -215,7 +255,12 @@ void Context::BuildPairData()
     {
         if (L[l].du.p && l + 1 < L.size())
         {
-            L[l].pext.alloc((size_t)L[l].cells);
+            if (L[l].sRS)
+            {
+                L[l].pext.alloc((size_t)L[l].sHalf);
+                L[l].pext.zero(st);
+            }
+            else L[l].pext.alloc((size_t)L[l].cells);
             LaunchBuildPext(L[l].view(), L[l + 1].view(), L[l].pext.p, st);
         }
         else L[l].pext.release();
@@ -234,7 +279,24 @@ void Context::RefillHierarchy()
         LaunchBuildCodes(L[l].view(), L[l].code.p, st);
     }
     BuildPairData();
+    BuildTailLists();
     NB_CK(cudaGetLastError());
+}
+
+// The tail levels' lists of unknowns by colour (they follow the cell types).
+void Context::BuildTailLists()
+{
+    if (tailStart >= (int)L.size())
+    {
+        tailLists.release();
+        tailCounts.release();
+        return;
+    }
+    std::vector<LevelView> views;
+    for (size_t q = (size_t)tailStart; q < L.size(); q++) views.push_back(L[q].view());
+    tailLists.alloc((size_t)TailListEntries(views.data(), (int)views.size()));
+    tailCounts.alloc(2 * kMaxTailLevels);
+    LaunchTailLists(views.data(), (int)views.size(), tailLists.p, tailCounts.p, st);
 }
 
 void Context::AllocVectors()
@@ -248,9 +310,10 @@ void Context::AllocVectors()
         const bool fused = FusedLevel((int)l);
         if (mixed)
         {
-            Lv.r32.alloc(c); Lv.r32.zero(st);
-            Lv.e32.alloc(c); Lv.e32.zero(st);
-            if (!last) { Lv.res32.alloc(c); Lv.res32.zero(st); }
+            const size_t c32 = Lv.VecLen(); // zeroed whole: the split layout's padding stays zero
+            Lv.r32.alloc(c32); Lv.r32.zero(st);
+            Lv.e32.alloc(c32); Lv.e32.zero(st);
+            if (!last) { Lv.res32.alloc(c32); Lv.res32.zero(st); }
             if (fused) { Lv.f32.alloc(c); Lv.f32.zero(st); } else Lv.f32.release();
             Lv.r64.release(); Lv.e64.release(); Lv.res64.release(); Lv.f64.release();
         }
@@ -269,9 +332,10 @@ void Context::AllocVectors()
     xb.alloc(c); xb.zero(st);
     if (mixed)
     {
-        for (auto &a : p32) { a.alloc(c); a.zero(st); }
-        q32.alloc(c); q32.zero(st);
-        x32.alloc(c); x32.zero(st);
+        const size_t c32 = VecLen0();
+        for (auto &a : p32) { a.alloc(c32); a.zero(st); }
+        q32.alloc(c32); q32.zero(st);
+        x32.alloc(c32); x32.zero(st);
         for (auto &a : p64) a.release();
         q64.release();
     }
@@ -535,7 +599,8 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
         std::vector<LevelView> views;
         for (size_t q = (size_t)l; q < L.size(); q++) views.push_back(L[q].view());
         prof(NB_K_COARSE, 0.0);
-        LaunchTail<T>(views.data(), (int)views.size(), r, e, PreSweeps(l), PostSweeps(l), opt.coarse_sweeps, st);
+        LaunchTail<T>(views.data(), (int)views.size(), r, e, PreSweeps(l), PostSweeps(l), opt.coarse_sweeps,
+                      tailLists.p, tailCounts.p, st);
         ProfEnd();
         return;
     }
@@ -553,6 +618,11 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
     }
     if constexpr (std::is_same<T, float>::value)
     {
+        if (Split(l))
+        {
+            VCycleSplit(l, r, e);
+            return;
+        }
         if (PairLevel(l))
         {
             VCyclePairs(l, r, e);
@@ -670,6 +740,70 @@ void Context::VCyclePairs(int l, float *r, float *e)
         }
 }
 
+// The V-cycle on a colour-split level (nb_split.cu): the first sweep from zero (one launch on a uniform level, a red
+// and a black one on a stretched level), further sweeps one colour per launch, the residual and the transfers on the
+// red cells (the black residual after a black half-sweep is zero; the post-smoothing's black half replaces the black
+// values without reading them), and on level 0 the (r.z, z, r) sums of the last sweep, black then red.
+void Context::VCycleSplit(int l, float *r, float *e)
+{
+    LevelData &Lv = L[l];
+    const LevelView v = Lv.view();
+    const bool stretched = v.stretched != 0;
+    const double s = sizeof(float), cells = (double)Lv.cells;
+    auto prof = [&](int id, double bytesPerCell) {
+        ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
+    };
+    const int pre = PreSweeps(l), post = PostSweeps(l);
+    // one colour: reads the other colour, and r and the bytes of its own; writes its own
+    const double half = (3.0 * s + 1.0) / 2.0;
+    const uint8_t *du = Lv.du.p;
+    if (stretched)
+    {
+        prof(NB_K_SMOOTH0, (2.0 * s + 1.0) / 2.0); // red from zero: reads r and the bytes of red, writes red
+        LaunchSplitFirst(v, du, r, e, st);
+        ProfEnd();
+        prof(NB_K_SMOOTH0, half);
+        LaunchSplitHalf(v, du, r, e, 1, st);
+        ProfEnd();
+    }
+    else
+    {
+        prof(NB_K_SMOOTH0, 2.0 * s + 1.0); // reads r and the bytes, writes e
+        LaunchSplitFirst(v, du, r, e, st);
+        ProfEnd();
+    }
+    for (int q = 1; q < pre; q++)
+        for (int c = 0; c < 2; c++)
+        {
+            prof(NB_K_SMOOTH0, half);
+            LaunchSplitHalf(v, du, r, e, c, st);
+            ProfEnd();
+        }
+    float *res = Lv.res<float>();
+    prof(NB_K_RESIDUAL0, (4.0 * s + 1.0) / 2.0); // reads e, and r and the bytes of red; writes red
+    LaunchSplitResidual(v, du, r, e, res, st);
+    ProfEnd();
+    LevelData &Lc = L[l + 1];
+    const LevelView vc = Lc.view();
+    prof(NB_K_RESTRICT0, (s + 1.0) / 2.0 + s / 8.0);
+    LaunchSplitRestrict(v, vc, Lv.pext.p, res, Lc.r<float>(), st);
+    ProfEnd();
+    VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
+    prof(NB_K_PROLONG0, s + 0.5 + s / 8.0); // reads and writes red e, reads the red bytes and the coarse e
+    LaunchSplitProlong(v, vc, Lv.pext.p, Lc.e<float>(), e, st);
+    ProfEnd();
+    for (int q = 0; q < post; q++)
+        for (int c = 1; c >= 0; c--)
+        {
+            prof(NB_K_SMOOTH0, half);
+            if (l == 0 && q + 1 == post) // z is final: r.z for CG here (IterBody skips its own)
+                LaunchSplitHalfDot(v, du, r, e, c, c == 0, red, iter.p, S_RZ0, S_RZ1, S_RZB, st);
+            else
+                LaunchSplitHalf(v, du, r, e, c, st);
+            ProfEnd();
+        }
+}
+
 // The V-cycle on a 3D level with one launch per red-black sweep (nb_fused.cu): the pre-smoothing from zero into f,
 // the residual and its restriction, the coarser levels, then the post-smoothing that reads f + P(e_coarse) and
 // writes e. On level 0 the last sweep also sums r.z for CG (IterBody then skips its own r.z launch).
@@ -731,6 +865,18 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
     VCycle<T>(0, r, z);
     if constexpr (std::is_same<T, float>::value)
     {
+        if (Split(0)) // r.z came with the V-cycle's last sweep
+        {
+            ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
+            LaunchSplitPApply(v0, L[0].du.p, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, st);
+            ProfEnd();
+            ProfBegin(NB_K_XR, 6.0 * s * cells);
+            LaunchLinXR((long long)VecLen0(), x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ,
+                        S_RR, st);
+            ProfEnd();
+            NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+            return;
+        }
         if (PairLevel(0))
         {
             // r.z came with the V-cycle's last sweep unless level 0 is itself the coarse end (tail or single level)
@@ -769,7 +915,7 @@ template <typename T>
 int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
                     double *rrEnd)
 {
-    NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * Cells(), st));
+    NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * VecLen0(), st));
     NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
     IterGraph *G = nullptr;
     if (opt.use_graphs)
@@ -850,7 +996,8 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
     xa.zero(st);
     float *r32 = L[0].r32.p, *z32 = L[0].e32.p;
     ProfBegin(NB_K_REFINE, (8.0 + 4.0) * (double)Cells());
-    LaunchScaleSum<float>(L[0].cells, b.p, r32, sfac, red, S_RES, st); // the residual of x = 0
+    if (Split(0)) LaunchSplitScaleSum(v0, b.p, r32, sfac, red, S_RES, st); // the residual of x = 0
+    else LaunchScaleSum<float>(L[0].cells, b.p, r32, sfac, red, S_RES, st);
     ProfEnd();
     const double bn2 = ReadSlot(S_RES);
     out->b_norm = std::sqrt(bn2);
@@ -879,7 +1026,9 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
             inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0,
                                    rr0 * opt.inner_tol * opt.inner_tol, std::max(1, opt.max_iters), false, &rrEnd);
             ProfBegin(NB_K_REFINE, (8.0 + 4.0 + 8.0 + 1.0 + 8.0 + 4.0) * (double)Cells());
-            if (PairLevel(0) && !nonuniform && dim == 3)
+            if (Split(0) && !nonuniform)
+                LaunchSplitRefine64(v0, L[0].du.p, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);
+            else if (PairLevel(0) && !nonuniform && dim == 3)
                 LaunchPairRefine64(v0, L[0].du.p, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);
             else
                 LaunchRefine64<float>(v0, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);

@@ -83,7 +83,8 @@ enum : int
     S_SUM = 10,  // compensated sum (sum, carry)
     S_DIV = 12,
     S_NUNK = 14, // the count of unknowns, read by the CG kernels on the device
-    S_COUNT = 16
+    S_RZB = 16,  // (r.z, sum z, sum r) of the black cells, summed by the black half of the last sweep
+    S_COUNT = 20
 };
 
 struct LevelData
@@ -96,8 +97,14 @@ struct LevelData
     DevArray<double> dw[3], dg[3];
     DevArray<float> dw32[3], dig32[3];
     DevArray<uint8_t> types, code;
-    DevArray<uint8_t> du;                 // diagonal units for the pair kernels (nb_pairs.cu); empty elsewhere
+    DevArray<uint8_t> du;                 // diagonal units for the pair kernels (nb_pairs.cu); empty elsewhere.
+                                          // Colour-split level: in that layout, and the codes on a stretched level
     DevArray<uint8_t> pext;               // unknown flag + moved prolongation weight toward the next coarser level
+                                          // (colour-split level: the red cells only)
+    // the colour-split layout of the FP32 vectors (nb_split.cu); sRS = 0: the grid layout
+    int sRS = 0, sPS = 0;
+    long long sHalf = 0;
+    size_t VecLen() const { return sRS ? (size_t)(2 * sHalf) : (size_t)cells; }
     DevArray<float> r32, e32, res32, f32; // f: the pre-smoothed iterate of a fused V-cycle
     DevArray<double> r64, e64, res64, f64;
     LevelView view() const;
@@ -123,6 +130,8 @@ struct Context
     std::vector<double> wt[3], gt[3];
     std::vector<LevelData> L;
     int tailStart = 0;                       // levels from here down run in one shared-memory block (nb_tail.cu)
+    DevArray<unsigned> tailLists;            // the tail levels' per-colour lists of unknowns (built per layout)
+    DevArray<int> tailCounts;
     DevArray<int32_t> idp;
     bool idpValid = false; // the numbering is made when first asked for (GetIdp, ExportMatrix, SolveLaplacian, Rhs)
     int n = 0;
@@ -240,7 +249,14 @@ struct Context
     bool FusedLevel(int l) const { return opt.fused_sweeps && dim == 3 && l < tailStart && l + 1 < (int)L.size(); }
     // the FP32 cell-pair kernels serve this level (its du is built)
     bool PairLevel(int l) const { return opt.pair_kernels && L[l].du.p != nullptr; }
+    // the FP32 vectors of this level are colour-split and its V-cycle runs the split kernels
+    bool Split(int l) const { return L[l].sRS != 0; }
+    // FP32 elements of a level-0 vector (the split layout pads its rows)
+    size_t VecLen0() const { return L[0].VecLen(); }
     void VCyclePairs(int l, float *r, float *e);
+    void VCycleSplit(int l, float *r, float *e);
+    void AssignSplit();
+    void BuildTailLists();
     template <typename T> void IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact);
     template <typename T>
     int RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,

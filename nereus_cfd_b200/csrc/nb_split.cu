@@ -1,0 +1,842 @@
+// Multigrid and PCG kernels for 3D FP32 levels in the colour-split layout (the inner solve of the mixed-precision
+// form), built so that each red-black half-sweep moves only the bytes the algorithm needs.
+//
+// Colour-split layout. Cell (i, j, k) has colour c = (i + j + k) & 1 and sits at c*H + i*PS + j*RS + (k >> 1) of a
+// level vector: each colour is an Ny x Nx x RS array whose rows hold the Nz/2 cells of that colour (RS = Nz/2
+// rounded up to 4, the padding kept at zero). In row (i, j) the cell of colour c at element m is k = 2m + q with
+// q = (i + j + c) & 1, and its six neighbours all have the other colour:
+//   (i +- 1, j, m), (i, j +- 1, m), (i, j, m) and (i, j, m + (q ? 1 : -1)).
+// A half-sweep of colour c therefore reads the other colour, r and the diagonal bytes of colour c, and writes
+// colour c: half of every array, where a cell-pair sweep reads and writes both colours.
+//
+// Quads. Thread t of a launch takes the four elements 4t .. 4t+3 of a plane of one colour (RS is a multiple of 4, so
+// a quad never crosses a row) and marches along i over up to kPairS planes, keeping planes i-1, i, i+1 in
+// registers. The j neighbours are the quads RS elements away; the element across the quad's edge comes from the
+// neighbouring lane (a shuffle; lanes 0 and 31 load it).
+//
+// Every vector is zero off the unknowns (and on the padding), so the neighbour sum runs over all six neighbours.
+// On a uniform level the coefficient is gamma everywhere and the diagonal is gamma/2 times the unit count in the
+// level's byte array (0x80 | units, 0 off the unknowns), divided through a 32-entry reciprocal table; on a
+// stretched level the byte array holds the cell codes and the coefficients come from the level's tables.
+//
+// The V-cycle on these levels (nb_solver.cu, VCycleSplit) uses two facts of red-black Gauss-Seidel:
+// - after a black half-sweep the black residual is zero (each black equation was just solved), so the residual and
+//   its restriction run over the red cells only;
+// - a black half-sweep does not read the black values it replaces, so the prolonged coarse correction is added to
+//   the red cells only before the post-smoothing, which starts black.
+#include "nb_kernels.h"
+
+namespace nb
+{
+
+namespace
+{
+
+struct F4
+{
+    float v[4];
+};
+
+__device__ __forceinline__ F4 L4(const float *p)
+{
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    return F4{{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ void S4(float *p, const F4 &a)
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(a.v[0], a.v[1], a.v[2], a.v[3]);
+}
+__device__ __forceinline__ unsigned LdU4(const uint8_t *p) { return *reinterpret_cast<const unsigned *>(p); }
+__device__ __forceinline__ unsigned Byte(unsigned d, int x) { return (d >> (8 * x)) & 0xFFu; }
+__device__ __forceinline__ float Unk(unsigned b) { return (b & 0x80u) ? 1.0f : 0.0f; }
+
+// 1 / (gamma/2 * units), entry 0 = 0
+__device__ __forceinline__ void FillInv(float *inv, double gamma)
+{
+    if (threadIdx.x < 32) inv[threadIdx.x] = threadIdx.x ? 1.0f / (0.5f * (float)gamma * (float)threadIdx.x) : 0.0f;
+    __syncthreads();
+}
+
+// Per-thread position of a quad kernel.
+struct QuadPos
+{
+    int lane;
+    bool valid;  // false for the clamped threads past the plane's last quad (they still load and shuffle)
+    int i0, i1;  // planes [i0, i1)
+    int j, m0;   // row and first element of the quad
+    int RS, PS;
+    long long off; // element of the quad on plane i0, within one colour
+};
+
+__device__ __forceinline__ QuadPos QuadStart(const LevelView &v)
+{
+    QuadPos p;
+    const int Q = v.sRS >> 2, nq = v.Nx * Q;
+    p.lane = threadIdx.x & 31;
+    int t = blockIdx.x * kPairThreads + threadIdx.x;
+    p.valid = t < nq;
+    if (!p.valid) t = nq - 1;
+    // grid.y splits the Ny-2 interior planes into chunks of S (the host sized it); a block past the last plane starts
+    // at the ring plane and marches none
+    const int S = (v.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
+    p.i0 = min(1 + (int)blockIdx.y * S, v.Ny - 1);
+    p.i1 = min(p.i0 + S, v.Ny - 1);
+    p.RS = v.sRS;
+    p.PS = v.sPS;
+    p.j = t / Q;
+    p.m0 = 4 * (t - p.j * Q);
+    p.off = (long long)p.i0 * v.sPS + 4LL * t;
+    return p;
+}
+
+// The launch grid of a quad kernel: planes per thread (1 .. kQuadMaxS) so that a launch has about `target` blocks.
+// The sweeps march far (each plane of the other colour is loaded once per chunk of planes, plus the two planes either
+// side); the kernels with more registers per thread take shorter chunks, so that their launches still fill several
+// waves of the 148 SMs.
+constexpr int kQuadMaxS = 16;
+constexpr long long kQuadBlocksSweep = 148 * 4; // first sweep, half-sweeps, residual (measured: 4 beats 8 and 16)
+constexpr long long kQuadBlocksOther = 148 * 8; // direction update and apply, prolongation (8 beats 24 and 48)
+
+inline dim3 QuadGrid(const LevelView &v, long long target)
+{
+    const long long nq = (long long)v.Nx * (v.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
+    const long long planes = v.Ny - 2 > 0 ? v.Ny - 2 : 1;
+    long long S = (planes * perPlane + target - 1) / target;
+    S = S < 1 ? 1 : (S > kQuadMaxS ? kQuadMaxS : S);
+    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
+}
+
+// The other colour's k neighbours of a quad: the element at m (c) and the one at m + (q ? 1 : -1) (returned).
+__device__ __forceinline__ F4 KShift(const F4 &c, float prevW, float nextX, int q)
+{
+    return q ? F4{{c.v[1], c.v[2], c.v[3], nextX}} : F4{{prevW, c.v[0], c.v[1], c.v[2]}};
+}
+
+// The elements just before and after this lane's quad in its row (0 past the row's ends; the values a lane takes
+// from a neighbouring row only reach ring or padding cells, whose results are masked).
+__device__ __forceinline__ void Edges(const QuadPos &P, const F4 &c, const float *row, float &prevW, float &nextX)
+{
+    prevW = __shfl_up_sync(0xffffffffu, c.v[3], 1);
+    nextX = __shfl_down_sync(0xffffffffu, c.v[0], 1);
+    if (P.lane == 0) prevW = P.m0 > 0 ? row[-1] : 0.f;
+    if (P.lane == 31) nextX = P.m0 + 4 < P.RS ? row[4] : 0.f;
+}
+
+// sum_q c_q x_q over the six neighbours of unknown cell (i, j, k) of a stretched level, and its diagonal
+__device__ __forceinline__ float StencilSum(const LevelView &v, int i, int j, int k, unsigned code, float nP, float nM,
+                                            float nJp, float nJm, float nKp, float nKm, float &diag)
+{
+    float cq[6];
+    const long long c = (long long)i * v.sI + (long long)j * v.sJ + k;
+    CodeStencil<float>(v, i, j, k, c, code, cq, diag);
+    return ((cq[0] * nP + cq[1] * nM) + (cq[2] * nJp + cq[3] * nJm)) + (cq[4] * nKp + cq[5] * nKm);
+}
+
+} // namespace
+
+// planes per thread at least in the pair-thread launches that end in a grid-wide sum
+constexpr int kSplitReduceS = 16;
+
+// ---------------------------------------------------------------------------------------------------------------
+// level bytes
+// ---------------------------------------------------------------------------------------------------------------
+// Scatter per-cell bytes (a level's codes) into the colour-split layout; `out` was zeroed (the padding stays 0).
+__global__ void k_split_bytes(LevelView v, const uint8_t *__restrict__ in, uint8_t *__restrict__ out)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < v.cells;
+         c += (long long)gridDim.x * blockDim.x)
+    {
+        const int k = (int)(c % v.Nz);
+        const long long rr = c / v.Nz;
+        const int j = (int)(rr % v.Nx), i = (int)(rr / v.Nx);
+        out[VecIdx(v, i, j, k)] = in[c];
+    }
+}
+
+void LaunchSplitBytes(const LevelView &v, const uint8_t *in, uint8_t *out, cudaStream_t st)
+{
+    int blocks = (int)((v.cells + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    NB_COUNT_LAUNCH();
+    k_split_bytes<<<blocks, 256, 0, st>>>(v, in, out);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// smoothing
+// ---------------------------------------------------------------------------------------------------------------
+
+// The first red-black sweep from a zero iterate on a uniform level, one launch: red e = r / diag, then black
+// e = (r + gamma * sum of the red neighbours) / diag with the red neighbours formed from r and the bytes. A thread
+// owns one quad position and writes the red and the black quad there.
+__global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const uint8_t *__restrict__ du,
+                                                              const float *__restrict__ r, float *__restrict__ e)
+{
+    __shared__ float inv[32];
+    FillInv(inv, v.gamma);
+    const QuadPos P = QuadStart(v);
+    const float g = (float)v.gamma;
+    const long long hb = v.sHalf;
+    const float *R0 = r + P.off, *R1 = r + hb + P.off;
+    const uint8_t *D0 = du + P.off, *D1 = du + hb + P.off;
+    float *X0 = e + P.off, *X1 = e + hb + P.off;
+    auto red = [&](long long o) {
+        F4 a = L4(R0 + o);
+        const unsigned d = LdU4(D0 + o);
+#pragma unroll
+        for (int x = 0; x < 4; x++) a.v[x] *= inv[Byte(d, x) & 0x7Fu];
+        return a;
+    };
+    auto red1 = [&](long long o) { return R0[o] * inv[D0[o] & 0x7Fu]; };
+    F4 RM = red(-P.PS), RC = red(0);
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i++, o += P.PS)
+    {
+        const F4 RP = red(o + P.PS), RJp = red(o + P.RS), RJm = red(o - P.RS);
+        const F4 rb = L4(R1 + o);
+        const unsigned db = LdU4(D1 + o);
+        float prevW = __shfl_up_sync(0xffffffffu, RC.v[3], 1), nextX = __shfl_down_sync(0xffffffffu, RC.v[0], 1);
+        if (P.lane == 0) prevW = P.m0 > 0 ? red1(o - 1) : 0.f;
+        if (P.lane == 31) nextX = P.m0 + 4 < P.RS ? red1(o + 4) : 0.f;
+        const F4 sh = KShift(RC, prevW, nextX, (i + P.j + 1) & 1);
+        F4 nb;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+        {
+            const float s = ((RP.v[x] + RM.v[x]) + (RJp.v[x] + RJm.v[x])) + (RC.v[x] + sh.v[x]);
+            nb.v[x] = (rb.v[x] + g * s) * inv[Byte(db, x) & 0x7Fu];
+        }
+        if (P.valid)
+        {
+            S4(X0 + o, RC);
+            S4(X1 + o, nb);
+        }
+        RM = RC;
+        RC = RP;
+    }
+}
+
+// One colour of a red-black sweep: e_c = (r_c + sum_q c_q e_q) / diag_c over the other colour's neighbours.
+// kSt: a stretched level (du holds the codes). kFirst (stretched only): the red pass from a zero iterate, r / diag.
+// kDot 1: (sum r.e, sum e, sum r) of this colour into out[partSlot..]; kDot 2: the same plus the totals already in
+// out[partSlot..], into the scalar block of the iteration's parity (the CG's r.z, sum z, sum r of the V-cycle's z).
+// du, r: this colour's halves; eo, ec: the other colour's and this colour's halves of e (disjoint).
+template <int kDot, bool kSt, bool kFirst>
+__global__ void __launch_bounds__(kPairThreads)
+    k_split_half(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ r,
+                 const float *__restrict__ eo, float *__restrict__ ec, int colour, Reducer R, const int *it,
+                 int baseEven, int baseOdd, int partSlot)
+{
+    float facc[3] = {0.f, 0.f, 0.f}; // a thread's terms in FP32, the block and grid sums in FP64
+    __shared__ float inv[32];
+    if (!kSt) FillInv(inv, v.gamma);
+    const QuadPos P = QuadStart(v);
+    const float g = (float)v.gamma;
+    const float *O = eo + P.off;
+    const float *Rr = r + P.off;
+    const uint8_t *D = du + P.off;
+    float *C = ec + P.off;
+    // the next plane's streamed values are loaded one iteration ahead
+    F4 oM{}, oC{}, oP{}, rr{};
+    unsigned d = 0;
+    if (P.i0 < P.i1)
+    {
+        rr = L4(Rr);
+        d = LdU4(D);
+        if (!kFirst)
+        {
+            oM = L4(O - P.PS);
+            oC = L4(O);
+            oP = L4(O + P.PS);
+        }
+    }
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i++, o += P.PS)
+    {
+        F4 oPn{}, rrn{};
+        unsigned dn = 0;
+        if (i + 1 < P.i1)
+        {
+            if (!kFirst) oPn = L4(O + o + 2 * P.PS);
+            rrn = L4(Rr + o + P.PS);
+            dn = LdU4(D + o + P.PS);
+        }
+        F4 oJp{}, oJm{}, sh{};
+        const int q = (i + P.j + colour) & 1;
+        if (!kFirst)
+        {
+            oJp = L4(O + o + P.RS);
+            oJm = L4(O + o - P.RS);
+            float prevW, nextX;
+            Edges(P, oC, O + o, prevW, nextX);
+            sh = KShift(oC, prevW, nextX, q);
+        }
+        F4 nv;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+        {
+            const unsigned b = Byte(d, x);
+            if (!kSt)
+            {
+                const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
+                nv.v[x] = (rr.v[x] + g * s) * inv[b & 0x7Fu];
+            }
+            else
+            {
+                nv.v[x] = 0.f;
+                if (b & CODE_UNKNOWN)
+                {
+                    const int k = 2 * (P.m0 + x) + q;
+                    float diag, s = 0.f;
+                    if (kFirst)
+                    {
+                        float cq[6];
+                        const long long c = (long long)i * v.sI + (long long)P.j * v.sJ + k;
+                        CodeStencil<float>(v, i, P.j, k, c, b, cq, diag);
+                    }
+                    else
+                    {
+                        const float kp = q ? sh.v[x] : oC.v[x], km = q ? oC.v[x] : sh.v[x];
+                        s = StencilSum(v, i, P.j, k, b, oP.v[x], oM.v[x], oJp.v[x], oJm.v[x], kp, km, diag);
+                    }
+                    nv.v[x] = diag != 0.f ? (rr.v[x] + s) / diag : 0.f;
+                }
+            }
+        }
+        if (P.valid)
+        {
+            S4(C + o, nv);
+            if (kDot)
+            {
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+                {
+                    facc[0] += rr.v[x] * nv.v[x];
+                    facc[1] += nv.v[x];
+                    facc[2] += rr.v[x];
+                }
+            }
+        }
+        if (!kFirst)
+        {
+            oM = oC;
+            oC = oP;
+            oP = oPn;
+        }
+        rr = rrn;
+        d = dn;
+    }
+    if (kDot == 1)
+    {
+        double acc[3] = {facc[0], facc[1], facc[2]};
+        GridReduce<3>(R, acc, partSlot);
+    }
+    else if (kDot == 2)
+    {
+        double acc[3] = {facc[0], facc[1], facc[2]};
+        GridReduce<3>(R, acc, (*it & 1) ? baseOdd : baseEven, 0, nullptr, partSlot);
+    }
+}
+
+// the arguments of k_split_half for colour c: its halves of du and r, the other colour's and its own halves of e
+#define NB_SPLIT_HALF_ARGS(c)                                                                                      \
+    v, du + (long long)(c) * v.sHalf, r + (long long)(c) * v.sHalf, e + (long long)((c) ^ 1) * v.sHalf,               \
+        e + (long long)(c) * v.sHalf, (c)
+
+void LaunchSplitFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
+    if (v.stretched)
+        k_split_half<0, true, true><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(0), Reducer{}, nullptr, 0, 0, 0);
+    else
+        k_split_first<<<grid, kPairThreads, 0, st>>>(v, du, r, e);
+}
+
+void LaunchSplitHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
+    if (v.stretched)
+        k_split_half<0, true, false><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), Reducer{}, nullptr, 0,
+                                                                     0, 0);
+    else
+        k_split_half<0, false, false><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), Reducer{}, nullptr, 0,
+                                                                      0, 0);
+}
+
+void LaunchSplitHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, bool last,
+                        const Reducer &R, const int *it, int baseEven, int baseOdd, int partSlot, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
+#define NB_SPLIT_HALF(DOT, ST)                                                                                     \
+    k_split_half<DOT, ST, false><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), R, it, baseEven, baseOdd, \
+                                                                partSlot)
+    if (last)
+    {
+        if (v.stretched) NB_SPLIT_HALF(2, true);
+        else NB_SPLIT_HALF(2, false);
+    }
+    else
+    {
+        if (v.stretched) NB_SPLIT_HALF(1, true);
+        else NB_SPLIT_HALF(1, false);
+    }
+#undef NB_SPLIT_HALF
+}
+#undef NB_SPLIT_HALF_ARGS
+
+// res = r - M e on the red cells (colour 0), into the first half of `res`; the black residual after a black
+// half-sweep is zero.
+template <bool kSt>
+__global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, const uint8_t *__restrict__ du,
+                                                                 const float *__restrict__ r,
+                                                                 const float *__restrict__ e, float *__restrict__ res)
+{
+    const QuadPos P = QuadStart(v);
+    const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
+    const float *O = e + v.sHalf + P.off;
+    const float *Xr = e + P.off;
+    const float *Rr = r + P.off;
+    const uint8_t *D = du + P.off;
+    float *Out = res + P.off;
+    F4 oM = L4(O - P.PS), oC = L4(O);
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i++, o += P.PS)
+    {
+        const F4 oP = L4(O + o + P.PS), oJp = L4(O + o + P.RS), oJm = L4(O + o - P.RS);
+        const F4 xc = L4(Xr + o), rr = L4(Rr + o);
+        const unsigned d = LdU4(D + o);
+        const int q = (i + P.j) & 1;
+        float prevW, nextX;
+        Edges(P, oC, O + o, prevW, nextX);
+        const F4 sh = KShift(oC, prevW, nextX, q);
+        F4 out;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+        {
+            const unsigned b = Byte(d, x);
+            out.v[x] = 0.f;
+            if (!(b & 0x80u)) continue;
+            if (!kSt)
+            {
+                const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
+                out.v[x] = rr.v[x] - (hg * (float)(b & 0x7Fu) * xc.v[x] - g * s);
+            }
+            else
+            {
+                const int k = 2 * (P.m0 + x) + q;
+                const float kp = q ? sh.v[x] : oC.v[x], km = q ? oC.v[x] : sh.v[x];
+                float diag;
+                const float s = StencilSum(v, i, P.j, k, b, oP.v[x], oM.v[x], oJp.v[x], oJm.v[x], kp, km, diag);
+                out.v[x] = rr.v[x] - (diag * xc.v[x] - s);
+            }
+        }
+        if (P.valid) S4(Out + o, out);
+        oM = oC;
+        oC = oP;
+    }
+}
+
+void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
+                         cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
+    if (v.stretched) k_split_residual<true><<<grid, kPairThreads, 0, st>>>(v, du, r, e, res);
+    else k_split_residual<false><<<grid, kPairThreads, 0, st>>>(v, du, r, e, res);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// transfers between a split level and the next coarser level (either layout): the operators of k_prolong and
+// k_restrict on the red cells
+// ---------------------------------------------------------------------------------------------------------------
+// Per red fine cell (colour-split, red half only): 0x80 for an unknown, plus in the low six bits the weight (in 1/64)
+// that the Neumann-aware prolongation moves from the cell's SOLID coarse contributors onto its parent.
+
+// e_f += P e_c on the red fine unknowns. Fine k = 2m + q (q = (a + b) & 1) lies between coarse k-cells m and m+1
+// with weights (3/4, 1/4) for q = 0 and (1/4, 3/4) for q = 1; its parent is m + q.
+__global__ void __launch_bounds__(kPairThreads) k_split_prolong(LevelView fv, LevelView cv,
+                                                                const uint8_t *__restrict__ pext,
+                                                                const float *__restrict__ ec, float *ef)
+{
+    const QuadPos P = QuadStart(fv);
+    const int b = P.j;
+    const int B = (b + 1) >> 1, B2 = B + ((b & 1) ? -1 : 1);
+    const int Dmax = cv.Nz - 1;
+    float *E = ef + P.off;
+    const uint8_t *X = pext + P.off;
+    long long o = 0;
+    for (int a = P.i0; a < P.i1; a++, o += P.PS)
+    {
+        const unsigned w = LdU4(X + o);
+        if (!P.valid || !(w & 0x80808080u)) continue;
+        const int A = (a + 1) >> 1, A2 = A + ((a & 1) ? -1 : 1);
+        const int q = (a + b) & 1;
+        float Cv[5], Par[5]; // coarse values interpolated across i and j at k-cells m0 .. m0+4, and the parent row's
+        if (cv.sRS && P.m0 + 4 <= Dmax)
+        {
+            // a colour-split coarse level: in coarse row (A', B') the k-cells m0, m0+2, m0+4 are elements m0/2 ..
+            // m0/2+2 of colour (A'+B') & 1 and m0+1, m0+3 elements m0/2, m0/2+1 of the other (m0 is a multiple of 4)
+            float row[4][5];
+            const int Ar[4] = {A, A, A2, A2}, Br[4] = {B, B2, B, B2};
+#pragma unroll
+            for (int n = 0; n < 4; n++)
+            {
+                const int ce = (Ar[n] + Br[n]) & 1;
+                const float *rb = ec + (long long)Ar[n] * cv.sPS + (long long)Br[n] * cv.sRS + (P.m0 >> 1);
+                const float2 ev = *reinterpret_cast<const float2 *>(rb + ce * cv.sHalf);
+                const float2 od = *reinterpret_cast<const float2 *>(rb + (ce ^ 1) * cv.sHalf);
+                row[n][0] = ev.x;
+                row[n][1] = od.x;
+                row[n][2] = ev.y;
+                row[n][3] = od.y;
+                row[n][4] = rb[ce * cv.sHalf + 2];
+            }
+#pragma unroll
+            for (int t = 0; t < 5; t++)
+            {
+                Cv[t] = 0.5625f * row[0][t] + 0.1875f * (row[1][t] + row[2][t]) + 0.0625f * row[3][t];
+                Par[t] = row[0][t];
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int t = 0; t < 5; t++)
+            {
+                const int D = min(P.m0 + t, Dmax); // past the row's end only for ring or padding cells (masked)
+                const float c00 = ec[VecIdx(cv, A, B, D)], c01 = ec[VecIdx(cv, A, B2, D)];
+                const float c10 = ec[VecIdx(cv, A2, B, D)], c11 = ec[VecIdx(cv, A2, B2, D)];
+                Cv[t] = 0.5625f * c00 + 0.1875f * (c01 + c10) + 0.0625f * c11;
+                Par[t] = c00;
+            }
+        }
+        F4 ev = L4(E + o);
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+        {
+            const unsigned px = Byte(w, x);
+            if (!(px & 0x80u)) continue;
+            const float lohi = q ? 0.25f * Cv[x] + 0.75f * Cv[x + 1] : 0.75f * Cv[x] + 0.25f * Cv[x + 1];
+            ev.v[x] += lohi + (float)(px & 0x3Fu) * (1.0f / 64.0f) * (q ? Par[x + 1] : Par[x]);
+        }
+        S4(E + o, ev);
+    }
+}
+
+void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
+                        float *eFine, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_split_prolong<<<QuadGrid(fine, kQuadBlocksOther), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+}
+
+// r_c = R res_f = P^T res_f at the coarse unknowns, from the red fine residual. A thread owns one coarse cell (K along
+// the 32 lanes, J across the 8 warps) and marches along I: fine planes 2I-2 .. 2I+1 enter as their (j, k)-weighted
+// 4x4 sums T(a), each kept for the next coarse plane; the red children's moved weights enter as X(a). In fine row
+// (a, b) the red cells among k = 2K-2 .. 2K+1 are elements K-1 and K, at k = 2K-2+q and 2K+q (q = (a + b) & 1),
+// and the red child of coarse K is element K - q.
+__device__ __forceinline__ void SplitRestrictPlane(const LevelView &fv, const uint8_t *pext, const float *res, int a,
+                                                   int J, int K, float &T, float &X)
+{
+    T = 0.f;
+    X = 0.f;
+    if (a > fv.Ny - 1) return;
+    const float wt[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+#pragma unroll
+    for (int dj = 0; dj < 4; dj++)
+    {
+        const int b = 2 * J - 2 + dj;
+        if (b > fv.Nx - 1) continue;
+        const int q = (a + b) & 1;
+        const long long row = (long long)a * fv.sPS + (long long)b * fv.sRS;
+        const float lo = res[row + K - 1], hi = res[row + K];
+        T += wt[dj] * (q ? 0.75f * lo + 0.25f * hi : 0.25f * lo + 0.75f * hi);
+        if (dj == 1 || dj == 2) X += (float)(pext[row + K - q] & 0x3Fu) * (q ? lo : hi);
+    }
+    X *= 1.0f / 64.0f;
+}
+
+__global__ void __launch_bounds__(256) k_split_restrict(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
+                                                        const float *__restrict__ res, float *__restrict__ rc)
+{
+    const int K = 1 + blockIdx.x * 32 + threadIdx.x, J = 1 + blockIdx.y * 8 + threadIdx.y;
+    if (K > cv.Nz - 2 || J > cv.Nx - 2) return;
+    const int S = (cv.Ny - 2 + (int)gridDim.z - 1) / (int)gridDim.z;
+    const int I0 = 1 + (int)blockIdx.z * S, I1 = min(I0 + S, cv.Ny - 1);
+    if (I0 >= I1) return;
+    float Tm2, Tm1, Xm1, Xdummy;
+    SplitRestrictPlane(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
+    SplitRestrictPlane(fv, pext, res, 2 * I0 - 1, J, K, Tm1, Xm1);
+    for (int I = I0; I < I1; I++)
+    {
+        float T0, X0, T1, X1;
+        SplitRestrictPlane(fv, pext, res, 2 * I, J, K, T0, X0);
+        SplitRestrictPlane(fv, pext, res, 2 * I + 1, J, K, T1, X1);
+        const long long c = (long long)I * cv.sI + (long long)J * cv.sJ + K;
+        if (cv.code[c] & CODE_UNKNOWN)
+            rc[VecIdx(cv, I, J, K)] = ((0.25f * Tm2 + 0.75f * Tm1) + (0.75f * T0 + 0.25f * T1)) + (Xm1 + X0);
+        Tm2 = T0;
+        Tm1 = T1;
+        Xm1 = X1;
+    }
+}
+
+void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
+                         float *rCoarse, cudaStream_t st)
+{
+    const long long perPlane = (long long)((coarse.Nz - 2 + 31) / 32) * ((coarse.Nx - 2 + 7) / 8);
+    const int S = MarchPlanes(coarse.Ny - 2, perPlane);
+    const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
+                    (unsigned)((coarse.Ny - 2 + S - 1) / S));
+    NB_COUNT_LAUNCH();
+    k_split_restrict<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// PCG on a split level 0 (the semantics of k_pair_papply)
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double SplitRzEff(const double *S, int base, double n, int singular)
+{
+    return singular ? S[base] - (S[base + 1] / n) * S[base + 2] : S[base];
+}
+
+// p_new = U (z - mean + beta p_old), q = M p_new, sum p_new.q, both colours at a thread's quad position.
+template <bool kSingular, bool kSt>
+__global__ void __launch_bounds__(kPairThreads, 4)
+    k_split_papply(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ z, float *p0, float *p1,
+                   float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd,
+                   int slotN, int slotPQ)
+{
+    const int iter = *it, par = iter & 1;
+    const float *__restrict__ pIn = par ? p1 : p0;
+    float *__restrict__ pOut = par ? p0 : p1;
+    const int baseNew = par ? baseOdd : baseEven, baseOld = par ? baseEven : baseOdd;
+    const double n = S[slotN];
+    const double beta =
+        iter == 0 ? 0.0 : SplitRzEff(S, baseNew, n, kSingular) / SplitRzEff(S, baseOld, n, kSingular);
+    const float bt = (float)beta;
+    const float mean = kSingular ? (float)(S[baseNew + 1] / n) : 0.f;
+    const QuadPos P = QuadStart(v);
+    const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
+    const long long hb = v.sHalf;
+    auto pn = [&](long long base) {
+        const F4 zz = L4(z + base), pv = L4(pIn + base);
+        F4 out;
+#pragma unroll
+        for (int x = 0; x < 4; x++) out.v[x] = (zz.v[x] - mean) + bt * pv.v[x];
+        if (kSingular)
+        {
+            const unsigned d = LdU4(du + base);
+#pragma unroll
+            for (int x = 0; x < 4; x++) out.v[x] *= Unk(Byte(d, x));
+        }
+        return out;
+    };
+    auto pn1 = [&](long long idx) {
+        float x = (z[idx] - mean) + bt * pIn[idx];
+        if (kSingular) x *= Unk(du[idx]);
+        return x;
+    };
+    const long long b0 = P.off, b1 = hb + P.off;
+    F4 M0 = pn(b0 - P.PS), M1 = pn(b1 - P.PS), C0 = pn(b0), C1 = pn(b1);
+    float facc = 0.f;
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i++, o += P.PS)
+    {
+        const F4 P0 = pn(b0 + o + P.PS), P1 = pn(b1 + o + P.PS);
+        const F4 Jp0 = pn(b0 + o + P.RS), Jp1 = pn(b1 + o + P.RS), Jm0 = pn(b0 + o - P.RS), Jm1 = pn(b1 + o - P.RS);
+        const unsigned d0 = LdU4(du + b0 + o), d1 = LdU4(du + b1 + o);
+        const int q0 = (i + P.j) & 1, q1 = q0 ^ 1;
+        float pw0 = __shfl_up_sync(0xffffffffu, C0.v[3], 1), nx0 = __shfl_down_sync(0xffffffffu, C0.v[0], 1);
+        float pw1 = __shfl_up_sync(0xffffffffu, C1.v[3], 1), nx1 = __shfl_down_sync(0xffffffffu, C1.v[0], 1);
+        if (P.lane == 0 && P.m0 > 0)
+        {
+            pw0 = pn1(b0 + o - 1);
+            pw1 = pn1(b1 + o - 1);
+        }
+        if (P.lane == 31 && P.m0 + 4 < P.RS)
+        {
+            nx0 = pn1(b0 + o + 4);
+            nx1 = pn1(b1 + o + 4);
+        }
+        // colour-0 cells see colour 1 shifted by q0, colour-1 cells see colour 0 shifted by q1
+        const F4 sh1 = KShift(C1, pw1, nx1, q0), sh0 = KShift(C0, pw0, nx0, q1);
+        F4 Q0, Q1;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+        {
+            const unsigned a0 = Byte(d0, x), a1 = Byte(d1, x);
+            if (!kSt)
+            {
+                const float s0 = ((P1.v[x] + M1.v[x]) + (Jp1.v[x] + Jm1.v[x])) + (C1.v[x] + sh1.v[x]);
+                const float s1 = ((P0.v[x] + M0.v[x]) + (Jp0.v[x] + Jm0.v[x])) + (C0.v[x] + sh0.v[x]);
+                Q0.v[x] = Unk(a0) * (hg * (float)(a0 & 0x7Fu) * C0.v[x] - g * s0);
+                Q1.v[x] = Unk(a1) * (hg * (float)(a1 & 0x7Fu) * C1.v[x] - g * s1);
+            }
+            else
+            {
+                Q0.v[x] = Q1.v[x] = 0.f;
+                float diag;
+                if (a0 & 0x80u)
+                {
+                    const int k = 2 * (P.m0 + x) + q0;
+                    const float kp = q0 ? sh1.v[x] : C1.v[x], km = q0 ? C1.v[x] : sh1.v[x];
+                    const float s = StencilSum(v, i, P.j, k, a0, P1.v[x], M1.v[x], Jp1.v[x], Jm1.v[x], kp, km, diag);
+                    Q0.v[x] = diag * C0.v[x] - s;
+                }
+                if (a1 & 0x80u)
+                {
+                    const int k = 2 * (P.m0 + x) + q1;
+                    const float kp = q1 ? sh0.v[x] : C0.v[x], km = q1 ? C0.v[x] : sh0.v[x];
+                    const float s = StencilSum(v, i, P.j, k, a1, P0.v[x], M0.v[x], Jp0.v[x], Jm0.v[x], kp, km, diag);
+                    Q1.v[x] = diag * C1.v[x] - s;
+                }
+            }
+        }
+        if (P.valid)
+        {
+            S4(pOut + b0 + o, C0);
+            S4(pOut + b1 + o, C1);
+            S4(q + b0 + o, Q0);
+            S4(q + b1 + o, Q1);
+#pragma unroll
+            for (int x = 0; x < 4; x++) facc += C0.v[x] * Q0.v[x] + C1.v[x] * Q1.v[x];
+        }
+        M0 = C0;
+        M1 = C1;
+        C0 = P0;
+        C1 = P1;
+    }
+    double acc[1] = {facc};
+    GridReduce<1>(R, acc, slotPQ);
+}
+
+void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
+                       const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
+                       int singular, int slotPQ, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    const dim3 grid = QuadGrid(v, kQuadBlocksOther);
+#define NB_SPLIT_PAPPLY(SING, ST)                                                                                  \
+    k_split_papply<SING, ST><<<grid, kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, \
+                                                            slotPQ)
+    if (singular)
+    {
+        if (v.stretched) NB_SPLIT_PAPPLY(true, true);
+        else NB_SPLIT_PAPPLY(true, false);
+    }
+    else
+    {
+        if (v.stretched) NB_SPLIT_PAPPLY(false, true);
+        else NB_SPLIT_PAPPLY(false, false);
+    }
+#undef NB_SPLIT_PAPPLY
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// the FP64 side of level 0: FP64 arrays in the grid layout, the FP32 vectors colour-split
+// ---------------------------------------------------------------------------------------------------------------
+// r = sfac * b (split) and (sum b^2, sum b): the residual of a zero iterate. One thread per cell pair (k0 even).
+__global__ void __launch_bounds__(256) k_split_scale_sum(LevelView v, const double *__restrict__ b,
+                                                         float *__restrict__ r, double sfac, Reducer R, int slot)
+{
+    double acc[2] = {0.0, 0.0};
+    const long long pairs = v.cells >> 1, stride = (long long)gridDim.x * blockDim.x;
+    const int H = v.Nz >> 1;
+    const double2 *b2 = reinterpret_cast<const double2 *>(b);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < pairs; t += stride)
+    {
+        const double2 x = b2[t];
+        const long long row = t / H; // i * Nx + j
+        const int m = (int)(t - row * H);
+        const int i = (int)(row / v.Nx), j = (int)(row - (long long)i * v.Nx);
+        const int par = (i + j) & 1; // the colour of the pair's first cell
+        const long long s = (long long)i * v.sPS + (long long)j * v.sRS + m;
+        r[par * v.sHalf + s] = (float)(x.x * sfac);
+        r[(par ^ 1) * v.sHalf + s] = (float)(x.y * sfac);
+        acc[0] += x.x * x.x + x.y * x.y;
+        acc[1] += x.x + x.y;
+    }
+    GridReduce<2>(R, acc, slot);
+}
+
+void LaunchSplitScaleSum(const LevelView &v, const double *b, float *r, double sfac, const Reducer &R, int slot,
+                         cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_split_scale_sum<<<148 * 8, 256, 0, st>>>(v, b, r, sfac, R, slot);
+}
+
+// The FP64 refinement step on a uniform split level 0 (k_pair_refine64's, with e read and r written split):
+// x_out = x_in + e; r = sfac (b - A x_out) in FP32; (sum (b - A x_out)^2, sum (b - A x_out)) in FP64. One thread per
+// cell pair of the grid layout; the pair (k0, k0+1) of row (i, j) is element k0/2 of colours (i+j)&1 and its other.
+__device__ __forceinline__ double2 Ld2d(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+
+__global__ void __launch_bounds__(kPairThreads, 4)
+    k_split_refine64(LevelView v, const uint8_t *__restrict__ du, const double *__restrict__ b,
+                     const double *__restrict__ xin, const float *__restrict__ e, double *__restrict__ xout,
+                     float *__restrict__ r, double scale, double sfac, Reducer R, int slot)
+{
+    const PairPos P = PairStart(v);
+    const long long sb = (long long)P.i0 * v.sPS + (long long)P.j * v.sRS + (P.k0 >> 1);
+    // the thread's element on plane i0 in colour 0 and colour 1
+    const float *e0 = e + sb, *e1 = e + v.sHalf + sb;
+    const uint8_t *d0p = du + sb, *d1p = du + v.sHalf + sb;
+    float *r0p = r + sb, *r1p = r + v.sHalf + sb;
+    const double *xp = xin + P.base;
+    // x_in + e at the pair `o` cells (grid layout) / `so` elements (split) away; par: the colour of its first cell
+    auto X = [&](long long o, long long so, int par) {
+        const double2 a = Ld2d(xp + o);
+        const float fa = e0[so], fb = e1[so];
+        return make_double2(a.x + (double)(par ? fb : fa), a.y + (double)(par ? fa : fb));
+    };
+    const int par0 = (P.i0 + P.j) & 1;
+    double2 XM = X(-P.sI, -v.sPS, par0 ^ 1), XC = X(0, 0, par0);
+    double acc[2] = {0.0, 0.0};
+    long long off = 0, so = 0;
+    for (int i = P.i0; i < P.i1; i++, off += P.sI, so += v.sPS)
+    {
+        const int par = (i + P.j) & 1;
+        const double2 XP = X(off + P.sI, so + v.sPS, par ^ 1);
+        const double2 XJp = X(off + P.sJ, so + v.sRS, par ^ 1), XJm = X(off - P.sJ, so - v.sRS, par ^ 1);
+        const double2 bb = Ld2d(b + P.base + off);
+        const unsigned da = d0p[so], db = d1p[so];
+        const unsigned d0 = par ? db : da, d1 = par ? da : db;
+        double left = __shfl_up_sync(0xffffffffu, XC.y, 1);
+        double right = __shfl_down_sync(0xffffffffu, XC.x, 1);
+        // cell k0-1 is element m-1 of the other colour, cell k0+2 element m+1 of this one (across a row's end: a ring
+        // cell's neighbour, masked)
+        if (P.lane == 0) left = xp[off - 1] + (double)(par ? e0[so - 1] : e1[so - 1]);
+        if (P.lane == 31) right = xp[off + 2] + (double)(par ? e1[so + 1] : e0[so + 1]);
+        const double s0 = ((XP.x + XM.x) + (XJp.x + XJm.x)) + (left + XC.y);
+        const double s1 = ((XP.y + XM.y) + (XJp.y + XJm.y)) + (XC.x + right);
+        const double r0 = (d0 & 0x80u) ? bb.x - scale * (s0 - 0.5 * (double)(d0 & 0x7Fu) * XC.x) : 0.0;
+        const double r1 = (d1 & 0x80u) ? bb.y - scale * (s1 - 0.5 * (double)(d1 & 0x7Fu) * XC.y) : 0.0;
+        if (P.valid)
+        {
+            *reinterpret_cast<double2 *>(xout + P.base + off) = XC;
+            const float f0 = (float)(r0 * sfac), f1 = (float)(r1 * sfac);
+            r0p[so] = par ? f1 : f0;
+            r1p[so] = par ? f0 : f1;
+            acc[0] += r0 * r0 + r1 * r1;
+            acc[1] += r0 + r1;
+        }
+        XM = XC;
+        XC = XP;
+    }
+    GridReduce<2>(R, acc, slot);
+}
+
+void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
+                         double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
+                         cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    k_split_refine64<<<PairGrid(v, kSplitReduceS), kPairThreads, 0, st>>>(v, du, b, xin, e, xout, r, scale, sfac, R,
+                                                                           slot);
+}
+
+} // namespace nb

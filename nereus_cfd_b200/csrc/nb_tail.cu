@@ -1,18 +1,29 @@
 // The coarse end of the multigrid V-cycle in one thread block: every level from `tailStart` down (at most a few
-// thousand cells each, about 16^3 and below) lives in shared memory, and the block runs their pre-smoothing,
-// residual, restriction, coarsest sweeps, prolongation and post-smoothing back to back with __syncthreads between
-// the phases. It reads the restricted residual of the first tail level from global memory and writes that level's
-// correction back; the finer levels' kernels on either side are unchanged. The operations are the ones of
-// nb_kernels.cu (same stencil, transfers and colour order), so the V-cycle stays the same symmetric operator.
+// thousand cells each) lives in shared memory, and the block runs their pre-smoothing, residual, restriction,
+// coarsest sweeps, prolongation and post-smoothing back to back. It reads the restricted residual of the first tail
+// level from global memory and writes that level's correction back; the finer levels' kernels on either side are
+// unchanged. The operations are the ones of nb_kernels.cu (same stencil, transfers and colour order), so the
+// V-cycle stays the same symmetric operator.
+//
+// What costs time here is latency, not bytes: each phase (one colour of a sweep, a residual, a transfer) is a short
+// loop over a level's unknowns followed by a barrier. So
+// - the per-colour lists of unknowns are built once per layout (k_tail_lists) and only copied in;
+// - a uniform level sums its six neighbours unmasked (every vector is zero off the unknowns) and divides through a
+//   per-level reciprocal table of the diagonal's half-units, computed once per launch;
+// - the levels with at most 32 unknowns of each colour (the last two or three) run in warp 0 alone, with __syncwarp
+//   between their phases instead of a block-wide barrier.
 #include "nb_kernels.h"
 
 namespace nb
 {
 
+constexpr int kTailThreads = 256;
+
 template <typename T> struct TailLevel
 {
     LevelView v;
-    unsigned off; // byte offset of the level's arrays in shared memory
+    unsigned off;     // byte offset of the level's arrays in shared memory
+    unsigned listOff; // entry offset of the level's list in the global list array
 };
 
 template <typename T> struct TailArgs
@@ -22,28 +33,29 @@ template <typename T> struct TailArgs
     const T *rIn; // residual of the first tail level (global)
     T *eOut;      // its correction (global)
     int pre, post, coarseSweeps;
+    const unsigned *lists; // per level: its cells' entries, red unknowns from the front, black ones from the back
+    const int *counts;     // [level][colour] unknowns
 };
 
-// The level's arrays in shared memory: r, e, res (T), then code and types (bytes), then the list of its unknowns
-// (4 bytes each: red ones from the front, black ones from the back), each padded to 16 bytes.
+// The level's arrays in shared memory: r, e, res (T), then code, types and diagonal units (bytes), then the list of
+// its unknowns (4 bytes each: red ones from the front, black ones from the back), each padded to 16 bytes.
 template <typename T> __host__ __device__ inline unsigned LevelBytes(long long cells)
 {
     const unsigned a = (unsigned)((cells * sizeof(T) + 15) / 16 * 16);
     const unsigned b = (unsigned)((cells + 15) / 16 * 16);
     const unsigned l = (unsigned)((cells * 4 + 15) / 16 * 16);
-    return 3 * a + 2 * b + l;
+    return 3 * a + 3 * b + l;
 }
 
 template <typename T> struct SmemLevel
 {
     LevelView v; // types/code point into shared memory
     T *r, *e, *res;
+    uint8_t *du;    // uniform level: 0x80 | diagonal half-units at an unknown, 0 elsewhere
     unsigned *list; // packed (i << 20 | j << 10 | k) of the unknowns; red [0, nRed), black [cells - nBlack, cells)
     int nRed, nBlack;
+    const double *inv; // 1 / (gamma/2 * units), entry 0 = 0
 };
-
-// unknowns per colour of each tail level, counted while the lists are built
-__shared__ int g_tailCount[kMaxTailLevels][2];
 
 __device__ __forceinline__ void Unpack(unsigned x, int &i, int &j, int &k)
 {
@@ -65,16 +77,10 @@ template <typename T> __device__ __forceinline__ SmemLevel<T> Bind(const TailLev
     s.res = (T *)(base + 2 * a);
     s.v.code = base + 3 * a;
     s.v.types = base + 3 * a + b;
-    s.list = (unsigned *)(base + 3 * a + 2 * b);
-    return s;
-}
-
-// the level bound with its unknown counts (valid once the lists are built)
-template <typename T> __device__ __forceinline__ SmemLevel<T> BindL(const TailLevel<T> &tl, unsigned char *smem, int l)
-{
-    SmemLevel<T> s = Bind<T>(tl, smem);
-    s.nRed = g_tailCount[l][0];
-    s.nBlack = g_tailCount[l][1];
+    s.du = base + 3 * a + 2 * b;
+    s.list = (unsigned *)(base + 3 * a + 3 * b);
+    s.nRed = s.nBlack = 0;
+    s.inv = nullptr;
     return s;
 }
 
@@ -100,15 +106,40 @@ __device__ __forceinline__ void Decode(const LevelView &v, long long c, int &i, 
     i = (int)(r / v.Nx);
 }
 
-template <typename T> __device__ void TSmooth(const SmemLevel<T> &L, int colour, bool first)
+// A phase runs over the whole block (kWarp false) or over warp 0 alone (kWarp true), and ends with the matching
+// barrier.
+template <bool kWarp> __device__ __forceinline__ int PhaseStart() { return kWarp ? (int)(threadIdx.x & 31) : (int)threadIdx.x; }
+template <bool kWarp> __device__ __forceinline__ int PhaseStride() { return kWarp ? 32 : (int)blockDim.x; }
+template <bool kWarp> __device__ __forceinline__ void PhaseSync()
+{
+    if (kWarp) __syncwarp();
+    else __syncthreads();
+}
+
+// the plain sum of a cell's neighbours on a uniform level (vectors are zero off the unknowns)
+template <typename T> __device__ __forceinline__ T NbrSum(const LevelView &v, const T *e, long long c)
+{
+    const T s = (e[c + v.sI] + e[c - v.sI]) + (e[c + v.sJ] + e[c - v.sJ]);
+    return v.dim == 3 ? s + (e[c + 1] + e[c - 1]) : s;
+}
+
+template <typename T, bool kWarp> __device__ void TSmooth(const SmemLevel<T> &L, int colour, bool first)
 {
     const LevelView &v = L.v;
     const int n = ListLen(L, colour);
-    for (int t = threadIdx.x; t < n; t += blockDim.x)
+    const T g = (T)v.gamma;
+    for (int t = PhaseStart<kWarp>(); t < n; t += PhaseStride<kWarp>())
     {
         int i, j, k;
         Unpack(ListAt(L, colour, t), i, j, k);
         const long long c = (long long)i * v.sI + (long long)j * v.sJ + k;
+        if (!v.stretched)
+        {
+            T rhs = L.r[c];
+            if (!first) rhs += g * NbrSum(v, L.e, c);
+            L.e[c] = rhs * (T)L.inv[L.du[c] & 0x7Fu];
+            continue;
+        }
         const unsigned code = v.code[c];
         T cq[6], diag;
         CodeStencil<T>(v, i, j, k, c, code, cq, diag);
@@ -124,18 +155,24 @@ template <typename T> __device__ void TSmooth(const SmemLevel<T> &L, int colour,
         }
         L.e[c] = diag != (T)0 ? rhs / diag : (T)0;
     }
-    __syncthreads();
+    PhaseSync<kWarp>();
 }
 
-template <typename T> __device__ void TResidual(const SmemLevel<T> &L)
+template <typename T, bool kWarp> __device__ void TResidual(const SmemLevel<T> &L)
 {
     const LevelView &v = L.v;
     const int n = ListLen(L, 2);
-    for (int t = threadIdx.x; t < n; t += blockDim.x)
+    const T g = (T)v.gamma, hg = (T)0.5 * (T)v.gamma;
+    for (int t = PhaseStart<kWarp>(); t < n; t += PhaseStride<kWarp>())
     {
         int i, j, k;
         Unpack(ListAt(L, 2, t), i, j, k);
         const long long c = (long long)i * v.sI + (long long)j * v.sJ + k;
+        if (!v.stretched)
+        {
+            L.res[c] = L.r[c] - (hg * (T)(L.du[c] & 0x7Fu) * L.e[c] - g * NbrSum(v, L.e, c));
+            continue;
+        }
         const unsigned code = v.code[c];
         T cq[6], diag;
         CodeStencil<T>(v, i, j, k, c, code, cq, diag);
@@ -148,7 +185,7 @@ template <typename T> __device__ void TResidual(const SmemLevel<T> &L)
         if (code & 32u) s -= cq[5] * L.e[c - 1];
         L.res[c] = L.r[c] - s;
     }
-    __syncthreads();
+    PhaseSync<kWarp>();
 }
 
 template <typename T>
@@ -169,11 +206,11 @@ __device__ __forceinline__ T TSolidWeight(const LevelView &cv, int I, int J, int
     return extra;
 }
 
-template <typename T> __device__ void TRestrict(const SmemLevel<T> &F, const SmemLevel<T> &C)
+template <typename T, bool kWarp> __device__ void TRestrict(const SmemLevel<T> &F, const SmemLevel<T> &C)
 {
     const LevelView &fv = F.v, &cv = C.v;
     const int n = ListLen(C, 2);
-    for (int t = threadIdx.x; t < n; t += blockDim.x)
+    for (int t = PhaseStart<kWarp>(); t < n; t += PhaseStride<kWarp>())
     {
         int I, J, K;
         Unpack(ListAt(C, 2, t), I, J, K);
@@ -216,14 +253,14 @@ template <typename T> __device__ void TRestrict(const SmemLevel<T> &F, const Sme
                 }
         C.r[c] = acc;
     }
-    __syncthreads();
+    PhaseSync<kWarp>();
 }
 
-template <typename T> __device__ void TProlong(const SmemLevel<T> &F, const SmemLevel<T> &C)
+template <typename T, bool kWarp> __device__ void TProlong(const SmemLevel<T> &F, const SmemLevel<T> &C)
 {
     const LevelView &fv = F.v, &cv = C.v;
     const int n = ListLen(F, 2);
-    for (int t = threadIdx.x; t < n; t += blockDim.x)
+    for (int t = PhaseStart<kWarp>(); t < n; t += PhaseStride<kWarp>())
     {
         int a, b, d;
         Unpack(ListAt(F, 2, t), a, b, d);
@@ -246,17 +283,63 @@ template <typename T> __device__ void TProlong(const SmemLevel<T> &F, const Smem
                 }
         F.e[c] += acc + extra * C.e[parent];
     }
-    __syncthreads();
+    PhaseSync<kWarp>();
 }
 
-template <typename T> __global__ void __launch_bounds__(1024) k_tail(TailArgs<T> A)
+// The descent through level l: the first sweep from zero, further sweeps, the residual and its restriction.
+template <typename T, bool kWarp>
+__device__ void TDown(const SmemLevel<T> &F, const SmemLevel<T> &C, int pre)
+{
+    TSmooth<T, kWarp>(F, 0, true);
+    TSmooth<T, kWarp>(F, 1, false);
+    for (int s = 1; s < pre; s++)
+    {
+        TSmooth<T, kWarp>(F, 0, false);
+        TSmooth<T, kWarp>(F, 1, false);
+    }
+    TResidual<T, kWarp>(F);
+    TRestrict<T, kWarp>(F, C);
+}
+
+// The coarsest level: symmetric sweep pairs from zero.
+template <typename T, bool kWarp> __device__ void TCoarsest(const SmemLevel<T> &C, int sweeps)
+{
+    TSmooth<T, kWarp>(C, 0, true);
+    TSmooth<T, kWarp>(C, 1, false);
+    for (int s = 1; s < sweeps; s++)
+    {
+        TSmooth<T, kWarp>(C, 0, false);
+        TSmooth<T, kWarp>(C, 1, false);
+    }
+    for (int s = 0; s < sweeps; s++)
+    {
+        TSmooth<T, kWarp>(C, 1, false);
+        TSmooth<T, kWarp>(C, 0, false);
+    }
+}
+
+// The ascent into level l: the prolonged correction, then the post-sweeps black first.
+template <typename T, bool kWarp> __device__ void TUp(const SmemLevel<T> &F, const SmemLevel<T> &C, int post)
+{
+    TProlong<T, kWarp>(F, C);
+    for (int s = 0; s < post; s++)
+    {
+        TSmooth<T, kWarp>(F, 1, false);
+        TSmooth<T, kWarp>(F, 0, false);
+    }
+}
+
+template <typename T> __global__ void __launch_bounds__(kTailThreads) k_tail(TailArgs<T> A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    // stage: cell types and codes of every tail level, zero corrections and residuals, the first level's r
+    __shared__ double sInv[kMaxTailLevels][32];
+    __shared__ int sCount[kMaxTailLevels][2];
+    // stage: cell types, codes and lists of every tail level, zero corrections and residuals, the first level's r
     for (int l = 0; l < A.nlev; l++)
     {
         const LevelView &g = A.lv[l].v;
         const SmemLevel<T> S = Bind<T>(A.lv[l], smem);
+        const unsigned *gl = A.lists + A.lv[l].listOff;
         for (long long c = threadIdx.x; c < g.cells; c += blockDim.x)
         {
             ((uint8_t *)S.v.code)[c] = g.code[c];
@@ -264,70 +347,125 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tail(TailArgs<T>
             S.e[c] = (T)0;
             S.res[c] = (T)0;
             S.r[c] = l == 0 ? A.rIn[c] : (T)0;
+            S.list[c] = gl[c];
+        }
+        if (threadIdx.x < 32)
+            sInv[l][threadIdx.x] = threadIdx.x ? 1.0 / (0.5 * g.gamma * (double)threadIdx.x) : 0.0;
+        if (threadIdx.x < 2) sCount[l][threadIdx.x] = A.counts[2 * l + threadIdx.x];
+    }
+    __syncthreads();
+    // the diagonal half-units of the uniform levels' unknowns: 2 per FLUID neighbour, 2 per interior Dirichlet
+    // neighbour, 4 per Dirichlet ring neighbour (ring factor 2)
+    for (int l = 0; l < A.nlev; l++)
+    {
+        const SmemLevel<T> S = Bind<T>(A.lv[l], smem);
+        const LevelView &v = S.v;
+        if (v.stretched) continue;
+        const int nq = v.dim == 3 ? 6 : 4;
+        for (long long c = threadIdx.x; c < v.cells; c += blockDim.x)
+        {
+            const unsigned code = v.code[c];
+            unsigned units = 0;
+            if (code & CODE_UNKNOWN)
+            {
+                units = 2u * (unsigned)__popc(code & CODE_FLUID_MASK);
+                if (code & CODE_DIRICHLET)
+                {
+                    int i, j, k;
+                    Decode(v, c, i, j, k);
+                    for (int q = 0; q < nq; q++)
+                        if (IsDirichlet(v.types[c + NbrOffset(v, q)]))
+                        {
+                            const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3),
+                                      nk = k + (q == 4) - (q == 5);
+                            units += OnRing(v, ni, nj, nk) ? 4u : 2u;
+                        }
+                }
+                units |= 0x80u;
+            }
+            S.du[c] = (uint8_t)units;
         }
     }
-    if (threadIdx.x < 2 * kMaxTailLevels) g_tailCount[threadIdx.x >> 1][threadIdx.x & 1] = 0;
     __syncthreads();
-    // the unknowns of every level by colour (i + j + k) & 1; their order within a colour does not matter (the
-    // cells of one colour are updated independently)
+    auto lev = [&](int l) {
+        SmemLevel<T> s = Bind<T>(A.lv[l], smem);
+        s.nRed = sCount[l][0];
+        s.nBlack = sCount[l][1];
+        s.inv = sInv[l];
+        return s;
+    };
+    const int last = A.nlev - 1;
+    // wl: the first level from which every coarser one has at most 32 unknowns of each colour (warp 0 runs those)
+    int wl = A.nlev;
+    for (int l = last; l >= 0 && sCount[l][0] <= 32 && sCount[l][1] <= 32; l--) wl = l;
+    const int top = wl < last ? wl : last;
+    for (int l = 0; l < top; l++) TDown<T, false>(lev(l), lev(l + 1), A.pre);
+    if (wl > last) TCoarsest<T, false>(lev(last), A.coarseSweeps);
+    else
+    {
+        if (threadIdx.x < 32)
+        {
+            for (int l = wl; l < last; l++) TDown<T, true>(lev(l), lev(l + 1), A.pre);
+            TCoarsest<T, true>(lev(last), A.coarseSweeps);
+            for (int l = last - 1; l >= wl; l--) TUp<T, true>(lev(l), lev(l + 1), A.post);
+        }
+        __syncthreads();
+    }
+    for (int l = top - 1; l >= 0; l--) TUp<T, false>(lev(l), lev(l + 1), A.post);
+    const SmemLevel<T> F0 = Bind<T>(A.lv[0], smem);
+    for (long long c = threadIdx.x; c < A.lv[0].v.cells; c += blockDim.x) A.eOut[c] = F0.e[c];
+}
+
+// The per-colour lists of every tail level's unknowns, once per layout: entries packed (i << 20 | j << 10 | k), red
+// ones from the front of the level's segment, black ones from the back; their order within a colour does not matter
+// (the cells of one colour are updated independently).
+__global__ void __launch_bounds__(1024) k_tail_lists(TailArgs<float> A)
+{
+    __shared__ int cnt[kMaxTailLevels][2];
+    if (threadIdx.x < 2 * kMaxTailLevels) cnt[threadIdx.x >> 1][threadIdx.x & 1] = 0;
+    __syncthreads();
     for (int l = 0; l < A.nlev; l++)
     {
         const LevelView &g = A.lv[l].v;
-        const SmemLevel<T> S = Bind<T>(A.lv[l], smem);
+        unsigned *list = const_cast<unsigned *>(A.lists) + A.lv[l].listOff;
         for (long long c = threadIdx.x; c < g.cells; c += blockDim.x)
         {
-            if (!(S.v.code[c] & CODE_UNKNOWN)) continue;
+            if (!(g.code[c] & CODE_UNKNOWN)) continue;
             int i, j, k;
             Decode(g, c, i, j, k);
             const int col = (i + j + k) & 1;
-            const int pos = atomicAdd(&g_tailCount[l][col], 1);
+            const int pos = atomicAdd(&cnt[l][col], 1);
             const unsigned packed = ((unsigned)i << 20) | ((unsigned)j << 10) | (unsigned)k;
-            if (col == 0) S.list[pos] = packed;
-            else S.list[g.cells - 1 - pos] = packed;
+            if (col == 0) list[pos] = packed;
+            else list[g.cells - 1 - pos] = packed;
         }
     }
     __syncthreads();
-    const int last = A.nlev - 1;
-    for (int l = 0; l < last; l++)
+    if (threadIdx.x < 2 * A.nlev) const_cast<int *>(A.counts)[threadIdx.x] = cnt[threadIdx.x >> 1][threadIdx.x & 1];
+}
+
+long long TailListEntries(const LevelView *levels, int nlev)
+{
+    long long n = 0;
+    for (int l = 0; l < nlev; l++) n += levels[l].cells;
+    return n;
+}
+
+void LaunchTailLists(const LevelView *levels, int nlev, unsigned *lists, int *counts, cudaStream_t st)
+{
+    TailArgs<float> A{};
+    unsigned off = 0;
+    for (int l = 0; l < nlev; l++)
     {
-        const SmemLevel<T> F = BindL<T>(A.lv[l], smem, l);
-        TSmooth<T>(F, 0, true);
-        TSmooth<T>(F, 1, false);
-        for (int s = 1; s < A.pre; s++)
-        {
-            TSmooth<T>(F, 0, false);
-            TSmooth<T>(F, 1, false);
-        }
-        TResidual<T>(F);
-        TRestrict<T>(F, BindL<T>(A.lv[l + 1], smem, l + 1));
+        A.lv[l].v = levels[l];
+        A.lv[l].listOff = off;
+        off += (unsigned)levels[l].cells;
     }
-    {
-        const SmemLevel<T> C = BindL<T>(A.lv[last], smem, last);
-        TSmooth<T>(C, 0, true);
-        TSmooth<T>(C, 1, false);
-        for (int s = 1; s < A.coarseSweeps; s++)
-        {
-            TSmooth<T>(C, 0, false);
-            TSmooth<T>(C, 1, false);
-        }
-        for (int s = 0; s < A.coarseSweeps; s++)
-        {
-            TSmooth<T>(C, 1, false);
-            TSmooth<T>(C, 0, false);
-        }
-    }
-    for (int l = last - 1; l >= 0; l--)
-    {
-        const SmemLevel<T> F = BindL<T>(A.lv[l], smem, l);
-        TProlong<T>(F, BindL<T>(A.lv[l + 1], smem, l + 1));
-        for (int s = 0; s < A.post; s++)
-        {
-            TSmooth<T>(F, 1, false);
-            TSmooth<T>(F, 0, false);
-        }
-    }
-    const SmemLevel<T> F0 = Bind<T>(A.lv[0], smem);
-    for (long long c = threadIdx.x; c < A.lv[0].v.cells; c += blockDim.x) A.eOut[c] = F0.e[c];
+    A.nlev = nlev;
+    A.lists = lists;
+    A.counts = counts;
+    NB_COUNT_LAUNCH();
+    k_tail_lists<<<1, 1024, 0, st>>>(A);
 }
 
 template <typename T> size_t TailSmemBytes(const LevelView *levels, int nlev)
@@ -346,15 +484,17 @@ template <typename T> bool PrepareTail(size_t bytes)
 
 template <typename T>
 void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pre, int post, int coarseSweeps,
-                cudaStream_t st)
+                const unsigned *lists, const int *counts, cudaStream_t st)
 {
     TailArgs<T> A{};
-    unsigned off = 0;
+    unsigned off = 0, listOff = 0;
     for (int l = 0; l < nlev; l++)
     {
         A.lv[l].v = levels[l];
         A.lv[l].off = off;
+        A.lv[l].listOff = listOff;
         off += LevelBytes<T>(levels[l].cells);
+        listOff += (unsigned)levels[l].cells;
     }
     A.nlev = nlev;
     A.rIn = rIn;
@@ -362,15 +502,19 @@ void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pr
     A.pre = pre < 1 ? 1 : pre;
     A.post = post < 1 ? 1 : post;
     A.coarseSweeps = coarseSweeps < 1 ? 1 : coarseSweeps;
+    A.lists = lists;
+    A.counts = counts;
     NB_COUNT_LAUNCH();
-    k_tail<T><<<1, 1024, off, st>>>(A);
+    k_tail<T><<<1, kTailThreads, off, st>>>(A);
 }
 
 template size_t TailSmemBytes<float>(const LevelView *, int);
 template size_t TailSmemBytes<double>(const LevelView *, int);
 template bool PrepareTail<float>(size_t);
 template bool PrepareTail<double>(size_t);
-template void LaunchTail<float>(const LevelView *, int, const float *, float *, int, int, int, cudaStream_t);
-template void LaunchTail<double>(const LevelView *, int, const double *, double *, int, int, int, cudaStream_t);
+template void LaunchTail<float>(const LevelView *, int, const float *, float *, int, int, int, const unsigned *,
+                                const int *, cudaStream_t);
+template void LaunchTail<double>(const LevelView *, int, const double *, double *, int, int, int, const unsigned *,
+                                 const int *, cudaStream_t);
 
 } // namespace nb
