@@ -238,6 +238,7 @@ void Context::BuildPairData()
         {
             if (Lv.sRS)
             {
+                PrepareSplitKernels();
                 Lv.du.alloc((size_t)(2 * Lv.sHalf));
                 Lv.du.zero(st); // the padding
                 if (v.stretched) LaunchSplitBytes(v, Lv.code.p, Lv.du.p, st);

@@ -89,21 +89,61 @@ __device__ __forceinline__ QuadPos QuadStart(const LevelView &v)
     return p;
 }
 
-// The launch grid of a quad kernel: planes per thread (1 .. kQuadMaxS) so that a launch has about `target` blocks.
-// The sweeps march far (each plane of the other colour is loaded once per chunk of planes, plus the two planes either
-// side); the kernels with more registers per thread take shorter chunks, so that their launches still fill several
-// waves of the 148 SMs.
-constexpr int kQuadMaxS = 16;
-constexpr long long kQuadBlocksSweep = 148 * 4; // first sweep, half-sweeps, residual (measured: 4 beats 8 and 16)
-constexpr long long kQuadBlocksOther = 148 * 8; // direction update and apply, prolongation (8 beats 24 and 48)
+// Resident blocks of a kernel per SM at kPairThreads threads (its registers and shared memory decide), and the SM
+// count of the current device.
+inline int ResidentBlocks(const void *fn)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kPairThreads, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
 
-inline dim3 QuadGrid(const LevelView &v, long long target)
+// read once per kernel (and before any stream capture: PrepareSplitKernels)
+template <auto kKernel> int Occ()
+{
+    static const int n = ResidentBlocks((const void *)kKernel);
+    return n;
+}
+
+inline int SmCount()
+{
+    int d = 0, c = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, d) != cudaSuccess || c < 1) c = 148;
+    return c;
+}
+
+// The launch grid of a quad kernel with `resident` blocks per SM: the longest march (planes per thread, at most
+// kQuadMaxS) whose launch fills the last wave of resident blocks to at least 90%; the longer the march, the fewer
+// planes of a neighbour array are loaded twice (a chunk of S planes loads S + 2). Measured on a 258^3 level: one
+// 92%-full wave of 16-plane chunks beats two waves of 8 (and 1.03 waves of 15 runs at half speed). With no such S,
+// the best-filled one (a small level fills no wave: S = 1, all the parallelism there is).
+constexpr int kQuadMaxS = 16;
+
+inline dim3 QuadGrid(const LevelView &v, int resident)
 {
     const long long nq = (long long)v.Nx * (v.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
     const long long planes = v.Ny - 2 > 0 ? v.Ny - 2 : 1;
-    long long S = (planes * perPlane + target - 1) / target;
-    S = S < 1 ? 1 : (S > kQuadMaxS ? kQuadMaxS : S);
-    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
+    const long long slots = (long long)SmCount() * (resident > 0 ? resident : 1);
+    long long bestS = 1;
+    double bestU = -1.0;
+    for (long long S = kQuadMaxS; S >= 1; S--)
+    {
+        const long long blocks = perPlane * ((planes + S - 1) / S);
+        const long long waves = (blocks + slots - 1) / slots;
+        const double u = (double)blocks / (double)(waves * slots);
+        if (u >= 0.9)
+        {
+            bestS = S;
+            break;
+        }
+        if (u > bestU + 1e-9)
+        {
+            bestU = u;
+            bestS = S;
+        }
+    }
+    return dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS));
 }
 
 // The other colour's k neighbours of a quad: the element at m (c) and the one at m + (q ? 1 : -1) (returned).
@@ -346,33 +386,47 @@ __global__ void __launch_bounds__(kPairThreads)
 void LaunchSplitFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
     if (v.stretched)
-        k_split_half<0, true, true><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(0), Reducer{}, nullptr, 0, 0, 0);
+    {
+        const int occ = Occ<k_split_half<0, true, true>>();
+        k_split_half<0, true, true><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(0), Reducer{},
+                                                                                 nullptr, 0, 0, 0);
+    }
     else
-        k_split_first<<<grid, kPairThreads, 0, st>>>(v, du, r, e);
+    {
+        const int occ = Occ<k_split_first>();
+        k_split_first<<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, r, e);
+    }
 }
 
 void LaunchSplitHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
     if (v.stretched)
-        k_split_half<0, true, false><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), Reducer{}, nullptr, 0,
-                                                                     0, 0);
+    {
+        const int occ = Occ<k_split_half<0, true, false>>();
+        k_split_half<0, true, false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), Reducer{},
+                                                                                  nullptr, 0, 0, 0);
+    }
     else
-        k_split_half<0, false, false><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), Reducer{}, nullptr, 0,
-                                                                      0, 0);
+    {
+        const int occ = Occ<k_split_half<0, false, false>>();
+        k_split_half<0, false, false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour),
+                                                                                   Reducer{}, nullptr, 0, 0, 0);
+    }
 }
 
 void LaunchSplitHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, bool last,
                         const Reducer &R, const int *it, int baseEven, int baseOdd, int partSlot, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
 #define NB_SPLIT_HALF(DOT, ST)                                                                                     \
-    k_split_half<DOT, ST, false><<<grid, kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), R, it, baseEven, baseOdd, \
-                                                                partSlot)
+    do                                                                                                             \
+    {                                                                                                              \
+        const int occ = Occ<k_split_half<DOT, ST, false>>();                         \
+        k_split_half<DOT, ST, false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), R, it,    \
+                                                                                baseEven, baseOdd, partSlot);      \
+    } while (0)
     if (last)
     {
         if (v.stretched) NB_SPLIT_HALF(2, true);
@@ -443,9 +497,16 @@ void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, 
                          cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    const dim3 grid = QuadGrid(v, kQuadBlocksSweep);
-    if (v.stretched) k_split_residual<true><<<grid, kPairThreads, 0, st>>>(v, du, r, e, res);
-    else k_split_residual<false><<<grid, kPairThreads, 0, st>>>(v, du, r, e, res);
+    if (v.stretched)
+    {
+        const int occ = Occ<k_split_residual<true>>();
+        k_split_residual<true><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, r, e, res);
+    }
+    else
+    {
+        const int occ = Occ<k_split_residual<false>>();
+        k_split_residual<false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, r, e, res);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -530,7 +591,8 @@ void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const ui
                         float *eFine, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_split_prolong<<<QuadGrid(fine, kQuadBlocksOther), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+    const int occ = Occ<k_split_prolong>();
+    k_split_prolong<<<QuadGrid(fine, occ), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
 }
 
 // r_c = R res_f = P^T res_f at the coarse unknowns, from the red fine residual. A thread owns one coarse cell (K along
@@ -719,10 +781,13 @@ void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, fl
                        int singular, int slotPQ, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    const dim3 grid = QuadGrid(v, kQuadBlocksOther);
 #define NB_SPLIT_PAPPLY(SING, ST)                                                                                  \
-    k_split_papply<SING, ST><<<grid, kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, \
-                                                            slotPQ)
+    do                                                                                                             \
+    {                                                                                                              \
+        const int occ = Occ<k_split_papply<SING, ST>>();                             \
+        k_split_papply<SING, ST><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven,  \
+                                                                            baseOdd, slotN, slotPQ);               \
+    } while (0)
     if (singular)
     {
         if (v.stretched) NB_SPLIT_PAPPLY(true, true);
@@ -837,6 +902,27 @@ void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b,
     NB_COUNT_LAUNCH();
     k_split_refine64<<<PairGrid(v, kSplitReduceS), kPairThreads, 0, st>>>(v, du, b, xin, e, xout, r, scale, sfac, R,
                                                                            slot);
+}
+
+
+// The occupancy of every split kernel, read outside any stream capture (the launchers size their grids from it).
+void PrepareSplitKernels()
+{
+    (void)Occ<k_split_first>();
+    (void)Occ<k_split_half<0, true, true>>();
+    (void)Occ<k_split_half<0, true, false>>();
+    (void)Occ<k_split_half<0, false, false>>();
+    (void)Occ<k_split_half<1, false, false>>();
+    (void)Occ<k_split_half<2, false, false>>();
+    (void)Occ<k_split_half<1, true, false>>();
+    (void)Occ<k_split_half<2, true, false>>();
+    (void)Occ<k_split_residual<true>>();
+    (void)Occ<k_split_residual<false>>();
+    (void)Occ<k_split_prolong>();
+    (void)Occ<k_split_papply<true, true>>();
+    (void)Occ<k_split_papply<true, false>>();
+    (void)Occ<k_split_papply<false, true>>();
+    (void)Occ<k_split_papply<false, false>>();
 }
 
 } // namespace nb
