@@ -517,74 +517,143 @@ void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, 
 // that the Neumann-aware prolongation moves from the cell's SOLID coarse contributors onto its parent.
 
 // e_f += P e_c on the red fine unknowns. Fine k = 2m + q (q = (a + b) & 1) lies between coarse k-cells m and m+1
-// with weights (3/4, 1/4) for q = 0 and (1/4, 3/4) for q = 1; its parent is m + q.
+// with weights (3/4, 1/4) for q = 0 and (1/4, 3/4) for q = 1; its parent is m + q. Fine row 2B-1 mixes coarse rows
+// B (3/4) and B-1 (1/4), row 2B rows B and B+1; planes the same way.
+//
+// A thread owns coarse row B and the fine quad m0 .. m0+3 of fine rows 2B-1 and 2B, and marches along the coarse
+// planes A: per coarse plane it interpolates three coarse rows across j once (k-cells m0 .. m0+4), and with the
+// neighbouring planes' rows (kept in registers) serves the four fine quads of fine planes 2A-1, 2A and rows 2B-1,
+// 2B, whose red values and bytes it loads together.
+
+// coarse k-cells m0 .. m0+4 of coarse row (A, B)
+__device__ __forceinline__ void CoarseRow5(const LevelView &cv, const float *__restrict__ ec, int A, int B, int m0,
+                                           float c[5])
+{
+    const int Dmax = cv.Nz - 1;
+    if (cv.sRS && m0 + 4 <= Dmax)
+    {
+        // a colour-split coarse level: k-cells m0, m0+2, m0+4 are elements m0/2 .. m0/2+2 of colour (A+B) & 1, and
+        // m0+1, m0+3 elements m0/2, m0/2+1 of the other (m0 is a multiple of 4)
+        const int ce = (A + B) & 1;
+        const float *rb = ec + (long long)A * cv.sPS + (long long)B * cv.sRS + (m0 >> 1);
+        const float2 ev = *reinterpret_cast<const float2 *>(rb + ce * cv.sHalf);
+        const float2 od = *reinterpret_cast<const float2 *>(rb + (ce ^ 1) * cv.sHalf);
+        c[0] = ev.x;
+        c[1] = od.x;
+        c[2] = ev.y;
+        c[3] = od.y;
+        c[4] = rb[ce * cv.sHalf + 2];
+        return;
+    }
+#pragma unroll
+    for (int t = 0; t < 5; t++) c[t] = ec[VecIdx(cv, A, B, min(m0 + t, Dmax))]; // past the row: masked cells only
+}
+
+// the coarse plane's rows interpolated across j for fine rows 2B-1 (y0) and 2B (y1), and row B itself (par)
+__device__ __forceinline__ void CoarsePlaneRows(const LevelView &cv, const float *__restrict__ ec, int A, int B,
+                                                int m0, float y0[5], float y1[5], float par[5])
+{
+    float cm[5], cp[5];
+    CoarseRow5(cv, ec, A, B, m0, par);
+    CoarseRow5(cv, ec, A, B - 1, m0, cm);
+    CoarseRow5(cv, ec, A, B + 1, m0, cp);
+#pragma unroll
+    for (int t = 0; t < 5; t++)
+    {
+        y0[t] = 0.75f * par[t] + 0.25f * cm[t];
+        y1[t] = 0.75f * par[t] + 0.25f * cp[t];
+    }
+}
+
 __global__ void __launch_bounds__(kPairThreads) k_split_prolong(LevelView fv, LevelView cv,
                                                                 const uint8_t *__restrict__ pext,
-                                                                const float *__restrict__ ec, float *ef)
+                                                                const float *__restrict__ ec, float *__restrict__ ef)
 {
-    const QuadPos P = QuadStart(fv);
-    const int b = P.j;
-    const int B = (b + 1) >> 1, B2 = B + ((b & 1) ? -1 : 1);
-    const int Dmax = cv.Nz - 1;
-    float *E = ef + P.off;
-    const uint8_t *X = pext + P.off;
-    long long o = 0;
-    for (int a = P.i0; a < P.i1; a++, o += P.PS)
+    const int Q = fv.sRS >> 2, nrow = cv.Nx - 2, nq = nrow * Q;
+    int t = blockIdx.x * kPairThreads + threadIdx.x;
+    const bool valid = t < nq;
+    if (!valid) t = nq - 1;
+    const int B = 1 + t / Q, m0 = 4 * (t - (B - 1) * Q);
+    const int S = (cv.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int A0 = min(1 + (int)blockIdx.y * S, cv.Ny - 1), A1 = min(A0 + S, cv.Ny - 1);
+    if (!valid || A0 >= A1) return;
+    float yM0[5], yM1[5], yC0[5], yC1[5], pC[5], pD[5];
+    CoarsePlaneRows(cv, ec, A0 - 1, B, m0, yM0, yM1, pD);
+    CoarsePlaneRows(cv, ec, A0, B, m0, yC0, yC1, pC);
+    const int fb0 = 2 * B - 1, fb1 = 2 * B;
+    for (int A = A0; A < A1; A++)
     {
-        const unsigned w = LdU4(X + o);
-        if (!P.valid || !(w & 0x80808080u)) continue;
-        const int A = (a + 1) >> 1, A2 = A + ((a & 1) ? -1 : 1);
-        const int q = (a + b) & 1;
-        float Cv[5], Par[5]; // coarse values interpolated across i and j at k-cells m0 .. m0+4, and the parent row's
-        if (cv.sRS && P.m0 + 4 <= Dmax)
+        float yP0[5], yP1[5], pP[5];
+        CoarsePlaneRows(cv, ec, A + 1, B, m0, yP0, yP1, pP);
+        // fine planes 2A-1 (with coarse plane A-1) and 2A (with A+1), rows 2B-1 and 2B
+#pragma unroll
+        for (int h = 0; h < 2; h++)
         {
-            // a colour-split coarse level: in coarse row (A', B') the k-cells m0, m0+2, m0+4 are elements m0/2 ..
-            // m0/2+2 of colour (A'+B') & 1 and m0+1, m0+3 elements m0/2, m0/2+1 of the other (m0 is a multiple of 4)
-            float row[4][5];
-            const int Ar[4] = {A, A, A2, A2}, Br[4] = {B, B2, B, B2};
+            const int fa = 2 * A - 1 + h;
+            const long long o0 = (long long)fa * fv.sPS + (long long)fb0 * fv.sRS + m0, o1 = o0 + fv.sRS;
+            const unsigned w0 = LdU4(pext + o0), w1 = LdU4(pext + o1);
+            F4 e0 = L4(ef + o0), e1 = L4(ef + o1);
+            const float *yo0 = h ? yP0 : yM0, *yo1 = h ? yP1 : yM1;
 #pragma unroll
-            for (int n = 0; n < 4; n++)
+            for (int rI = 0; rI < 2; rI++)
             {
-                const int ce = (Ar[n] + Br[n]) & 1;
-                const float *rb = ec + (long long)Ar[n] * cv.sPS + (long long)Br[n] * cv.sRS + (P.m0 >> 1);
-                const float2 ev = *reinterpret_cast<const float2 *>(rb + ce * cv.sHalf);
-                const float2 od = *reinterpret_cast<const float2 *>(rb + (ce ^ 1) * cv.sHalf);
-                row[n][0] = ev.x;
-                row[n][1] = od.x;
-                row[n][2] = ev.y;
-                row[n][3] = od.y;
-                row[n][4] = rb[ce * cv.sHalf + 2];
-            }
+                const unsigned w = rI ? w1 : w0;
+                if (!(w & 0x80808080u)) continue;
+                const int q = (fa + (rI ? fb1 : fb0)) & 1;
+                float z[5];
 #pragma unroll
-            for (int t = 0; t < 5; t++)
-            {
-                Cv[t] = 0.5625f * row[0][t] + 0.1875f * (row[1][t] + row[2][t]) + 0.0625f * row[3][t];
-                Par[t] = row[0][t];
-            }
-        }
-        else
-        {
+                for (int k = 0; k < 5; k++)
+                    z[k] = rI ? 0.75f * yC1[k] + 0.25f * yo1[k] : 0.75f * yC0[k] + 0.25f * yo0[k];
+                F4 &ev = rI ? e1 : e0;
 #pragma unroll
-            for (int t = 0; t < 5; t++)
-            {
-                const int D = min(P.m0 + t, Dmax); // past the row's end only for ring or padding cells (masked)
-                const float c00 = ec[VecIdx(cv, A, B, D)], c01 = ec[VecIdx(cv, A, B2, D)];
-                const float c10 = ec[VecIdx(cv, A2, B, D)], c11 = ec[VecIdx(cv, A2, B2, D)];
-                Cv[t] = 0.5625f * c00 + 0.1875f * (c01 + c10) + 0.0625f * c11;
-                Par[t] = c00;
+                for (int x = 0; x < 4; x++)
+                {
+                    const unsigned px = Byte(w, x);
+                    if (!(px & 0x80u)) continue;
+                    const float lohi = q ? 0.25f * z[x] + 0.75f * z[x + 1] : 0.75f * z[x] + 0.25f * z[x + 1];
+                    ev.v[x] += lohi + (float)(px & 0x3Fu) * (1.0f / 64.0f) * (q ? pC[x + 1] : pC[x]);
+                }
+                S4(ef + (rI ? o1 : o0), ev);
             }
         }
-        F4 ev = L4(E + o);
 #pragma unroll
-        for (int x = 0; x < 4; x++)
+        for (int k = 0; k < 5; k++)
         {
-            const unsigned px = Byte(w, x);
-            if (!(px & 0x80u)) continue;
-            const float lohi = q ? 0.25f * Cv[x] + 0.75f * Cv[x + 1] : 0.75f * Cv[x] + 0.25f * Cv[x + 1];
-            ev.v[x] += lohi + (float)(px & 0x3Fu) * (1.0f / 64.0f) * (q ? Par[x + 1] : Par[x]);
+            yM0[k] = yC0[k];
+            yM1[k] = yC1[k];
+            yC0[k] = yP0[k];
+            yC1[k] = yP1[k];
+            pC[k] = pP[k];
         }
-        S4(E + o, ev);
     }
+}
+
+// The grid of k_split_prolong: threads over (coarse row, fine quad), grid.y chunks of coarse planes sized like
+// QuadGrid's (the longest march with a full last wave).
+inline dim3 ProlongGrid(const LevelView &fine, const LevelView &coarse, int resident)
+{
+    const long long nq = (long long)(coarse.Nx - 2) * (fine.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
+    const long long planes = coarse.Ny - 2 > 0 ? coarse.Ny - 2 : 1;
+    const long long slots = (long long)SmCount() * (resident > 0 ? resident : 1);
+    long long bestS = 1;
+    double bestU = -1.0;
+    for (long long S = kQuadMaxS; S >= 1; S--)
+    {
+        const long long blocks = perPlane * ((planes + S - 1) / S);
+        const long long waves = (blocks + slots - 1) / slots;
+        const double u = (double)blocks / (double)(waves * slots);
+        if (u >= 0.9)
+        {
+            bestS = S;
+            break;
+        }
+        if (u > bestU + 1e-9)
+        {
+            bestU = u;
+            bestS = S;
+        }
+    }
+    return dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS));
 }
 
 void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
@@ -592,7 +661,7 @@ void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const ui
 {
     NB_COUNT_LAUNCH();
     const int occ = Occ<k_split_prolong>();
-    k_split_prolong<<<QuadGrid(fine, occ), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+    k_split_prolong<<<ProlongGrid(fine, coarse, occ), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
 }
 
 // r_c = R res_f = P^T res_f at the coarse unknowns, from the red fine residual. A thread owns one coarse cell (K along
