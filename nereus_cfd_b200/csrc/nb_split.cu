@@ -664,12 +664,86 @@ void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const ui
     k_split_prolong<<<ProlongGrid(fine, coarse, occ), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
 }
 
-// r_c = R res_f = P^T res_f at the coarse unknowns, from the red fine residual. A thread owns one coarse cell (K along
-// the 32 lanes, J across the 8 warps) and marches along I: fine planes 2I-2 .. 2I+1 enter as their (j, k)-weighted
-// 4x4 sums T(a), each kept for the next coarse plane; the red children's moved weights enter as X(a). In fine row
-// (a, b) the red cells among k = 2K-2 .. 2K+1 are elements K-1 and K, at k = 2K-2+q and 2K+q (q = (a + b) & 1),
-// and the red child of coarse K is element K - q.
-__device__ __forceinline__ void SplitRestrictPlane(const LevelView &fv, const uint8_t *pext, const float *res, int a,
+// r_c = R res_f = P^T res_f at the coarse unknowns, from the red fine residual. A thread owns four consecutive coarse
+// cells K0 .. K0+3 (K0 = 1 + 4 t) of coarse row J (one flat index over (J, t)) and marches along I: fine planes
+// 2I-2 .. 2I+1 enter as their (j, k)-weighted 4x4 sums T(a), each kept for the next coarse plane; the red children's
+// moved weights enter as X(a). In fine row (a, b) the red cells among k = 2K-2 .. 2K+1 are elements K-1 and K, at
+// k = 2K-2+q and 2K+q (q = (a + b) & 1), and the red child of coarse K is element K - q; the five elements
+// K0-1 .. K0+3 of a row are one aligned float4 and one more.
+__device__ __forceinline__ void SplitRestrictPlane(const LevelView &fv, const uint8_t *__restrict__ pext,
+                                                   const float *__restrict__ res, int a, int J, int K0, bool five,
+                                                   float T[4], float X[4])
+{
+#pragma unroll
+    for (int x = 0; x < 4; x++) T[x] = X[x] = 0.f;
+    if (a > fv.Ny - 1) return;
+    const float wt[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+#pragma unroll
+    for (int dj = 0; dj < 4; dj++)
+    {
+        const int b = 2 * J - 2 + dj;
+        if (b > fv.Nx - 1) continue;
+        const int q = (a + b) & 1;
+        const long long row = (long long)a * fv.sPS + (long long)b * fv.sRS + (K0 - 1);
+        const F4 r4 = L4(res + row);
+        const float R[5] = {r4.v[0], r4.v[1], r4.v[2], r4.v[3], five ? res[row + 4] : 0.f};
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+            T[x] += wt[dj] * (q ? 0.75f * R[x] + 0.25f * R[x + 1] : 0.25f * R[x] + 0.75f * R[x + 1]);
+        if (dj == 1 || dj == 2)
+        {
+            const unsigned w = LdU4(pext + row);
+            const unsigned w4 = five ? pext[row + 4] : 0u;
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+            {
+                // the red child of coarse K0 + x is element K0 + x - q: index x + 1 - q of the five
+                const unsigned pw = q ? Byte(w, x) : (x < 3 ? Byte(w, x + 1) : w4);
+                X[x] += (float)(pw & 0x3Fu) * R[x + 1 - q];
+            }
+        }
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++) X[x] *= 1.0f / 64.0f;
+}
+
+__global__ void __launch_bounds__(kPairThreads) k_split_restrict(LevelView fv, LevelView cv,
+                                                                 const uint8_t *__restrict__ pext,
+                                                                 const float *__restrict__ res, float *__restrict__ rc)
+{
+    const int nq = (cv.Nz - 2 + 3) / 4, nt = (cv.Nx - 2) * nq;
+    const int t = blockIdx.x * kPairThreads + threadIdx.x;
+    if (t >= nt) return;
+    const int J = 1 + t / nq, K0 = 1 + 4 * (t - (J - 1) * nq);
+    const int S = (cv.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int I0 = 1 + (int)blockIdx.y * S, I1 = min(I0 + S, cv.Ny - 1);
+    if (I0 >= I1) return;
+    const bool five = K0 + 3 <= cv.Nz - 2; // element K0+3 is read only for coarse cell K0+3
+    float Tm2[4], Tm1[4], Xm1[4], Xd[4];
+    SplitRestrictPlane(fv, pext, res, 2 * I0 - 2, J, K0, five, Tm2, Xd);
+    SplitRestrictPlane(fv, pext, res, 2 * I0 - 1, J, K0, five, Tm1, Xm1);
+    for (int I = I0; I < I1; I++)
+    {
+        float T0[4], X0[4], T1[4], X1[4];
+        SplitRestrictPlane(fv, pext, res, 2 * I, J, K0, five, T0, X0);
+        SplitRestrictPlane(fv, pext, res, 2 * I + 1, J, K0, five, T1, X1);
+        const long long c = (long long)I * cv.sI + (long long)J * cv.sJ + K0;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+        {
+            if (K0 + x <= cv.Nz - 2 && (cv.code[c + x] & CODE_UNKNOWN))
+                rc[VecIdx(cv, I, J, K0 + x)] =
+                    ((0.25f * Tm2[x] + 0.75f * Tm1[x]) + (0.75f * T0[x] + 0.25f * T1[x])) + (Xm1[x] + X0[x]);
+            Tm2[x] = T0[x];
+            Tm1[x] = T1[x];
+            Xm1[x] = X1[x];
+        }
+    }
+}
+
+// The same restriction with one thread per coarse cell (K along the 32 lanes, J across the 8 warps), for the smaller
+// coarse levels: more threads, and their launches are latency-bound.
+__device__ __forceinline__ void SplitRestrictPlane1(const LevelView &fv, const uint8_t *pext, const float *res, int a,
                                                    int J, int K, float &T, float &X)
 {
     T = 0.f;
@@ -690,7 +764,7 @@ __device__ __forceinline__ void SplitRestrictPlane(const LevelView &fv, const ui
     X *= 1.0f / 64.0f;
 }
 
-__global__ void __launch_bounds__(256) k_split_restrict(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
+__global__ void __launch_bounds__(256) k_split_restrict1(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
                                                         const float *__restrict__ res, float *__restrict__ rc)
 {
     const int K = 1 + blockIdx.x * 32 + threadIdx.x, J = 1 + blockIdx.y * 8 + threadIdx.y;
@@ -699,13 +773,13 @@ __global__ void __launch_bounds__(256) k_split_restrict(LevelView fv, LevelView 
     const int I0 = 1 + (int)blockIdx.z * S, I1 = min(I0 + S, cv.Ny - 1);
     if (I0 >= I1) return;
     float Tm2, Tm1, Xm1, Xdummy;
-    SplitRestrictPlane(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
-    SplitRestrictPlane(fv, pext, res, 2 * I0 - 1, J, K, Tm1, Xm1);
+    SplitRestrictPlane1(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
+    SplitRestrictPlane1(fv, pext, res, 2 * I0 - 1, J, K, Tm1, Xm1);
     for (int I = I0; I < I1; I++)
     {
         float T0, X0, T1, X1;
-        SplitRestrictPlane(fv, pext, res, 2 * I, J, K, T0, X0);
-        SplitRestrictPlane(fv, pext, res, 2 * I + 1, J, K, T1, X1);
+        SplitRestrictPlane1(fv, pext, res, 2 * I, J, K, T0, X0);
+        SplitRestrictPlane1(fv, pext, res, 2 * I + 1, J, K, T1, X1);
         const long long c = (long long)I * cv.sI + (long long)J * cv.sJ + K;
         if (cv.code[c] & CODE_UNKNOWN)
             rc[VecIdx(cv, I, J, K)] = ((0.25f * Tm2 + 0.75f * Tm1) + (0.75f * T0 + 0.25f * T1)) + (Xm1 + X0);
@@ -715,15 +789,46 @@ __global__ void __launch_bounds__(256) k_split_restrict(LevelView fv, LevelView 
     }
 }
 
+// Coarse levels with at least kRestrictQuadCells cells take the quad kernel (4x fewer loads per coarse cell), the
+// smaller ones the per-cell kernel.
+constexpr long long kRestrictQuadCells = 1LL << 20;
+
 void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
                          float *rCoarse, cudaStream_t st)
 {
-    const long long perPlane = (long long)((coarse.Nz - 2 + 31) / 32) * ((coarse.Nx - 2 + 7) / 8);
-    const int S = MarchPlanes(coarse.Ny - 2, perPlane);
-    const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
-                    (unsigned)((coarse.Ny - 2 + S - 1) / S));
     NB_COUNT_LAUNCH();
-    k_split_restrict<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
+    if (coarse.cells < kRestrictQuadCells)
+    {
+        const long long perPlane = (long long)((coarse.Nz - 2 + 31) / 32) * ((coarse.Nx - 2 + 7) / 8);
+        const int S = MarchPlanes(coarse.Ny - 2, perPlane);
+        const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
+                        (unsigned)((coarse.Ny - 2 + S - 1) / S));
+        k_split_restrict1<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
+        return;
+    }
+    const long long nt = (long long)(coarse.Nx - 2) * ((coarse.Nz - 2 + 3) / 4);
+    const long long perPlane = (nt + kPairThreads - 1) / kPairThreads, planes = coarse.Ny - 2 > 0 ? coarse.Ny - 2 : 1;
+    const long long slots = (long long)SmCount() * Occ<k_split_restrict>();
+    long long bestS = 1;
+    double bestU = -1.0;
+    for (long long S = kQuadMaxS; S >= 1; S--)
+    {
+        const long long blocks = perPlane * ((planes + S - 1) / S);
+        const long long waves = (blocks + slots - 1) / slots;
+        const double u = (double)blocks / (double)(waves * slots);
+        if (u >= 0.9)
+        {
+            bestS = S;
+            break;
+        }
+        if (u > bestU + 1e-9)
+        {
+            bestU = u;
+            bestS = S;
+        }
+    }
+    k_split_restrict<<<dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS)), kPairThreads, 0, st>>>(
+        fine, coarse, pext, resFine, rCoarse);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -988,6 +1093,7 @@ void PrepareSplitKernels()
     (void)Occ<k_split_residual<true>>();
     (void)Occ<k_split_residual<false>>();
     (void)Occ<k_split_prolong>();
+    (void)Occ<k_split_restrict>();
     (void)Occ<k_split_papply<true, true>>();
     (void)Occ<k_split_papply<true, false>>();
     (void)Occ<k_split_papply<false, true>>();
