@@ -153,7 +153,10 @@ void Context::BuildHierarchy()
         const int nx = F.Nx - 2, ny = F.Ny - 2, nz = dim == 3 ? F.Nz - 2 : 1;
         const int mn = dim == 3 ? std::min(nx, std::min(ny, nz)) : std::min(nx, ny);
         const long long interior = (long long)nx * ny * nz;
-        if (mn < 4 || interior <= 8) break; // down to about 2 cells a side: the coarse end runs in shared memory
+        // down to 4 .. 7 cells a side (at most a few hundred unknowns), solved by sweeps in the shared-memory tail:
+        // one level more, of a handful of unknowns, made no difference to the iteration counts measured and only
+        // lengthened the tail's serial phases
+        if (mn < 8 || interior <= 64) break;
         LevelData C = take(L.size());
         C.dim = dim;
         C.Nx = (nx + 1) / 2 + 2;
@@ -203,12 +206,13 @@ void Context::BuildHierarchy()
     cudaGetLastError(); // an attribute the device refuses leaves the per-colour path, checked at launch
 }
 
-// The colour-split levels (pair_kernels = 2, mixed precision): the 3D levels with Nz even above the coarse end, as
-// long as every finer level is one too (a level's transfers read and write the next coarser level in either layout,
-// the grid-layout kernels only the grid layout).
+// The colour-split levels (pair_kernels = 2, mixed precision): the uniform 3D levels with Nz even above the coarse
+// end, as long as every finer level is one too (a level's transfers read and write the next coarser level in either
+// layout, the grid-layout kernels only the grid layout). A stretched grid keeps the cell-pair kernels: its
+// per-cell coefficients make the split kernels compute-bound (measured slower on the stretched cylinder).
 void Context::AssignSplit()
 {
-    const bool on = opt.precision == NB_PRECISION_MIXED && opt.pair_kernels == 2 && !opt.fused_sweeps;
+    const bool on = opt.precision == NB_PRECISION_MIXED && opt.pair_kernels == 2 && !opt.fused_sweeps && !nonuniform;
     bool finer = true;
     for (size_t l = 0; l < L.size(); l++)
     {
