@@ -407,6 +407,30 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
     }
 }
 
+// ---- programmatic dependent launch: a kernel launched by LaunchPdl may be scheduled while the previous kernel on
+// its stream drains. It calls PdlWait() before reading anything an earlier kernel wrote (the wait returns once that
+// grid has completed and its writes are visible), then PdlTrigger(), which lets the next kernel start launching in
+// turn. A kernel launched plainly runs both as no-ops. ----
+__device__ __forceinline__ void PdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void PdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t LaunchPdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                             Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Grid size for a level's line kernels: enough blocks to cover the lines, at most a few waves of the 148 SMs.
 inline int LineGrid(int nLines, int maxBlocks)
 {

@@ -101,11 +101,10 @@ void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const flo
                  int slotPQ, int slotRR, cudaStream_t st);
 
 // ---- nb_split.cu: FP32 kernels for 3D levels with Nz even in the colour-split layout (LevelView::sRS) ----
-// du: the level's bytes in that layout (diagonal units; the codes on a stretched level); pext: the red cells' bytes
-void LaunchSplitBytes(const LevelView &v, const uint8_t *in, uint8_t *out, cudaStream_t st);
+// uniform levels only; du: the level's diagonal units in that layout; pext: the red cells' bytes
 // reads the kernels' occupancy (their grids follow it); call before capturing launches into a graph
 void PrepareSplitKernels();
-// the first red-black sweep from a zero iterate (a stretched level: its red half; the black half follows)
+// the first red-black sweep from a zero iterate
 void LaunchSplitFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st);
 void LaunchSplitHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st);
 // the post-smoothing's last sweep on level 0: the black half (last = false) sums its (r.z, z, r) into

@@ -800,6 +800,8 @@ __global__ void __launch_bounds__(256) k_lin_xr(long long cells, float *__restri
                                                 Reducer R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
                                                 int singular, int slotPQ, int slotRR)
 {
+    PdlWait();
+    PdlTrigger();
     const int par = *it & 1;
     const float *__restrict__ p = par ? p0 : p1;
     const int base = par ? baseOdd : baseEven;
@@ -840,8 +842,8 @@ void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const flo
                  int slotPQ, int slotRR, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_lin_xr<<<kLinBlocks, 256, 0, st>>>(cells, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, singular, slotPQ,
-                                         slotRR);
+    LaunchPdl(k_lin_xr, dim3(kLinBlocks), dim3(256), 0, st, cells, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN,
+              singular, slotPQ, slotRR);
 }
 
 } // namespace nb

@@ -245,8 +245,7 @@ void Context::BuildPairData()
                 PrepareSplitKernels();
                 Lv.du.alloc((size_t)(2 * Lv.sHalf));
                 Lv.du.zero(st); // the padding
-                if (v.stretched) LaunchSplitBytes(v, Lv.code.p, Lv.du.p, st);
-                else LaunchBuildDu(v, Lv.du.p, st);
+                LaunchBuildDu(v, Lv.du.p, st);
             }
             else
             {
@@ -745,15 +744,14 @@ void Context::VCyclePairs(int l, float *r, float *e)
         }
 }
 
-// The V-cycle on a colour-split level (nb_split.cu): the first sweep from zero (one launch on a uniform level, a red
-// and a black one on a stretched level), further sweeps one colour per launch, the residual and the transfers on the
+// The V-cycle on a colour-split level (nb_split.cu): the first sweep from zero in one launch, further sweeps one
+// colour per launch, the residual and the transfers on the
 // red cells (the black residual after a black half-sweep is zero; the post-smoothing's black half replaces the black
 // values without reading them), and on level 0 the (r.z, z, r) sums of the last sweep, black then red.
 void Context::VCycleSplit(int l, float *r, float *e)
 {
     LevelData &Lv = L[l];
     const LevelView v = Lv.view();
-    const bool stretched = v.stretched != 0;
     const double s = sizeof(float), cells = (double)Lv.cells;
     auto prof = [&](int id, double bytesPerCell) {
         ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
@@ -762,21 +760,9 @@ void Context::VCycleSplit(int l, float *r, float *e)
     // one colour: reads the other colour, and r and the bytes of its own; writes its own
     const double half = (3.0 * s + 1.0) / 2.0;
     const uint8_t *du = Lv.du.p;
-    if (stretched)
-    {
-        prof(NB_K_SMOOTH0, (2.0 * s + 1.0) / 2.0); // red from zero: reads r and the bytes of red, writes red
-        LaunchSplitFirst(v, du, r, e, st);
-        ProfEnd();
-        prof(NB_K_SMOOTH0, half);
-        LaunchSplitHalf(v, du, r, e, 1, st);
-        ProfEnd();
-    }
-    else
-    {
-        prof(NB_K_SMOOTH0, 2.0 * s + 1.0); // reads r and the bytes, writes e
-        LaunchSplitFirst(v, du, r, e, st);
-        ProfEnd();
-    }
+    prof(NB_K_SMOOTH0, 2.0 * s + 1.0); // reads r and the bytes, writes e
+    LaunchSplitFirst(v, du, r, e, st);
+    ProfEnd();
     for (int q = 1; q < pre; q++)
         for (int c = 0; c < 2; c++)
         {

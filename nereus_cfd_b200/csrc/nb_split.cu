@@ -14,10 +14,10 @@
 // registers. The j neighbours are the quads RS elements away; the element across the quad's edge comes from the
 // neighbouring lane (a shuffle; lanes 0 and 31 load it).
 //
-// Every vector is zero off the unknowns (and on the padding), so the neighbour sum runs over all six neighbours.
-// On a uniform level the coefficient is gamma everywhere and the diagonal is gamma/2 times the unit count in the
-// level's byte array (0x80 | units, 0 off the unknowns), divided through a 32-entry reciprocal table; on a
-// stretched level the byte array holds the cell codes and the coefficients come from the level's tables.
+// Every vector is zero off the unknowns (and on the padding), so the neighbour sum runs over all six neighbours. The
+// levels are uniform (a stretched grid keeps the cell-pair kernels of nb_pairs.cu): the coefficient is gamma
+// everywhere and the diagonal is gamma/2 times the unit count in the level's byte array (0x80 | units, 0 off the
+// unknowns), divided through a 32-entry reciprocal table.
 //
 // The V-cycle on these levels (nb_solver.cu, VCycleSplit) uses two facts of red-black Gauss-Seidel:
 // - after a black half-sweep the black residual is zero (each black equation was just solved), so the residual and
@@ -162,45 +162,10 @@ __device__ __forceinline__ void Edges(const QuadPos &P, const F4 &c, const float
     if (P.lane == 31) nextX = P.m0 + 4 < P.RS ? row[4] : 0.f;
 }
 
-// sum_q c_q x_q over the six neighbours of unknown cell (i, j, k) of a stretched level, and its diagonal
-__device__ __forceinline__ float StencilSum(const LevelView &v, int i, int j, int k, unsigned code, float nP, float nM,
-                                            float nJp, float nJm, float nKp, float nKm, float &diag)
-{
-    float cq[6];
-    const long long c = (long long)i * v.sI + (long long)j * v.sJ + k;
-    CodeStencil<float>(v, i, j, k, c, code, cq, diag);
-    return ((cq[0] * nP + cq[1] * nM) + (cq[2] * nJp + cq[3] * nJm)) + (cq[4] * nKp + cq[5] * nKm);
-}
-
 } // namespace
 
 // planes per thread at least in the pair-thread launches that end in a grid-wide sum
 constexpr int kSplitReduceS = 16;
-
-// ---------------------------------------------------------------------------------------------------------------
-// level bytes
-// ---------------------------------------------------------------------------------------------------------------
-// Scatter per-cell bytes (a level's codes) into the colour-split layout; `out` was zeroed (the padding stays 0).
-__global__ void k_split_bytes(LevelView v, const uint8_t *__restrict__ in, uint8_t *__restrict__ out)
-{
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < v.cells;
-         c += (long long)gridDim.x * blockDim.x)
-    {
-        const int k = (int)(c % v.Nz);
-        const long long rr = c / v.Nz;
-        const int j = (int)(rr % v.Nx), i = (int)(rr / v.Nx);
-        out[VecIdx(v, i, j, k)] = in[c];
-    }
-}
-
-void LaunchSplitBytes(const LevelView &v, const uint8_t *in, uint8_t *out, cudaStream_t st)
-{
-    int blocks = (int)((v.cells + 255) / 256);
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    if (blocks < 1) blocks = 1;
-    NB_COUNT_LAUNCH();
-    k_split_bytes<<<blocks, 256, 0, st>>>(v, in, out);
-}
 
 // ---------------------------------------------------------------------------------------------------------------
 // smoothing
@@ -212,6 +177,8 @@ void LaunchSplitBytes(const LevelView &v, const uint8_t *in, uint8_t *out, cudaS
 __global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const uint8_t *__restrict__ du,
                                                               const float *__restrict__ r, float *__restrict__ e)
 {
+    PdlWait();
+    PdlTrigger();
     __shared__ float inv[32];
     FillInv(inv, v.gamma);
     const QuadPos P = QuadStart(v);
@@ -256,20 +223,21 @@ __global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const
     }
 }
 
-// One colour of a red-black sweep: e_c = (r_c + sum_q c_q e_q) / diag_c over the other colour's neighbours.
-// kSt: a stretched level (du holds the codes). kFirst (stretched only): the red pass from a zero iterate, r / diag.
+// One colour of a red-black sweep: e_c = (r_c + gamma * sum of the other colour's six neighbours) / diag_c.
 // kDot 1: (sum r.e, sum e, sum r) of this colour into out[partSlot..]; kDot 2: the same plus the totals already in
 // out[partSlot..], into the scalar block of the iteration's parity (the CG's r.z, sum z, sum r of the V-cycle's z).
 // du, r: this colour's halves; eo, ec: the other colour's and this colour's halves of e (disjoint).
-template <int kDot, bool kSt, bool kFirst>
+template <int kDot>
 __global__ void __launch_bounds__(kPairThreads)
     k_split_half(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ r,
                  const float *__restrict__ eo, float *__restrict__ ec, int colour, Reducer R, const int *it,
                  int baseEven, int baseOdd, int partSlot)
 {
+    PdlWait();
+    PdlTrigger();
     float facc[3] = {0.f, 0.f, 0.f}; // a thread's terms in FP32, the block and grid sums in FP64
     __shared__ float inv[32];
-    if (!kSt) FillInv(inv, v.gamma);
+    FillInv(inv, v.gamma);
     const QuadPos P = QuadStart(v);
     const float g = (float)v.gamma;
     const float *O = eo + P.off;
@@ -283,12 +251,9 @@ __global__ void __launch_bounds__(kPairThreads)
     {
         rr = L4(Rr);
         d = LdU4(D);
-        if (!kFirst)
-        {
-            oM = L4(O - P.PS);
-            oC = L4(O);
-            oP = L4(O + P.PS);
-        }
+        oM = L4(O - P.PS);
+        oC = L4(O);
+        oP = L4(O + P.PS);
     }
     long long o = 0;
     for (int i = P.i0; i < P.i1; i++, o += P.PS)
@@ -297,51 +262,20 @@ __global__ void __launch_bounds__(kPairThreads)
         unsigned dn = 0;
         if (i + 1 < P.i1)
         {
-            if (!kFirst) oPn = L4(O + o + 2 * P.PS);
+            oPn = L4(O + o + 2 * P.PS);
             rrn = L4(Rr + o + P.PS);
             dn = LdU4(D + o + P.PS);
         }
-        F4 oJp{}, oJm{}, sh{};
-        const int q = (i + P.j + colour) & 1;
-        if (!kFirst)
-        {
-            oJp = L4(O + o + P.RS);
-            oJm = L4(O + o - P.RS);
-            float prevW, nextX;
-            Edges(P, oC, O + o, prevW, nextX);
-            sh = KShift(oC, prevW, nextX, q);
-        }
+        const F4 oJp = L4(O + o + P.RS), oJm = L4(O + o - P.RS);
+        float prevW, nextX;
+        Edges(P, oC, O + o, prevW, nextX);
+        const F4 sh = KShift(oC, prevW, nextX, (i + P.j + colour) & 1);
         F4 nv;
 #pragma unroll
         for (int x = 0; x < 4; x++)
         {
-            const unsigned b = Byte(d, x);
-            if (!kSt)
-            {
-                const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
-                nv.v[x] = (rr.v[x] + g * s) * inv[b & 0x7Fu];
-            }
-            else
-            {
-                nv.v[x] = 0.f;
-                if (b & CODE_UNKNOWN)
-                {
-                    const int k = 2 * (P.m0 + x) + q;
-                    float diag, s = 0.f;
-                    if (kFirst)
-                    {
-                        float cq[6];
-                        const long long c = (long long)i * v.sI + (long long)P.j * v.sJ + k;
-                        CodeStencil<float>(v, i, P.j, k, c, b, cq, diag);
-                    }
-                    else
-                    {
-                        const float kp = q ? sh.v[x] : oC.v[x], km = q ? oC.v[x] : sh.v[x];
-                        s = StencilSum(v, i, P.j, k, b, oP.v[x], oM.v[x], oJp.v[x], oJm.v[x], kp, km, diag);
-                    }
-                    nv.v[x] = diag != 0.f ? (rr.v[x] + s) / diag : 0.f;
-                }
-            }
+            const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
+            nv.v[x] = (rr.v[x] + g * s) * inv[Byte(d, x) & 0x7Fu];
         }
         if (P.valid)
         {
@@ -357,12 +291,9 @@ __global__ void __launch_bounds__(kPairThreads)
                 }
             }
         }
-        if (!kFirst)
-        {
-            oM = oC;
-            oC = oP;
-            oP = oPn;
-        }
+        oM = oC;
+        oC = oP;
+        oP = oPn;
         rr = rrn;
         d = dn;
     }
@@ -386,68 +317,37 @@ __global__ void __launch_bounds__(kPairThreads)
 void LaunchSplitFirst(const LevelView &v, const uint8_t *du, const float *r, float *e, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    if (v.stretched)
-    {
-        const int occ = Occ<k_split_half<0, true, true>>();
-        k_split_half<0, true, true><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(0), Reducer{},
-                                                                                 nullptr, 0, 0, 0);
-    }
-    else
-    {
-        const int occ = Occ<k_split_first>();
-        k_split_first<<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, r, e);
-    }
+    LaunchPdl(k_split_first, QuadGrid(v, Occ<k_split_first>()), kPairThreads, 0, st, v, du, r, e);
 }
 
 void LaunchSplitHalf(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    if (v.stretched)
-    {
-        const int occ = Occ<k_split_half<0, true, false>>();
-        k_split_half<0, true, false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), Reducer{},
-                                                                                  nullptr, 0, 0, 0);
-    }
-    else
-    {
-        const int occ = Occ<k_split_half<0, false, false>>();
-        k_split_half<0, false, false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour),
-                                                                                   Reducer{}, nullptr, 0, 0, 0);
-    }
+    LaunchPdl(k_split_half<0>, QuadGrid(v, Occ<k_split_half<0>>()), kPairThreads, 0, st, NB_SPLIT_HALF_ARGS(colour),
+              Reducer{}, (const int *)nullptr, 0, 0, 0);
 }
 
 void LaunchSplitHalfDot(const LevelView &v, const uint8_t *du, const float *r, float *e, int colour, bool last,
                         const Reducer &R, const int *it, int baseEven, int baseOdd, int partSlot, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-#define NB_SPLIT_HALF(DOT, ST)                                                                                     \
-    do                                                                                                             \
-    {                                                                                                              \
-        const int occ = Occ<k_split_half<DOT, ST, false>>();                         \
-        k_split_half<DOT, ST, false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(NB_SPLIT_HALF_ARGS(colour), R, it,    \
-                                                                                baseEven, baseOdd, partSlot);      \
-    } while (0)
     if (last)
-    {
-        if (v.stretched) NB_SPLIT_HALF(2, true);
-        else NB_SPLIT_HALF(2, false);
-    }
+        LaunchPdl(k_split_half<2>, QuadGrid(v, Occ<k_split_half<2>>()), kPairThreads, 0, st,
+                  NB_SPLIT_HALF_ARGS(colour), R, it, baseEven, baseOdd, partSlot);
     else
-    {
-        if (v.stretched) NB_SPLIT_HALF(1, true);
-        else NB_SPLIT_HALF(1, false);
-    }
-#undef NB_SPLIT_HALF
+        LaunchPdl(k_split_half<1>, QuadGrid(v, Occ<k_split_half<1>>()), kPairThreads, 0, st,
+                  NB_SPLIT_HALF_ARGS(colour), R, it, baseEven, baseOdd, partSlot);
 }
 #undef NB_SPLIT_HALF_ARGS
 
 // res = r - M e on the red cells (colour 0), into the first half of `res`; the black residual after a black
 // half-sweep is zero.
-template <bool kSt>
 __global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, const uint8_t *__restrict__ du,
                                                                  const float *__restrict__ r,
                                                                  const float *__restrict__ e, float *__restrict__ res)
 {
+    PdlWait();
+    PdlTrigger();
     const QuadPos P = QuadStart(v);
     const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
     const float *O = e + v.sHalf + P.off;
@@ -462,30 +362,16 @@ __global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, co
         const F4 oP = L4(O + o + P.PS), oJp = L4(O + o + P.RS), oJm = L4(O + o - P.RS);
         const F4 xc = L4(Xr + o), rr = L4(Rr + o);
         const unsigned d = LdU4(D + o);
-        const int q = (i + P.j) & 1;
         float prevW, nextX;
         Edges(P, oC, O + o, prevW, nextX);
-        const F4 sh = KShift(oC, prevW, nextX, q);
+        const F4 sh = KShift(oC, prevW, nextX, (i + P.j) & 1);
         F4 out;
 #pragma unroll
         for (int x = 0; x < 4; x++)
         {
             const unsigned b = Byte(d, x);
-            out.v[x] = 0.f;
-            if (!(b & 0x80u)) continue;
-            if (!kSt)
-            {
-                const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
-                out.v[x] = rr.v[x] - (hg * (float)(b & 0x7Fu) * xc.v[x] - g * s);
-            }
-            else
-            {
-                const int k = 2 * (P.m0 + x) + q;
-                const float kp = q ? sh.v[x] : oC.v[x], km = q ? oC.v[x] : sh.v[x];
-                float diag;
-                const float s = StencilSum(v, i, P.j, k, b, oP.v[x], oM.v[x], oJp.v[x], oJm.v[x], kp, km, diag);
-                out.v[x] = rr.v[x] - (diag * xc.v[x] - s);
-            }
+            const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
+            out.v[x] = (b & 0x80u) ? rr.v[x] - (hg * (float)(b & 0x7Fu) * xc.v[x] - g * s) : 0.f;
         }
         if (P.valid) S4(Out + o, out);
         oM = oC;
@@ -497,16 +383,7 @@ void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, 
                          cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    if (v.stretched)
-    {
-        const int occ = Occ<k_split_residual<true>>();
-        k_split_residual<true><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, r, e, res);
-    }
-    else
-    {
-        const int occ = Occ<k_split_residual<false>>();
-        k_split_residual<false><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, r, e, res);
-    }
+    LaunchPdl(k_split_residual, QuadGrid(v, Occ<k_split_residual>()), kPairThreads, 0, st, v, du, r, e, res);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -569,6 +446,8 @@ __global__ void __launch_bounds__(kPairThreads) k_split_prolong(LevelView fv, Le
                                                                 const uint8_t *__restrict__ pext,
                                                                 const float *__restrict__ ec, float *__restrict__ ef)
 {
+    PdlWait();
+    PdlTrigger();
     const int Q = fv.sRS >> 2, nrow = cv.Nx - 2, nq = nrow * Q;
     int t = blockIdx.x * kPairThreads + threadIdx.x;
     const bool valid = t < nq;
@@ -661,7 +540,8 @@ void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const ui
 {
     NB_COUNT_LAUNCH();
     const int occ = Occ<k_split_prolong>();
-    k_split_prolong<<<ProlongGrid(fine, coarse, occ), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+    LaunchPdl(k_split_prolong, ProlongGrid(fine, coarse, occ), kPairThreads, 0, st, fine, coarse, pext, eCoarse,
+              eFine);
 }
 
 // r_c = R res_f = P^T res_f at the coarse unknowns, from the red fine residual. A thread owns four consecutive coarse
@@ -711,6 +591,8 @@ __global__ void __launch_bounds__(kPairThreads) k_split_restrict(LevelView fv, L
                                                                  const uint8_t *__restrict__ pext,
                                                                  const float *__restrict__ res, float *__restrict__ rc)
 {
+    PdlWait();
+    PdlTrigger();
     const int nq = (cv.Nz - 2 + 3) / 4, nt = (cv.Nx - 2) * nq;
     const int t = blockIdx.x * kPairThreads + threadIdx.x;
     if (t >= nt) return;
@@ -767,6 +649,8 @@ __device__ __forceinline__ void SplitRestrictPlane1(const LevelView &fv, const u
 __global__ void __launch_bounds__(256) k_split_restrict1(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
                                                         const float *__restrict__ res, float *__restrict__ rc)
 {
+    PdlWait();
+    PdlTrigger();
     const int K = 1 + blockIdx.x * 32 + threadIdx.x, J = 1 + blockIdx.y * 8 + threadIdx.y;
     if (K > cv.Nz - 2 || J > cv.Nx - 2) return;
     const int S = (cv.Ny - 2 + (int)gridDim.z - 1) / (int)gridDim.z;
@@ -803,7 +687,7 @@ void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const u
         const int S = MarchPlanes(coarse.Ny - 2, perPlane);
         const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
                         (unsigned)((coarse.Ny - 2 + S - 1) / S));
-        k_split_restrict1<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
+        LaunchPdl(k_split_restrict1, grid, dim3(32, 8), 0, st, fine, coarse, pext, resFine, rCoarse);
         return;
     }
     const long long nt = (long long)(coarse.Nx - 2) * ((coarse.Nz - 2 + 3) / 4);
@@ -827,8 +711,8 @@ void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const u
             bestS = S;
         }
     }
-    k_split_restrict<<<dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS)), kPairThreads, 0, st>>>(
-        fine, coarse, pext, resFine, rCoarse);
+    LaunchPdl(k_split_restrict, dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS)), kPairThreads, 0,
+              st, fine, coarse, pext, resFine, rCoarse);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -840,12 +724,14 @@ __device__ __forceinline__ double SplitRzEff(const double *S, int base, double n
 }
 
 // p_new = U (z - mean + beta p_old), q = M p_new, sum p_new.q, both colours at a thread's quad position.
-template <bool kSingular, bool kSt>
+template <bool kSingular>
 __global__ void __launch_bounds__(kPairThreads, 4)
     k_split_papply(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ z, float *p0, float *p1,
                    float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd,
                    int slotN, int slotPQ)
 {
+    PdlWait();
+    PdlTrigger();
     const int iter = *it, par = iter & 1;
     const float *__restrict__ pIn = par ? p1 : p0;
     float *__restrict__ pOut = par ? p0 : p1;
@@ -905,32 +791,10 @@ __global__ void __launch_bounds__(kPairThreads, 4)
         for (int x = 0; x < 4; x++)
         {
             const unsigned a0 = Byte(d0, x), a1 = Byte(d1, x);
-            if (!kSt)
-            {
-                const float s0 = ((P1.v[x] + M1.v[x]) + (Jp1.v[x] + Jm1.v[x])) + (C1.v[x] + sh1.v[x]);
-                const float s1 = ((P0.v[x] + M0.v[x]) + (Jp0.v[x] + Jm0.v[x])) + (C0.v[x] + sh0.v[x]);
-                Q0.v[x] = Unk(a0) * (hg * (float)(a0 & 0x7Fu) * C0.v[x] - g * s0);
-                Q1.v[x] = Unk(a1) * (hg * (float)(a1 & 0x7Fu) * C1.v[x] - g * s1);
-            }
-            else
-            {
-                Q0.v[x] = Q1.v[x] = 0.f;
-                float diag;
-                if (a0 & 0x80u)
-                {
-                    const int k = 2 * (P.m0 + x) + q0;
-                    const float kp = q0 ? sh1.v[x] : C1.v[x], km = q0 ? C1.v[x] : sh1.v[x];
-                    const float s = StencilSum(v, i, P.j, k, a0, P1.v[x], M1.v[x], Jp1.v[x], Jm1.v[x], kp, km, diag);
-                    Q0.v[x] = diag * C0.v[x] - s;
-                }
-                if (a1 & 0x80u)
-                {
-                    const int k = 2 * (P.m0 + x) + q1;
-                    const float kp = q1 ? sh0.v[x] : C0.v[x], km = q1 ? C0.v[x] : sh0.v[x];
-                    const float s = StencilSum(v, i, P.j, k, a1, P0.v[x], M0.v[x], Jp0.v[x], Jm0.v[x], kp, km, diag);
-                    Q1.v[x] = diag * C1.v[x] - s;
-                }
-            }
+            const float s0 = ((P1.v[x] + M1.v[x]) + (Jp1.v[x] + Jm1.v[x])) + (C1.v[x] + sh1.v[x]);
+            const float s1 = ((P0.v[x] + M0.v[x]) + (Jp0.v[x] + Jm0.v[x])) + (C0.v[x] + sh0.v[x]);
+            Q0.v[x] = Unk(a0) * (hg * (float)(a0 & 0x7Fu) * C0.v[x] - g * s0);
+            Q1.v[x] = Unk(a1) * (hg * (float)(a1 & 0x7Fu) * C1.v[x] - g * s1);
         }
         if (P.valid)
         {
@@ -955,24 +819,12 @@ void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, fl
                        int singular, int slotPQ, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-#define NB_SPLIT_PAPPLY(SING, ST)                                                                                  \
-    do                                                                                                             \
-    {                                                                                                              \
-        const int occ = Occ<k_split_papply<SING, ST>>();                             \
-        k_split_papply<SING, ST><<<QuadGrid(v, occ), kPairThreads, 0, st>>>(v, du, z, p0, p1, q, R, S, it, baseEven,  \
-                                                                            baseOdd, slotN, slotPQ);               \
-    } while (0)
     if (singular)
-    {
-        if (v.stretched) NB_SPLIT_PAPPLY(true, true);
-        else NB_SPLIT_PAPPLY(true, false);
-    }
+        LaunchPdl(k_split_papply<true>, QuadGrid(v, Occ<k_split_papply<true>>()), kPairThreads, 0, st, v, du, z, p0,
+                  p1, q, R, S, it, baseEven, baseOdd, slotN, slotPQ);
     else
-    {
-        if (v.stretched) NB_SPLIT_PAPPLY(false, true);
-        else NB_SPLIT_PAPPLY(false, false);
-    }
-#undef NB_SPLIT_PAPPLY
+        LaunchPdl(k_split_papply<false>, QuadGrid(v, Occ<k_split_papply<false>>()), kPairThreads, 0, st, v, du, z, p0,
+                  p1, q, R, S, it, baseEven, baseOdd, slotN, slotPQ);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -1083,21 +935,14 @@ void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b,
 void PrepareSplitKernels()
 {
     (void)Occ<k_split_first>();
-    (void)Occ<k_split_half<0, true, true>>();
-    (void)Occ<k_split_half<0, true, false>>();
-    (void)Occ<k_split_half<0, false, false>>();
-    (void)Occ<k_split_half<1, false, false>>();
-    (void)Occ<k_split_half<2, false, false>>();
-    (void)Occ<k_split_half<1, true, false>>();
-    (void)Occ<k_split_half<2, true, false>>();
-    (void)Occ<k_split_residual<true>>();
-    (void)Occ<k_split_residual<false>>();
+    (void)Occ<k_split_half<0>>();
+    (void)Occ<k_split_half<1>>();
+    (void)Occ<k_split_half<2>>();
+    (void)Occ<k_split_residual>();
     (void)Occ<k_split_prolong>();
     (void)Occ<k_split_restrict>();
-    (void)Occ<k_split_papply<true, true>>();
-    (void)Occ<k_split_papply<true, false>>();
-    (void)Occ<k_split_papply<false, true>>();
-    (void)Occ<k_split_papply<false, false>>();
+    (void)Occ<k_split_papply<true>>();
+    (void)Occ<k_split_papply<false>>();
 }
 
 } // namespace nb

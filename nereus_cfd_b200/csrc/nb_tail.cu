@@ -331,6 +331,8 @@ template <typename T, bool kWarp> __device__ void TUp(const SmemLevel<T> &F, con
 
 template <typename T> __global__ void __launch_bounds__(kTailThreads) k_tail(TailArgs<T> A)
 {
+    PdlWait();
+    PdlTrigger();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double sInv[kMaxTailLevels][32];
     __shared__ int sCount[kMaxTailLevels][2];
@@ -505,7 +507,7 @@ void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pr
     A.lists = lists;
     A.counts = counts;
     NB_COUNT_LAUNCH();
-    k_tail<T><<<1, kTailThreads, off, st>>>(A);
+    LaunchPdl(k_tail<T>, dim3(1), dim3(kTailThreads), (size_t)off, st, A);
 }
 
 template size_t TailSmemBytes<float>(const LevelView *, int);
