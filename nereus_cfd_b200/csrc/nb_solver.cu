@@ -396,7 +396,7 @@ Context::~Context()
 }
 
 // ---- per-kernel timing: events from a pool, bracketing launches of the selected kernel ids ----
-void Context::ProfBegin(int id, double bytes)
+void Context::ProfBegin(int id, double bytes, int launches)
 {
     if (!(profMask >> id & 1u)) return;
     cudaEvent_t a;
@@ -421,6 +421,7 @@ void Context::ProfBegin(int id, double bytes)
     NB_CK(capturing ? cudaEventRecordWithFlags(profA, st, cudaEventRecordExternal) : cudaEventRecord(profA, st));
     profOpen = id;
     profBytes = bytes;
+    profLaunches = launches;
 }
 
 void Context::ProfEnd()
@@ -435,7 +436,7 @@ void Context::ProfEnd()
     else
         b = evPool[evUsed++];
     NB_CK(capturing ? cudaEventRecordWithFlags(b, st, cudaEventRecordExternal) : cudaEventRecord(b, st));
-    (capturing ? capturing->prof : prof).push_back({profOpen, profA, b, profBytes});
+    (capturing ? capturing->prof : prof).push_back({profOpen, profA, b, profBytes, profLaunches});
     profOpen = -1;
 }
 
@@ -445,7 +446,7 @@ static void Accumulate(const std::vector<Context::ProfRecord> &recs, Context::Pr
     {
         float m = 0.0f;
         NB_CK(cudaEventElapsedTime(&m, r.a, r.b));
-        tot[r.id].launches += 1;
+        tot[r.id].launches += r.launches;
         tot[r.id].ms += m;
         tot[r.id].bytes += r.bytes;
     }
@@ -784,15 +785,18 @@ void Context::VCycleSplit(int l, float *r, float *e)
     LaunchSplitProlong(v, vc, Lv.pext.p, Lc.e<float>(), e, st);
     ProfEnd();
     for (int q = 0; q < post; q++)
+    {
+        // the black and the red half back to back: one pair of events around both (half the events' own cost)
+        ProfBegin(l == 0 ? NB_K_SMOOTH0 : NB_K_COARSE, l == 0 ? 2.0 * half * cells : 0.0, 2);
         for (int c = 1; c >= 0; c--)
         {
-            prof(NB_K_SMOOTH0, half);
             if (l == 0 && q + 1 == post) // z is final: r.z for CG here (IterBody skips its own)
                 LaunchSplitHalfDot(v, du, r, e, c, c == 0, red, iter.p, S_RZ0, S_RZ1, S_RZB, st);
             else
                 LaunchSplitHalf(v, du, r, e, c, st);
-            ProfEnd();
         }
+        ProfEnd();
+    }
 }
 
 // The V-cycle on a 3D level with one launch per red-black sweep (nb_fused.cu): the pre-smoothing from zero into f,

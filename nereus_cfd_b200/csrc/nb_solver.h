@@ -164,7 +164,8 @@ struct Context
     {
         int id;
         cudaEvent_t a, b;
-        double bytes;
+        double bytes;      // of all the launches between the two events
+        int launches = 1;  // launches of kernel `id` between them (back to back)
     };
     struct ProfTotal
     {
@@ -179,7 +180,9 @@ struct Context
     int profOpen = -1;
     cudaEvent_t profA = nullptr;
     double profBytes = 0.0;
-    void ProfBegin(int id, double bytes);
+    int profLaunches = 1;
+    // events around the next `launches` launches of kernel `id` (back to back on the stream), `bytes` in all
+    void ProfBegin(int id, double bytes, int launches = 1);
     void ProfEnd();
     void ProfClear();
     void ProfFlush();
