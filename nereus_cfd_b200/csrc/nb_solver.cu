@@ -481,6 +481,11 @@ void Context::ProfRead(int id, int *launches, double *ms, double *bytesPerLaunch
 
 void Context::IterGraph::Release()
 {
+    if (loopExec) cudaGraphExecDestroy(loopExec);
+    if (loop) cudaGraphDestroy(loop);
+    loopExec = nullptr;
+    loop = nullptr;
+    loopFailed = false;
     if (exec) cudaGraphExecDestroy(exec);
     if (g) cudaGraphDestroy(g);
     for (cudaEvent_t e : events) cudaEventDestroy(e);
@@ -852,7 +857,7 @@ template <typename T> void Context::VCycleFused(int l, T *r, T *e)
 
 // One CG iteration on level 0: z = V-cycle(r), r.z, p = z + beta p (and q = M p, p.q), x += alpha p, r -= alpha q,
 // r.r copied to the host. The iteration number and the parity of the p buffers live on the device.
-template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact)
+template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact, bool copyRR)
 {
     const LevelView v0 = L[0].view();
     const double s = sizeof(T), cells = (double)Cells();
@@ -869,7 +874,8 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
             LaunchLinXR((long long)VecLen0(), x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ,
                         S_RR, st);
             ProfEnd();
-            NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (copyRR)
+                NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
             return;
         }
         if (PairLevel(0))
@@ -887,7 +893,8 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
             ProfBegin(NB_K_XR, 6.0 * s * cells);
             LaunchLinXR(L[0].cells, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, S_RR, st);
             ProfEnd();
-            NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (copyRR)
+                NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
             return;
         }
     }
@@ -903,7 +910,64 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
     ProfBegin(NB_K_XR, 6.0 * s * cells);
     LaunchUpdateXR<T>(v0, x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, S_RR, st);
     ProfEnd();
-    NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (copyRR) NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+}
+
+// The loop condition of the device-side CG loop, after an iteration's x/r update: go on while the iterations done are
+// below the cap, r.r is above its target and finite (the host loop's test).
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, double *S, const int *it, int slotRR, int slotTgt,
+                            int slotMax, int slotIts)
+{
+    const double rr = S[slotRR];
+    const int n = *it;
+    S[slotIts] = (double)n;
+    const bool go = n < (int)S[slotMax] && rr > S[slotTgt] && isfinite(rr);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+template <typename T> void Context::BuildLoop(IterGraph *G, T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact)
+{
+    cudaGraph_t loop = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto unavailable = [&]() {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (loop) cudaGraphDestroy(loop);
+        G->loopFailed = true;
+    };
+    cudaGraphConditionalHandle h = 0;
+    if (cudaGraphCreate(&loop, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&h, loop, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return unavailable();
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaGraphAddNode(&node, loop, nullptr, 0, &np) != cudaSuccess) return unavailable();
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    const long long before = g_launches.load();
+    if (cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return unavailable();
+    bool ok = true;
+    try
+    {
+        IterBody<T>(x, r, z, p0, p1, q, exact, false);
+        NB_COUNT_LAUNCH();
+        k_loop_cond<<<1, 1, 0, st>>>(h, slots.p, iter.p, S_RR, S_TGT, S_MAXIT, S_ITS);
+    }
+    catch (...)
+    {
+        ok = false;
+    }
+    cudaGraph_t out = nullptr;
+    if (cudaStreamEndCapture(st, &out) != cudaSuccess || !ok) return unavailable();
+    if (cudaGraphInstantiate(&exec, loop, 0) != cudaSuccess) return unavailable();
+    G->loop = loop;
+    G->loopExec = exec;
+    G->loopLaunches = g_launches.load() - before; // counted when run, not when recorded
+    NB_COUNT_LAUNCHES(-G->loopLaunches);
 }
 
 template <typename T>
@@ -912,6 +976,32 @@ int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double
 {
     NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * VecLen0(), st));
     NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
+    if (opt.use_graphs && profMask == 0)
+    {
+        // the whole loop on the device: one launch, one synchronisation
+        IterGraph *L = &graphs[sizeof(T) == 8 ? 1 : 0];
+        if (!L->loopExec && !L->loopFailed) BuildLoop<T>(L, x, r, z, p0, p1, q, exact);
+        if (L->loopExec)
+        {
+            if (!(maxIt > 0 && rrStart > rrTarget))
+            {
+                *rrEnd = rrStart;
+                return 0;
+            }
+            hostSlots[S_TGT] = rrTarget;
+            hostSlots[S_MAXIT] = (double)maxIt;
+            NB_CK(cudaMemcpyAsync(slots.p + S_TGT, hostSlots + S_TGT, 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+            NB_CK(cudaGraphLaunch(L->loopExec, st));
+            NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+            NB_CK(cudaMemcpyAsync(hostSlots + S_ITS, slots.p + S_ITS, sizeof(double), cudaMemcpyDeviceToHost, st));
+            NB_CK(cudaStreamSynchronize(st));
+            NB_CK(cudaGetLastError());
+            const int it = (int)hostSlots[S_ITS];
+            NB_COUNT_LAUNCHES(it * L->loopLaunches);
+            *rrEnd = hostSlots[S_RR];
+            return it;
+        }
+    }
     IterGraph *G = nullptr;
     if (opt.use_graphs)
     {

@@ -84,7 +84,10 @@ enum : int
     S_DIV = 12,
     S_NUNK = 14, // the count of unknowns, read by the CG kernels on the device
     S_RZB = 16,  // (r.z, sum z, sum r) of the black cells, summed by the black half of the last sweep
-    S_COUNT = 20
+    S_TGT = 19,  // the device-side CG loop: r.r target, iteration cap, iterations done
+    S_MAXIT = 20,
+    S_ITS = 21,
+    S_COUNT = 22
 };
 
 struct LevelData
@@ -197,6 +200,12 @@ struct Context
         std::vector<cudaEvent_t> events;
         unsigned mask = 0;
         long long launches = 0; // kernels one replay runs
+        // the whole CG loop as one graph: a WHILE node whose body is the iteration, the condition set on the device
+        // (no profiling events inside); built once, or marked unavailable when the runtime refuses it
+        cudaGraph_t loop = nullptr;
+        cudaGraphExec_t loopExec = nullptr;
+        long long loopLaunches = 0; // kernels one loop iteration runs
+        bool loopFailed = false;
         void Release();
     };
     IterGraph graphs[2]; // [0] float, [1] double
@@ -260,7 +269,9 @@ struct Context
     void VCycleSplit(int l, float *r, float *e);
     void AssignSplit();
     void BuildTailLists();
-    template <typename T> void IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact);
+    // copyRR: end with the copy of r.r to the host (not inside the device-side loop)
+    template <typename T> void IterBody(T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact, bool copyRR = true);
+    template <typename T> void BuildLoop(IterGraph *G, T *x, T *r, T *z, T *p0, T *p1, T *q, bool exact);
     template <typename T>
     int RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double rrTarget, int maxIt, bool exact,
                double *rrEnd);
