@@ -976,7 +976,7 @@ int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double
 {
     NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * VecLen0(), st));
     NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
-    if (opt.use_graphs && profMask == 0)
+    if (opt.use_graphs >= 2 && profMask == 0)
     {
         // the whole loop on the device: one launch, one synchronisation
         IterGraph *L = &graphs[sizeof(T) == 8 ? 1 : 0];

@@ -99,15 +99,15 @@ def test_split_repeat_is_bit_identical(nb):
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_device_loop_equals_host_loop(nb, precision):
-    """The CG loop as one graph with a device-side WHILE condition (use_graphs = 1) runs the same kernels in the same
-    order as launching them iteration by iteration from the host (use_graphs = 0): the same iterations and the same
-    bits."""
+    """The CG loop as one graph with a device-side WHILE condition (use_graphs = 2), one graph per iteration
+    (use_graphs = 1) and plain launches iteration by iteration from the host (use_graphs = 0) run the same kernels in
+    the same order: the same iterations and the same bits."""
     case = W.sphere_outlet_3d(40)
     g = case.grid
     types = capi.label_cells(g, case.scene)
     u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
     out = []
-    for graphs in (1, 0):
+    for graphs in (2, 1, 0):
         m = MACGrid(g, types.copy(), u.copy(), v.copy(), w.copy(), np.zeros(g.cells), case.rho, case.dt)
         s = PressureSolver(precision, use_graphs=graphs)
         r = s.SolvePressure(m, tol=1e-9)
@@ -118,8 +118,9 @@ def test_device_loop_equals_host_loop(nb, precision):
         s.DestroyPressureSolver()
         assert np.array_equal(m.p, m2.p) and r.iters_inner == r2.iters_inner
         out.append((r.iters_inner, r.iters_outer, m.p, m.u))
-    assert out[0][:2] == out[1][:2]
-    assert np.array_equal(out[0][2], out[1][2]) and np.array_equal(out[0][3], out[1][3])
+    for o in out[1:]:
+        assert out[0][:2] == o[:2]
+        assert np.array_equal(out[0][2], o[2]) and np.array_equal(out[0][3], o[3])
 
 
 def test_device_loop_stops_at_the_iteration_cap(nb):
