@@ -25,7 +25,8 @@ def lib():
     return capi.load()
 
 
-def test_header_declares_the_survey_entry_points():
+def test_header_declares_the_backend_entry_points():
+    """The calls a NEREUS pressure backend needs: context, layout, the projection step and SolveLaplacian."""
     syms = declared_symbols()
     for s in ["nereus_b200_create", "nereus_b200_destroy", "nereus_b200_set_layout", "nereus_b200_project",
               "nereus_b200_solve_laplacian"]:
