@@ -435,6 +435,14 @@ def channel_2d_stretched(nx: int = 24, ny: int = 12, seed: int = 5) -> Case:
                                                                          regions=[disc]), seed)
 
 
+def cavity_outlet_2d(n: int = 32, seed: int = 9) -> Case:
+    """2D unit square, uniform n x n, a solid disc at (0.4, 0.5) radius 0.15, no-slip walls and a p = 0 pressure outlet
+    on the x = 1 face: a uniform 2D scene of the kind the EXPLICIT method runs."""
+    g = uniform_grid(2, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    disc = Region(REGION_SOLID, PRIM_CYLINDER, (0.4, 0.5, 0.0), radius=0.15, axis=2)
+    return Case("cavity_outlet_2d_%d" % n, g, walls_scene(2, outlet_face=1, regions=[disc]), seed)
+
+
 def inflow_outflow_3d(n: int = 8, seed: int = 6) -> Case:
     """3D unit cube with a velocity inlet at x = 0 and a continuity outflow at x = 1 (both Neumann for the
     pressure: a singular system, compatibility on)."""

@@ -21,7 +21,10 @@
 // hdr: dim, grid_mode, grid_size, nxi, nyi, nzi, label_mode, needs_compat, scheme, solver, max_iters, threads,
 //      method_kind (0 Eulerian/ADI-like, 1 hybrid/FLIP-like), repeats, Nx, Ny (expected, ring included).
 // scheme: 0 Chorin; 1 incremental (SolvePressure with SYSTEM.scheme = PRESSURE_INCREMENTAL from gridAnt, then
-// ProjectPressure + AccumulatePressureIncrement as Project does); 2 Chorin with the warm start from gridAnt.
+// ProjectPressure + AccumulatePressureIncrement as Project does); 2 Chorin with the warm start from gridAnt;
+// 3 (2D, uniform) the EXPLICIT method's own pressure step and projection (src/Methods/Explicit/Explicit2D.cpp:48-120,
+// SOR to tol * max|b| in the max norm with at most max_iters sweeps), after the shared assembly that A, IDP and b
+// (written as for Chorin, with the relative residual of the SOR solution in that system) come from; iterations -1.
 // The result file then ends with double ref_norm (IncrementReferenceNorm, 0 for Chorin) and double p_final[cells]
 // (the pressure after Project).
 #include <algorithm>
@@ -77,6 +80,7 @@
 #include "headers/Core/Scene.h"
 #include "Methods/PPESolver/PressureSolver2D.h"
 #include "Methods/PPESolver/PressureSolver3D.h"
+#include "Methods/Explicit/ExplicitSettings.h"
 #undef private
 #undef protected
 
@@ -343,10 +347,21 @@ int main(int argc, char **argv)
 
     // Cold solve (AMGCL builds its hierarchy here), then warm repeats of the same solve (Chorin only).
     double t1 = Now();
-    if (dim == 3) PressureSolver3D::SolvePressure(ant, &grid, nullptr, time);
-    else PressureSolver2D::SolvePressure(ant, &grid, nullptr, time);
+    int iters = -1;
+    if (scheme == 3)
+    {
+        // Explicit2D::Pressure enforces the ring at its time + dt, so it is handed time - dt
+        EXPLICIT_SETTINGS.tolerance = tol;
+        EXPLICIT_SETTINGS.maxIterations = h[10];
+        Explicit2D::Pressure(nullptr, &grid, nullptr, time - SIMULATION.dt);
+    }
+    else
+    {
+        if (dim == 3) PressureSolver3D::SolvePressure(ant, &grid, nullptr, time);
+        else PressureSolver2D::SolvePressure(ant, &grid, nullptr, time);
+        iters = PRESSURE_TELEMETRY.lastIterations;
+    }
     const double tCold = Now() - t1;
-    int iters = PRESSURE_TELEMETRY.lastIterations;
     const int repeats = scheme == 0 ? h[13] : 0;
     double tWarm = 0.0;
     std::vector<double> tEach(repeats > 0 ? repeats : 0);
@@ -374,7 +389,8 @@ int main(int argc, char **argv)
     }
 
     t1 = Now();
-    if (dim == 3) PressureSolver3D::ProjectPressure(&grid);
+    if (scheme == 3) Explicit2D::Projection(nullptr, &grid, nullptr, time);
+    else if (dim == 3) PressureSolver3D::ProjectPressure(&grid);
     else PressureSolver2D::ProjectPressure(&grid);
     const double tProject = Now() - t1;
     if (scheme == 1) // the rest of Project under the incremental scheme

@@ -65,7 +65,8 @@ class RefResult:
     p_final: np.ndarray = None  # the pressure after Project (schemes 1 and 2)
 
 
-SCHEME_CHORIN, SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM = 0, 1, 2
+SCHEME_CHORIN, SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM, SCHEME_EXPLICIT = 0, 1, 2, 3
+_PREV_SCHEMES = (SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM)  # the schemes that read and write a previous step
 
 
 def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000,
@@ -94,7 +95,7 @@ def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, 
         f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
         if g.dim == 3:
             f.write(np.ascontiguousarray(w, dtype="<f8").tobytes())
-        if scheme != SCHEME_CHORIN:
+        if scheme in _PREV_SCHEMES:
             f.write(np.ascontiguousarray(p_prev, dtype="<f8").reshape(-1).tobytes())
 
 
@@ -140,7 +141,7 @@ def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
         (nr,) = struct.unpack_from("<i", data, off); off += 4
         t_each = take("<f8", nr)
     ref_norm, p_final = 0.0, None
-    if scheme != SCHEME_CHORIN:
+    if scheme in _PREV_SCHEMES:
         (ref_norm,) = struct.unpack_from("<d", data, off); off += 8
         p_final = take("<f8", cells)
     return RefResult(Nx, Ny, Nz, n, iters, bool(sing), thr, tA, tC, tW, tP, rr, md, dh, types, idp, rowptr, col, val,

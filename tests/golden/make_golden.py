@@ -2,7 +2,7 @@
 
 Run in a checkout that has the reference sources (it builds oracle/_ref/ref_harness from them first):
 
-    python tests/golden/make_golden.py [REF_ROOT]
+    python tests/golden/make_golden.py [REF_ROOT] [--only explicit]
 
 Each fixture is one small case: the inputs both sides read (face velocities, the prescribed ring pressure) and what
 the reference computed from them (cell types, IDP, the CSR matrix, b before and after the compatibility step, the
@@ -47,6 +47,14 @@ SCHEME_CASES = [
 ]
 
 
+# the EXPLICIT method's own pressure step and projection (2D, uniform): (fixture name, builder, kwargs, SOR tolerance
+# relative to max |b| in the max norm)
+EXPLICIT_CASES = [
+    ("explicit_cavity_outlet_2d_32", "cavity_outlet_2d", {"n": 32, "seed": 21}, 1e-13),
+    ("explicit_closed_box_2d_16", "closed_box_2d", {"n": 16, "seed": 22}, 1e-13),
+]
+
+
 def build_case(builder: str, kwargs: dict) -> W.Case:
     return getattr(W, builder)(**kwargs)
 
@@ -87,9 +95,35 @@ def write_scheme_case(name, builder, kwargs, tol, scheme, time):
         name, ref.n, ref.iters, cold.iters, ref.rel_res, ref.max_div, ref.ref_norm, os.path.getsize(out) // 1024))
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def write_explicit_case(name, builder, kwargs, tol):
+    """The reference's Explicit2D::Pressure + Projection on a uniform 2D case, with the shared assembly's IDP, b and
+    matrix beside it (rel_res: the SOR solution's relative residual in that system)."""
+    case = build_case(builder, kwargs)
+    g = case.grid
+    probe = refcase.run(case, np.zeros(int(np.prod(g.u_shape()))), np.zeros(int(np.prod(g.v_shape()))), np.zeros(0),
+                        tol=1e-6)
+    types = probe.types
+    u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
+    ref = refcase.run(case, u, v, w, tol=tol, max_iters=2000000, scheme=refcase.SCHEME_EXPLICIT)
+    p_in = np.where(ref.types == W.PRESSURE, ref.p, 0.0)
+    meta = dict(name=name, builder=builder, kwargs=kwargs, tol=tol, needs_compat=case.needs_compat, rho=case.rho,
+                dt=case.dt, n=ref.n, singular=ref.singular, rel_res=ref.rel_res, max_div=ref.max_div, dh=ref.dh,
+                scheme=refcase.SCHEME_EXPLICIT)
+    out = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(
+        out, meta=np.array(json.dumps(meta)), u=u.ravel(), v=v.ravel(), w=w.ravel(), p_in=p_in, types=ref.types,
+        idp=ref.idp, b=ref.b, x=ref.x, p=ref.p, u_out=ref.u, v_out=ref.v)
+    print("%-36s n=%-6d rel_res=%.2e max_div=%.2e singular=%d  %d KB" % (
+        name, ref.n, ref.rel_res, ref.max_div, ref.singular, os.path.getsize(out) // 1024))
+
+
+def main(ref_root: str = "/root/reference", only: str = "") -> None:
     if not refcase.build(ref_root):
         raise SystemExit("the reference harness could not be built from %s" % ref_root)
+    if only == "explicit":
+        for args in EXPLICIT_CASES:
+            write_explicit_case(*args)
+        return
     for name, builder, kwargs, tol in CASES:
         case = build_case(builder, kwargs)
         g = case.grid
@@ -114,7 +148,15 @@ def main(ref_root: str = "/root/reference") -> None:
             name, ref.n, ref.iters, ref.rel_res, ref.max_div, os.path.getsize(out) // 1024))
     for args in SCHEME_CASES:
         write_scheme_case(*args)
+    for args in EXPLICIT_CASES:
+        write_explicit_case(*args)
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    argv = sys.argv[1:]
+    only = ""
+    if "--only" in argv:
+        k = argv.index("--only")
+        only = argv[k + 1]
+        argv = argv[:k] + argv[k + 2:]
+    main(*argv, only=only)
