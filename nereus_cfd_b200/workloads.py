@@ -423,6 +423,86 @@ def flip_tank_3d(n: int = 128, seed: int = 4, a: Optional[float] = None, b: Opti
                 fp32_velocity=True, method=1)
 
 
+def flip_tank_2d(n: int = 32, seed: int = 10, a: float = 0.55, b: float = 0.45) -> Case:
+    """A 2D FLIP-style tank: unit square, uniform n^2, interior cells with centre x < a and y < b liquid (FLUID), the
+    rest air (EMPTY), no-slip walls and an open top (a pressure outlet without p=, so its ring cells are EMPTY)."""
+    g = uniform_grid(2, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    air = Region(REGION_EMPTY, PRIM_BOX, (-1.0, -1.0, -1.0), (2.0, 2.0, 2.0))
+    liquid = Region(REGION_FLUID, PRIM_BOX, (-1.0, -1.0, -1.0), (a, b, 2.0))
+    return Case("flip_tank_2d_%d" % n, g, walls_scene(2, outlet_face=3, regions=[air, liquid]), seed,
+                velocity_rule="liquid", fp32_velocity=True, method=1)
+
+
+def _uniforms(seed: int, stream: int, count: int) -> np.ndarray:
+    z = splitmix64(stream_seed(seed, stream), 0, count)
+    return ((z >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
+
+
+def flip_particles(case: Case, types: np.ndarray, seed: int, ppc: int = 4, hole_fraction: float = 0.03,
+                   features: bool = True) -> np.ndarray:
+    """Seeded FLIP particle positions, (count, 3) float64 (z = 0 in 2D), for a relabelling step on ``case``:
+    ``ppc`` particles jittered uniformly inside every interior FLUID cell of ``types``, except that the cells of
+    a ``hole_fraction`` draw hold none. With ``features``, also: straight runs of 4 empty cells along each axis
+    inside the liquid (each filled only when its lower neighbour was filled first); a 2 x 2 block of empty cells; a
+    few spray particles in air; particles exactly on a face coordinate, within one cell below the grid's first face,
+    and far beyond its last face (the index clamp)."""
+    g = case.grid
+    t = types.reshape(g.shape)
+    nd = g.dim
+    faces = [ax.face for ax in g.axes]  # x, y, z face coordinates, ring included
+    dh = g.dh
+    liquid = np.zeros(g.shape, dtype=bool)
+    sl = tuple(slice(1, -1) for _ in range(nd)) + (() if nd == 3 else (slice(None),))
+    liquid[sl] = t[sl] == FLUID
+    cells = np.argwhere(liquid)  # (i, j, k) in the (y, x, z) layout
+    drop = _uniforms(seed, 1, len(cells)) < hole_fraction
+    if features and len(cells):
+        lo, hi = cells.min(axis=0), cells.max(axis=0)
+        mid = (lo + hi) // 2
+        holes = set()
+        axes = (0, 1, 2) if nd == 3 else (0, 1)
+        for n_ax, ax in enumerate(axes):
+            c0 = mid.copy()
+            for other in axes:
+                if other != ax:
+                    c0[other] = min(max(lo[other] + 1, mid[other] + (2 * n_ax - 2)), hi[other] - 1)
+            c0[ax] = max(lo[ax] + 1, mid[ax] - 2)
+            for s in range(4):
+                c = c0.copy()
+                c[ax] = min(c0[ax] + s, hi[ax] - 1)
+                holes.add(tuple(int(v) for v in c))
+        b0 = [min(max(lo[a] + 1, lo[a] + 1), hi[a] - 2) for a in range(3)]
+        for di in (0, 1):
+            for dj in (0, 1):
+                holes.add((b0[0] + di, b0[1] + dj, b0[2]))
+        for n_c, c in enumerate(cells):
+            if tuple(int(v) for v in c) in holes:
+                drop[n_c] = True
+    keep = cells[~drop]
+    r = _uniforms(seed, 2, len(keep) * ppc * 3).reshape(len(keep), ppc, 3)
+    # (i, j, k) -> x from column j, y from row i, z from k
+    x = faces[0][keep[:, 1]][:, None] + dh * r[:, :, 0]
+    y = faces[1][keep[:, 0]][:, None] + dh * r[:, :, 1]
+    z = faces[2][keep[:, 2]][:, None] + dh * r[:, :, 2] if nd == 3 else np.zeros_like(x)
+    pts = [np.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], axis=1)]
+    if features:
+        ext = []
+        air = np.argwhere(t == EMPTY)
+        if len(air):
+            pick = (_uniforms(seed, 3, 3) * len(air)).astype(np.int64)
+            for q in pick:
+                i, j, k = air[q]
+                ext.append([faces[0][j] + 0.5 * dh, faces[1][i] + 0.5 * dh,
+                            faces[2][k] + 0.5 * dh if nd == 3 else 0.0])
+        zc = faces[2][g.Nz // 2] + 0.25 * dh if nd == 3 else 0.0
+        ext.append([faces[0][2], faces[1][2], faces[2][2] if nd == 3 else 0.0])  # exactly on faces
+        ext.append([faces[0][0] - 0.4 * dh, faces[1][1] + 0.5 * dh, zc])  # within one cell below the first face
+        ext.append([faces[0][g.Nx // 2] + 0.5 * dh, faces[1][-1] + 7.0 * dh, zc])  # beyond the top: clamped
+        ext.append([1.0e3, faces[1][g.Ny // 2], zc])  # far beyond x: clamped
+        pts.append(np.array(ext, dtype=np.float64))
+    return np.ascontiguousarray(np.concatenate(pts, axis=0))
+
+
 def channel_2d_stretched(nx: int = 24, ny: int = 12, seed: int = 5) -> Case:
     """2D channel [0,2.2]x[0,0.41], x stretched by 1.04 away from a band at x = 0.5, a solid disc at (0.5, 0.2)
     radius 0.05, inlet at x = 0, p = 0 outlet at x = 2.2."""

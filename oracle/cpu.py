@@ -67,6 +67,8 @@ def lib():
         L.or_max_divergence.restype = ctypes.c_double
         L.or_residual_norm.argtypes = [_ip, _ip, _dp, ctypes.c_int, _dp, _dp]
         L.or_residual_norm.restype = ctypes.c_double
+        L.or_update_fluid_cells.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 4 + [_dp, ctypes.c_longlong, _u8]
+        L.or_update_fluid_cells.restype = ctypes.c_longlong
     return _LIB
 
 
@@ -118,6 +120,18 @@ def label_cells(grid, scene) -> np.ndarray:
     lib().or_label_cells(grid.dim, grid.Nx, grid.Ny, grid.Nz if grid.dim == 3 else 1, _p(cx, _dp), _p(cy, _dp),
                          _p(cz, _dp), ctypes.byref(s), _p(out, _u8))
     return out
+
+
+def update_fluid_cells(grid, types, xyz, origin, dh=None):
+    """FLIP's re-labelling from particle positions (``or_update_fluid_cells``): returns the new cell types and the
+    number of particles skipped as out of range. xyz: (count, 3) float64 positions; origin: FacePos(X|Y|Z, 0)."""
+    out = np.ascontiguousarray(types, dtype=np.uint8).reshape(-1).copy()
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    dh = grid.dh if dh is None else dh
+    oz = origin[2] if len(origin) > 2 else 0.0
+    skipped = lib().or_update_fluid_cells(grid.dim, grid.Nx, grid.Ny, grid.Nz if grid.dim == 3 else 1,
+                                          origin[0], origin[1], oz, dh, _p(xyz, _dp), xyz.shape[0], _p(out, _u8))
+    return out, int(skipped)
 
 
 @dataclass

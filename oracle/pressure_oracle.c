@@ -564,3 +564,68 @@ double or_residual_norm(const int32_t *rp, const int32_t *cl, const double *val,
     }
     return sqrt(s);
 }
+
+/* One particle coordinate to a cell index along an axis with N cells, as UpdateFluidCells does it
+ * (src/Methods/FLIP/FLIP3D.cpp:796-802): truncation toward zero of (x - origin) / dh, clamped above to N - 1. The
+ * reference has no lower clamp: an index below 0 (x more than one cell below the grid's first face) or a non-finite
+ * coordinate reads outside the labels there. Here such a particle is skipped (-1), and so is it in the B200 kernel.
+ * A quotient at or beyond N (including +inf) takes N - 1 without converting it. */
+static inline int ParticleIndex(double x, double origin, double dh, int N)
+{
+    const double q = (x - origin) / dh;
+    if (!(q > -1.0)) return -1;
+    if (q >= (double)N) return N - 1;
+    return (int)q;
+}
+
+/* FLIP3D::UpdateFluidCells (src/Methods/FLIP/FLIP3D.cpp:784-833) and FLIP2D::UpdateFluidCells
+ * (src/Methods/FLIP/FLIP2D.cpp:648-691), in their order:
+ *   1. MAC::ResetFluidCells (src/MAC.cpp:556-589): every cell that is not SOLID, INFLOW, OUTFLOW or PRESSURE becomes
+ *      EMPTY, ring included;
+ *   2. each particle's cell, if EMPTY, becomes FLUID;
+ *   3. one pass over the interior cells in (i, j, k) order, in place: an EMPTY cell with at least 5 (3D) or 3 (2D)
+ *      FLUID neighbours among its 6 (4) becomes FLUID. In place means that a cell filled earlier in the pass counts
+ *      for the cells after it, so the (i-1), (j-1), (k-1) neighbours are read after their own visit.
+ * xyz holds count particles as (x, y, z) triples (z unread in 2D); (ox, oy, oz) are FacePos(X|Y|Z, 0), the low face
+ * of the first ring cell. Returns the number of particles skipped by ParticleIndex. */
+long long or_update_fluid_cells(int dim, int Nx, int Ny, int Nz, double ox, double oy, double oz, double dh,
+                                const double *xyz, long long count, uint8_t *types)
+{
+    const int nz = dim == 3 ? Nz : 1;
+    const size_t cells = (size_t)Nx * Ny * nz;
+    for (size_t c = 0; c < cells; c++)
+    {
+        const int t = types[c];
+        if (t != SOLID && t != INFLOW && t != OUTFLOW && t != PRESSURE) types[c] = EMPTY;
+    }
+    long long skipped = 0;
+    for (long long p = 0; p < count; p++)
+    {
+        const int i = ParticleIndex(xyz[3 * p + 1], oy, dh, Ny);
+        const int j = ParticleIndex(xyz[3 * p + 0], ox, dh, Nx);
+        const int k = dim == 3 ? ParticleIndex(xyz[3 * p + 2], oz, dh, Nz) : 0;
+        if (i < 0 || j < 0 || k < 0) { skipped++; continue; }
+        const size_t c = ((size_t)i * Nx + j) * nz + k;
+        if (types[c] == EMPTY) types[c] = FLUID;
+    }
+    for (int i = 1; i < Ny - 1; i++)
+        for (int j = 1; j < Nx - 1; j++)
+        {
+            if (dim == 2)
+            {
+                const size_t c = (size_t)i * Nx + j;
+                const int f = (types[c + 1] == FLUID) + (types[c - 1] == FLUID) + (types[c + Nx] == FLUID) +
+                              (types[c - Nx] == FLUID);
+                if (types[c] == EMPTY && f >= 3) types[c] = FLUID;
+                continue;
+            }
+            for (int k = 1; k < Nz - 1; k++)
+            {
+                const size_t c = ((size_t)i * Nx + j) * Nz + k, sj = Nz, si = (size_t)Nx * Nz;
+                const int f = (types[c + sj] == FLUID) + (types[c - sj] == FLUID) + (types[c + si] == FLUID) +
+                              (types[c - si] == FLUID) + (types[c + 1] == FLUID) + (types[c - 1] == FLUID);
+                if (types[c] == EMPTY && f >= 5) types[c] = FLUID;
+            }
+        }
+    return skipped;
+}

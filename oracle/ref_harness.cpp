@@ -1,7 +1,8 @@
 // ORACLE / TEST INFRASTRUCTURE ONLY -- never linked into or called by the product library.
 //
 // A driver for the NEREUS reference's own pressure path, compiled from the reference sources where they lie
-// (src/MAC.cpp, src/Utils.cpp, src/Methods/PPESolver/PressureSolver{2,3}D.cpp, include/tinyexpr/tinyexpr.c) by
+// (src/MAC.cpp, src/Utils.cpp, src/Methods/PPESolver/PressureSolver{2,3}D.cpp, src/Methods/Explicit/Explicit2D.cpp,
+// src/Methods/FLIP/{FLIP,DiffusionSolver}{2,3}D.cpp, include/tinyexpr/tinyexpr.c) by
 // oracle/Makefile into oracle/_ref/ref_harness. It reads one case file, drives the reference exactly the way its
 // own harnesses do (tests/suite_pressure.cpp:84-122: build a MAC, set the cell types, InitializePressureSolver,
 // SolvePressure, ProjectPressure), and writes what the reference computed:
@@ -25,8 +26,13 @@
 // 3 (2D, uniform) the EXPLICIT method's own pressure step and projection (src/Methods/Explicit/Explicit2D.cpp:48-120,
 // SOR to tol * max|b| in the max norm with at most max_iters sweeps), after the shared assembly that A, IDP and b
 // (written as for Chorin, with the relative residual of the SOR solution in that system) come from; iterations -1.
-// The result file then ends with double ref_norm (IncrementReferenceNorm, 0 for Chorin) and double p_final[cells]
-// (the pressure after Project).
+// 4 FLIP's re-labelling (FLIP3D::UpdateFluidCells, src/Methods/FLIP/FLIP3D.cpp:784-833; FLIP2D::UpdateFluidCells,
+// src/Methods/FLIP/FLIP2D.cpp:648-691) from the particle positions of the case file, then the Chorin step on the new
+// labels.
+// [scheme 1 or 2] The result file then ends with double ref_norm (IncrementReferenceNorm, 0 for Chorin) and double
+// p_final[cells] (the pressure after Project).
+// [scheme 4] The case file ends with int64 count and double xyz[3 * count] (x, y, z per particle); the result file
+// with double origin[3] (FacePos(X|Y|Z, 0)) and uint8 types_before[cells] (the labels UpdateFluidCells started from).
 #include <algorithm>
 #include <array>
 #include <cctype>
@@ -81,6 +87,8 @@
 #include "Methods/PPESolver/PressureSolver2D.h"
 #include "Methods/PPESolver/PressureSolver3D.h"
 #include "Methods/Explicit/ExplicitSettings.h"
+#include "Methods/FLIP/FLIP2D.h"
+#include "Methods/FLIP/FLIP3D.h"
 #undef private
 #undef protected
 
@@ -291,6 +299,31 @@ int main(int argc, char **argv)
         ReadN(f, gridAnt.p.data(), gridAnt.p.size());
         ant = &gridAnt;
     }
+    std::vector<uint8_t> typesBefore;
+    double origin[3] = {0.0, 0.0, 0.0};
+    if (scheme == 4)
+    {
+        int64_t np = 0;
+        ReadN(f, &np, 1);
+        std::vector<double> xyz((size_t)np * 3);
+        ReadN(f, xyz.data(), xyz.size());
+        static ParticleSet particles;
+        particles.data.assign((size_t)np, Particle{});
+        particles.count = (int)np;
+        for (int64_t q = 0; q < np; q++)
+        {
+            particles.data[q].isActive = true;
+            particles.data[q].x = xyz[3 * q];
+            particles.data[q].y = xyz[3 * q + 1];
+            particles.data[q].z = xyz[3 * q + 2];
+        }
+        typesBefore.assign(grid.cellTypes.data(), grid.cellTypes.data() + cells);
+        origin[0] = grid.FacePos(MAC::X, 0);
+        origin[1] = grid.FacePos(MAC::Y, 0);
+        origin[2] = dim == 3 ? grid.FacePos(MAC::Z, 0) : 0.0;
+        if (dim == 3) FLIP3D::UpdateFluidCells(&grid, &particles);
+        else FLIP2D::UpdateFluidCells(&grid, &particles);
+    }
     std::fclose(f);
 
     // The pressure ring as the step sees it (SolveScheme's first call, PressureSolver3D.cpp:281).
@@ -448,6 +481,11 @@ int main(int argc, char **argv)
     {
         WriteN(o, &refNorm, 1);
         WriteN(o, grid.p.data(), grid.p.size());
+    }
+    if (scheme == 4)
+    {
+        WriteN(o, origin, 3);
+        WriteN(o, typesBefore.data(), cells);
     }
     std::fclose(o);
     return 0;

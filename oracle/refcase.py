@@ -63,14 +63,16 @@ class RefResult:
     t_each: np.ndarray  # wall time of each warm repeat
     ref_norm: float = 0.0  # IncrementReferenceNorm (incremental scheme)
     p_final: np.ndarray = None  # the pressure after Project (schemes 1 and 2)
+    origin: tuple = None  # FacePos(X|Y|Z, 0) (scheme 4)
+    types_before: np.ndarray = None  # the labels UpdateFluidCells started from (scheme 4)
 
 
-SCHEME_CHORIN, SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM, SCHEME_EXPLICIT = 0, 1, 2, 3
+SCHEME_CHORIN, SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM, SCHEME_EXPLICIT, SCHEME_FLIP_RELABEL = 0, 1, 2, 3, 4
 _PREV_SCHEMES = (SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM)  # the schemes that read and write a previous step
 
 
 def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000,
-               threads=1, repeats=0, scheme=SCHEME_CHORIN, p_prev=None, time=0.0):
+               threads=1, repeats=0, scheme=SCHEME_CHORIN, p_prev=None, time=0.0, particles=None):
     g = case.grid
     grid_mode = 0 if not g.nonuniform else 1
     nxi, nyi = g.Nx - 2, g.Ny - 2
@@ -97,6 +99,10 @@ def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, 
             f.write(np.ascontiguousarray(w, dtype="<f8").tobytes())
         if scheme in _PREV_SCHEMES:
             f.write(np.ascontiguousarray(p_prev, dtype="<f8").reshape(-1).tobytes())
+        if scheme == SCHEME_FLIP_RELABEL:
+            xyz = np.ascontiguousarray(particles, dtype="<f8").reshape(-1, 3)
+            f.write(struct.pack("<q", xyz.shape[0]))
+            f.write(xyz.tobytes())
 
 
 def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
@@ -144,12 +150,16 @@ def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
     if scheme in _PREV_SCHEMES:
         (ref_norm,) = struct.unpack_from("<d", data, off); off += 8
         p_final = take("<f8", cells)
+    origin, types_before = None, None
+    if scheme == SCHEME_FLIP_RELABEL:
+        origin = tuple(take("<f8", 3))
+        types_before = take(np.uint8, cells)
     return RefResult(Nx, Ny, Nz, n, iters, bool(sing), thr, tA, tC, tW, tP, rr, md, dh, types, idp, rowptr, col, val,
-                     b_raw, b, x, p, u, v, w, width, gap, centre, t_each, ref_norm, p_final)
+                     b_raw, b, x, p, u, v, w, width, gap, centre, t_each, ref_norm, p_final, origin, types_before)
 
 
 def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000, threads=1,
-        repeats=0, timeout=3600, scheme=SCHEME_CHORIN, p_prev=None, time=0.0) -> RefResult:
+        repeats=0, timeout=3600, scheme=SCHEME_CHORIN, p_prev=None, time=0.0, particles=None) -> RefResult:
     """Runs the reference on ``case`` with face velocities u, v, w; labels from the scene text (label_mode 0) or
     the given ``types`` (label_mode 1)."""
     if not available():
@@ -157,7 +167,7 @@ def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max
     with tempfile.TemporaryDirectory() as td:
         cp, rp = os.path.join(td, "case.bin"), os.path.join(td, "res.bin")
         write_case(cp, case, u, v, w, label_mode, types, solver, tol, max_iters, threads, repeats, scheme, p_prev,
-                   time)
+                   time, particles)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         r = subprocess.run([HARNESS, cp, rp], capture_output=True, text=True, timeout=timeout, env=env, cwd=td)
         if r.returncode != 0:

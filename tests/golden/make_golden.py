@@ -2,7 +2,7 @@
 
 Run in a checkout that has the reference sources (it builds oracle/_ref/ref_harness from them first):
 
-    python tests/golden/make_golden.py [REF_ROOT] [--only explicit]
+    python tests/golden/make_golden.py [REF_ROOT] [--only explicit|flip]
 
 Each fixture is one small case: the inputs both sides read (face velocities, the prescribed ring pressure) and what
 the reference computed from them (cell types, IDP, the CSR matrix, b before and after the compatibility step, the
@@ -52,6 +52,14 @@ SCHEME_CASES = [
 EXPLICIT_CASES = [
     ("explicit_cavity_outlet_2d_32", "cavity_outlet_2d", {"n": 32, "seed": 21}, 1e-13),
     ("explicit_closed_box_2d_16", "closed_box_2d", {"n": 16, "seed": 22}, 1e-13),
+]
+
+
+# FLIP's re-labelling from particles, then the Chorin step on the new labels: (fixture name, builder, kwargs,
+# particle seed, particles per cell)
+FLIP_CASES = [
+    ("flip_relabel_tank_3d_16", "flip_tank_3d", {"n": 16, "seed": 41}, 57, 4),
+    ("flip_relabel_tank_2d_24", "flip_tank_2d", {"n": 24, "seed": 32}, 56, 4),
 ]
 
 
@@ -117,12 +125,43 @@ def write_explicit_case(name, builder, kwargs, tol):
         name, ref.n, ref.rel_res, ref.max_div, ref.singular, os.path.getsize(out) // 1024))
 
 
+def write_flip_case(name, builder, kwargs, particle_seed, ppc):
+    """The reference's FLIP{2,3}D::UpdateFluidCells from seeded particles (W.flip_particles) on the scene's labels,
+    then its Chorin step on the new labels."""
+    case = build_case(builder, kwargs)
+    g = case.grid
+    probe = refcase.run(case, *[np.zeros(int(np.prod(s))) if s != (0,) else np.zeros(0)
+                                for s in (g.u_shape(), g.v_shape(), g.w_shape())], tol=1e-6)
+    xyz = W.flip_particles(case, probe.types, particle_seed, ppc)
+    u, v, w = W.face_velocities(g, probe.types, case.seed, case.velocity_rule, case.fp32_velocity)
+    tol = 1e-12
+    ref = refcase.run(case, u, v, w, tol=tol, scheme=refcase.SCHEME_FLIP_RELABEL, particles=xyz)
+    assert np.array_equal(ref.types_before, probe.types)
+    p_in = np.where(ref.types == W.PRESSURE, ref.p, 0.0)
+    meta = dict(name=name, builder=builder, kwargs=kwargs, particle_seed=particle_seed, ppc=ppc, tol=tol,
+                needs_compat=case.needs_compat, rho=case.rho, dt=case.dt, n=ref.n, iters=ref.iters,
+                singular=ref.singular, rel_res=ref.rel_res, max_div=ref.max_div, dh=ref.dh,
+                origin=[float(o) for o in ref.origin], scheme=refcase.SCHEME_FLIP_RELABEL)
+    out = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(
+        out, meta=np.array(json.dumps(meta)), xyz=xyz, types_in=ref.types_before, u=u.ravel(), v=v.ravel(),
+        w=w.ravel(), p_in=p_in, types=ref.types, idp=ref.idp, b=ref.b, x=ref.x, p=ref.p, u_out=ref.u, v_out=ref.v,
+        w_out=ref.w)
+    changed = int((ref.types != ref.types_before).sum())
+    print("%-36s particles=%-6d relabelled=%-5d n=%-6d rel_res=%.2e  %d KB" % (
+        name, xyz.shape[0], changed, ref.n, ref.rel_res, os.path.getsize(out) // 1024))
+
+
 def main(ref_root: str = "/root/reference", only: str = "") -> None:
     if not refcase.build(ref_root):
         raise SystemExit("the reference harness could not be built from %s" % ref_root)
     if only == "explicit":
         for args in EXPLICIT_CASES:
             write_explicit_case(*args)
+        return
+    if only == "flip":
+        for args in FLIP_CASES:
+            write_flip_case(*args)
         return
     for name, builder, kwargs, tol in CASES:
         case = build_case(builder, kwargs)
@@ -150,6 +189,8 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
         write_scheme_case(*args)
     for args in EXPLICIT_CASES:
         write_explicit_case(*args)
+    for args in FLIP_CASES:
+        write_flip_case(*args)
 
 
 if __name__ == "__main__":
