@@ -215,6 +215,34 @@ typedef struct nb_scene
 int nereus_b200_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, const double *cy, const double *cz,
                             const nb_scene *scene, uint8_t *cellTypes);
 
+/* ---- FLIP's re-labelling from particle positions: FLIP3D::UpdateFluidCells (src/Methods/FLIP/FLIP3D.cpp:784-833)
+ *      and FLIP2D::UpdateFluidCells (src/Methods/FLIP/FLIP2D.cpp:648-691), with MAC::ResetFluidCells
+ *      (src/MAC.cpp:556-589). The labels come out byte for byte as the reference's serial loops leave them:
+ *      every cell not SOLID, INFLOW, OUTFLOW or PRESSURE is reset to EMPTY, each particle's cell that is EMPTY
+ *      becomes FLUID, then one in-place pass over the interior in (i, j, k) order fills an EMPTY cell with at least
+ *      5 (3D) or 3 (2D) FLUID neighbours, a cell filled earlier in the pass counting for the later ones. ----
+ * (ox, oy, oz) are the grid's FacePos(X|Y|Z, 0) (the low face of the first ring cell) and dh is SIMULATION.dh.
+ * Particle p's coordinates are px[p * stride], py[p * stride], pz[p * stride] (pz unread in 2D, may be NULL): the
+ * reference's own Particle array has stride 7 with px = &data[0].x, py = &data[0].y, pz = &data[0].z; separate
+ * position arrays have stride 1. A particle's index along an axis is trunc((x - origin) / dh), at most N - 1, as in
+ * the reference; a particle more than one cell below the grid's first face, or with a non-finite coordinate, which
+ * the reference would index outside its labels with, is skipped and counted in *skipped.
+ * Host form: host pointers; the call copies in and out and returns when done. skipped may be NULL. */
+int nereus_b200_update_fluid_cells(int dim, int Nx, int Ny, int Nz, double ox, double oy, double oz, double dh,
+                                   const double *px, const double *py, const double *pz, int64_t count,
+                                   int64_t stride, uint8_t *cellTypes, int64_t *skipped);
+/* Device form: cellTypes, px/py/pz, scratch and skipped (one int64, may be NULL) are DEVICE pointers on `device`;
+ * the work is queued on `stream` (a cudaStream_t, NULL = the default stream) with no allocation and no host wait, so
+ * it may be captured in a CUDA graph. scratch (4-byte aligned) holds the cells that the in-place pass leaves
+ * undecided; nereus_b200_update_fluid_cells_scratch_bytes gives a size that always suffices (16 bytes + 4 per
+ * interior cell). With less (16 bytes at least) the result is the same, and only slower when the undecided cells
+ * overflow it. Calls that overlap in time on one scratch buffer race. */
+size_t nereus_b200_update_fluid_cells_scratch_bytes(int dim, int Nx, int Ny, int Nz);
+int nereus_b200_update_fluid_cells_device(int device, int dim, int Nx, int Ny, int Nz, double ox, double oy,
+                                          double oz, double dh, const double *px, const double *py, const double *pz,
+                                          int64_t count, int64_t stride, uint8_t *cellTypes, void *scratch,
+                                          size_t scratch_bytes, int64_t *skipped, void *stream);
+
 /* ---- batched and served solves. The reference has one solve per call from the manager thread
  *      (SimulationManager.h:345-353 -> PressureSolver3D::SolvePressure + Project); a server runs many independent
  *      pressure steps (tanks of a batch, requests of a stream) concurrently on one or more devices. Each device

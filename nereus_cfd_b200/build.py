@@ -2,8 +2,8 @@
 
     python -m nereus_cfd_b200.build [--verbose]
 
-nb_exact.cu is compiled with -fmad=false (its results must round like the reference's host code); the solver
-kernels keep fused multiply-adds. The object files go to nereus_cfd_b200/_build/.
+nb_exact.cu and nb_relabel.cu are compiled with -fmad=false (their results must round like the reference's host
+code); the solver kernels keep fused multiply-adds. The object files go to nereus_cfd_b200/_build/.
 """
 from __future__ import annotations
 
@@ -30,6 +30,7 @@ SOURCES = {
     "nb_solver.cu": [],
     "nb_capi.cu": [],
     "nb_noalloc.cu": [],
+    "nb_relabel.cu": ["-fmad=false"],
     "nb_server.cu": [],
 }
 HEADERS = ["nb_device.cuh", "nb_kernels.h", "nb_solver.h", "nb_guard.h"]

@@ -139,6 +139,14 @@ SIGNATURES = {
     "nereus_b200_number_unknowns_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "nereus_b200_update_fluid_cells": (ctypes.c_int, [ctypes.c_int] * 4 + [ctypes.c_double] * 4 +
+                                       [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_int64, _u8,
+                                                                ctypes.POINTER(ctypes.c_int64)]),
+    "nereus_b200_update_fluid_cells_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
+    "nereus_b200_update_fluid_cells_device": (ctypes.c_int, [ctypes.c_int] * 5 + [ctypes.c_double] * 4 +
+                                              [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_int64] +
+                                              [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                               ctypes.c_void_p]),
 }
 
 # kernel ids of nereus_b200_profile_* (include/nereus_b200.h)
@@ -212,6 +220,26 @@ def scene_struct(scene) -> SceneStruct:
             s.regions[n].p0[a], s.regions[n].p1[a] = r.p0[a], r.p1[a]
         s.regions[n].radius = r.radius
     return s
+
+
+def update_fluid_cells(grid, types, xyz, origin, dh=None):
+    """FLIP{2,3}D::UpdateFluidCells on the device from host arrays (nereus_b200_update_fluid_cells): returns the new
+    cell types and the number of particles skipped as outside the labels. xyz: (count, 3) float64 positions, or any
+    float64 array whose rows start with x, y, z (the reference's 7-double Particle rows included); origin:
+    FacePos(X|Y|Z, 0)."""
+    out = np.ascontiguousarray(types, dtype=np.uint8).reshape(-1).copy()
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    xyz = xyz.reshape(xyz.shape[0], -1) if xyz.size else np.zeros((0, 3))
+    count, stride = xyz.shape
+    base = xyz.ctypes.data
+    pz = ctypes.c_void_p(base + 16) if grid.dim == 3 else None
+    skipped = ctypes.c_int64(0)
+    oz = origin[2] if len(origin) > 2 else 0.0
+    check(load().nereus_b200_update_fluid_cells(
+        grid.dim, grid.Nx, grid.Ny, grid.Nz if grid.dim == 3 else 1, origin[0], origin[1], oz,
+        grid.dh if dh is None else dh, ctypes.c_void_p(base), ctypes.c_void_p(base + 8), pz, count, stride,
+        ptr(out, _u8), ctypes.byref(skipped)))
+    return out, int(skipped.value)
 
 
 def label_cells(grid, scene) -> np.ndarray:

@@ -285,6 +285,84 @@ int nereus_b200_number_unknowns_noalloc(int device, int dim, int Nx, int Ny, int
     });
 }
 
+size_t nereus_b200_update_fluid_cells_scratch_bytes(int dim, int Nx, int Ny, int Nz)
+{
+    return nb::RelabelScratchBytes(dim, Nx, Ny, Nz);
+}
+
+int nereus_b200_update_fluid_cells_device(int device, int dim, int Nx, int Ny, int Nz, double ox, double oy,
+                                          double oz, double dh, const double *px, const double *py, const double *pz,
+                                          int64_t count, int64_t stride, uint8_t *cellTypes, void *scratch,
+                                          size_t scratch_bytes, int64_t *skipped, void *stream)
+{
+    static_assert(sizeof(int64_t) == sizeof(unsigned long long), "skipped is a 64-bit counter");
+    return Guard([&] {
+        int ndev = 0;
+        NB_CK(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) throw nb::InputError("no such device");
+        int prev = 0;
+        NB_CK(cudaGetDevice(&prev));
+        NB_CK(cudaSetDevice(device));
+        try
+        {
+            nb::UpdateFluidCellsDevice(dim, Nx, Ny, Nz, ox, oy, oz, dh, px, py, pz, count, stride, cellTypes, scratch,
+                                       scratch_bytes, (unsigned long long *)skipped, (cudaStream_t)stream);
+        }
+        catch (...)
+        {
+            cudaSetDevice(prev);
+            throw;
+        }
+        NB_CK(cudaSetDevice(prev));
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_update_fluid_cells(int dim, int Nx, int Ny, int Nz, double ox, double oy, double oz, double dh,
+                                   const double *px, const double *py, const double *pz, int64_t count,
+                                   int64_t stride, uint8_t *cellTypes, int64_t *skipped)
+{
+    if (!cellTypes) return Fail(NB_BAD_INPUT, "null argument");
+    if ((dim != 2 && dim != 3) || Nx < 1 || Ny < 1 || (dim == 3 && Nz < 1)) return Fail(NB_BAD_INPUT, "bad sizes");
+    if (count < 0) return Fail(NB_BAD_INPUT, "negative particle count");
+    if (count > 0 && (!px || !py || (dim == 3 && !pz))) return Fail(NB_BAD_INPUT, "null particle coordinates");
+    if (count > 0 && stride < 1) return Fail(NB_BAD_INPUT, "particle stride must be at least 1");
+    return Guard([&] {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return Fail(NB_NO_DEVICE, "no CUDA device");
+        const int nz = dim == 3 ? Nz : 1;
+        const size_t cells = (size_t)Nx * Ny * nz;
+        // the positions packed as three plain arrays: 24 bytes per particle cross PCIe instead of the whole struct
+        std::vector<double> xyz((size_t)count * (dim == 3 ? 3 : 2));
+        double *hx = xyz.data(), *hy = hx + count, *hz = dim == 3 ? hy + count : nullptr;
+        for (int64_t p = 0; p < count; p++)
+        {
+            hx[p] = px[p * stride];
+            hy[p] = py[p * stride];
+            if (hz) hz[p] = pz[p * stride];
+        }
+        cudaStream_t st;
+        NB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{st};
+        nb::DevArray<double> P;
+        nb::DevArray<uint8_t> T, S;
+        nb::DevArray<unsigned long long> K;
+        P.upload(xyz.data(), xyz.size(), st);
+        T.upload(cellTypes, cells, st);
+        const size_t sb = nb::RelabelScratchBytes(dim, Nx, Ny, Nz);
+        S.alloc(sb);
+        K.alloc(1);
+        const double *dx = P.p, *dy = P.p ? P.p + count : nullptr, *dz = (P.p && dim == 3) ? P.p + 2 * count : nullptr;
+        nb::UpdateFluidCellsDevice(dim, Nx, Ny, Nz, ox, oy, oz, dh, dx, dy, dz, count, 1, T.p, S.p, sb, K.p, st);
+        unsigned long long k = 0;
+        NB_CK(cudaMemcpyAsync(cellTypes, T.p, cells, cudaMemcpyDeviceToHost, st));
+        NB_CK(cudaMemcpyAsync(&k, K.p, sizeof(k), cudaMemcpyDeviceToHost, st));
+        NB_CK(cudaStreamSynchronize(st));
+        if (skipped) *skipped = (int64_t)k;
+        return (int)NB_OK;
+    });
+}
+
 int nereus_b200_export_matrix(nb_ctx *ctx, int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singular)
 {
     if (!ctx || !ctx->c || !rowptr || !col || !val || !nnz || !singular) return Fail(NB_BAD_INPUT, "null argument");

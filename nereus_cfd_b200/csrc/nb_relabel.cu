@@ -1,0 +1,316 @@
+// FLIP's re-labelling from particle positions on the device: FLIP3D::UpdateFluidCells
+// (src/Methods/FLIP/FLIP3D.cpp:784-833) and FLIP2D::UpdateFluidCells (src/Methods/FLIP/FLIP2D.cpp:648-691), with
+// MAC::ResetFluidCells (src/MAC.cpp:556-589). The labels come out byte for byte as the reference's serial loops leave
+// them, so the pressure step that follows (set_layout) numbers and assembles the same system.
+//
+// The reference's three steps and how they run here (five launches on one stream, no allocation, no host wait, so a
+// caller may capture them in a graph):
+//   1. reset: every cell that is not SOLID, INFLOW, OUTFLOW or PRESSURE becomes EMPTY. k_relabel_reset, 16 bytes per
+//      thread; it also zeroes the pending-list counter and the skipped-particle count.
+//   2. mark: each particle's cell, if EMPTY, becomes FLUID. k_relabel_mark, grid-stride over the particles, reading
+//      x, y, z through a stride so that the reference's own Particle array (x, y, z at doubles 1..3 of 7) and plain
+//      position arrays both serve. The index is the reference's (truncation of (x - origin) / dh toward zero, clamped
+//      above); a particle more than one cell below the grid or with a non-finite coordinate, which the reference
+//      would index outside its labels with, is skipped and counted.
+//   3. hole filling: one pass over the interior in (i, j, k) order, IN PLACE: an EMPTY cell with >= 5 (3D) / >= 3
+//      (2D) FLUID neighbours becomes FLUID, and a cell filled earlier in the pass counts for the later ones. So a cell
+//      sees its upper neighbours (i+1, j+1, k+1) as they were before the pass and its lower ones (i-1, j-1, k-1) as
+//      the pass left them. The result is the unique solution of that recurrence, which is what is computed here:
+//        k_relabel_fill: one thread per interior column, marching the fast axis (k; j in 2D) upwards, so runs along
+//          it resolve in order. Filled cells get the marker kFilled, which counts as FLUID for the cells above and
+//          not at all for the cells below (they read the label from before the pass). A cell still EMPTY that could
+//          yet be filled once its lower neighbours are (the count with every EMPTY interior lower neighbour taken as
+//          filled reaches the threshold) goes on a pending list.
+//        k_relabel_settle: one block iterates over the pending list until a pass fills nothing. Every fill is
+//          justified by neighbours that belong to the solution, and every cell of the solution not yet filled is on
+//          the list, so the fixed point is the solution; each pass but the last fills at least one cell, which bounds
+//          the passes by the list's length + 1. When the list outgrew the caller's scratch, the block runs the same
+//          passes over every interior cell instead.
+//        k_relabel_finish: kFilled -> FLUID.
+#include "nb_solver.h"
+
+#include <cstdint>
+
+namespace nb
+{
+
+namespace
+{
+
+constexpr uint8_t kFilled = 0x80; // an EMPTY cell the hole pass filled, until k_relabel_finish
+constexpr int kThreads = 256;
+constexpr int kSettleThreads = 1024;
+constexpr int kHeaderInts = 4; // scratch: [0] pending count, [1..3] unused, then the list
+
+struct RelabelGrid
+{
+    int dim, Nx, Ny, Nz;       // Nz = 1 in 2D
+    long long cells;
+    long long sI, sJ;          // strides of i and j (2D: sJ = 1 is the march axis)
+    int colsX;                 // interior columns along the second axis (3D: Nx - 2; 2D: 1)
+    int nCols;                 // interior columns
+    int march;                 // interior cells along the march axis (3D: Nz - 2; 2D: Nx - 2)
+    int thr;                   // FLUID neighbours that fill a hole: 5 (3D), 3 (2D)
+};
+
+__device__ __forceinline__ uint8_t ResetByte(uint8_t b)
+{
+    return (b == SOLID || b == INFLOW || b == OUTFLOW || b == PRESSURE) ? b : (uint8_t)EMPTY;
+}
+
+__device__ __forceinline__ uint32_t ResetWord(uint32_t w)
+{
+    uint32_t o = 0;
+#pragma unroll
+    for (int s = 0; s < 32; s += 8) o |= (uint32_t)ResetByte((uint8_t)(w >> s)) << s;
+    return o;
+}
+
+__device__ __forceinline__ uint32_t FinishWord(uint32_t w)
+{
+    uint32_t o = 0;
+#pragma unroll
+    for (int s = 0; s < 32; s += 8)
+    {
+        const uint8_t b = (uint8_t)(w >> s);
+        o |= (uint32_t)(b == kFilled ? (uint8_t)FLUID : b) << s;
+    }
+    return o;
+}
+
+// A byte map over the whole label array: the bytes before the first 16-byte boundary and after the last one
+// one at a time, the rest as uint4.
+template <bool kFinish>
+__device__ __forceinline__ void MapLabels(uint8_t *__restrict__ t, long long cells)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    const long long mis = (long long)((16 - ((uintptr_t)t & 15)) & 15);
+    const long long head = mis < cells ? mis : cells;
+    const long long nvec = (cells - head) >> 4;
+    for (long long c = tid; c < head; c += nt)
+        t[c] = kFinish ? (t[c] == kFilled ? (uint8_t)FLUID : t[c]) : ResetByte(t[c]);
+    uint4 *v = (uint4 *)(t + head);
+    for (long long q = tid; q < nvec; q += nt)
+    {
+        uint4 x = v[q];
+        if (kFinish)
+        {
+            x.x = FinishWord(x.x); x.y = FinishWord(x.y); x.z = FinishWord(x.z); x.w = FinishWord(x.w);
+        }
+        else
+        {
+            x.x = ResetWord(x.x); x.y = ResetWord(x.y); x.z = ResetWord(x.z); x.w = ResetWord(x.w);
+        }
+        v[q] = x;
+    }
+    for (long long c = head + (nvec << 4) + tid; c < cells; c += nt)
+        t[c] = kFinish ? (t[c] == kFilled ? (uint8_t)FLUID : t[c]) : ResetByte(t[c]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_relabel_reset(uint8_t *__restrict__ t, long long cells, int *hdr,
+                                                            unsigned long long *skipped)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        hdr[0] = 0;
+        if (skipped) *skipped = 0ull;
+    }
+    MapLabels<false>(t, cells);
+}
+
+__global__ void __launch_bounds__(kThreads) k_relabel_finish(uint8_t *__restrict__ t, long long cells)
+{
+    MapLabels<true>(t, cells);
+}
+
+// UpdateFluidCells' index of one coordinate (FLIP3D.cpp:796-802): trunc((x - origin) / dh), at most N - 1; -1 for a
+// quotient at or below -1 or not finite (outside the labels in the reference). A quotient at or above N takes N - 1
+// without a conversion.
+__device__ __forceinline__ int ParticleIndex(double x, double origin, double dh, int N)
+{
+    const double q = (x - origin) / dh;
+    if (!(q > -1.0)) return -1;
+    if (q >= (double)N) return N - 1;
+    return (int)q;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_relabel_mark(const double *__restrict__ px, const double *__restrict__ py, const double *__restrict__ pz,
+                   long long count, long long stride, RelabelGrid g, double ox, double oy, double oz, double dh,
+                   uint8_t *__restrict__ t, unsigned long long *skipped)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    unsigned long long mine = 0;
+    for (long long p = tid; p < count; p += nt)
+    {
+        const long long o = p * stride;
+        const int i = ParticleIndex(__ldg(py + o), oy, dh, g.Ny);
+        const int j = ParticleIndex(__ldg(px + o), ox, dh, g.Nx);
+        const int k = g.dim == 3 ? ParticleIndex(__ldg(pz + o), oz, dh, g.Nz) : 0;
+        if ((i | j | k) < 0)
+        {
+            mine++;
+            continue;
+        }
+        const long long c = ((long long)i * g.Nx + j) * g.Nz + k;
+        if (t[c] == EMPTY) t[c] = (uint8_t)FLUID;
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, s);
+    if (skipped && (threadIdx.x & 31) == 0 && mine) atomicAdd(skipped, mine);
+}
+
+// FLUID neighbours of interior cell c as the in-place pass sees them: the upper ones (c + sI, c + sJ, c + 1) only if
+// FLUID before the pass, the lower ones if FLUID or filled by it. In 2D the sJ terms are the march axis's own, so
+// they are left out (sJ = 1 = the +-1 terms).
+__device__ __forceinline__ int FluidCount(const RelabelGrid &g, const uint8_t *t, long long c)
+{
+    int up = (t[c + g.sI] == FLUID) + (t[c + 1] == FLUID);
+    const uint8_t a = t[c - g.sI], b = t[c - 1];
+    int lo = (a == FLUID || a == kFilled) + (b == FLUID || b == kFilled);
+    if (g.dim == 3)
+    {
+        up += t[c + g.sJ] == FLUID;
+        const uint8_t d = t[c - g.sJ];
+        lo += d == FLUID || d == kFilled;
+    }
+    return up + lo;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_relabel_fill(RelabelGrid g, uint8_t *t, int *hdr, int *list, int cap)
+{
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= g.nCols) return;
+    // 3D: column (i, j) marching k; 2D: row i marching j
+    const int i = 1 + col / g.colsX;
+    const int j = g.dim == 3 ? 1 + col % g.colsX : 0;
+    const long long base = g.dim == 3 ? ((long long)i * g.Nx + j) * g.Nz : (long long)i * g.Nx;
+    for (int m = 1; m <= g.march; m++)
+    {
+        const long long c = base + m;
+        if (t[c] != EMPTY) continue;
+        const int f = FluidCount(g, t, c);
+        if (f >= g.thr)
+        {
+            t[c] = kFilled;
+            continue;
+        }
+        // lower neighbours that are EMPTY interior cells may still be filled by the settling passes
+        int maybe = (m > 1 && t[c - 1] == EMPTY) + (i > 1 && t[c - g.sI] == EMPTY);
+        if (g.dim == 3) maybe += j > 1 && t[c - g.sJ] == EMPTY;
+        if (f + maybe >= g.thr)
+        {
+            const int slot = atomicAdd(hdr, 1);
+            if (slot < cap) list[slot] = (int)c;
+        }
+    }
+}
+
+// Interior cell number q (0 .. interior cells - 1) in (i, j, k) order.
+__device__ __forceinline__ long long InteriorCell(const RelabelGrid &g, long long q)
+{
+    const long long col = q / g.march;
+    const int m = 1 + (int)(q - col * g.march);
+    const int i = 1 + (int)(col / g.colsX);
+    const int j = g.dim == 3 ? 1 + (int)(col % g.colsX) : 0;
+    return (g.dim == 3 ? ((long long)i * g.Nx + j) * g.Nz : (long long)i * g.Nx) + m;
+}
+
+__global__ void __launch_bounds__(kSettleThreads)
+    k_relabel_settle(RelabelGrid g, uint8_t *t, const int *hdr, const int *list, int cap)
+{
+    __shared__ int changed;
+    const int pending = hdr[0];
+    const bool all = pending > cap; // the list overflowed: pass over every interior cell
+    const long long n = all ? (long long)g.nCols * g.march : pending;
+    for (long long pass = 0; pass <= n; pass++)
+    {
+        if (threadIdx.x == 0) changed = 0;
+        __syncthreads();
+        bool any = false;
+        for (long long q = threadIdx.x; q < n; q += blockDim.x)
+        {
+            const long long c = all ? InteriorCell(g, q) : (long long)list[q];
+            if (t[c] == EMPTY && FluidCount(g, t, c) >= g.thr)
+            {
+                t[c] = kFilled;
+                any = true;
+            }
+        }
+        if (any) changed = 1;
+        __syncthreads();
+        const bool more = changed != 0;
+        __syncthreads();
+        if (!more) break;
+    }
+}
+
+int Blocks(long long work, int perBlock, int cap)
+{
+    long long b = (work + perBlock - 1) / perBlock;
+    if (b < 1) b = 1;
+    return (int)(b < cap ? b : cap);
+}
+
+} // namespace
+
+size_t RelabelScratchBytes(int dim, int Nx, int Ny, int Nz)
+{
+    const long long nz = dim == 3 ? (long long)(Nz > 2 ? Nz - 2 : 0) : 1;
+    const long long interior = (long long)(Nx > 2 ? Nx - 2 : 0) * (Ny > 2 ? Ny - 2 : 0) * nz;
+    return (size_t)(kHeaderInts + interior) * sizeof(int);
+}
+
+void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double oy, double oz, double dh,
+                            const double *px, const double *py, const double *pz, long long count, long long stride,
+                            uint8_t *cellTypes, void *scratch, size_t scratchBytes, unsigned long long *skipped,
+                            cudaStream_t st)
+{
+    if (dim != 2 && dim != 3) throw InputError("dim must be 2 or 3");
+    const int nz = dim == 3 ? Nz : 1;
+    if (Nx < 1 || Ny < 1 || nz < 1) throw InputError("bad sizes");
+    const long long cells = (long long)Nx * Ny * nz;
+    if (cells >= (1ll << 31)) throw InputError("at most 2^31 - 1 cells");
+    if (!cellTypes || !scratch) throw InputError("null argument");
+    if (count < 0) throw InputError("negative particle count");
+    if (count > 0 && (!px || !py || (dim == 3 && !pz))) throw InputError("null particle coordinates");
+    if (count > 0 && stride < 1) throw InputError("particle stride must be at least 1");
+    if (!(dh > 0.0) || !std::isfinite(dh)) throw InputError("dh must be positive and finite");
+    if (scratchBytes < kHeaderInts * sizeof(int) || ((uintptr_t)scratch & 3)) throw InputError("scratch too small or misaligned");
+
+    RelabelGrid g;
+    g.dim = dim; g.Nx = Nx; g.Ny = Ny; g.Nz = nz; g.cells = cells;
+    g.sI = (long long)Nx * nz;
+    g.sJ = dim == 3 ? nz : 1;
+    g.colsX = dim == 3 ? (Nx > 2 ? Nx - 2 : 0) : 1;
+    g.nCols = (Ny > 2 ? Ny - 2 : 0) * g.colsX;
+    g.march = dim == 3 ? (nz > 2 ? nz - 2 : 0) : (Nx > 2 ? Nx - 2 : 0);
+    g.thr = 2 * dim - 1;
+    int *hdr = (int *)scratch;
+    int *list = hdr + kHeaderInts;
+    const long long capLL = (long long)(scratchBytes / sizeof(int)) - kHeaderInts;
+    const int cap = (int)(capLL < (1ll << 31) - 1 ? capLL : (1ll << 31) - 1);
+
+    const int sms = 148;
+    NB_COUNT_LAUNCH();
+    k_relabel_reset<<<Blocks(cells / 16 + 1, kThreads, sms * 8), kThreads, 0, st>>>(cellTypes, cells, hdr, skipped);
+    if (count > 0)
+    {
+        NB_COUNT_LAUNCH();
+        k_relabel_mark<<<Blocks(count, kThreads, sms * 16), kThreads, 0, st>>>(px, py, pz, count, stride, g, ox, oy,
+                                                                              oz, dh, cellTypes, skipped);
+    }
+    if (g.nCols > 0 && g.march > 0)
+    {
+        NB_COUNT_LAUNCHES(3);
+        k_relabel_fill<<<Blocks(g.nCols, kThreads, 1 << 30), kThreads, 0, st>>>(g, cellTypes, hdr, list, cap);
+        k_relabel_settle<<<1, kSettleThreads, 0, st>>>(g, cellTypes, hdr, list, cap);
+        k_relabel_finish<<<Blocks(cells / 16 + 1, kThreads, sms * 8), kThreads, 0, st>>>(cellTypes, cells);
+    }
+    NB_CK(cudaGetLastError());
+}
+
+} // namespace nb

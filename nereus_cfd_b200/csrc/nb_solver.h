@@ -283,4 +283,12 @@ constexpr int kNoAllocMaxLines = 1 << 18;
 void NumberUnknownsNoAlloc(int device, int dim, int Nx, int Ny, int Nz, const uint8_t *types, int32_t *idp,
                            int32_t *n, cudaStream_t st);
 
+// FLIP's re-labelling from particles (nb_relabel.cu): the labels FLIP{2,3}D::UpdateFluidCells leaves, on `st`, no
+// allocation. skipped (device, may be null) gets the number of particles outside the labels.
+size_t RelabelScratchBytes(int dim, int Nx, int Ny, int Nz);
+void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double oy, double oz, double dh,
+                            const double *px, const double *py, const double *pz, long long count, long long stride,
+                            uint8_t *cellTypes, void *scratch, size_t scratchBytes, unsigned long long *skipped,
+                            cudaStream_t st);
+
 } // namespace nb

@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import ROOT, cuda_ok
@@ -71,3 +72,25 @@ def test_null_arguments_are_bad_input(lib):
     assert lib.nereus_b200_project(None, None, None, None, None, 1.0, 1.0, 0, 0, 1e-8, None) == capi.NB_BAD_INPUT
     assert lib.nereus_b200_system_size(None) == 0
     lib.nereus_b200_destroy(None)  # a no-op
+
+
+def test_relabel_checks_its_arguments_before_the_device(lib):
+    """nereus_b200_update_fluid_cells refuses bad sizes and pointers before it looks for a device."""
+    t = np.zeros(27, dtype=np.uint8)
+    xyz = np.zeros((2, 3))
+    px = ctypes.c_void_p(xyz.ctypes.data)
+    args = lambda **kw: dict(dict(dim=3, N=3, t=capi.ptr(t, capi._u8), px=px, count=2, stride=3), **kw)
+
+    def call(a):
+        return lib.nereus_b200_update_fluid_cells(a["dim"], a["N"], a["N"], a["N"], 0.0, 0.0, 0.0, 1.0, a["px"],
+                                                  a["px"], a["px"], a["count"], a["stride"], a["t"], None)
+    assert call(args(t=None)) == capi.NB_BAD_INPUT
+    assert call(args(dim=4)) == capi.NB_BAD_INPUT
+    assert call(args(N=0)) == capi.NB_BAD_INPUT
+    assert call(args(count=-1)) == capi.NB_BAD_INPUT
+    assert call(args(stride=0)) == capi.NB_BAD_INPUT
+    assert call(args(px=None)) == capi.NB_BAD_INPUT
+    if not cuda_ok():
+        assert call(args()) == capi.NB_NO_DEVICE
+        sb = lib.nereus_b200_update_fluid_cells_scratch_bytes(3, 10, 10, 10)
+        assert sb == 16 + 4 * 8 ** 3
