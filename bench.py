@@ -290,6 +290,7 @@ def run_b200(args, rank, world, dist):
     stretched = run_stretched(args, dev) if args.stretched_steps > 0 and world == 1 else None
     tanks = run_tanks(args, rank, world, dist, dev) if args.tanks > 0 else None
     trace = run_trace(args, dev) if args.trace > 0 and world == 1 else None
+    relabel = run_relabel(args, dev) if args.relabel_steps > 0 and world == 1 else None
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -303,7 +304,7 @@ def run_b200(args, rank, world, dist):
         "latency_ms": {"p50": round(percentile(lat, 0.5), 3), "p99": round(percentile(lat, 0.99), 3)},
         "solve": {k: mixed_res[k] for k in ("iters_outer", "iters_inner", "rel_res", "max_div", "status")},
         "fp64_plain": fp64, "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": int(launches),
-        "stretched_cylinder": stretched, "batched_tanks": tanks, "serving_trace": trace,
+        "stretched_cylinder": stretched, "batched_tanks": tanks, "serving_trace": trace, "flip_relabel": relabel,
     }
     return out
 
@@ -408,6 +409,102 @@ def run_stretched(args, dev):
         out["unknowns"] = res.n
         s.DestroyPressureSolver()
     out["speedup_mixed_over_fp64"] = round(out["mixed"]["value"] / out["fp64"]["value"], 3)
+    return out
+
+
+def run_relabel(args, dev):
+    """FLIP's re-labelling from particles (nereus_b200_update_fluid_cells_device; FLIP3D::UpdateFluidCells): the
+    free-surface tank at 256^3 (liquid where x < 0.5 and z < 0.5), 8 particles per liquid cell seeded cell by cell
+    (the reference's seeding order) with 3% of the liquid cells left empty, positions as (x, y, z) rows of float64
+    and as the reference's 7-double Particle rows. The call resets the labels itself, so repeated steps start from
+    the previous step's labels exactly as the reference's do. CUDA events on the launching stream; the position rows
+    (805 MB) are larger than L2. The host form (host arrays in, labels out) is timed by wall clock, and the oracle's
+    serial restatement on one host core is the CPU baseline."""
+    import torch
+
+    from nereus_cfd_b200 import capi, workloads as W
+
+    lib = capi.load()
+    n = args.relabel_size
+    case = W.flip_tank_3d(n=n, seed=4, a=0.5, b=0.5)
+    g = case.grid
+    types = capi.label_cells(g, case.scene)
+    org = [ax.face[0] for ax in g.axes]
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(4)
+    liquid = torch.nonzero(torch.from_numpy(types.reshape(g.shape) == W.FLUID).to("cuda"))  # (i, j, k) in order
+    keep = torch.rand(liquid.shape[0], device="cuda", generator=gen, dtype=torch.float64) >= 0.03
+    cells = liquid[keep].repeat_interleave(8, dim=0)
+    faces = [torch.from_numpy(ax.face).to("cuda") for ax in g.axes]
+    jit = torch.rand(cells.shape[0], 3, device="cuda", generator=gen, dtype=torch.float64)
+    rows = torch.stack([faces[0][cells[:, 1]], faces[1][cells[:, 0]], faces[2][cells[:, 2]]], dim=1) + g.dh * jit
+    rows = rows.contiguous()
+    del cells, jit
+    count = rows.shape[0]
+    t = torch.from_numpy(types).to("cuda")
+    sb = lib.nereus_b200_update_fluid_cells_scratch_bytes(3, g.Nx, g.Ny, g.Nz)
+    scratch = torch.zeros(sb // 4 + 1, dtype=torch.int32, device="cuda")
+    skipped = torch.zeros(1, dtype=torch.int64, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def step(px, py, pz, stride):
+        capi.check(lib.nereus_b200_update_fluid_cells_device(
+            dev, 3, g.Nx, g.Ny, g.Nz, org[0], org[1], org[2], g.dh, ctypes.c_void_p(px), ctypes.c_void_p(py),
+            ctypes.c_void_p(pz), count, stride, ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(scratch.data_ptr()),
+            sb, ctypes.c_void_p(skipped.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+
+    def timed(px, py, pz, stride):
+        for _ in range(3):
+            step(px, py, pz, stride)
+        evs = []
+        l0 = lib.nereus_b200_kernel_launches()
+        for _ in range(args.relabel_steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            step(px, py, pz, stride)
+            b.record(st)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs], lib.nereus_b200_kernel_launches() - l0
+
+    base = rows.data_ptr()
+    ms, launches = timed(base, base + 8, base + 16, 3)
+    peak, peak_kind = measured_peaks()
+    algo = 24 * count + 5 * g.cells  # positions; labels: reset r+w, fill r, finish r+w
+    med = statistics.median(ms)
+    out = {"workload": "flip_tank_3d_%d, 8 particles per liquid cell" % n, "particles": count, "cells": g.cells,
+           "value": round(count / med / 1e3, 1), "unit": "M particles/s", "ms": round(med, 4),
+           "steps": len(ms), "gpu_launches": int(launches), "skipped": int(skipped.item()),
+           "roofline": {"bound": "hbm", "achieved": round(algo / med / 1e6, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(algo / med / 1e6 / peak, 3), "peak_kind": peak_kind,
+                        "algorithmic_bytes": int(algo),
+                        "bytes_per_unit": "24 B per particle (x, y, z) + 5 B per cell (labels reset, read, finished)"}}
+    # the reference's own Particle layout: 7 doubles a particle, x at the second
+    aos = torch.zeros(count, 7, dtype=torch.float64, device="cuda")
+    aos[:, 1:4] = rows
+    ab = aos.data_ptr()
+    ms7, _ = timed(ab + 8, ab + 16, ab + 24, 7)
+    out["particle_rows_7"] = {"value": round(count / statistics.median(ms7) / 1e3, 1), "unit": "M particles/s",
+                              "ms": round(statistics.median(ms7), 4)}
+    del aos
+    # host form end to end: host positions and labels in, labels out
+    hx = rows.cpu().numpy()
+    ts = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        capi.update_fluid_cells(g, types, hx, org)
+        ts.append(time.perf_counter() - t0)
+    out["e2e"] = {"value": round(count / min(ts) / 1e6, 1), "unit": "M particles/s", "ms": round(1e3 * min(ts), 2),
+                  "api": "nereus_b200_update_fluid_cells (host arrays)", "h2d_bytes_per_step": 24 * count + g.cells,
+                  "d2h_bytes_per_step": g.cells + 8}
+    if not args.no_cpu_baseline:
+        from oracle import cpu
+
+        t0 = time.perf_counter()
+        cpu.update_fluid_cells(g, types, hx, org)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(count / dt / 1e6, 2), "unit": "M particles/s", "cores": 1,
+                               "kind": "port", "sample": "the whole cloud, oracle/pressure_oracle.c serial"}
     return out
 
 
@@ -562,6 +659,8 @@ def main():
     ap.add_argument("--trace", type=int, default=200, help="requests of the serving trace (0: skip)")
     ap.add_argument("--stretched-steps", type=int, default=5, help="steps of the stretched workload (0: skip)")
     ap.add_argument("--trace-fp64", type=int, default=40, help="trace requests solved one at a time in plain FP64")
+    ap.add_argument("--relabel-steps", type=int, default=10, help="timed steps of FLIP's re-labelling (0: skip)")
+    ap.add_argument("--relabel-size", type=int, default=256)
     args = ap.parse_args()
     args.solver_opts = {k: int(v) if v.lstrip("-").isdigit() else float(v)
                         for k, v in (o.split("=", 1) for o in args.opt)}

@@ -7,7 +7,8 @@
 // caller may capture them in a graph):
 //   1. reset: every cell that is not SOLID, INFLOW, OUTFLOW or PRESSURE becomes EMPTY. k_relabel_reset, 16 bytes per
 //      thread; it also zeroes the pending-list counter and the skipped-particle count.
-//   2. mark: each particle's cell, if EMPTY, becomes FLUID. k_relabel_mark, grid-stride over the particles, reading
+//   2. mark: each particle's cell, if EMPTY, becomes FLUID. k_relabel_mark, one wave of threads striding over the
+//      particles four at a time, reading
 //      x, y, z through a stride so that the reference's own Particle array (x, y, z at doubles 1..3 of 7) and plain
 //      position arrays both serve. The index is the reference's (truncation of (x - origin) / dh toward zero, clamped
 //      above); a particle more than one cell below the grid or with a non-finite coordinate, which the reference
@@ -16,11 +17,12 @@
 //      (2D) FLUID neighbours becomes FLUID, and a cell filled earlier in the pass counts for the later ones. So a cell
 //      sees its upper neighbours (i+1, j+1, k+1) as they were before the pass and its lower ones (i-1, j-1, k-1) as
 //      the pass left them. The result is the unique solution of that recurrence, which is what is computed here:
-//        k_relabel_fill: one thread per interior column, marching the fast axis (k; j in 2D) upwards, so runs along
-//          it resolve in order. Filled cells get the marker kFilled, which counts as FLUID for the cells above and
-//          not at all for the cells below (they read the label from before the pass). A cell still EMPTY that could
-//          yet be filled once its lower neighbours are (the count with every EMPTY interior lower neighbour taken as
-//          filled reaches the threshold) goes on a pending list.
+//        k_relabel_fill: one thread per interior cell, consecutive threads along the fast axis. Filled cells get the
+//          marker kFilled, which counts as FLUID for the cells above and not at all for the cells below (they read
+//          the label from before the pass). A filled cell has at most one uncounted neighbour, so at most one of its
+//          upper neighbours can continue a chain of fills: the thread walks up that chain at once. A cell still EMPTY
+//          that could yet be filled once its lower neighbours are (the count with every EMPTY interior lower
+//          neighbour taken as filled reaches the threshold) goes on a pending list.
 //        k_relabel_settle: one block iterates over the pending list until a pass fills nothing. Every fill is
 //          justified by neighbours that belong to the solution, and every cell of the solution not yet filled is on
 //          the list, so the fixed point is the solution; each pass but the last fills at least one cell, which bounds
@@ -135,7 +137,9 @@ __device__ __forceinline__ int ParticleIndex(double x, double origin, double dh,
     return (int)q;
 }
 
-__global__ void __launch_bounds__(kThreads)
+constexpr int kMarkBatch = 4; // particles in flight per thread
+
+__global__ void __launch_bounds__(kThreads, 4)
     k_relabel_mark(const double *__restrict__ px, const double *__restrict__ py, const double *__restrict__ pz,
                    long long count, long long stride, RelabelGrid g, double ox, double oy, double oz, double dh,
                    uint8_t *__restrict__ t, unsigned long long *skipped)
@@ -143,19 +147,42 @@ __global__ void __launch_bounds__(kThreads)
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
     unsigned long long mine = 0;
-    for (long long p = tid; p < count; p += nt)
-    {
-        const long long o = p * stride;
-        const int i = ParticleIndex(__ldg(py + o), oy, dh, g.Ny);
-        const int j = ParticleIndex(__ldg(px + o), ox, dh, g.Nx);
-        const int k = g.dim == 3 ? ParticleIndex(__ldg(pz + o), oz, dh, g.Nz) : 0;
-        if ((i | j | k) < 0)
+    const long long step = nt * kMarkBatch;
+    double x[kMarkBatch], y[kMarkBatch], z[kMarkBatch];
+    // positions of particles p, p + nt, ..., p + 3 nt (the first one again past the end: it is in range)
+    auto load = [&](long long p) {
+#pragma unroll
+        for (int b = 0; b < kMarkBatch; b++)
         {
-            mine++;
-            continue;
+            const long long o = (p + b * nt < count ? p + b * nt : p) * stride;
+            x[b] = __ldg(px + o);
+            y[b] = __ldg(py + o);
+            z[b] = g.dim == 3 ? __ldg(pz + o) : 0.0;
         }
-        const long long c = ((long long)i * g.Nx + j) * g.Nz + k;
-        if (t[c] == EMPTY) t[c] = (uint8_t)FLUID;
+    };
+    long long p0 = tid;
+    if (p0 < count) load(p0);
+    while (p0 < count)
+    {
+        long long c[kMarkBatch];
+#pragma unroll
+        for (int b = 0; b < kMarkBatch; b++)
+        {
+            const int i = ParticleIndex(y[b], oy, dh, g.Ny);
+            const int j = ParticleIndex(x[b], ox, dh, g.Nx);
+            const int k = g.dim == 3 ? ParticleIndex(z[b], oz, dh, g.Nz) : 0;
+            const bool live = p0 + b * nt < count;
+            const bool out = (i | j | k) < 0;
+            mine += live && out;
+            c[b] = live && !out ? ((long long)i * g.Nx + j) * g.Nz + k : -1;
+        }
+        // the next batch's positions are in flight while this batch's labels are read and written
+        const long long p1 = p0 + step;
+        if (p1 < count) load(p1);
+#pragma unroll
+        for (int b = 0; b < kMarkBatch; b++)
+            if (c[b] >= 0 && t[c[b]] == EMPTY) t[c[b]] = (uint8_t)FLUID;
+        p0 = p1;
     }
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, s);
@@ -179,33 +206,40 @@ __device__ __forceinline__ int FluidCount(const RelabelGrid &g, const uint8_t *t
     return up + lo;
 }
 
-__global__ void __launch_bounds__(kThreads)
-    k_relabel_fill(RelabelGrid g, uint8_t *t, int *hdr, int *list, int cap)
+// Interior coordinates of cell c: (i, j, m) with m the march-axis index (k in 3D, j in 2D; j = 0 in 2D).
+__device__ __forceinline__ void CellCoords(const RelabelGrid &g, long long c, int &i, int &j, int &m)
 {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= g.nCols) return;
-    // 3D: column (i, j) marching k; 2D: row i marching j
-    const int i = 1 + col / g.colsX;
-    const int j = g.dim == 3 ? 1 + col % g.colsX : 0;
-    const long long base = g.dim == 3 ? ((long long)i * g.Nx + j) * g.Nz : (long long)i * g.Nx;
-    for (int m = 1; m <= g.march; m++)
+    i = (int)(c / g.sI);
+    const long long r = c - (long long)i * g.sI;
+    if (g.dim == 3)
     {
-        const long long c = base + m;
-        if (t[c] != EMPTY) continue;
-        const int f = FluidCount(g, t, c);
-        if (f >= g.thr)
-        {
-            t[c] = kFilled;
-            continue;
-        }
-        // lower neighbours that are EMPTY interior cells may still be filled by the settling passes
-        int maybe = (m > 1 && t[c - 1] == EMPTY) + (i > 1 && t[c - g.sI] == EMPTY);
-        if (g.dim == 3) maybe += j > 1 && t[c - g.sJ] == EMPTY;
-        if (f + maybe >= g.thr)
-        {
-            const int slot = atomicAdd(hdr, 1);
-            if (slot < cap) list[slot] = (int)c;
-        }
+        j = (int)(r / g.sJ);
+        m = (int)(r - (long long)j * g.sJ);
+    }
+    else
+    {
+        j = 0;
+        m = (int)r;
+    }
+}
+
+// Cell c was just filled. A filled cell has at most one neighbour that counts as non-FLUID, so at most one of its
+// upper neighbours can still be EMPTY: if that one now reaches the threshold it is filled too, and the walk goes on
+// from it. Every step fills a cell that was EMPTY, which bounds the walk by the number of interior cells.
+__device__ __forceinline__ void ChaseUp(const RelabelGrid &g, uint8_t *t, long long c)
+{
+    int i, j, m;
+    CellCoords(g, c, i, j, m);
+    for (;;)
+    {
+        const int lastM = g.dim == 3 ? g.Nz - 2 : g.Nx - 2;
+        long long u = -1;
+        if (m < lastM && t[c + 1] == EMPTY) { u = c + 1; m++; }
+        else if (g.dim == 3 && j < g.Nx - 2 && t[c + g.sJ] == EMPTY) { u = c + g.sJ; j++; }
+        else if (i < g.Ny - 2 && t[c + g.sI] == EMPTY) { u = c + g.sI; i++; }
+        if (u < 0 || FluidCount(g, t, u) < g.thr) return;
+        t[u] = kFilled;
+        c = u;
     }
 }
 
@@ -217,6 +251,37 @@ __device__ __forceinline__ long long InteriorCell(const RelabelGrid &g, long lon
     const int i = 1 + (int)(col / g.colsX);
     const int j = g.dim == 3 ? 1 + (int)(col % g.colsX) : 0;
     return (g.dim == 3 ? ((long long)i * g.Nx + j) * g.Nz : (long long)i * g.Nx) + m;
+}
+
+// One thread per interior cell, consecutive threads along the march axis. A cell that reaches the threshold with
+// the labels as this thread reads them is filled (and the chain above it followed); one that could still reach it
+// once its EMPTY lower neighbours are filled goes on the pending list.
+__global__ void __launch_bounds__(kThreads)
+    k_relabel_fill(RelabelGrid g, uint8_t *t, int *hdr, int *list, int cap)
+{
+    const long long n = (long long)g.nCols * g.march;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += nt)
+    {
+        const long long c = InteriorCell(g, q);
+        if (t[c] != EMPTY) continue;
+        const int f = FluidCount(g, t, c);
+        if (f >= g.thr)
+        {
+            t[c] = kFilled;
+            ChaseUp(g, t, c);
+            continue;
+        }
+        int i, j, m;
+        CellCoords(g, c, i, j, m);
+        int maybe = (m > 1 && t[c - 1] == EMPTY) + (i > 1 && t[c - g.sI] == EMPTY);
+        if (g.dim == 3) maybe += j > 1 && t[c - g.sJ] == EMPTY;
+        if (f + maybe >= g.thr)
+        {
+            const int slot = atomicAdd(hdr, 1);
+            if (slot < cap) list[slot] = (int)c;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kSettleThreads)
@@ -237,6 +302,7 @@ __global__ void __launch_bounds__(kSettleThreads)
             if (t[c] == EMPTY && FluidCount(g, t, c) >= g.thr)
             {
                 t[c] = kFilled;
+                ChaseUp(g, t, c);
                 any = true;
             }
         }
@@ -294,19 +360,22 @@ void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double o
     const long long capLL = (long long)(scratchBytes / sizeof(int)) - kHeaderInts;
     const int cap = (int)(capLL < (1ll << 31) - 1 ? capLL : (1ll << 31) - 1);
 
-    const int sms = 148;
+    int dev = 0, sms = 148;
+    NB_CK(cudaGetDevice(&dev));
+    NB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     NB_COUNT_LAUNCH();
     k_relabel_reset<<<Blocks(cells / 16 + 1, kThreads, sms * 8), kThreads, 0, st>>>(cellTypes, cells, hdr, skipped);
     if (count > 0)
     {
         NB_COUNT_LAUNCH();
-        k_relabel_mark<<<Blocks(count, kThreads, sms * 16), kThreads, 0, st>>>(px, py, pz, count, stride, g, ox, oy,
-                                                                              oz, dh, cellTypes, skipped);
+        k_relabel_mark<<<Blocks((count + kMarkBatch - 1) / kMarkBatch, kThreads, sms * 4), kThreads, 0, st>>>(
+            px, py, pz, count, stride, g, ox, oy, oz, dh, cellTypes, skipped);
     }
     if (g.nCols > 0 && g.march > 0)
     {
         NB_COUNT_LAUNCHES(3);
-        k_relabel_fill<<<Blocks(g.nCols, kThreads, 1 << 30), kThreads, 0, st>>>(g, cellTypes, hdr, list, cap);
+        k_relabel_fill<<<Blocks((long long)g.nCols * g.march, kThreads, sms * 8), kThreads, 0, st>>>(g, cellTypes, hdr,
+                                                                                                  list, cap);
         k_relabel_settle<<<1, kSettleThreads, 0, st>>>(g, cellTypes, hdr, list, cap);
         k_relabel_finish<<<Blocks(cells / 16 + 1, kThreads, sms * 8), kThreads, 0, st>>>(cellTypes, cells);
     }
