@@ -17,7 +17,8 @@
 //      (2D) FLUID neighbours becomes FLUID, and a cell filled earlier in the pass counts for the later ones. So a cell
 //      sees its upper neighbours (i+1, j+1, k+1) as they were before the pass and its lower ones (i-1, j-1, k-1) as
 //      the pass left them. The result is the unique solution of that recurrence, which is what is computed here:
-//        k_relabel_fill: one thread per interior cell, consecutive threads along the fast axis. Filled cells get the
+//        k_relabel_fill: one thread per interior cell, consecutive threads along the fast axis, whole columns per
+//          block step. Filled cells get the
 //          marker kFilled, which counts as FLUID for the cells above and not at all for the cells below (they read
 //          the label from before the pass). A filled cell has at most one uncounted neighbour, so at most one of its
 //          upper neighbours can continue a chain of fills: the thread walks up that chain at once. A cell still EMPTY
@@ -129,9 +130,18 @@ __global__ void __launch_bounds__(kThreads) k_relabel_finish(uint8_t *__restrict
 // UpdateFluidCells' index of one coordinate (FLIP3D.cpp:796-802): trunc((x - origin) / dh), at most N - 1; -1 for a
 // quotient at or below -1 or not finite (outside the labels in the reference). A quotient at or above N takes N - 1
 // without a conversion.
-__device__ __forceinline__ int ParticleIndex(double x, double origin, double dh, int N)
+// The quotient is first taken as (x - origin) * inv with inv = 1 / dh rounded, which is within 2^-51 |q| of the
+// correctly rounded quotient q (two roundings of 2^-53 each, plus the one of q). Every decision below compares q with
+// an integer (the truncation, -1, N), so where the product lies farther than that bound (2^-48 |q| here, with margin)
+// from both integers around it, q lies strictly between the same two integers and every decision agrees; otherwise
+// (and for a non-finite product) the exact IEEE division decides.
+__device__ __forceinline__ int ParticleIndex(double x, double origin, double dh, double inv, int N)
 {
-    const double q = (x - origin) / dh;
+    const double d = x - origin;
+    double q = d * inv;
+    const double fl = floor(q);
+    const double tol = fabs(q) * 0x1p-48 + 0x1p-60;
+    if (!(q - fl > tol && fl + 1.0 - q > tol)) q = d / dh;
     if (!(q > -1.0)) return -1;
     if (q >= (double)N) return N - 1;
     return (int)q;
@@ -142,7 +152,7 @@ constexpr int kMarkBatch = 4; // particles in flight per thread
 __global__ void __launch_bounds__(kThreads, 4)
     k_relabel_mark(const double *__restrict__ px, const double *__restrict__ py, const double *__restrict__ pz,
                    long long count, long long stride, RelabelGrid g, double ox, double oy, double oz, double dh,
-                   uint8_t *__restrict__ t, unsigned long long *skipped)
+                   double inv, uint8_t *__restrict__ t, unsigned long long *skipped)
 {
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
@@ -168,9 +178,9 @@ __global__ void __launch_bounds__(kThreads, 4)
 #pragma unroll
         for (int b = 0; b < kMarkBatch; b++)
         {
-            const int i = ParticleIndex(y[b], oy, dh, g.Ny);
-            const int j = ParticleIndex(x[b], ox, dh, g.Nx);
-            const int k = g.dim == 3 ? ParticleIndex(z[b], oz, dh, g.Nz) : 0;
+            const int i = ParticleIndex(y[b], oy, dh, inv, g.Ny);
+            const int j = ParticleIndex(x[b], ox, dh, inv, g.Nx);
+            const int k = g.dim == 3 ? ParticleIndex(z[b], oz, dh, inv, g.Nz) : 0;
             const bool live = p0 + b * nt < count;
             const bool out = (i | j | k) < 0;
             mine += live && out;
@@ -206,15 +216,17 @@ __device__ __forceinline__ int FluidCount(const RelabelGrid &g, const uint8_t *t
     return up + lo;
 }
 
-// Interior coordinates of cell c: (i, j, m) with m the march-axis index (k in 3D, j in 2D; j = 0 in 2D).
+// Coordinates of cell c: (i, j, m) with m the march-axis index (k in 3D, j in 2D; j = 0 in 2D). Cells number
+// below 2^31, so 32-bit arithmetic serves.
 __device__ __forceinline__ void CellCoords(const RelabelGrid &g, long long c, int &i, int &j, int &m)
 {
-    i = (int)(c / g.sI);
-    const long long r = c - (long long)i * g.sI;
+    const unsigned cu = (unsigned)c, sI = (unsigned)g.sI, sJ = (unsigned)g.sJ;
+    i = (int)(cu / sI);
+    const unsigned r = cu - (unsigned)i * sI;
     if (g.dim == 3)
     {
-        j = (int)(r / g.sJ);
-        m = (int)(r - (long long)j * g.sJ);
+        j = (int)(r / sJ);
+        m = (int)(r - (unsigned)j * sJ);
     }
     else
     {
@@ -226,10 +238,8 @@ __device__ __forceinline__ void CellCoords(const RelabelGrid &g, long long c, in
 // Cell c was just filled. A filled cell has at most one neighbour that counts as non-FLUID, so at most one of its
 // upper neighbours can still be EMPTY: if that one now reaches the threshold it is filled too, and the walk goes on
 // from it. Every step fills a cell that was EMPTY, which bounds the walk by the number of interior cells.
-__device__ __forceinline__ void ChaseUp(const RelabelGrid &g, uint8_t *t, long long c)
+__device__ __forceinline__ void ChaseUp(const RelabelGrid &g, uint8_t *t, long long c, int i, int j, int m)
 {
-    int i, j, m;
-    CellCoords(g, c, i, j, m);
     for (;;)
     {
         const int lastM = g.dim == 3 ? g.Nz - 2 : g.Nx - 2;
@@ -246,40 +256,50 @@ __device__ __forceinline__ void ChaseUp(const RelabelGrid &g, uint8_t *t, long l
 // Interior cell number q (0 .. interior cells - 1) in (i, j, k) order.
 __device__ __forceinline__ long long InteriorCell(const RelabelGrid &g, long long q)
 {
-    const long long col = q / g.march;
-    const int m = 1 + (int)(q - col * g.march);
-    const int i = 1 + (int)(col / g.colsX);
-    const int j = g.dim == 3 ? 1 + (int)(col % g.colsX) : 0;
+    const unsigned qu = (unsigned)q, march = (unsigned)g.march;
+    const unsigned col = qu / march;
+    const int m = 1 + (int)(qu - col * march);
+    const int i = 1 + (int)(col / (unsigned)g.colsX);
+    const int j = g.dim == 3 ? 1 + (int)(col % (unsigned)g.colsX) : 0;
     return (g.dim == 3 ? ((long long)i * g.Nx + j) * g.Nz : (long long)i * g.Nx) + m;
 }
 
-// One thread per interior cell, consecutive threads along the march axis. A cell that reaches the threshold with
-// the labels as this thread reads them is filled (and the chain above it followed); one that could still reach it
-// once its EMPTY lower neighbours are filled goes on the pending list.
+// Each block step takes whole columns: `span` threads per column along the march axis (consecutive threads on
+// consecutive cells), kThreads / span columns per step. A cell that reaches the threshold with the labels as this
+// thread reads them is filled (and the chain above it followed); one that could still reach it once its EMPTY lower
+// neighbours are filled goes on the pending list.
 __global__ void __launch_bounds__(kThreads)
     k_relabel_fill(RelabelGrid g, uint8_t *t, int *hdr, int *list, int cap)
 {
-    const long long n = (long long)g.nCols * g.march;
-    const long long nt = (long long)gridDim.x * blockDim.x;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += nt)
+    const int span = g.march < kThreads ? g.march : kThreads;
+    const int cpb = kThreads / span;
+    const int lc = threadIdx.x / span, lm = threadIdx.x - lc * span;
+    if (lc >= cpb) return;
+    for (int col0 = blockIdx.x * cpb; col0 < g.nCols; col0 += gridDim.x * cpb)
     {
-        const long long c = InteriorCell(g, q);
-        if (t[c] != EMPTY) continue;
-        const int f = FluidCount(g, t, c);
-        if (f >= g.thr)
+        const int col = col0 + lc;
+        if (col >= g.nCols) return;
+        const int i = 1 + col / g.colsX;
+        const int j = g.dim == 3 ? 1 + (col - (i - 1) * g.colsX) : 0;
+        const long long base = g.dim == 3 ? ((long long)i * g.Nx + j) * g.Nz : (long long)i * g.Nx;
+        for (int m = 1 + lm; m <= g.march; m += span)
         {
-            t[c] = kFilled;
-            ChaseUp(g, t, c);
-            continue;
-        }
-        int i, j, m;
-        CellCoords(g, c, i, j, m);
-        int maybe = (m > 1 && t[c - 1] == EMPTY) + (i > 1 && t[c - g.sI] == EMPTY);
-        if (g.dim == 3) maybe += j > 1 && t[c - g.sJ] == EMPTY;
-        if (f + maybe >= g.thr)
-        {
-            const int slot = atomicAdd(hdr, 1);
-            if (slot < cap) list[slot] = (int)c;
+            const long long c = base + m;
+            if (t[c] != EMPTY) continue;
+            const int f = FluidCount(g, t, c);
+            if (f >= g.thr)
+            {
+                t[c] = kFilled;
+                ChaseUp(g, t, c, i, g.dim == 3 ? j : 0, m);
+                continue;
+            }
+            int maybe = (m > 1 && t[c - 1] == EMPTY) + (i > 1 && t[c - g.sI] == EMPTY);
+            if (g.dim == 3) maybe += j > 1 && t[c - g.sJ] == EMPTY;
+            if (f + maybe >= g.thr)
+            {
+                const int slot = atomicAdd(hdr, 1);
+                if (slot < cap) list[slot] = (int)c;
+            }
         }
     }
 }
@@ -302,7 +322,9 @@ __global__ void __launch_bounds__(kSettleThreads)
             if (t[c] == EMPTY && FluidCount(g, t, c) >= g.thr)
             {
                 t[c] = kFilled;
-                ChaseUp(g, t, c);
+                int i, j, m;
+                CellCoords(g, c, i, j, m);
+                ChaseUp(g, t, c, i, j, m);
                 any = true;
             }
         }
@@ -369,13 +391,13 @@ void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double o
     {
         NB_COUNT_LAUNCH();
         k_relabel_mark<<<Blocks((count + kMarkBatch - 1) / kMarkBatch, kThreads, sms * 4), kThreads, 0, st>>>(
-            px, py, pz, count, stride, g, ox, oy, oz, dh, cellTypes, skipped);
+            px, py, pz, count, stride, g, ox, oy, oz, dh, 1.0 / dh, cellTypes, skipped);
     }
     if (g.nCols > 0 && g.march > 0)
     {
         NB_COUNT_LAUNCHES(3);
-        k_relabel_fill<<<Blocks((long long)g.nCols * g.march, kThreads, sms * 8), kThreads, 0, st>>>(g, cellTypes, hdr,
-                                                                                                  list, cap);
+        const int span = g.march < kThreads ? g.march : kThreads;
+        k_relabel_fill<<<Blocks(g.nCols, kThreads / span, sms * 8), kThreads, 0, st>>>(g, cellTypes, hdr, list, cap);
         k_relabel_settle<<<1, kSettleThreads, 0, st>>>(g, cellTypes, hdr, list, cap);
         k_relabel_finish<<<Blocks(cells / 16 + 1, kThreads, sms * 8), kThreads, 0, st>>>(cellTypes, cells);
     }
