@@ -232,6 +232,7 @@ class Scene:
     regions: List[Region]
     at_centre: bool = True
     pressure_expr: Optional[str] = None  # the p="..." of pressure-outlet faces with has_p
+    face_params: Optional[dict] = None  # face index -> extra boundary parameters (u="..." v="..." w="...")
 
     def face_arrays(self):
         kind = [BC_NOSLIP] * 6
@@ -249,6 +250,8 @@ class Scene:
             line = "boundary %s %s" % (FACE_NAMES[f], BC_NAMES[k])
             if hp:
                 line += ' p="%s"' % (self.pressure_expr or "0")
+            if self.face_params and f in self.face_params:
+                line += " " + self.face_params[f]
             lines.append(line)
         for r in self.regions:
             kind = {REGION_SOLID: "solid", REGION_FLUID: "fluid", REGION_EMPTY: "empty"}[r.region]
@@ -421,6 +424,27 @@ def flip_tank_3d(n: int = 128, seed: int = 4, a: Optional[float] = None, b: Opti
     sc = walls_scene(3, regions=[air, liquid])
     return Case("flip_tank_3d_%d_a%.4f_b%.4f" % (n, a, b), g, sc, seed, velocity_rule="liquid",
                 fp32_velocity=True, method=1)
+
+
+def bc_channel_3d(n: int = 12, seed: int = 23) -> Case:
+    """Every boundary kind the velocity replay handles, on a unit cube n^3 with a solid sphere at (0.5, 0.5, 0.5)
+    radius 0.2: a space- and time-dependent inlet at x = 0, an outflow (continuity) at x = 1, slip walls at y = 0
+    and y = 1, a wall sliding along x at z = 1 and a no-slip wall at z = 0."""
+    g = uniform_grid(3, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    sphere = Region(REGION_SOLID, PRIM_SPHERE, (0.5, 0.5, 0.5), radius=0.2)
+    faces = [(4, BC_NOSLIP, 0), (2, BC_SLIP, 0), (3, BC_SLIP, 0), (5, BC_MOVING, 0), (0, BC_INLET, 0),
+             (1, BC_OUTFLOW, 0)]
+    params = {0: 'u="1+0.25*sin(3*t)*y" v="0.1*z" w="0"', 5: 'u="0.5+t"'}
+    return Case("bc_channel_3d_%d" % n, g, Scene(faces, [sphere], True, None, params), seed)
+
+
+def bc_outlet_2d(n: int = 20, seed: int = 24) -> Case:
+    """The 2D replay with a prescribed outlet pressure: unit square n^2, a parabolic inlet at x = 0, a pressure
+    outlet p = 0.1 t + y at x = 1, a slip wall at y = 0, a no-slip wall at y = 1."""
+    g = uniform_grid(2, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    faces = [(3, BC_NOSLIP, 0), (2, BC_SLIP, 0), (0, BC_INLET, 0), (1, BC_PRESSURE_OUTLET, 1)]
+    params = {0: 'u="4*y*(1-y)" v="0"'}
+    return Case("bc_outlet_2d_%d" % n, g, Scene(faces, [], True, "0.1*t+y", params), seed)
 
 
 def flip_tank_2d(n: int = 32, seed: int = 10, a: float = 0.55, b: float = 0.45) -> Case:

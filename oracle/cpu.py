@@ -69,6 +69,10 @@ def lib():
         L.or_residual_norm.restype = ctypes.c_double
         L.or_update_fluid_cells.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 4 + [_dp, ctypes.c_longlong, _u8]
         L.or_update_fluid_cells.restype = ctypes.c_longlong
+        _i = ctypes.POINTER(ctypes.c_int32)
+        L.or_bc_velocity.argtypes = ([_dp] * 3 + [_i] * 4 + [_i, _i, _dp, ctypes.c_int] + [_i] * 3 + [ctypes.c_int] +
+                                     [_i, _i, _dp, _dp, ctypes.c_int] + [_i] * 3 + [_dp, _dp, ctypes.c_int])
+        L.or_bc_pressure.argtypes = [_dp, _i, _i, _i, _dp, ctypes.c_int]
     return _LIB
 
 
@@ -132,6 +136,38 @@ def update_fluid_cells(grid, types, xyz, origin, dh=None):
     skipped = lib().or_update_fluid_cells(grid.dim, grid.Nx, grid.Ny, grid.Nz if grid.dim == 3 else 1,
                                           origin[0], origin[1], oz, dh, _p(xyz, _dp), xyz.shape[0], _p(out, _u8))
     return out, int(skipped)
+
+
+def bc_replay(lists, u, v, w, p, with_velocity_function=True):
+    """EnforceVelocityBC + EnforcePressureBC from the reference's lists (``lists``: the arrays of a bc_* fixture, or
+    what refcase.run_bc returned): new copies of u, v, w, p."""
+    L = lib()
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    _i = ctypes.POINTER(ctypes.c_int32)
+    u, v, p = f64(u).copy(), f64(v).copy(), f64(p).copy()
+    two_d = len(w) == 0
+    w = np.zeros(1) if two_d else f64(w).copy()
+    keep = []
+
+    def P(a, t):
+        keep.append(a)
+        return a.ctypes.data_as(t)
+    solid = [i32(lists["solid%d" % c]) for c in range(3)]
+    nsolid = np.array([len(x) for x in solid], dtype=np.int32)
+    pv = f64(lists["presc_value"]) if with_velocity_function else None
+    L.or_bc_velocity(P(u, _dp), P(v, _dp), P(w, _dp), P(solid[0], _i), P(solid[1], _i), P(solid[2], _i),
+                     P(nsolid, _i), P(i32(lists["presc_comp"]), _i), P(i32(lists["presc_index"]), _i),
+                     P(pv, _dp) if pv is not None else None, len(lists["presc_comp"]),
+                     P(i32(lists["copy_comp"]), _i), P(i32(lists["copy_dst"]), _i), P(i32(lists["copy_src"]), _i),
+                     len(lists["copy_comp"]), P(i32(lists["inlet_comp"]), _i), P(i32(lists["inlet_index"]), _i),
+                     P(f64(lists["inlet_area"]), _dp), P(f64(lists["inlet_sign"]), _dp), len(lists["inlet_comp"]),
+                     P(i32(lists["outflow_comp"]), _i), P(i32(lists["outflow_index"]), _i),
+                     P(i32(lists["outflow_outer"]), _i), P(f64(lists["outflow_area"]), _dp),
+                     P(f64(lists["outflow_sign"]), _dp), len(lists["outflow_comp"]))
+    L.or_bc_pressure(P(p, _dp), P(i32(lists["ring_dst"]), _i), P(i32(lists["ring_kind"]), _i),
+                     P(i32(lists["ring_src"]), _i), P(f64(lists["ring_value"]), _dp), len(lists["ring_dst"]))
+    return u, v, (np.zeros(0) if two_d else w), p
 
 
 @dataclass

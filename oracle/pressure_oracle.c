@@ -629,3 +629,51 @@ long long or_update_fluid_cells(int dim, int Nx, int Ny, int Nz, double ox, doub
         }
     return skipped;
 }
+
+/* MAC::EnforceVelocityBC (src/MAC.cpp:833-858) from the lists MAC::BuildBoundaryLists made, in their order:
+ * every solidFaceList[c] entry of field c set to 0; then, when the scene has a boundary velocity function
+ * (presc_value not NULL), each prescribedList entry set to its value; then each copyList entry f[dst] = f[src]; then
+ * ApplyOutflowFlux (:811-831): with qIn = -sum(sign * f[index] * area) over the inlet faces and qOut =
+ * sum(sign * f[index] * area), aOut = sum(area) over the outflow faces, each accumulated in list order,
+ * delta = (qIn - qOut) / aOut and each outflow face f[index] += sign * delta, f[outer] = f[index].
+ * Fields: comp 0 u, 1 v, 2 w. */
+void or_bc_velocity(double *u, double *v, double *w, const int32_t *solid0, const int32_t *solid1,
+                    const int32_t *solid2, const int32_t *nsolid, const int32_t *presc_comp,
+                    const int32_t *presc_index, const double *presc_value, int npresc, const int32_t *copy_comp,
+                    const int32_t *copy_dst, const int32_t *copy_src, int ncopy, const int32_t *in_comp,
+                    const int32_t *in_index, const double *in_area, const double *in_sign, int nin,
+                    const int32_t *out_comp, const int32_t *out_index, const int32_t *out_outer,
+                    const double *out_area, const double *out_sign, int nout)
+{
+    double *f[3] = {u, v, w};
+    const int32_t *solid[3] = {solid0, solid1, solid2};
+    for (int c = 0; c < 3; c++)
+        for (int q = 0; q < nsolid[c]; q++) f[c][solid[c][q]] = 0.0;
+    if (presc_value)
+        for (int q = 0; q < npresc; q++) f[presc_comp[q]][presc_index[q]] = presc_value[q];
+    for (int q = 0; q < ncopy; q++) f[copy_comp[q]][copy_dst[q]] = f[copy_comp[q]][copy_src[q]];
+    if (nout == 0) return;
+    double qIn = 0.0, qOut = 0.0, aOut = 0.0;
+    for (int q = 0; q < nin; q++) qIn -= in_sign[q] * f[in_comp[q]][in_index[q]] * in_area[q];
+    for (int q = 0; q < nout; q++)
+    {
+        qOut += out_sign[q] * f[out_comp[q]][out_index[q]] * out_area[q];
+        aOut += out_area[q];
+    }
+    if (aOut <= 0.0) return;
+    const double delta = (qIn - qOut) / aOut;
+    for (int q = 0; q < nout; q++)
+    {
+        double *g = f[out_comp[q]];
+        g[out_index[q]] += out_sign[q] * delta;
+        g[out_outer[q]] = g[out_index[q]];
+    }
+}
+
+/* MAC::EnforcePressureBC (src/MAC.cpp:860-865) from ringList, in order: kind 0 sets p[dst] = 0, kind 1 the
+ * prescribed value (value[q], PrescribedPressure at the entry's cell), kind 2 copies p[src]. */
+void or_bc_pressure(double *p, const int32_t *dst, const int32_t *kind, const int32_t *src, const double *value,
+                    int n)
+{
+    for (int q = 0; q < n; q++) p[dst[q]] = kind[q] == 0 ? 0.0 : (kind[q] == 1 ? value[q] : p[src[q]]);
+}

@@ -33,6 +33,13 @@
 // p_final[cells] (the pressure after Project).
 // [scheme 4] The case file ends with int64 count and double xyz[3 * count] (x, y, z per particle); the result file
 // with double origin[3] (FacePos(X|Y|Z, 0)) and uint8 types_before[cells] (the labels UpdateFluidCells started from).
+// 5 the boundary-condition replay alone (MAC::EnforceVelocityBC and EnforcePressureBC, src/MAC.cpp:613-871): the
+// case file ends with double p[cells], the pressure the ring is enforced on; the boundary functions are the scene's.
+// The result file is then "NBBC0001", int32 {Nx, Ny, Nz, nsolid[3], npresc, ncopy, nring, ninlet, noutflow}, the
+// lists BuildBoundaryLists made, in their order (solidFaceList[c]; prescribedList as int32 c[], index[] and the
+// double value the boundary function gave each entry at `time`; copyList as int32 c[], dst[], src[]; ringList as
+// int32 dst[], kind[], src[] and double value[] (PrescribedPressure for kind 1, else 0); inletFaces then
+// outflowFaces as int32 c[], index[], outer[], double area[], sign[]), then u, v, (w,) p after the two calls.
 #include <algorithm>
 #include <array>
 #include <cctype>
@@ -200,6 +207,93 @@ static void InitStretched(MAC &g, int dim, const double *dom, const std::vector<
     g.BuildStrides();
 }
 
+// Scheme 5: the reference's own boundary-condition replay on the case's fields, with the lists it built.
+static int BoundaryReplay(MAC &grid, int dim, double time, const std::vector<double> &pIn, const char *out)
+{
+    if (dim == 3) grid.SetBoundaryFunctions(SIMULATION.VelocityBoundaryFunction, SIMULATION.PressureBoundaryFunction);
+    else grid.SetBoundaryFunctions(SIMULATION.VelocityBoundaryFunction2D, SIMULATION.PressureBoundaryFunction2D);
+    for (size_t c = 0; c < pIn.size(); c++) grid.p[c] = pIn[c];
+    grid.EnforceVelocityBC(time);
+    grid.EnforcePressureBC(time);
+
+    FILE *o = std::fopen(out, "wb");
+    if (!o) { std::fprintf(stderr, "cannot write %s\n", out); return 2; }
+    std::fwrite("NBBC0001", 1, 8, o);
+    const int32_t hdr[11] = {grid.Nx, grid.Ny, dim == 3 ? grid.Nz : 1, (int32_t)grid.solidFaceList[0].size(),
+                             (int32_t)grid.solidFaceList[1].size(), (int32_t)grid.solidFaceList[2].size(),
+                             (int32_t)grid.prescribedList.size(), (int32_t)grid.copyList.size(),
+                             (int32_t)grid.ringList.size(), (int32_t)grid.inletFaces.size(),
+                             (int32_t)grid.outflowFaces.size()};
+    WriteN(o, hdr, 11);
+    for (int c = 0; c < 3; c++)
+    {
+        std::vector<int32_t> v(grid.solidFaceList[c].begin(), grid.solidFaceList[c].end());
+        WriteN(o, v.data(), v.size());
+    }
+    {
+        const size_t n = grid.prescribedList.size();
+        std::vector<int32_t> comp(n), index(n);
+        std::vector<double> value(n);
+        for (size_t q = 0; q < n; q++)
+        {
+            const MAC::PrescribedEntry &e = grid.prescribedList[q];
+            comp[q] = (int32_t)e.c;
+            index[q] = e.index;
+            if (dim == 3)
+            {
+                const Vec3 vel = grid.boundaryVelocity3D(e.x, e.y, e.z, time);
+                value[q] = e.c == MAC::U ? vel.u : (e.c == MAC::V ? vel.v : vel.w);
+            }
+            else
+            {
+                const Vec2 vel = grid.boundaryVelocity2D(e.x, e.y, time);
+                value[q] = e.c == MAC::U ? vel.u : vel.v;
+            }
+        }
+        WriteN(o, comp.data(), n); WriteN(o, index.data(), n); WriteN(o, value.data(), n);
+    }
+    {
+        const size_t n = grid.copyList.size();
+        std::vector<int32_t> comp(n), dst(n), src(n);
+        for (size_t q = 0; q < n; q++)
+        {
+            comp[q] = (int32_t)grid.copyList[q].c; dst[q] = grid.copyList[q].dst; src[q] = grid.copyList[q].src;
+        }
+        WriteN(o, comp.data(), n); WriteN(o, dst.data(), n); WriteN(o, src.data(), n);
+    }
+    {
+        const size_t n = grid.ringList.size();
+        std::vector<int32_t> dst(n), kind(n), src(n);
+        std::vector<double> value(n, 0.0);
+        for (size_t q = 0; q < n; q++)
+        {
+            const MAC::RingEntry &e = grid.ringList[q];
+            dst[q] = e.dst; kind[q] = e.kind; src[q] = e.src;
+            if (e.kind == 1) value[q] = grid.PrescribedPressure(e.i, e.j, e.k, time);
+        }
+        WriteN(o, dst.data(), n); WriteN(o, kind.data(), n); WriteN(o, src.data(), n); WriteN(o, value.data(), n);
+    }
+    for (const std::vector<MAC::FluxFace> *faces : {&grid.inletFaces, &grid.outflowFaces})
+    {
+        const size_t n = faces->size();
+        std::vector<int32_t> comp(n), index(n), outer(n);
+        std::vector<double> area(n), sign(n);
+        for (size_t q = 0; q < n; q++)
+        {
+            const MAC::FluxFace &e = (*faces)[q];
+            comp[q] = (int32_t)e.c; index[q] = e.index; outer[q] = e.outer; area[q] = e.area; sign[q] = e.sign;
+        }
+        WriteN(o, comp.data(), n); WriteN(o, index.data(), n); WriteN(o, outer.data(), n);
+        WriteN(o, area.data(), n); WriteN(o, sign.data(), n);
+    }
+    WriteN(o, grid.u.data(), grid.u.size());
+    WriteN(o, grid.v.data(), grid.v.size());
+    if (dim == 3) WriteN(o, grid.w.data(), grid.w.size());
+    WriteN(o, grid.p.data(), grid.p.size());
+    std::fclose(o);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
     if (argc != 3) { std::fprintf(stderr, "usage: ref_harness case.bin result.bin\n"); return 2; }
@@ -299,6 +393,12 @@ int main(int argc, char **argv)
         ReadN(f, gridAnt.p.data(), gridAnt.p.size());
         ant = &gridAnt;
     }
+    std::vector<double> pBC;
+    if (scheme == 5)
+    {
+        pBC.resize(grid.p.size());
+        ReadN(f, pBC.data(), pBC.size());
+    }
     std::vector<uint8_t> typesBefore;
     double origin[3] = {0.0, 0.0, 0.0};
     if (scheme == 4)
@@ -325,6 +425,7 @@ int main(int argc, char **argv)
         else FLIP2D::UpdateFluidCells(&grid, &particles);
     }
     std::fclose(f);
+    if (scheme == 5) return BoundaryReplay(grid, dim, time, pBC, argv[2]);
 
     // The pressure ring as the step sees it (SolveScheme's first call, PressureSolver3D.cpp:281).
     grid.EnforcePressureBC(time);

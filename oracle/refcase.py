@@ -68,6 +68,7 @@ class RefResult:
 
 
 SCHEME_CHORIN, SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM, SCHEME_EXPLICIT, SCHEME_FLIP_RELABEL = 0, 1, 2, 3, 4
+SCHEME_BC_REPLAY = 5
 _PREV_SCHEMES = (SCHEME_INCREMENTAL, SCHEME_CHORIN_WARM)  # the schemes that read and write a previous step
 
 
@@ -97,7 +98,7 @@ def write_case(path, case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, 
         f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
         if g.dim == 3:
             f.write(np.ascontiguousarray(w, dtype="<f8").tobytes())
-        if scheme in _PREV_SCHEMES:
+        if scheme in _PREV_SCHEMES or scheme == SCHEME_BC_REPLAY:
             f.write(np.ascontiguousarray(p_prev, dtype="<f8").reshape(-1).tobytes())
         if scheme == SCHEME_FLIP_RELABEL:
             xyz = np.ascontiguousarray(particles, dtype="<f8").reshape(-1, 3)
@@ -173,3 +174,49 @@ def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max
         if r.returncode != 0:
             raise RuntimeError("ref_harness failed (%d): %s %s" % (r.returncode, r.stdout[-2000:], r.stderr[-2000:]))
         return read_result(rp, case.grid.dim, scheme)
+
+
+def read_bc_result(path, dim) -> dict:
+    """The lists and fields of a boundary-replay run (scheme 5), as named arrays."""
+    with open(path, "rb") as f:
+        data = f.read()
+    assert data[:8] == b"NBBC0001", "bad result file"
+    off = 8
+    Nx, Ny, Nz, s0, s1, s2, npresc, ncopy, nring, nin, nout = struct.unpack_from("<11i", data, off)
+    off += 44
+
+    def take(dtype, count):
+        nonlocal off
+        a = np.frombuffer(data, dtype=dtype, count=count, offset=off).copy()
+        off += a.nbytes
+        return a
+
+    r = {"Nx": Nx, "Ny": Ny, "Nz": Nz}
+    for c, n in enumerate((s0, s1, s2)):
+        r["solid%d" % c] = take("<i4", n)
+    r["presc_comp"], r["presc_index"], r["presc_value"] = take("<i4", npresc), take("<i4", npresc), take("<f8", npresc)
+    r["copy_comp"], r["copy_dst"], r["copy_src"] = take("<i4", ncopy), take("<i4", ncopy), take("<i4", ncopy)
+    r["ring_dst"], r["ring_kind"], r["ring_src"], r["ring_value"] = (take("<i4", nring), take("<i4", nring),
+                                                                     take("<i4", nring), take("<f8", nring))
+    for name, n in (("inlet", nin), ("outflow", nout)):
+        r[name + "_comp"], r[name + "_index"], r[name + "_outer"] = take("<i4", n), take("<i4", n), take("<i4", n)
+        r[name + "_area"], r[name + "_sign"] = take("<f8", n), take("<f8", n)
+    r["u"] = take("<f8", (Nx + 1) * Ny * Nz)
+    r["v"] = take("<f8", Nx * (Ny + 1) * Nz)
+    r["w"] = take("<f8", Nx * Ny * (Nz + 1)) if dim == 3 else np.zeros(0)
+    r["p"] = take("<f8", Nx * Ny * Nz)
+    assert off == len(data), "trailing bytes in the result"
+    return r
+
+
+def run_bc(case, u, v, w, p, time=0.0, timeout=600) -> dict:
+    """The reference's EnforceVelocityBC + EnforcePressureBC on the given fields (labels from the scene text)."""
+    if not available():
+        raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+    with tempfile.TemporaryDirectory() as td:
+        cp, rp = os.path.join(td, "case.bin"), os.path.join(td, "res.bin")
+        write_case(cp, case, u, v, w, scheme=SCHEME_BC_REPLAY, p_prev=p, time=time)
+        r = subprocess.run([HARNESS, cp, rp], capture_output=True, text=True, timeout=timeout, cwd=td)
+        if r.returncode != 0:
+            raise RuntimeError("ref_harness failed (%d): %s %s" % (r.returncode, r.stdout[-2000:], r.stderr[-2000:]))
+        return read_bc_result(rp, case.grid.dim)

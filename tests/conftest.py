@@ -20,12 +20,13 @@ def pytest_configure(config):
 SCHEME_PREFIXES = ("incremental_", "warm_")
 EXPLICIT_PREFIX = "explicit_"
 FLIP_PREFIX = "flip_relabel_"
+BC_PREFIX = "bc_"
 
 
 def golden_names():
     """The Chorin fixtures (one solve from zero)."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
-    return [n for n in names if not n.startswith(SCHEME_PREFIXES + (EXPLICIT_PREFIX, FLIP_PREFIX))]
+    return [n for n in names if not n.startswith(SCHEME_PREFIXES + (EXPLICIT_PREFIX, FLIP_PREFIX, BC_PREFIX))]
 
 
 def explicit_golden_names():
@@ -38,6 +39,12 @@ def flip_golden_names():
     """The fixtures of FLIP's re-labelling from particles followed by the Chorin step."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
     return [n for n in names if n.startswith(FLIP_PREFIX)]
+
+
+def bc_golden_names():
+    """The fixtures of the boundary-condition replay (EnforceVelocityBC + EnforcePressureBC)."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    return [n for n in names if n.startswith(BC_PREFIX)]
 
 
 def scheme_golden_names():

@@ -2,7 +2,7 @@
 
 Run in a checkout that has the reference sources (it builds oracle/_ref/ref_harness from them first):
 
-    python tests/golden/make_golden.py [REF_ROOT] [--only explicit|flip]
+    python tests/golden/make_golden.py [REF_ROOT] [--only explicit|flip|bc]
 
 Each fixture is one small case: the inputs both sides read (face velocities, the prescribed ring pressure) and what
 the reference computed from them (cell types, IDP, the CSR matrix, b before and after the compatibility step, the
@@ -60,6 +60,17 @@ EXPLICIT_CASES = [
 FLIP_CASES = [
     ("flip_relabel_tank_3d_16", "flip_tank_3d", {"n": 16, "seed": 41}, 57, 4),
     ("flip_relabel_tank_2d_24", "flip_tank_2d", {"n": 24, "seed": 32}, 56, 4),
+]
+
+
+# the boundary-condition replay (EnforceVelocityBC + EnforcePressureBC) on seeded N(0,1) fields: (fixture name,
+# builder, kwargs, time)
+BC_CASES = [
+    ("bc_channel_3d_12", "bc_channel_3d", {"n": 12, "seed": 23}, 0.3),
+    ("bc_outlet_2d_20", "bc_outlet_2d", {"n": 20, "seed": 24}, 0.7),
+    ("bc_inflow_outflow_3d_8", "inflow_outflow_3d", {"n": 8, "seed": 25}, 0.1),
+    ("bc_pressure_outlet_3d_12", "pressure_outlet_3d", {"n": 12, "seed": 26}, 0.45),
+    ("bc_sphere_outlet_3d_10", "sphere_outlet_3d", {"n": 10, "seed": 27}, 0.0),
 ]
 
 
@@ -152,6 +163,27 @@ def write_flip_case(name, builder, kwargs, particle_seed, ppc):
         name, xyz.shape[0], changed, ref.n, ref.rel_res, os.path.getsize(out) // 1024))
 
 
+def write_bc_case(name, builder, kwargs, time):
+    """The reference's EnforceVelocityBC and EnforcePressureBC on seeded fields: its lists (with the values its
+    boundary functions gave at `time`) and the fields before and after."""
+    case = build_case(builder, kwargs)
+    g = case.grid
+    seed = kwargs["seed"]
+    u = W.normals(W.stream_seed(seed, 10), int(np.prod(g.u_shape())))
+    v = W.normals(W.stream_seed(seed, 11), int(np.prod(g.v_shape())))
+    w = W.normals(W.stream_seed(seed, 12), int(np.prod(g.w_shape()))) if g.dim == 3 else np.zeros(0)
+    p = W.normals(W.stream_seed(seed, 13), g.cells)
+    r = refcase.run_bc(case, u, v, w, p, time)
+    meta = dict(name=name, builder=builder, kwargs=kwargs, time=time)
+    arrays = {k: val for k, val in r.items() if isinstance(val, np.ndarray) and k not in ("u", "v", "w", "p")}
+    out = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(out, meta=np.array(json.dumps(meta)), u_in=u, v_in=v, w_in=w, p_in=p, u_out=r["u"],
+                        v_out=r["v"], w_out=r["w"], p_out=r["p"], **arrays)
+    print("%-36s presc=%-5d copies=%-5d ring=%-5d outflow=%-4d  %d KB" % (
+        name, len(r["presc_comp"]), len(r["copy_comp"]), len(r["ring_dst"]), len(r["outflow_comp"]),
+        os.path.getsize(out) // 1024))
+
+
 def main(ref_root: str = "/root/reference", only: str = "") -> None:
     if not refcase.build(ref_root):
         raise SystemExit("the reference harness could not be built from %s" % ref_root)
@@ -162,6 +194,10 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
     if only == "flip":
         for args in FLIP_CASES:
             write_flip_case(*args)
+        return
+    if only == "bc":
+        for args in BC_CASES:
+            write_bc_case(*args)
         return
     for name, builder, kwargs, tol in CASES:
         case = build_case(builder, kwargs)
@@ -191,6 +227,8 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
         write_explicit_case(*args)
     for args in FLIP_CASES:
         write_flip_case(*args)
+    for args in BC_CASES:
+        write_bc_case(*args)
 
 
 if __name__ == "__main__":
