@@ -243,6 +243,49 @@ int nereus_b200_update_fluid_cells_device(int device, int dim, int Nx, int Ny, i
                                           int64_t count, int64_t stride, uint8_t *cellTypes, void *scratch,
                                           size_t scratch_bytes, int64_t *skipped, void *stream);
 
+/* ---- boundary-condition replay on device fields: MAC::EnforceVelocityBC and MAC::EnforcePressureBC
+ *      (src/MAC.cpp:811-865) from the lists MAC::BuildBoundaryLists makes on the host (src/MAC.cpp:613-1090), so that
+ *      a stepping loop keeps u, v, w and p on the device between its sub-steps. The fields come out bit for bit as the
+ *      reference's replay leaves them, ApplyOutflowFlux included. ----
+ * The lists are the MAC's own, entry by entry in its order (MAC.h:450-458): solidFaceList[c]; prescribedList's
+ * component and field index; copyList; ringList (kind 0 zero, 1 prescribed, 2 copy); inletFaces and outflowFaces.
+ * Field indices are MAC::FieldIndex's. Components: 0 u, 1 v, 2 w. nereus_b200_bc_create copies and checks them (every
+ * index inside its field, else NB_BAD_INPUT) and allocates its device memory; the enforce calls allocate nothing
+ * and wait for nothing, so they may be captured in a CUDA graph. */
+typedef struct nb_bc_lists
+{
+    int dim, Nx, Ny, Nz;                 /* ring included; Nz unread in 2D */
+    const int32_t *solid[3];             /* solidFaceList[c] */
+    int32_t nsolid[3];
+    const int32_t *presc_comp, *presc_index; /* prescribedList */
+    int32_t npresc;
+    const int32_t *copy_comp, *copy_dst, *copy_src; /* copyList */
+    int32_t ncopy;
+    const int32_t *ring_dst, *ring_kind, *ring_src; /* ringList */
+    int32_t nring;
+    const int32_t *inlet_comp, *inlet_index; /* inletFaces */
+    const double *inlet_area, *inlet_sign;
+    int32_t ninlet;
+    const int32_t *outflow_comp, *outflow_index, *outflow_outer; /* outflowFaces */
+    const double *outflow_area, *outflow_sign;
+    int32_t noutflow;
+} nb_bc_lists;
+typedef struct nb_bc nb_bc;
+int nereus_b200_bc_create(int device, const nb_bc_lists *lists, nb_bc **out);
+/* EnforceVelocityBC on device fields u, v, w (w unread in 2D), queued on `stream` (a cudaStream_t; NULL = the default
+ * stream). presc_values: a device array of npresc doubles, entry q the boundary velocity function's component at
+ * prescribedList[q]'s point and time (the caller evaluates the scene's expressions, as the reference does); NULL when
+ * the scene has no boundary velocity function, which leaves the prescribed entries unwritten as the reference does. */
+int nereus_b200_bc_enforce_velocity(nb_bc *bc, double *u, double *v, double *w, const double *presc_values,
+                                    void *stream);
+/* EnforcePressureBC on device field p. ring_values: a device array of nring doubles, read at kind-1 entries
+ * (PrescribedPressure at the entry's cell and time); NULL writes 0 there, as PrescribedPressure does without a
+ * pressure function. */
+int nereus_b200_bc_enforce_pressure(nb_bc *bc, double *p, const double *ring_values, void *stream);
+/* The number of dependency levels (launches) of each replay. */
+int nereus_b200_bc_levels(const nb_bc *bc, int *velocity_levels, int *pressure_levels);
+void nereus_b200_bc_destroy(nb_bc *bc);
+
 /* ---- batched and served solves. The reference has one solve per call from the manager thread
  *      (SimulationManager.h:345-353 -> PressureSolver3D::SolvePressure + Project); a server runs many independent
  *      pressure steps (tanks of a batch, requests of a stream) concurrently on one or more devices. Each device

@@ -2,7 +2,7 @@
 
     python -m nereus_cfd_b200.build [--verbose]
 
-nb_exact.cu and nb_relabel.cu are compiled with -fmad=false (their results must round like the reference's host
+nb_exact.cu, nb_relabel.cu and nb_bc.cu are compiled with -fmad=false (their results must round like the reference's host
 code); the solver kernels keep fused multiply-adds. The object files go to nereus_cfd_b200/_build/.
 """
 from __future__ import annotations
@@ -31,6 +31,7 @@ SOURCES = {
     "nb_capi.cu": [],
     "nb_noalloc.cu": [],
     "nb_relabel.cu": ["-fmad=false"],
+    "nb_bc.cu": ["-fmad=false"],
     "nb_server.cu": [],
 }
 HEADERS = ["nb_device.cuh", "nb_kernels.h", "nb_solver.h", "nb_guard.h"]

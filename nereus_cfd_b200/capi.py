@@ -82,6 +82,23 @@ class SceneStruct(ctypes.Structure):
 
 
 # Every exported symbol of include/nereus_b200.h with its ctypes signature.
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+class BcLists(ctypes.Structure):
+    """nb_bc_lists (include/nereus_b200.h): the MAC's boundary lists for nereus_b200_bc_create."""
+
+    _fields_ = [("dim", ctypes.c_int), ("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+                ("solid", _i32p * 3), ("nsolid", ctypes.c_int32 * 3),
+                ("presc_comp", _i32p), ("presc_index", _i32p), ("npresc", ctypes.c_int32),
+                ("copy_comp", _i32p), ("copy_dst", _i32p), ("copy_src", _i32p), ("ncopy", ctypes.c_int32),
+                ("ring_dst", _i32p), ("ring_kind", _i32p), ("ring_src", _i32p), ("nring", ctypes.c_int32),
+                ("inlet_comp", _i32p), ("inlet_index", _i32p), ("inlet_area", _dp), ("inlet_sign", _dp),
+                ("ninlet", ctypes.c_int32),
+                ("outflow_comp", _i32p), ("outflow_index", _i32p), ("outflow_outer", _i32p), ("outflow_area", _dp),
+                ("outflow_sign", _dp), ("noutflow", ctypes.c_int32)]
+
+
 SIGNATURES = {
     "nereus_b200_default_options": (None, [ctypes.POINTER(Options)]),
     "nereus_b200_last_error": (ctypes.c_char_p, []),
@@ -143,6 +160,12 @@ SIGNATURES = {
                                        [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_int64, _u8,
                                                                 ctypes.POINTER(ctypes.c_int64)]),
     "nereus_b200_update_fluid_cells_scratch_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
+    "nereus_b200_bc_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(BcLists), ctypes.POINTER(ctypes.c_void_p)]),
+    "nereus_b200_bc_enforce_velocity": (ctypes.c_int, [ctypes.c_void_p] * 6),
+    "nereus_b200_bc_enforce_pressure": (ctypes.c_int, [ctypes.c_void_p] * 4),
+    "nereus_b200_bc_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int)]),
+    "nereus_b200_bc_destroy": (None, [ctypes.c_void_p]),
     "nereus_b200_update_fluid_cells_device": (ctypes.c_int, [ctypes.c_int] * 5 + [ctypes.c_double] * 4 +
                                               [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_int64] +
                                               [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,

@@ -285,6 +285,92 @@ int nereus_b200_number_unknowns_noalloc(int device, int dim, int Nx, int Ny, int
     });
 }
 
+} // extern "C"
+
+struct nb_bc
+{
+    nb::BcReplay *r = nullptr;
+    ~nb_bc() { nb::DestroyBcReplay(r); }
+};
+
+namespace
+{
+// Runs f with `device` current, restoring the caller's device afterwards.
+template <typename F> void OnDevice(int device, F &&f)
+{
+    int prev = 0;
+    NB_CK(cudaGetDevice(&prev));
+    NB_CK(cudaSetDevice(device));
+    try
+    {
+        f();
+    }
+    catch (...)
+    {
+        cudaSetDevice(prev);
+        throw;
+    }
+    NB_CK(cudaSetDevice(prev));
+}
+} // namespace
+
+extern "C" {
+
+int nereus_b200_bc_create(int device, const nb_bc_lists *lists, nb_bc **out)
+{
+    if (!lists || !out) return Fail(NB_BAD_INPUT, "null argument");
+    *out = nullptr;
+    return Guard([&] {
+        nb::CheckBcLists(*lists); // bad lists fail here, before any device
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return Fail(NB_NO_DEVICE, "no CUDA device");
+        if (device < 0 || device >= ndev) throw nb::InputError("no such device");
+        std::unique_ptr<nb_bc> b(new nb_bc);
+        OnDevice(device, [&] { b->r = nb::CreateBcReplay(device, *lists); });
+        *out = b.release();
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_bc_enforce_velocity(nb_bc *bc, double *u, double *v, double *w, const double *presc_values,
+                                    void *stream)
+{
+    if (!bc || !bc->r) return Fail(NB_BAD_INPUT, "null argument");
+    return Guard([&] {
+        OnDevice(nb::BcDevice(*bc->r), [&] {
+            nb::EnforceVelocityDevice(*bc->r, u, v, w, presc_values, (cudaStream_t)stream);
+        });
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_bc_enforce_pressure(nb_bc *bc, double *p, const double *ring_values, void *stream)
+{
+    if (!bc || !bc->r) return Fail(NB_BAD_INPUT, "null argument");
+    return Guard([&] {
+        OnDevice(nb::BcDevice(*bc->r), [&] { nb::EnforcePressureDevice(*bc->r, p, ring_values, (cudaStream_t)stream); });
+        return (int)NB_OK;
+    });
+}
+
+int nereus_b200_bc_levels(const nb_bc *bc, int *velocity_levels, int *pressure_levels)
+{
+    if (!bc || !bc->r) return Fail(NB_BAD_INPUT, "null argument");
+    if (velocity_levels) *velocity_levels = nb::BcLevels(*bc->r, 0);
+    if (pressure_levels) *pressure_levels = nb::BcLevels(*bc->r, 1);
+    return NB_OK;
+}
+
+void nereus_b200_bc_destroy(nb_bc *bc)
+{
+    if (!bc) return;
+    int prev = 0;
+    const bool ok = cudaGetDevice(&prev) == cudaSuccess;
+    if (bc->r) cudaSetDevice(nb::BcDevice(*bc->r));
+    delete bc;
+    if (ok) cudaSetDevice(prev);
+}
+
 size_t nereus_b200_update_fluid_cells_scratch_bytes(int dim, int Nx, int Ny, int Nz)
 {
     return nb::RelabelScratchBytes(dim, Nx, Ny, Nz);

@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -290,5 +291,17 @@ void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double o
                             const double *px, const double *py, const double *pz, long long count, long long stride,
                             uint8_t *cellTypes, void *scratch, size_t scratchBytes, unsigned long long *skipped,
                             cudaStream_t st);
+
+// Boundary-condition replay (nb_bc.cu): the reference's lists as leveled device write programs.
+struct BcReplay;
+// Checks the lists on the host (every index inside its field); throws InputError on a bad list.
+void CheckBcLists(const nb_bc_lists &lists);
+// The checked, levelled lists on the current device.
+BcReplay *CreateBcReplay(int device, const nb_bc_lists &lists);
+void DestroyBcReplay(BcReplay *b);
+int BcLevels(const BcReplay &b, int pressure);
+int BcDevice(const BcReplay &b);
+void EnforceVelocityDevice(BcReplay &b, double *u, double *v, double *w, const double *prescValues, cudaStream_t st);
+void EnforcePressureDevice(BcReplay &b, double *p, const double *ringValues, cudaStream_t st);
 
 } // namespace nb
