@@ -1,8 +1,9 @@
 /*
  * ORACLE / TEST INFRASTRUCTURE ONLY.
  *
- * A plain-C restatement of the NEREUS pressure projection (RaphaelLaroca/NEREUS_CFD), used by tests/ and by
- * bench.py's CPU-baseline leg as the checker. The product library never links, loads or calls this file.
+ * A plain-C restatement of the NEREUS pressure projection (RaphaelLaroca/NEREUS_CFD): tests/ check the B200 path's
+ * results against it, and bench.py's CPU-baseline leg times it. The product library never links, loads or calls this
+ * file.
  *
  * Parity pin: tests/test_oracle_golden.py checks every function here against the reference's own outputs
  * (the .npz fixtures under tests/golden, written by tests/golden/make_golden.py from oracle/_ref/ref_harness, which is compiled from
