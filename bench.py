@@ -290,7 +290,12 @@ def run_b200(args, rank, world, dist):
     stretched = run_stretched(args, dev) if args.stretched_steps > 0 and world == 1 else None
     tanks = run_tanks(args, rank, world, dist, dev) if args.tanks > 0 else None
     trace = run_trace(args, dev) if args.trace > 0 and world == 1 else None
-    relabel = run_relabel(args, dev) if args.relabel_steps > 0 and world == 1 else None
+    relabel = None
+    if args.relabel_steps > 0 and world == 1:
+        try:
+            relabel = run_relabel(args, dev)
+        except Exception as e:  # a side measurement: reported, never fatal to the headline line
+            relabel = {"unavailable": "%s: %s" % (type(e).__name__, str(e)[:300])}
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
