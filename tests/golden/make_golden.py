@@ -53,6 +53,11 @@ EXPLICIT_CASES = [
     ("explicit_cavity_outlet_2d_32", "cavity_outlet_2d", {"n": 32, "seed": 21}, 1e-13),
     ("explicit_closed_box_2d_16", "closed_box_2d", {"n": 16, "seed": 22}, 1e-13),
 ]
+# a scene outside the equivalence: air (EMPTY) cells inside the grid, toward which EXPLICIT's coefficient is 2 and the
+# shared system's ring factor 1
+EXPLICIT_LIMIT_CASES = [
+    ("limit_explicit_tank_2d_24", "flip_tank_2d", {"n": 24, "seed": 28}, 1e-13),
+]
 
 
 # FLIP's re-labelling from particles, then the Chorin step on the new labels: (fixture name, builder, kwargs,
@@ -188,7 +193,7 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
     if not refcase.build(ref_root):
         raise SystemExit("the reference harness could not be built from %s" % ref_root)
     if only == "explicit":
-        for args in EXPLICIT_CASES:
+        for args in EXPLICIT_CASES + EXPLICIT_LIMIT_CASES:
             write_explicit_case(*args)
         return
     if only == "flip":
@@ -223,7 +228,7 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
             name, ref.n, ref.iters, ref.rel_res, ref.max_div, os.path.getsize(out) // 1024))
     for args in SCHEME_CASES:
         write_scheme_case(*args)
-    for args in EXPLICIT_CASES:
+    for args in EXPLICIT_CASES + EXPLICIT_LIMIT_CASES:
         write_explicit_case(*args)
     for args in FLIP_CASES:
         write_flip_case(*args)

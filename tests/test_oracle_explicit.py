@@ -44,3 +44,17 @@ def test_oracle_chorin_step_reproduces_explicit(name):
     scale = max(np.abs(z["u"]).max(), np.abs(z["v"]).max())
     assert np.abs(o.u - z["u_out"]).max() <= 1e-9 * scale
     assert np.abs(o.v - z["v_out"]).max() <= 1e-9 * scale
+
+
+def test_interior_air_is_outside_the_equivalence():
+    """With EMPTY cells inside the grid (a free surface), EXPLICIT's coefficient toward them is 2 and the shared
+    system's ring factor 1 (interior Dirichlet cells are not ring cells): the two pressures differ, so the routing
+    holds only where every EMPTY and PRESSURE cell lies on the ring (tests/golden/limit_explicit_tank_2d_24.npz)."""
+    case, meta, z = load_golden("limit_explicit_tank_2d_24")
+    g = case.grid
+    t = z["types"].reshape(g.Ny, g.Nx)
+    assert (t[1:-1, 1:-1] == 2).any()  # EMPTY inside
+    assert meta["rel_res"] > 1e-2  # EXPLICIT's pressure does not solve the shared system
+    o = cpu.solve_projection(g, z["types"], z["u"], z["v"], z["w"], z["p_in"], meta["rho"], meta["dt"],
+                             meta["needs_compat"], 1e-13)
+    assert np.linalg.norm(o.x - z["x"]) / np.linalg.norm(z["x"]) > 1e-2
