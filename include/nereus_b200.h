@@ -284,6 +284,11 @@ int nereus_b200_bc_enforce_velocity(nb_bc *bc, double *u, double *v, double *w, 
 int nereus_b200_bc_enforce_pressure(nb_bc *bc, double *p, const double *ring_values, void *stream);
 /* The number of dependency levels (launches) of each replay. */
 int nereus_b200_bc_levels(const nb_bc *bc, int *velocity_levels, int *pressure_levels);
+/* Host only, no device: the level each list entry is replayed in, as nereus_b200_bc_create would plan it.
+ * velocity_level gets nsolid[0] + nsolid[1] + nsolid[2] + npresc + ncopy entries in that order (the reference's replay
+ * order), pressure_level nring; either may be NULL. The counts of levels go to *velocity_levels, *pressure_levels. */
+int nereus_b200_bc_plan(const nb_bc_lists *lists, int32_t *velocity_level, int32_t *pressure_level,
+                        int *velocity_levels, int *pressure_levels);
 void nereus_b200_bc_destroy(nb_bc *bc);
 
 /* ---- batched and served solves. The reference has one solve per call from the manager thread

@@ -166,6 +166,8 @@ SIGNATURES = {
     "nereus_b200_bc_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int)]),
     "nereus_b200_bc_destroy": (None, [ctypes.c_void_p]),
+    "nereus_b200_bc_plan": (ctypes.c_int, [ctypes.POINTER(BcLists), ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "nereus_b200_update_fluid_cells_device": (ctypes.c_int, [ctypes.c_int] * 5 + [ctypes.c_double] * 4 +
                                               [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_int64] +
                                               [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,

@@ -97,14 +97,15 @@ __global__ void __launch_bounds__(kFluxThreads) k_bc_outflow(FluxFaces ff, doubl
     }
 }
 
-// Levels of a sequential write program (see the top of this file); returns the operations sorted by level (stable)
-// and the start of each level.
-void LevelProgram(const std::vector<BcOp> &seq, std::vector<BcOp> &sorted, std::vector<int> &start)
+// Levels of a sequential write program (see the top of this file); returns the operations sorted by level (stable),
+// the start of each level and each operation's level in program order.
+void LevelProgram(const std::vector<BcOp> &seq, std::vector<BcOp> &sorted, std::vector<int> &start,
+                  std::vector<int> &level)
 {
     std::unordered_map<long long, int> lastWrite, lastRead;
     lastWrite.reserve(seq.size() * 2);
     lastRead.reserve(seq.size());
-    std::vector<int> level(seq.size());
+    level.assign(seq.size(), 0);
     int nlev = 0;
     auto key = [](int c, int i) { return ((long long)c << 32) | (unsigned)i; };
     for (size_t q = 0; q < seq.size(); q++)
@@ -156,6 +157,7 @@ struct BcHost
     int dim = 3, npresc = 0, nring = 0, nin = 0, nout = 0;
     std::vector<BcOp> vel, pres;
     std::vector<int> velStart, presStart;
+    std::vector<int> velLevel, presLevel; // each operation's level, in list order
     std::vector<int32_t> fluxI;
     std::vector<double> fluxD;
     double aOut = 0.0;
@@ -259,8 +261,8 @@ static BcHost BuildBcHost(const nb_bc_lists &L)
     h.dim = L.dim;
     h.npresc = L.npresc;
     h.nring = L.nring;
-    LevelProgram(seq, h.vel, h.velStart);
-    LevelProgram(pseq, h.pres, h.presStart);
+    LevelProgram(seq, h.vel, h.velStart, h.velLevel);
+    LevelProgram(pseq, h.pres, h.presStart, h.presLevel);
     h.fluxI.swap(fi);
     h.fluxD.swap(fd);
     h.nin = nin;
@@ -299,6 +301,13 @@ static BcReplay *CreateBcReplay(int device, const BcHost &h)
 }
 
 void CheckBcLists(const nb_bc_lists &lists) { (void)BuildBcHost(lists); }
+
+void PlanBcLevels(const nb_bc_lists &lists, std::vector<int> &velocity, std::vector<int> &pressure)
+{
+    BcHost h = BuildBcHost(lists);
+    velocity.swap(h.velLevel);
+    pressure.swap(h.presLevel);
+}
 
 BcReplay *CreateBcReplay(int device, const nb_bc_lists &lists) { return CreateBcReplay(device, BuildBcHost(lists)); }
 

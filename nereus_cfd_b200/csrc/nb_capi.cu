@@ -353,6 +353,30 @@ int nereus_b200_bc_enforce_pressure(nb_bc *bc, double *p, const double *ring_val
     });
 }
 
+int nereus_b200_bc_plan(const nb_bc_lists *lists, int32_t *velocity_level, int32_t *pressure_level,
+                        int *velocity_levels, int *pressure_levels)
+{
+    if (!lists) return Fail(NB_BAD_INPUT, "null argument");
+    return Guard([&] {
+        std::vector<int> vel, pres;
+        nb::PlanBcLevels(*lists, vel, pres);
+        int nv = 0, np = 0;
+        for (size_t q = 0; q < vel.size(); q++)
+        {
+            if (velocity_level) velocity_level[q] = vel[q];
+            if (vel[q] + 1 > nv) nv = vel[q] + 1;
+        }
+        for (size_t q = 0; q < pres.size(); q++)
+        {
+            if (pressure_level) pressure_level[q] = pres[q];
+            if (pres[q] + 1 > np) np = pres[q] + 1;
+        }
+        if (velocity_levels) *velocity_levels = nv;
+        if (pressure_levels) *pressure_levels = np;
+        return (int)NB_OK;
+    });
+}
+
 int nereus_b200_bc_levels(const nb_bc *bc, int *velocity_levels, int *pressure_levels)
 {
     if (!bc || !bc->r) return Fail(NB_BAD_INPUT, "null argument");

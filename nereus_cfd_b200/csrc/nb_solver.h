@@ -296,6 +296,9 @@ void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double o
 struct BcReplay;
 // Checks the lists on the host (every index inside its field); throws InputError on a bad list.
 void CheckBcLists(const nb_bc_lists &lists);
+// The level of each operation of the two replays, in list order (solid faces of u, v, w, prescribed entries, copies;
+// ring entries), on the host.
+void PlanBcLevels(const nb_bc_lists &lists, std::vector<int> &velocity, std::vector<int> &pressure);
 // The checked, levelled lists on the current device.
 BcReplay *CreateBcReplay(int device, const nb_bc_lists &lists);
 void DestroyBcReplay(BcReplay *b);

@@ -233,6 +233,7 @@ class Scene:
     at_centre: bool = True
     pressure_expr: Optional[str] = None  # the p="..." of pressure-outlet faces with has_p
     face_params: Optional[dict] = None  # face index -> extra boundary parameters (u="..." v="..." w="...")
+    pressure_exprs: Optional[dict] = None  # face index -> its own p="..." (else pressure_expr)
 
     def face_arrays(self):
         kind = [BC_NOSLIP] * 6
@@ -249,7 +250,8 @@ class Scene:
         for f, k, hp in self.faces:
             line = "boundary %s %s" % (FACE_NAMES[f], BC_NAMES[k])
             if hp:
-                line += ' p="%s"' % (self.pressure_expr or "0")
+                expr = (self.pressure_exprs or {}).get(f, self.pressure_expr or "0")
+                line += ' p="%s"' % expr
             if self.face_params and f in self.face_params:
                 line += " " + self.face_params[f]
             lines.append(line)
@@ -445,6 +447,41 @@ def bc_outlet_2d(n: int = 20, seed: int = 24) -> Case:
     faces = [(3, BC_NOSLIP, 0), (2, BC_SLIP, 0), (0, BC_INLET, 0), (1, BC_PRESSURE_OUTLET, 1)]
     params = {0: 'u="4*y*(1-y)" v="0"'}
     return Case("bc_outlet_2d_%d" % n, g, Scene(faces, [], True, "0.1*t+y", params), seed)
+
+
+def bc_suite_scene(scene: int, dim: int, seed: int = 29) -> Case:
+    """The four scenes of the reference's own boundary-condition test (tests/suite_units.cpp:453-480), on its grids
+    (unit square 24^2 or unit cube 12^3, uniform):
+    0 a closed box with a moving lid (u = 1, w = 0.5 x), a slip side, walls and an interior solid box;
+    1 a channel with a time-dependent inlet and pressure outlets on three faces meeting at corners, a solid sphere;
+    2 prescribed pressures on three faces, an outlet at p = 0, an inlet, a slip wall, a solid box;
+    3 an inlet whose flux leaves through a continuity outflow, slip walls, a solid sphere."""
+    n = 24 if dim == 2 else 12
+    g = uniform_grid(dim, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    XMIN, XMAX, YMIN, YMAX, ZMIN, ZMAX = range(6)
+    if scene == 0:
+        faces = [(XMIN, BC_NOSLIP, 0), (XMAX, BC_SLIP, 0), (YMIN, BC_NOSLIP, 0), (ZMIN, BC_SLIP, 0),
+                 (ZMAX, BC_NOSLIP, 0), (YMAX, BC_MOVING, 0)]
+        params, pexprs = {YMAX: 'u="1" w="0.5*x"'}, None
+        regions = [Region(REGION_SOLID, PRIM_BOX, (0.35, 0.3, 0.3), (0.6, 0.55, 0.6))]
+    elif scene == 1:
+        faces = [(XMIN, BC_INLET, 0), (XMAX, BC_PRESSURE_OUTLET, 0), (YMIN, BC_NOSLIP, 0),
+                 (ZMIN, BC_PRESSURE_OUTLET, 0), (ZMAX, BC_NOSLIP, 0), (YMAX, BC_PRESSURE_OUTLET, 0)]
+        params, pexprs = {XMIN: 'u="1 + 0.5*sin(3*t) + y" v="0.2*y" w="0.1*z"'}, None
+        regions = [Region(REGION_SOLID, PRIM_SPHERE, (0.5, 0.5, 0.5), radius=0.18)]
+    elif scene == 2:
+        faces = [(XMIN, BC_PRESSURE_OUTLET, 1), (XMAX, BC_PRESSURE_OUTLET, 1), (YMIN, BC_PRESSURE_OUTLET, 0),
+                 (YMAX, BC_INLET, 0), (ZMIN, BC_PRESSURE_OUTLET, 1), (ZMAX, BC_SLIP, 0)]
+        params = {YMAX: 'u="0.2" v="-0.5*x" w="0"'}
+        pexprs = {XMIN: "1 + y + t", XMAX: "0.5*t - x", ZMIN: "2*z"}
+        regions = [Region(REGION_SOLID, PRIM_BOX, (0.4, 0.4, 0.4), (0.6, 0.7, 0.55))]
+    else:
+        faces = [(XMIN, BC_INLET, 0), (XMAX, BC_OUTFLOW, 0), (YMIN, BC_NOSLIP, 0), (YMAX, BC_SLIP, 0),
+                 (ZMIN, BC_SLIP, 0), (ZMAX, BC_SLIP, 0)]
+        params, pexprs = {XMIN: 'u="1 - (y - 1)^2 + 0.3*z"'}, None
+        regions = [Region(REGION_SOLID, PRIM_SPHERE, (0.5, 0.4, 0.5), radius=0.15)]
+    sc = Scene(faces, regions, True, None, params, pexprs)
+    return Case("bc_suite_scene%d_%dd_%d" % (scene, dim, n), g, sc, seed)
 
 
 def flip_tank_2d(n: int = 32, seed: int = 10, a: float = 0.55, b: float = 0.45) -> Case:
