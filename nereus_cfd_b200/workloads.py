@@ -449,15 +449,23 @@ def bc_outlet_2d(n: int = 20, seed: int = 24) -> Case:
     return Case("bc_outlet_2d_%d" % n, g, Scene(faces, [], True, "0.1*t+y", params), seed)
 
 
-def bc_suite_scene(scene: int, dim: int, seed: int = 29) -> Case:
+def bc_suite_scene(scene: int, dim: int, seed: int = 29, stretched: bool = False) -> Case:
     """The four scenes of the reference's own boundary-condition test (tests/suite_units.cpp:453-480), on its grids
     (unit square 24^2 or unit cube 12^3, uniform):
     0 a closed box with a moving lid (u = 1, w = 0.5 x), a slip side, walls and an interior solid box;
     1 a channel with a time-dependent inlet and pressure outlets on three faces meeting at corners, a solid sphere;
     2 prescribed pressures on three faces, an outlet at p = 0, an inlet, a slip wall, a solid box;
-    3 an inlet whose flux leaves through a continuity outflow, slip walls, a solid sphere."""
+    3 an inlet whose flux leaves through a continuity outflow, slip walls, a solid sphere.
+    ``stretched`` grades y and z by 1.15 per cell away from a 4-cell band (the reference's test grades its grids too).
+    """
     n = 24 if dim == 2 else 12
-    g = uniform_grid(dim, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
+    if stretched:
+        # graded in y and z (x uniform), so the faces of an x boundary differ in area
+        wy = band_stretched_widths(n, 1.0, 4, 0.75, 1.15)
+        wz = band_stretched_widths(n, 1.0, 4, 0.15, 1.15)
+        g = stretched_grid(dim, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), [np.full(n, 1.0 / n), wy, wz][:dim])
+    else:
+        g = uniform_grid(dim, (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), n)
     XMIN, XMAX, YMIN, YMAX, ZMIN, ZMAX = range(6)
     if scene == 0:
         faces = [(XMIN, BC_NOSLIP, 0), (XMAX, BC_SLIP, 0), (YMIN, BC_NOSLIP, 0), (ZMIN, BC_SLIP, 0),
@@ -481,7 +489,7 @@ def bc_suite_scene(scene: int, dim: int, seed: int = 29) -> Case:
         params, pexprs = {XMIN: 'u="1 - (y - 1)^2 + 0.3*z"'}, None
         regions = [Region(REGION_SOLID, PRIM_SPHERE, (0.5, 0.4, 0.5), radius=0.15)]
     sc = Scene(faces, regions, True, None, params, pexprs)
-    return Case("bc_suite_scene%d_%dd_%d" % (scene, dim, n), g, sc, seed)
+    return Case("bc_suite_scene%d_%dd_%d%s" % (scene, dim, n, "_stretched" if stretched else ""), g, sc, seed)
 
 
 def flip_tank_2d(n: int = 32, seed: int = 10, a: float = 0.55, b: float = 0.45) -> Case:

@@ -77,7 +77,9 @@ BC_CASES = [
     ("bc_pressure_outlet_3d_12", "pressure_outlet_3d", {"n": 12, "seed": 26}, 0.45),
     ("bc_sphere_outlet_3d_10", "sphere_outlet_3d", {"n": 10, "seed": 27}, 0.0),
 ] + [("bc_suite_scene%d_%dd" % (k, d), "bc_suite_scene", {"scene": k, "dim": d, "seed": 30 + 2 * k + d}, t)
-     for k in range(4) for d, t in ((3, 0.25), (2, 0.6))]  # the reference's own boundary test scenes
+     for k in range(4) for d, t in ((3, 0.25), (2, 0.6))] + [  # the reference's own boundary test scenes
+    ("bc_suite_scene%d_%dd_stretched" % (k, d), "bc_suite_scene",
+     {"scene": k, "dim": d, "seed": 40 + 2 * k + d, "stretched": True}, 0.45) for k in (1, 3) for d in (3, 2)]
 
 
 def build_case(builder: str, kwargs: dict) -> W.Case:
