@@ -156,4 +156,59 @@ class PressureSolver
     bool warmStart_ = false;
 };
 
+// FLIP3D::UpdateFluidCells / FLIP2D::UpdateFluidCells (src/Methods/FLIP/FLIP3D.cpp:784-833,
+// src/Methods/FLIP/FLIP2D.cpp:648-691) on host labels, in place. x0 points at the first particle's x with y and z the
+// next two doubles, rows `stride` doubles apart: the reference's Particle array is &particles->data[0].x, stride 7.
+// origin = FacePos(X|Y|Z, 0) (origin[2] unread in 2D), dh = SIMULATION.dh. Returns the number of particles skipped
+// as outside the labels (the reference would index outside them).
+inline int64_t UpdateFluidCells(int dim, int Nx, int Ny, int Nz, const double origin[3], double dh, const double *x0,
+                                int64_t count, int64_t stride, uint8_t *cellTypes)
+{
+    int64_t skipped = 0;
+    const double *y0 = x0 ? x0 + 1 : nullptr, *z0 = (x0 && dim == 3) ? x0 + 2 : nullptr;
+    const int st = nereus_b200_update_fluid_cells(dim, Nx, Ny, Nz, origin[0], origin[1], dim == 3 ? origin[2] : 0.0,
+                                                  dh, x0, y0, z0, count, stride, cellTypes, &skipped);
+    if (st != NB_OK) throw Error(st, nereus_b200_last_error());
+    return skipped;
+}
+
+// MAC::EnforceVelocityBC and MAC::EnforcePressureBC (src/MAC.cpp:811-865) on device fields, from the lists
+// MAC::BuildBoundaryLists made (rebuild the object when the MAC rebuilds them). The calls queue work on `stream`.
+class BoundaryReplay
+{
+  public:
+    BoundaryReplay(int device, const nb_bc_lists &lists)
+    {
+        const int st = nereus_b200_bc_create(device, &lists, &bc_);
+        if (st != NB_OK) throw Error(st, nereus_b200_last_error());
+    }
+    ~BoundaryReplay() { nereus_b200_bc_destroy(bc_); }
+    BoundaryReplay(const BoundaryReplay &) = delete;
+    BoundaryReplay &operator=(const BoundaryReplay &) = delete;
+
+    // prescValues: the boundary velocity function at each prescribedList entry (device), or null without one.
+    void EnforceVelocityBC(double *u, double *v, double *w, const double *prescValues, void *stream = nullptr)
+    {
+        const int st = nereus_b200_bc_enforce_velocity(bc_, u, v, w, prescValues, stream);
+        if (st != NB_OK) throw Error(st, nereus_b200_last_error());
+    }
+    // ringValues: PrescribedPressure at each ringList entry of kind 1 (device), or null for 0 there.
+    void EnforcePressureBC(double *p, const double *ringValues, void *stream = nullptr)
+    {
+        const int st = nereus_b200_bc_enforce_pressure(bc_, p, ringValues, stream);
+        if (st != NB_OK) throw Error(st, nereus_b200_last_error());
+    }
+    int VelocityLevels() const { return Levels(0); }
+    int PressureLevels() const { return Levels(1); }
+
+  private:
+    int Levels(int pressure) const
+    {
+        int v = 0, p = 0;
+        nereus_b200_bc_levels(bc_, &v, &p);
+        return pressure ? p : v;
+    }
+    nb_bc *bc_ = nullptr;
+};
+
 } // namespace nereus_b200

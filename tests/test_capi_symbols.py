@@ -94,3 +94,16 @@ def test_relabel_checks_its_arguments_before_the_device(lib):
         assert call(args()) == capi.NB_NO_DEVICE
         sb = lib.nereus_b200_update_fluid_cells_scratch_bytes(3, 10, 10, 10)
         assert sb == 16 + 4 * 8 ** 3
+
+
+@pytest.mark.skipif(cuda_ok(), reason="checks the no-GPU behaviour")
+def test_cpp_host_side_errors_without_a_device(lib, tmp_path):
+    """include/nereus_b200_solver.hpp's UpdateFluidCells and BoundaryReplay: NB_BAD_INPUT for bad arguments,
+    NB_NO_DEVICE (an exception, not a host fallback) for a good call without a GPU."""
+    exe = str(tmp_path / "shim_errors")
+    libdir = os.path.dirname(capi.LIB_PATH)
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-I" + os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "shim_errors.cpp"), "-o", exe, "-L" + libdir,
+                           "-lnereus_b200", "-Wl,-rpath," + libdir])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
