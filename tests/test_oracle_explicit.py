@@ -58,3 +58,18 @@ def test_interior_air_is_outside_the_equivalence():
     o = cpu.solve_projection(g, z["types"], z["u"], z["v"], z["w"], z["p_in"], meta["rho"], meta["dt"],
                              meta["needs_compat"], 1e-13)
     assert np.linalg.norm(o.x - z["x"]) / np.linalg.norm(z["x"]) > 1e-2
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_compatibility_on_changes_nothing_unless_singular(name):
+    """The routing passes needsCompat = true: the compatibility step and the levelling act only on a singular system
+    (PressureSolver3D.cpp:300-307, 181-211), which is when EXPLICIT removes its mean, so the flag leaves a
+    non-singular step as it was."""
+    case, meta, z = load_golden(name)
+    args = (case.grid, z["types"], z["u"], z["v"], z["w"], z["p_in"], meta["rho"], meta["dt"])
+    on = cpu.solve_projection(*args, True, 1e-13)
+    off = cpu.solve_projection(*args, meta["needs_compat"], 1e-13)
+    if not meta["singular"]:
+        assert np.array_equal(on.x, off.x) and np.array_equal(on.u, off.u)
+    x, xr = on.x - on.x.mean(), z["x"] - z["x"].mean()
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) <= 1e-9
