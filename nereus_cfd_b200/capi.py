@@ -256,6 +256,8 @@ def update_fluid_cells(grid, types, xyz, origin, dh=None):
     xyz = np.ascontiguousarray(xyz, dtype=np.float64)
     xyz = xyz.reshape(xyz.shape[0], -1) if xyz.size else np.zeros((0, 3))
     count, stride = xyz.shape
+    if count and stride < grid.dim:
+        raise ValueError("positions need x, y%s in each row" % (", z" if grid.dim == 3 else ""))
     base = xyz.ctypes.data
     pz = ctypes.c_void_p(base + 16) if grid.dim == 3 else None
     skipped = ctypes.c_int64(0)

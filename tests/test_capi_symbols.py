@@ -107,3 +107,12 @@ def test_cpp_host_side_errors_without_a_device(lib, tmp_path):
                            "-lnereus_b200", "-Wl,-rpath," + libdir])
     r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_relabel_wrapper_wants_a_coordinate_per_axis(lib):
+    """capi.update_fluid_cells reads x, y (, z) from each row: a 3D call with two columns is refused in Python."""
+    from nereus_cfd_b200 import workloads as W
+
+    g = W.flip_tank_3d(n=4, seed=1).grid
+    with pytest.raises(ValueError):
+        capi.update_fluid_cells(g, np.zeros(g.cells, dtype=np.uint8), np.zeros((3, 2)), [0.0, 0.0, 0.0])
