@@ -216,6 +216,30 @@ __device__ __forceinline__ int FluidCount(const RelabelGrid &g, const uint8_t *t
     return up + lo;
 }
 
+// The same count for the owner of cell c at (i, j, m), with `maybe`, its EMPTY interior lower neighbours (those that
+// may still be filled), taken from ONE read of each lower neighbour. Other threads fill cells meanwhile; had the two
+// figures come from separate reads, a neighbour filled between them would be in neither and c could be left out of
+// both the fills and the pending list. From one read, every lower neighbour that belongs to the solution is either
+// FLUID/filled (counted) or EMPTY (in `maybe`), so a cell of the solution that is not filled is always listed. The
+// upper neighbours' "FLUID before the pass" never changes during the pass.
+__device__ __forceinline__ int FluidCountOnce(const RelabelGrid &g, const uint8_t *t, long long c, int i, int j, int m,
+                                              int &maybe)
+{
+    const volatile uint8_t *vt = t;
+    int up = (t[c + g.sI] == FLUID) + (t[c + 1] == FLUID);
+    const uint8_t a = vt[c - g.sI], b = vt[c - 1];
+    int lo = (a == FLUID || a == kFilled) + (b == FLUID || b == kFilled);
+    maybe = (i > 1 && a == EMPTY) + (m > 1 && b == EMPTY);
+    if (g.dim == 3)
+    {
+        up += t[c + g.sJ] == FLUID;
+        const uint8_t d = vt[c - g.sJ];
+        lo += d == FLUID || d == kFilled;
+        maybe += j > 1 && d == EMPTY;
+    }
+    return up + lo;
+}
+
 // Coordinates of cell c: (i, j, m) with m the march-axis index (k in 3D, j in 2D; j = 0 in 2D). Cells number
 // below 2^31, so 32-bit arithmetic serves.
 __device__ __forceinline__ void CellCoords(const RelabelGrid &g, long long c, int &i, int &j, int &m)
@@ -286,15 +310,14 @@ __global__ void __launch_bounds__(kThreads)
         {
             const long long c = base + m;
             if (t[c] != EMPTY) continue;
-            const int f = FluidCount(g, t, c);
+            int maybe = 0;
+            const int f = FluidCountOnce(g, t, c, i, j, m, maybe);
             if (f >= g.thr)
             {
                 t[c] = kFilled;
-                ChaseUp(g, t, c, i, g.dim == 3 ? j : 0, m);
+                ChaseUp(g, t, c, i, j, m);
                 continue;
             }
-            int maybe = (m > 1 && t[c - 1] == EMPTY) + (i > 1 && t[c - g.sI] == EMPTY);
-            if (g.dim == 3) maybe += j > 1 && t[c - g.sJ] == EMPTY;
             if (f + maybe >= g.thr)
             {
                 const int slot = atomicAdd(hdr, 1);
