@@ -482,8 +482,11 @@ def run_relabel(args, dev):
            "steps": len(ms), "gpu_launches": int(launches), "skipped": int(skipped.item()),
            "roofline": {"bound": "hbm", "achieved": round(algo / med / 1e6, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(algo / med / 1e6 / peak, 3), "peak_kind": peak_kind,
-                        "algorithmic_bytes": int(algo),
+                        "traffic": None, "algorithmic_bytes": int(algo),
                         "bytes_per_unit": "24 B per particle (x, y, z) + 5 B per cell (labels reset, read, finished)"}}
+    tr = ncu_traffic("relabel_call")  # DRAM bytes of one call from the committed ncu summary, scaled by cells
+    if tr is not None:
+        out["roofline"]["traffic"] = int(tr[0] * g.cells / tr[1])
     # the reference's own Particle layout: 7 doubles a particle, x at the second
     aos = torch.zeros(count, 7, dtype=torch.float64, device="cuda")
     aos[:, 1:4] = rows
