@@ -66,8 +66,10 @@ typedef struct nb_options
                             per pass); 1: one captured graph per CG iteration (V-cycle included), the loop on the
                             host; 0: plain launches. The server's slots run 2 as 1: with several slots on one GPU
                             the per-iteration graphs were measured 6% faster */
-    int fused_sweeps;    /* 1: 3D levels smooth with one shared-memory tiled launch per red-black sweep, the
-                            prolongation and r.z fused in; 0 (default): one launch per colour */
+    int transfer_kernels; /* the restriction of colour-split levels: 0 (default): one thread per 4 coarse cells
+                             where the coarse level has at least 2^20 cells, else one thread per coarse cell;
+                             1: one thread per coarse cell everywhere; 2: one thread per 4 coarse cells everywhere.
+                             All three give the same result */
     int pair_kernels;    /* FP32 kernels of the mixed form on 3D levels with Nz even (uniform or stretched):
                             2 (default): the colour-split layout, red and black cells in separate arrays, so that
                             one colour's sweep moves half the bytes; 1: cell pairs in the grid layout; 0: the

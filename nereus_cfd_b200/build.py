@@ -24,7 +24,6 @@ SOURCES = {
     "nb_exact.cu": ["-fmad=false"],
     "nb_kernels.cu": [],
     "nb_tail.cu": [],
-    "nb_fused.cu": [],
     "nb_pairs.cu": [],
     "nb_split.cu": [],
     "nb_solver.cu": [],

@@ -28,7 +28,7 @@ class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("max_iters", ctypes.c_int),
                 ("max_outer", ctypes.c_int), ("inner_tol", ctypes.c_double), ("pre_sweeps", ctypes.c_int),
                 ("post_sweeps", ctypes.c_int), ("coarse_sweeps", ctypes.c_int), ("max_levels", ctypes.c_int),
-                ("stream", ctypes.c_void_p), ("use_graphs", ctypes.c_int), ("fused_sweeps", ctypes.c_int),
+                ("stream", ctypes.c_void_p), ("use_graphs", ctypes.c_int), ("transfer_kernels", ctypes.c_int),
                 ("pair_kernels", ctypes.c_int), ("tail_cells", ctypes.c_int), ("stretched_sweeps", ctypes.c_int)]
 
 

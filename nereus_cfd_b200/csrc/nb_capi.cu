@@ -38,7 +38,7 @@ void nereus_b200_default_options(nb_options *o)
     o->max_levels = 16;
     o->stream = nullptr;
     o->use_graphs = 2;
-    o->fused_sweeps = 0;
+    o->transfer_kernels = 0;
     o->pair_kernels = 2;
     o->tail_cells = 2048;
     o->stretched_sweeps = 2;

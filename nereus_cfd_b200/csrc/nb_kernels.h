@@ -48,13 +48,6 @@ void LaunchGather(const LevelView &v, const int32_t *idp, const double *grid, do
 void LaunchScatterVolume(const LevelView &v, const int32_t *idp, const double *compact, double *grid, int volume,
                          cudaStream_t st);
 
-// ---- nb_fused.cu: one red-black sweep per launch on 3D levels (shared-memory tiles, slow-axis marching) ----
-template <typename T> void PrepareSweeps();
-template <typename T>
-void LaunchRBSweep(const LevelView &v, const LevelView &cv, const T *r, const T *eIn, const T *ec, T *eOut,
-                   int firstColour, bool first, bool prolong, bool dot, const Reducer &R, const int *it, int baseEven,
-                   int baseOdd, cudaStream_t st);
-
 // ---- nb_tail.cu: the coarse end of the V-cycle in one thread block, in shared memory ----
 constexpr int kMaxTailLevels = 8;
 constexpr size_t kTailMaxSmem = 200 * 1024;
@@ -116,8 +109,9 @@ void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, 
                          cudaStream_t st);
 void LaunchSplitProlong(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *eCoarse,
                         float *eFine, cudaStream_t st);
+// mode: 0 by the coarse level's size, 1 one thread per coarse cell, 2 one thread per 4 coarse cells (same result)
 void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
-                         float *rCoarse, cudaStream_t st);
+                         float *rCoarse, int mode, cudaStream_t st);
 void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
                        const Reducer &R, const double *S, const int *it, int baseEven, int baseOdd, int slotN,
                        int singular, int slotPQ, cudaStream_t st);

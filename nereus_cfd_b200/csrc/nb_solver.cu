@@ -75,8 +75,6 @@ template <> float *LevelData::e<float>() { return e32.p; }
 template <> double *LevelData::e<double>() { return e64.p; }
 template <> float *LevelData::res<float>() { return res32.p; }
 template <> double *LevelData::res<double>() { return res64.p; }
-template <> float *LevelData::f<float>() { return f32.p; }
-template <> double *LevelData::f<double>() { return f64.p; }
 
 static void UploadTables(LevelData &Lv, cudaStream_t st)
 {
@@ -201,9 +199,6 @@ void Context::BuildHierarchy()
     BuildPairData();
     BuildTailLists();
     NB_CK(cudaGetLastError());
-    if (mixed) PrepareSweeps<float>();
-    else PrepareSweeps<double>();
-    cudaGetLastError(); // an attribute the device refuses leaves the per-colour path, checked at launch
 }
 
 // The colour-split levels (pair_kernels = 2, mixed precision): the uniform 3D levels with Nz even above the coarse
@@ -212,7 +207,7 @@ void Context::BuildHierarchy()
 // per-cell coefficients make the split kernels compute-bound (measured slower on the stretched cylinder).
 void Context::AssignSplit()
 {
-    const bool on = opt.precision == NB_PRECISION_MIXED && opt.pair_kernels == 2 && !opt.fused_sweeps && !nonuniform;
+    const bool on = opt.precision == NB_PRECISION_MIXED && opt.pair_kernels == 2 && !nonuniform;
     bool finer = true;
     for (size_t l = 0; l < L.size(); l++)
     {
@@ -311,23 +306,20 @@ void Context::AllocVectors()
         LevelData &Lv = L[l];
         const size_t c = (size_t)Lv.cells;
         const bool last = l + 1 == L.size();
-        const bool fused = FusedLevel((int)l);
         if (mixed)
         {
             const size_t c32 = Lv.VecLen(); // zeroed whole: the split layout's padding stays zero
             Lv.r32.alloc(c32); Lv.r32.zero(st);
             Lv.e32.alloc(c32); Lv.e32.zero(st);
             if (!last) { Lv.res32.alloc(c32); Lv.res32.zero(st); }
-            if (fused) { Lv.f32.alloc(c); Lv.f32.zero(st); } else Lv.f32.release();
-            Lv.r64.release(); Lv.e64.release(); Lv.res64.release(); Lv.f64.release();
+            Lv.r64.release(); Lv.e64.release(); Lv.res64.release();
         }
         else
         {
             Lv.r64.alloc(c); Lv.r64.zero(st);
             Lv.e64.alloc(c); Lv.e64.zero(st);
             if (!last) { Lv.res64.alloc(c); Lv.res64.zero(st); }
-            if (fused) { Lv.f64.alloc(c); Lv.f64.zero(st); } else Lv.f64.release();
-            Lv.r32.release(); Lv.e32.release(); Lv.res32.release(); Lv.f32.release();
+            Lv.r32.release(); Lv.e32.release(); Lv.res32.release();
         }
     }
     const size_t c = Cells();
@@ -621,11 +613,6 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
         ProfEnd();
         return;
     }
-    if (FusedLevel(l))
-    {
-        VCycleFused<T>(l, r, e);
-        return;
-    }
     if constexpr (std::is_same<T, float>::value)
     {
         if (Split(l))
@@ -783,7 +770,7 @@ void Context::VCycleSplit(int l, float *r, float *e)
     LevelData &Lc = L[l + 1];
     const LevelView vc = Lc.view();
     prof(NB_K_RESTRICT0, (s + 1.0) / 2.0 + s / 8.0);
-    LaunchSplitRestrict(v, vc, Lv.pext.p, res, Lc.r<float>(), st);
+    LaunchSplitRestrict(v, vc, Lv.pext.p, res, Lc.r<float>(), opt.transfer_kernels, st);
     ProfEnd();
     VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
     prof(NB_K_PROLONG0, s + 0.5 + s / 8.0); // reads and writes red e, reads the red bytes and the coarse e
@@ -801,57 +788,6 @@ void Context::VCycleSplit(int l, float *r, float *e)
                 LaunchSplitHalf(v, du, r, e, c, st);
         }
         ProfEnd();
-    }
-}
-
-// The V-cycle on a 3D level with one launch per red-black sweep (nb_fused.cu): the pre-smoothing from zero into f,
-// the residual and its restriction, the coarser levels, then the post-smoothing that reads f + P(e_coarse) and
-// writes e. On level 0 the last sweep also sums r.z for CG (IterBody then skips its own r.z launch).
-template <typename T> void Context::VCycleFused(int l, T *r, T *e)
-{
-    LevelData &Lv = L[l];
-    const LevelView v = Lv.view();
-    LevelData &Lc = L[l + 1];
-    const LevelView vc = Lc.view();
-    const double s = sizeof(T), cells = (double)Lv.cells;
-    auto prof = [&](int id, double bytesPerCell) {
-        ProfBegin(l == 0 ? id : NB_K_COARSE, l == 0 ? bytesPerCell * cells : 0.0);
-    };
-    const int pre = PreSweeps(l), post = PostSweeps(l);
-    T *f = Lv.f<T>(), *res = Lv.res<T>();
-    // pre-smoothing: the first sweep from zero (reads r, codes; writes the iterate), the rest in turn, ending in f
-    T *dst = (pre % 2 == 1) ? f : e;
-    prof(NB_K_SMOOTH0, s + 1.0 + s);
-    LaunchRBSweep<T>(v, vc, r, nullptr, nullptr, dst, 0, true, false, false, red, iter.p, S_RZ0, S_RZ1, st);
-    ProfEnd();
-    for (int q = 1; q < pre; q++)
-    {
-        T *src = dst;
-        dst = (src == f) ? e : f;
-        prof(NB_K_SMOOTH0, 3.0 * s + 1.0);
-        LaunchRBSweep<T>(v, vc, r, src, nullptr, dst, 0, false, false, false, red, iter.p, S_RZ0, S_RZ1, st);
-        ProfEnd();
-    }
-    prof(NB_K_RESIDUAL0, 3.0 * s + 1.0);
-    LaunchLevelResidual<T>(v, r, f, res, st);
-    ProfEnd();
-    prof(NB_K_RESTRICT0, s + s / 8.0);
-    LaunchRestrict<T>(v, vc, res, Lc.r<T>(), st);
-    ProfEnd();
-    VCycle<T>(l + 1, Lc.r<T>(), Lc.e<T>());
-    // post-smoothing, black first: the first sweep adds the prolonged coarse correction, the last ends in e
-    const bool dotHere = l == 0;
-    T *src = f;
-    dst = (post % 2 == 1) ? e : res;
-    for (int q = 0; q < post; q++)
-    {
-        const bool lastSweep = q + 1 == post;
-        prof(q == 0 ? NB_K_PROLONG0 : NB_K_SMOOTH0, 3.0 * s + 1.0 + (q == 0 ? s / 8.0 : 0.0));
-        LaunchRBSweep<T>(v, vc, r, src, Lc.e<T>(), dst, 1, false, q == 0, dotHere && lastSweep, red, iter.p, S_RZ0,
-                         S_RZ1, st);
-        ProfEnd();
-        src = dst;
-        dst = (src == e) ? res : e;
     }
 }
 
@@ -898,12 +834,9 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
             return;
         }
     }
-    if (!FusedLevel(0)) // else the V-cycle's last sweep summed r.z already
-    {
-        ProfBegin(NB_K_DOT, 2.0 * s * cells);
-        LaunchDot<T>(v0, r, z, red, iter.p, S_RZ0, S_RZ1, st);
-        ProfEnd();
-    }
+    ProfBegin(NB_K_DOT, 2.0 * s * cells);
+    LaunchDot<T>(v0, r, z, red, iter.p, S_RZ0, S_RZ1, st);
+    ProfEnd();
     ProfBegin(NB_K_PAPPLY, (4.0 * s + 1.0) * cells);
     LaunchUpdatePApply<T>(v0, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, exact ? 1 : 0, st);
     ProfEnd();
@@ -1421,7 +1354,5 @@ void Context::GetIdp(int32_t *out)
 
 template void Context::VCycle<float>(int, float *, float *);
 template void Context::VCycle<double>(int, double *, double *);
-template void Context::VCycleFused<float>(int, float *, float *);
-template void Context::VCycleFused<double>(int, double *, double *);
 
 } // namespace nb

@@ -109,13 +109,12 @@ struct LevelData
     int sRS = 0, sPS = 0;
     long long sHalf = 0;
     size_t VecLen() const { return sRS ? (size_t)(2 * sHalf) : (size_t)cells; }
-    DevArray<float> r32, e32, res32, f32; // f: the pre-smoothed iterate of a fused V-cycle
-    DevArray<double> r64, e64, res64, f64;
+    DevArray<float> r32, e32, res32;
+    DevArray<double> r64, e64, res64;
     LevelView view() const;
     template <typename T> T *r();
     template <typename T> T *e();
     template <typename T> T *res();
-    template <typename T> T *f();
 };
 
 struct Context
@@ -255,11 +254,9 @@ struct Context
     // the initial residual of the guess, and the tolerance the refNorm floor turns `tol` into; false: nothing to do
     bool StartFrom(const double *guess, double refNorm, double tol, double bn2, double *tolEff);
     template <typename T> void VCycle(int l, T *r, T *e);
-    template <typename T> void VCycleFused(int l, T *r, T *e);
     // red-black sweeps before / after the coarse correction on level l (stretched levels take stretched_sweeps)
     int PreSweeps(int l) const { return std::max(1, L[l].stretched ? opt.stretched_sweeps : opt.pre_sweeps); }
     int PostSweeps(int l) const { return std::max(1, L[l].stretched ? opt.stretched_sweeps : opt.post_sweeps); }
-    bool FusedLevel(int l) const { return opt.fused_sweeps && dim == 3 && l < tailStart && l + 1 < (int)L.size(); }
     // the FP32 cell-pair kernels serve this level (its du is built)
     bool PairLevel(int l) const { return opt.pair_kernels && L[l].du.p != nullptr; }
     // the FP32 vectors of this level are colour-split and its V-cycle runs the split kernels

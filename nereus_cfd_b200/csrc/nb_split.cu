@@ -674,14 +674,15 @@ __global__ void __launch_bounds__(256) k_split_restrict1(LevelView fv, LevelView
 }
 
 // Coarse levels with at least kRestrictQuadCells cells take the quad kernel (4x fewer loads per coarse cell), the
-// smaller ones the per-cell kernel.
+// smaller ones the per-cell kernel (mode 0); mode 1 takes the per-cell kernel and mode 2 the quad kernel everywhere.
+// Both sum the same products in the same order.
 constexpr long long kRestrictQuadCells = 1LL << 20;
 
 void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const uint8_t *pext, const float *resFine,
-                         float *rCoarse, cudaStream_t st)
+                         float *rCoarse, int mode, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    if (coarse.cells < kRestrictQuadCells)
+    if (mode == 1 || (mode != 2 && coarse.cells < kRestrictQuadCells))
     {
         const long long perPlane = (long long)((coarse.Nz - 2 + 31) / 32) * ((coarse.Nx - 2 + 7) / 8);
         const int S = MarchPlanes(coarse.Ny - 2, perPlane);

@@ -29,6 +29,8 @@
 // 4 FLIP's re-labelling (FLIP3D::UpdateFluidCells, src/Methods/FLIP/FLIP3D.cpp:784-833; FLIP2D::UpdateFluidCells,
 // src/Methods/FLIP/FLIP2D.cpp:648-691) from the particle positions of the case file, then the Chorin step on the new
 // labels.
+// With NB_REF_LEAN=1 in the environment the result leaves out cell types, IDP, the CSR matrix and both right-hand
+// sides (nnz is written as 0 and the header's last double as 1.0), for grids where those run to gigabytes.
 // [scheme 1 or 2] The result file then ends with double ref_norm (IncrementReferenceNorm, 0 for Chorin) and double
 // p_final[cells] (the pressure after Project).
 // [scheme 4] The case file ends with int64 count and double xyz[3 * count] (x, y, z per particle); the result file
@@ -543,25 +545,32 @@ int main(int argc, char **argv)
                 maxDiv = std::max(maxDiv, std::fabs(d));
             }
 
+    // NB_REF_LEAN=1 (large grids): the labels, numbering, matrix and right-hand sides are left out of the result
+    // (flag 1 in the last double of the header); x, p, the fields, the tables and the times stay
+    const char *leanEnv = std::getenv("NB_REF_LEAN");
+    const bool lean = leanEnv && leanEnv[0] == '1';
     FILE *o = std::fopen(argv[2], "wb");
     if (!o) { std::fprintf(stderr, "cannot write %s\n", argv[2]); return 2; }
     std::fwrite("NBRES001", 1, 8, o);
     const int32_t nnz = (int32_t)S.A.nonZeros();
-    const int32_t oh[8] = {Nx, Ny, Nz, n, nnz, iters, S.singular ? 1 : 0, THREAD_COUNT};
+    const int32_t oh[8] = {Nx, Ny, Nz, n, lean ? 0 : nnz, iters, S.singular ? 1 : 0, THREAD_COUNT};
     WriteN(o, oh, 8);
-    const double od[8] = {tAssemble, tCold, tWarm, tProject, relres, maxDiv, grid.dh, 0.0};
+    const double od[8] = {tAssemble, tCold, tWarm, tProject, relres, maxDiv, grid.dh, lean ? 1.0 : 0.0};
     WriteN(o, od, 8);
-    WriteN(o, grid.cellTypes.data(), cells);
-    std::vector<int32_t> idp(IDP.begin(), IDP.end());
-    WriteN(o, idp.data(), cells);
-    std::vector<int32_t> rp(n + 1), cl(nnz);
-    for (int r = 0; r <= n; r++) rp[r] = S.A.outerIndexPtr()[r];
-    for (int q = 0; q < nnz; q++) cl[q] = S.A.innerIndexPtr()[q];
-    WriteN(o, rp.data(), n + 1);
-    WriteN(o, cl.data(), nnz);
-    WriteN(o, S.A.valuePtr(), nnz);
-    WriteN(o, braw.data(), n);
-    WriteN(o, b.data(), n);
+    if (!lean)
+    {
+        WriteN(o, grid.cellTypes.data(), cells);
+        std::vector<int32_t> idp(IDP.begin(), IDP.end());
+        WriteN(o, idp.data(), cells);
+        std::vector<int32_t> rp(n + 1), cl(nnz);
+        for (int r = 0; r <= n; r++) rp[r] = S.A.outerIndexPtr()[r];
+        for (int q = 0; q < nnz; q++) cl[q] = S.A.innerIndexPtr()[q];
+        WriteN(o, rp.data(), n + 1);
+        WriteN(o, cl.data(), nnz);
+        WriteN(o, S.A.valuePtr(), nnz);
+        WriteN(o, braw.data(), n);
+        WriteN(o, b.data(), n);
+    }
     WriteN(o, x.data(), n);
     WriteN(o, pAfter.data(), pAfter.size());
     WriteN(o, grid.u.data(), grid.u.size());

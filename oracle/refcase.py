@@ -113,9 +113,10 @@ def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
     off = 8
     Nx, Ny, Nz, n, nnz, iters, sing, thr = struct.unpack_from("<8i", data, off)
     off += 32
-    tA, tC, tW, tP, rr, md, dh, _ = struct.unpack_from("<8d", data, off)
+    tA, tC, tW, tP, rr, md, dh, lean = struct.unpack_from("<8d", data, off)
     off += 64
     cells = Nx * Ny * Nz
+    lean = lean == 1.0  # NB_REF_LEAN: no labels, numbering, matrix or right-hand sides in the file
 
     def take(dtype, count):
         nonlocal off
@@ -123,13 +124,13 @@ def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
         off += a.nbytes
         return a
 
-    types = take(np.uint8, cells)
-    idp = take("<i4", cells)
-    rowptr = take("<i4", n + 1)
+    types = take(np.uint8, 0 if lean else cells)
+    idp = take("<i4", 0 if lean else cells)
+    rowptr = take("<i4", 0 if lean else n + 1)
     col = take("<i4", nnz)
     val = take("<f8", nnz)
-    b_raw = take("<f8", n)
-    b = take("<f8", n)
+    b_raw = take("<f8", 0 if lean else n)
+    b = take("<f8", 0 if lean else n)
     x = take("<f8", n)
     p = take("<f8", cells)
     u = take("<f8", (Nx + 1) * Ny * Nz)
@@ -160,16 +161,18 @@ def read_result(path, dim, scheme=SCHEME_CHORIN) -> RefResult:
 
 
 def run(case, u, v, w, label_mode=0, types=None, solver=SOLVER_CG, tol=None, max_iters=1000000, threads=1,
-        repeats=0, timeout=3600, scheme=SCHEME_CHORIN, p_prev=None, time=0.0, particles=None) -> RefResult:
+        repeats=0, timeout=3600, scheme=SCHEME_CHORIN, p_prev=None, time=0.0, particles=None,
+        lean=False) -> RefResult:
     """Runs the reference on ``case`` with face velocities u, v, w; labels from the scene text (label_mode 0) or
-    the given ``types`` (label_mode 1)."""
+    the given ``types`` (label_mode 1). lean: the result leaves out labels, IDP, the matrix and the right-hand sides
+    (empty arrays here), for large grids."""
     if not available():
         raise RuntimeError("oracle/_ref/ref_harness is not built (make -C oracle ref)")
     with tempfile.TemporaryDirectory() as td:
         cp, rp = os.path.join(td, "case.bin"), os.path.join(td, "res.bin")
         write_case(cp, case, u, v, w, label_mode, types, solver, tol, max_iters, threads, repeats, scheme, p_prev,
                    time, particles)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), NB_REF_LEAN="1" if lean else "0")
         r = subprocess.run([HARNESS, cp, rp], capture_output=True, text=True, timeout=timeout, env=env, cwd=td)
         if r.returncode != 0:
             raise RuntimeError("ref_harness failed (%d): %s %s" % (r.returncode, r.stdout[-2000:], r.stderr[-2000:]))

@@ -2,7 +2,7 @@
 
 Run in a checkout that has the reference sources (it builds oracle/_ref/ref_harness from them first):
 
-    python tests/golden/make_golden.py [REF_ROOT] [--only explicit|flip|bc]
+    python tests/golden/make_golden.py [REF_ROOT] [--only explicit|flip|bc|<fixture name>]
 
 Each fixture is one small case: the inputs both sides read (face velocities, the prescribed ring pressure) and what
 the reference computed from them (cell types, IDP, the CSR matrix, b before and after the compatibility step, the
@@ -35,6 +35,8 @@ CASES = [
     ("channel_2d_stretched_24x12", "channel_2d_stretched", {"nx": 24, "ny": 12, "seed": 15}, 1e-12),
     ("inflow_outflow_3d_8", "inflow_outflow_3d", {"n": 8, "seed": 16}, 1e-12),
     ("all_solid_3d_6", "all_solid_3d", {"n": 6, "seed": 17}, 1e-12),
+    # the 2D 128^2 closed box at full size (all-Neumann, compatibility on; the case's own tolerance is 1e-10)
+    ("closed_box_2d_128", "closed_box_2d", {"n": 128, "seed": 1}, 1e-12),
 ]
 
 
@@ -208,6 +210,8 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
             write_bc_case(*args)
         return
     for name, builder, kwargs, tol in CASES:
+        if only and only != name:
+            continue
         case = build_case(builder, kwargs)
         g = case.grid
         # labels from the reference's own scene code (label_mode 0), then velocities from those labels
@@ -229,6 +233,8 @@ def main(ref_root: str = "/root/reference", only: str = "") -> None:
             **{"centre%d" % a: ref.centre[a] for a in range(3)})
         print("%-36s n=%-6d iters=%-4d rel_res=%.2e max_div=%.2e  %d KB" % (
             name, ref.n, ref.iters, ref.rel_res, ref.max_div, os.path.getsize(out) // 1024))
+    if only:
+        return
     for args in SCHEME_CASES:
         write_scheme_case(*args)
     for args in EXPLICIT_CASES + EXPLICIT_LIMIT_CASES:
