@@ -554,70 +554,141 @@ def run_relabel(args, dev):
 
 
 def run_tanks(args, rank, world, dist, dev):
-    """The batched form: `tanks` FLIP-style n^3 tanks (liquid where x < a, z < b; a, b ~ U(0.3, 0.7) per tank),
-    each one pressure step to 1e-8 through the server (`slots` concurrent solves on this rank's device; the tanks'
-    fields resident on the device as in a simulation step, each request bringing its own cell labels), split over the
-    ranks by the least-loaded plan; against the same tanks solved one at a time in plain FP64 on the device. Wall
-    clock from the first submission to the last completion, max over ranks."""
-    import copy
+    """The batched form (cfg4): `tanks` FLIP-style n^3 tanks (liquid where x < a, z < b; a, b ~ U(0.3, 0.7) per tank),
+    each step one pressure projection of every tank to 1e-8 as ONE batched call (nereus_b200_batch_project_device:
+    every kernel of a CG iteration is one launch over all tanks still iterating, the iteration a captured graph with
+    a WHILE node, launch shapes autotuned on the first call). The tanks' fields stay on the device and are restored
+    from a copy inside every step. Against the same tanks one at a time, each on its own context holding its layout,
+    in plain FP64 (the single-solve form) and in the mixed form. CUDA events on one stream; steps repeated until the
+    timed region passes one second. With N ranks the tanks are split by the least-loaded plan; max over ranks."""
+    import torch
 
     from nereus_cfd_b200 import capi, serving
     from nereus_cfd_b200.pressure import PressureSolver
 
+    lib = capi.load()
     cases = serving.tank_batch(args.tanks, args.tank_size)
+    stream = torch.cuda.current_stream()
     summary = {}
-
-    import torch
 
     def execute(mine):
         jobs = [serving.to_device(serving.job_from_case(c, tol=TOL), dev) for c in mine]
         if not jobs:
             return {"seconds": 0.0, "completed": 0, "latencies": []}
-        with serving.Server(devices=(dev,), slots_per_device=args.slots, **args.solver_opts) as srv:
-            warm = [copy.deepcopy(j) for j in jobs[: args.slots]]
-            serving.serve_jobs(warm, srv)  # each slot's context, graphs and buffers
-            out = serving.serve_jobs(jobs, srv)
-        out["iters_inner"] = [j.result["iters_inner"] for j in jobs if j.result]
-        # one at a time in plain FP64 on a sample of the same tanks, fields on the device likewise
-        sample = [serving.to_device(serving.job_from_case(c, tol=TOL), dev) for c in mine[: args.fp64_tanks]]
-        s = PressureSolver("fp64", device=dev, **args.solver_opts)
-        lib = capi.load()
+        keys = ("u", "v", "w", "p")
+        orig = [{k: j.device_fields[k].clone() for k in keys} for j in jobs]
 
-        def one(j):
-            s.EnsureSystem(j.grid)
-            f, res = j.device_fields, capi.Result()
-            capi.check(lib.nereus_b200_project_device(s.ctx, f["u"].data_ptr(), f["v"].data_ptr(), f["w"].data_ptr(),
-                                                      f["p"].data_ptr(), j.grid.rho, j.grid.dt, 0, TOL,
-                                                      ctypes.byref(res)), allow=(0, 1))
+        def restore(i):
+            for k in keys:
+                jobs[i].device_fields[k].copy_(orig[i][k])
 
-        s.InitializePressureSolver(sample[0].grid)
-        one(copy.deepcopy(sample[0]))  # warm-up
+        def events():
+            return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        # ---- the batched form ----
+        batch = serving.Batch(len(jobs), device=dev, stream=stream.cuda_stream, **args.solver_opts)
+        for i, j in enumerate(jobs):
+            batch.set_layout(i, j.grid)
+        items = batch.items(jobs)
+
+        def step():
+            for i in range(len(jobs)):
+                restore(i)
+            return batch.project(jobs, items=items)
+
+        for _ in range(2):  # the first call tunes and captures
+            step()
+        a, b = events()
+        a.record(stream)
+        step()
+        b.record(stream)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for j in sample:
-            one(j)
+        one = a.elapsed_time(b) / 1e3
+        steps = max(args.tank_steps, int(1.0 / max(one, 1e-6)) + 1)
+        lat = []
+        l0 = lib.nereus_b200_kernel_launches()
+        a, b = events()
+        a.record(stream)
+        for _ in range(steps):
+            x, y = events()
+            x.record(stream)
+            res = step()
+            y.record(stream)
+            lat.append((x, y))
+        b.record(stream)
         torch.cuda.synchronize()
-        out["fp64_seconds_each"] = (time.perf_counter() - t0) / len(sample)
-        s.DestroyPressureSolver()
+        secs = a.elapsed_time(b) / 1e3
+        launches = lib.nereus_b200_kernel_launches() - l0
+        lat = [x.elapsed_time(y) for x, y in lat]
+        info = batch.info()
+        batch.close()
+        out = {"seconds": secs, "completed": steps * len(jobs), "steps": steps, "latencies": lat,
+               "iters_inner": [r["iters_inner"] for r in res], "rel_res_max": max(r["rel_res"] for r in res),
+               "status": sorted({r["status"] for r in res}), "gpu_launches": launches, "batch": info}
+
+        # ---- one at a time, each tank on its own context (its layout kept), fields restored each time ----
+        def one_at_a_time(precision):
+            ss = []
+            for j in jobs:
+                s = PressureSolver(precision, device=dev, stream=stream.cuda_stream, **args.solver_opts)
+                s.InitializePressureSolver(j.grid)
+                ss.append(s)
+            r = capi.Result()
+
+            def solve(i):
+                restore(i)
+                f = jobs[i].device_fields
+                capi.check(lib.nereus_b200_project_device(ss[i].ctx, f["u"].data_ptr(), f["v"].data_ptr(),
+                                                          f["w"].data_ptr(), f["p"].data_ptr(), jobs[i].grid.rho,
+                                                          jobs[i].grid.dt, 0, TOL, ctypes.byref(r)),
+                           allow=(0, 1))
+
+            for i in range(len(jobs)):  # warm: each context's graphs
+                solve(i)
+            a, b = events()
+            a.record(stream)
+            for i in range(len(jobs)):
+                solve(i)
+            b.record(stream)
+            torch.cuda.synchronize()
+            sec = a.elapsed_time(b) / 1e3
+            for s in ss:
+                s.DestroyPressureSolver()
+            return {"value": round(len(jobs) / sec, 3), "unit": "solves/s", "tanks": len(jobs),
+                    "seconds": round(sec, 4)}
+
+        out["fp64_one_at_a_time"] = one_at_a_time("fp64")
+        out["mixed_one_at_a_time"] = one_at_a_time("mixed")
         summary.update(out)
         return out
 
     res = serving.run_sharded(cases, lambda c: c.grid.cells, execute, dist)
-    fp64_each = summary.get("fp64_seconds_each")
+    fp64 = summary.get("fp64_one_at_a_time", {}).get("seconds")
+    mixed1 = summary.get("mixed_one_at_a_time", {}).get("seconds")
     if dist:
         vals = [None] * world
-        dist.all_gather_object(vals, fp64_each)
-        fp64_each = max(v for v in vals if v is not None)
-    fp64_rate = world / fp64_each if fp64_each else None
+        dist.all_gather_object(vals, (fp64, mixed1))
+        fp64 = max(v[0] for v in vals if v[0] is not None)
+        mixed1 = max(v[1] for v in vals if v[1] is not None)
+    fp64_rate = args.tanks / fp64 if fp64 else None
+    mixed1_rate = args.tanks / mixed1 if mixed1 else None
     its = summary.get("iters_inner", [])
+    lat = summary.get("latencies", [])
     return {"workload": "flip_tanks_%dx%d^3" % (args.tanks, args.tank_size), "tanks": args.tanks,
-            "slots_per_device": args.slots, "value": round(res["solves_per_s"], 3), "unit": "solves/s",
-            "p50_ms": round(res["p50_ms"], 3), "p99_ms": round(res["p99_ms"], 3), "seconds": round(res["seconds"], 4),
-            "scaling": "strong", "iters_inner_rank0": [int(min(its)), int(max(its))] if its else None,
+            "form": "one batched call per step (nereus_b200_batch_project_device)",
+            "value": round(res["solves_per_s"], 3), "unit": "solves/s", "steps": summary.get("steps"),
+            "seconds": round(res["seconds"], 4), "step_p50_ms": round(percentile(lat, 0.5), 3) if lat else None,
+            "step_p99_ms": round(percentile(lat, 0.99), 3) if lat else None, "scaling": "strong",
+            "iters_inner_rank0": [int(min(its)), int(max(its))] if its else None,
+            "rel_res_max_rank0": summary.get("rel_res_max"), "status_rank0": summary.get("status"),
+            "gpu_launches_rank0": summary.get("gpu_launches"), "batch_rank0": summary.get("batch"),
             "fp64_one_at_a_time": {"value": round(fp64_rate, 3) if fp64_rate else None, "unit": "solves/s",
-                                   "sample_tanks": args.fp64_tanks},
+                                   "tanks": args.tanks},
+            "mixed_one_at_a_time": {"value": round(mixed1_rate, 3) if mixed1_rate else None, "unit": "solves/s",
+                                    "tanks": args.tanks},
             "speedup_over_fp64_one_at_a_time": round(res["solves_per_s"] / fp64_rate, 3) if fp64_rate else None,
-            "timing": "host wall clock, first submission to last completion, max over ranks",
+            "speedup_over_mixed_one_at_a_time": round(res["solves_per_s"] / mixed1_rate, 3) if mixed1_rate else None,
+            "timing": "CUDA events on one stream, fields restored inside each step; max over ranks",
             "per_rank": res["per_rank"]}
 
 
@@ -742,8 +813,8 @@ def main():
     ap.add_argument("--opt", action="append", default=[], help="solver option key=value (nb_options field)")
     ap.add_argument("--tanks", type=int, default=64, help="batched tanks (0: skip the batched form)")
     ap.add_argument("--tank-size", type=int, default=128)
-    ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device in the batched form")
-    ap.add_argument("--fp64-tanks", type=int, default=4, help="tanks solved one at a time in plain FP64")
+    ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device of the serving trace")
+    ap.add_argument("--tank-steps", type=int, default=5, help="batched steps at least (the timed region >= 1 s)")
     ap.add_argument("--trace", type=int, default=200, help="requests of the serving trace (0: skip)")
     ap.add_argument("--stretched-steps", type=int, default=5, help="steps of the stretched workload (0: skip)")
     ap.add_argument("--trace-fp64", type=int, default=40, help="trace requests solved one at a time in plain FP64")

@@ -78,6 +78,9 @@ typedef struct nb_options
                             cells (and shared memory for all of them); 0: no such block */
     int stretched_sweeps; /* red-black sweeps before and after the coarse correction on a stretched grid's levels
                              (their anisotropy asks for more smoothing); pre_sweeps/post_sweeps apply to uniform ones */
+    int autotune;        /* batches: 1 (default): the launch shapes of the smoothing, residual and transfer kernels
+                            are timed on the batch's first step and the fastest kept (cached per grid, level, kernel
+                            and capacity); 0: the shapes a single solve takes. Neither changes a result */
 } nb_options;
 
 typedef struct nb_result
@@ -360,15 +363,66 @@ double nereus_b200_request_bytes(int dim, int Nx, int Ny, int Nz, int precision)
  * in submission order, each goes to the device with the smallest assigned total (lowest index on ties). */
 int nereus_b200_plan(const double *costs, int n, int k, int *device_of);
 
-/* ---- IDP numbering without allocation. No counterpart in the reference: its IDP loop runs inside
- *      AssembleSystem (PressureSolver3D.cpp:133-139); this is the same numbering as nereus_b200_get_idp gives after
- *      nereus_b200_set_layout, for callers that must not allocate device memory at the point they renumber. ----
+/* ---- batched solves: one pressure step for each of many grids of the same shape, advanced together. Replaces, for
+ *      a caller with many independent systems (FLIP tanks, ensemble members), one SolvePressureSystem call per
+ *      system (PressureSettings.h:578-624), each of which waits for its solver alone. Every kernel of a CG iteration
+ *      is one launch over all requests still iterating (a device-side work list of requests, compacted after each
+ *      iteration as requests converge), the iteration runs as a captured CUDA graph with a WHILE node, and each
+ *      request keeps its own labels, multigrid hierarchy, vectors, reductions, tolerance and iteration count. A
+ *      request's result is bit for bit what nereus_b200_project_device gives it alone with the same options.
+ *      Mixed precision; uniform 3D grids whose multigrid levels above the coarse end have Nz even. ---- */
+typedef struct nb_batch nb_batch;
+
+typedef struct nb_batch_item
+{
+    double *u, *v, *w, *p; /* device fields of the request's slot (as nereus_b200_project_device) */
+    double rho, dt;
+    int needs_compat;
+    double tol;
+} nb_batch_item;
+
+#define NB_BATCH_MAX_LEVELS 16
+typedef struct nb_batch_info
+{
+    int capacity, levels, tail_start;
+    long long loop_launches;                   /* kernels one batched CG iteration launches */
+    double tune_ms;                            /* device time the autotuner spent */
+    int march[NB_BATCH_MAX_LEVELS][5];         /* per split level: the march length of the first sweep, a half-sweep,
+                                                  the residual, the restriction, the prolongation */
+    int restrict_mode[NB_BATCH_MAX_LEVELS];    /* 1: one thread per coarse cell; 2: one per four */
+} nb_batch_info;
+
+/* capacity: the most requests one call takes (1 .. 1024); opt->precision must be NB_PRECISION_MIXED */
+int nereus_b200_batch_create(nb_batch **batch, const nb_options *opt, int capacity);
+void nereus_b200_batch_destroy(nb_batch *batch);
+/* the layout of slot `slot` (as nereus_b200_set_layout; unchanged bytes keep its hierarchy) */
+int nereus_b200_batch_set_layout(nb_batch *batch, int slot, int dim, int Nx, int Ny, int Nz, const uint8_t *cellTypes,
+                                 const double *const width[3], const double *const gap[3], int nonUniform, double dh);
+/* The Chorin step of slots 0 .. count-1 with items[i]'s device fields; results[i] gets each one's report. Returns the
+ * worst status. NB_BAD_INPUT when the slots' shapes differ or do not take the batched form. */
+int nereus_b200_batch_project_device(nb_batch *batch, int count, const nb_batch_item *items, nb_result *results);
+int nereus_b200_batch_info(nb_batch *batch, nb_batch_info *info);
+/* The autotuner (host only). choose: the candidate index to keep given the candidates' times (the fastest, unless
+ * the fallback is within 3% of it; ties within 0.5% to the earlier one). key: the cache key of a (grid, level,
+ * kernel kind 0-4, capacity) into buf, returning its length. The cache holds one line per key, "key|S|mode|us":
+ * dump writes it into buf (returning its full length), load adds lines of that form (returning the count, or
+ * NB_BAD_INPUT for a malformed text), clear empties it. */
+int nereus_b200_tune_choose(int n, const double *times, int fallback);
+int nereus_b200_tune_key(int Nx, int Ny, int Nz, int level, int kind, int capacity, char *buf, int size);
+int nereus_b200_tune_cache_dump(char *buf, int size);
+int nereus_b200_tune_cache_load(const char *text);
+void nereus_b200_tune_cache_clear(void);
+
+/* ---- IDP numbering without allocation. No counterpart in the reference. It gives the same numbering as
+ *      nereus_b200_get_idp after nereus_b200_set_layout, for callers that must not allocate device memory at the
+ *      point they renumber. ----
  * cellTypes (Nx*Ny*Nz bytes), idp (Nx*Ny*Nz int32) and n (one int32) are DEVICE pointers on `device`; the call is
  * asynchronous on `stream` (a cudaStream_t, NULL = the default stream). idp gets -1 off the system, *n the count.
  * Makes no cudaMalloc/cudaFree: its scratch is one fixed 2 MiB array per device, enough for grids of at most
  * NB_NOALLOC_MAX_LINES interior lines ((Ny-2)*(Nx-2) in 3D, Ny-2 in 2D); larger grids get NB_BAD_INPUT.
  * The first call on a device looks up that array's address (and may load the library's device code), so make it
- * before any stream capture begins. Calls that overlap in time on one device share the scratch and race. */
+ * before any stream capture begins; after a cudaDeviceReset the next call looks it up again, so make that one
+ * before any capture too. Calls that overlap in time on one device share the scratch and race. */
 #define NB_NOALLOC_MAX_LINES 262144
 int nereus_b200_number_unknowns_noalloc(int device, int dim, int Nx, int Ny, int Nz, const uint8_t *cellTypes,
                                         int32_t *idp, int32_t *n, void *stream);

@@ -32,8 +32,9 @@ SOURCES = {
     "nb_relabel.cu": ["-fmad=false"],
     "nb_bc.cu": ["-fmad=false"],
     "nb_server.cu": [],
+    "nb_batch.cu": [],
 }
-HEADERS = ["nb_device.cuh", "nb_kernels.h", "nb_solver.h", "nb_guard.h"]
+HEADERS = ["nb_device.cuh", "nb_batch.cuh", "nb_kernels.h", "nb_solver.h", "nb_guard.h"]
 
 
 def _newest_input() -> float:

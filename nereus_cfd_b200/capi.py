@@ -29,7 +29,8 @@ class Options(ctypes.Structure):
                 ("max_outer", ctypes.c_int), ("inner_tol", ctypes.c_double), ("pre_sweeps", ctypes.c_int),
                 ("post_sweeps", ctypes.c_int), ("coarse_sweeps", ctypes.c_int), ("max_levels", ctypes.c_int),
                 ("stream", ctypes.c_void_p), ("use_graphs", ctypes.c_int), ("transfer_kernels", ctypes.c_int),
-                ("pair_kernels", ctypes.c_int), ("tail_cells", ctypes.c_int), ("stretched_sweeps", ctypes.c_int)]
+                ("pair_kernels", ctypes.c_int), ("tail_cells", ctypes.c_int), ("stretched_sweeps", ctypes.c_int),
+                ("autotune", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -79,6 +80,31 @@ class Region(ctypes.Structure):
 class SceneStruct(ctypes.Structure):
     _fields_ = [("face_kind", ctypes.c_int * 6), ("face_has_p", ctypes.c_int * 6), ("face_order", ctypes.c_int * 6),
                 ("nregions", ctypes.c_int), ("regions", Region * 16)]
+
+
+class BatchItem(ctypes.Structure):
+    """nb_batch_item: one request of a batched step (device fields of its slot)."""
+
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p), ("p", ctypes.c_void_p),
+                ("rho", ctypes.c_double), ("dt", ctypes.c_double), ("needs_compat", ctypes.c_int),
+                ("tol", ctypes.c_double)]
+
+
+BATCH_MAX_LEVELS = 16
+BATCH_KINDS = ["first", "half", "residual", "restrict", "prolong"]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_int), ("levels", ctypes.c_int), ("tail_start", ctypes.c_int),
+                ("loop_launches", ctypes.c_longlong), ("tune_ms", ctypes.c_double),
+                ("march", (ctypes.c_int * 5) * BATCH_MAX_LEVELS), ("restrict_mode", ctypes.c_int * BATCH_MAX_LEVELS)]
+
+    def as_dict(self):
+        n = max(0, self.tail_start)
+        return {"capacity": self.capacity, "levels": self.levels, "tail_start": self.tail_start,
+                "loop_launches": self.loop_launches, "tune_ms": round(self.tune_ms, 3),
+                "march": [dict(zip(BATCH_KINDS, list(self.march[l]))) for l in range(n)],
+                "restrict_mode": [self.restrict_mode[l] for l in range(n)]}
 
 
 # Every exported symbol of include/nereus_b200.h with its ctypes signature.
@@ -168,6 +194,20 @@ SIGNATURES = {
     "nereus_b200_bc_destroy": (None, [ctypes.c_void_p]),
     "nereus_b200_bc_plan": (ctypes.c_int, [ctypes.POINTER(BcLists), ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "nereus_b200_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(Options),
+                                                ctypes.c_int]),
+    "nereus_b200_batch_destroy": (None, [ctypes.c_void_p]),
+    "nereus_b200_batch_set_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.c_int, _u8, _dp * 3, _dp * 3, ctypes.c_int,
+                                                    ctypes.c_double]),
+    "nereus_b200_batch_project_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchItem),
+                                                        ctypes.POINTER(Result)]),
+    "nereus_b200_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchInfo)]),
+    "nereus_b200_tune_choose": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int]),
+    "nereus_b200_tune_key": (ctypes.c_int, [ctypes.c_int] * 6 + [ctypes.c_char_p, ctypes.c_int]),
+    "nereus_b200_tune_cache_dump": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "nereus_b200_tune_cache_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "nereus_b200_tune_cache_clear": (None, []),
     "nereus_b200_update_fluid_cells_device": (ctypes.c_int, [ctypes.c_int] * 5 + [ctypes.c_double] * 4 +
                                               [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_int64] +
                                               [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,

@@ -284,18 +284,18 @@ struct PairPos
     long long base; // cell index of the pair's first cell on plane i0
 };
 
-__device__ __forceinline__ PairPos PairStart(const LevelView &v)
+__device__ __forceinline__ PairPos PairStart(const LevelView &v, int bx, int by, int gy)
 {
     PairPos p;
     const int P = (int)(v.sI >> 1);
     p.lane = threadIdx.x & 31;
-    int q = blockIdx.x * kPairThreads + threadIdx.x;
+    int q = bx * kPairThreads + threadIdx.x;
     p.valid = q < P;
     if (!p.valid) q = P - 1;
     // the launch's grid.y splits the Ny-2 interior planes into chunks of S (the host sized it); a block past the
     // last plane starts at the ring plane and marches none
-    const int S = (v.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
-    p.i0 = min(1 + (int)blockIdx.y * S, v.Ny - 1);
+    const int S = (v.Ny - 2 + gy - 1) / gy;
+    p.i0 = min(1 + by * S, v.Ny - 1);
     p.i1 = min(p.i0 + S, v.Ny - 1);
     p.sI = (int)v.sI;
     p.sJ = (int)v.sJ;
@@ -304,6 +304,10 @@ __device__ __forceinline__ PairPos PairStart(const LevelView &v)
     p.k0 = cin - p.j * v.Nz;
     p.base = (long long)p.i0 * v.sI + cin;
     return p;
+}
+__device__ __forceinline__ PairPos PairStart(const LevelView &v)
+{
+    return PairStart(v, (int)blockIdx.x, (int)blockIdx.y, (int)gridDim.y);
 }
 
 // ---- reductions ----
@@ -341,17 +345,17 @@ constexpr int kWarps = kBlock / 32;
 // bump: when not null, the last block adds 1 to *bump after storing the totals (the PCG iteration counter, which
 // every block of the launch has read before any block can be the last).
 // addSlot0 >= 0 (sums only): each total also adds out[addSlot0 + s], the totals an earlier launch left there.
+// GridReduceB: the same over the blocks bid = 0 .. nblk-1 of one reduction (a batched launch runs one reduction per
+// request, each over its own blocks and Reducer).
 template <int NV>
-__device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], int slot0, int op = 0,
-                                           int *bump = nullptr, int addSlot0 = -1)
+__device__ __forceinline__ void GridReduceB(const Reducer &R, double (&val)[NV], int slot0, unsigned bid,
+                                            unsigned nblk, int op = 0, int *bump = nullptr, int addSlot0 = -1)
 {
     __shared__ double sh[NV][32];
     __shared__ bool amLast;
     const int nthr = blockDim.x * blockDim.y * blockDim.z;
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     const int lane = tid & 31, warp = tid >> 5, nwarp = (nthr + 31) >> 5;
-    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
 #pragma unroll
     for (int s = 0; s < NV; s++)
     {
@@ -406,6 +410,24 @@ __device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], 
         *R.counter = 0u;
     }
 }
+
+template <int NV>
+__device__ __forceinline__ void GridReduce(const Reducer &R, double (&val)[NV], int slot0, int op = 0,
+                                           int *bump = nullptr, int addSlot0 = -1)
+{
+    GridReduceB<NV>(R, val, slot0, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                    gridDim.x * gridDim.y * gridDim.z, op, bump, addSlot0);
+}
+
+// The block coordinates of a launch's blocks within one request's grid: a single launch passes blockIdx and gridDim,
+// a batched launch (blockIdx.z = the request's place in the active list) the same x and y.
+struct Blk
+{
+    int x, y, gx, gy;
+};
+__device__ __forceinline__ Blk ThisBlk() { return Blk{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y}; }
+__device__ __forceinline__ unsigned BlkId(const Blk &b) { return (unsigned)(b.x + b.gx * b.y); }
+__device__ __forceinline__ unsigned BlkCount(const Blk &b) { return (unsigned)(b.gx * b.gy); }
 
 // ---- programmatic dependent launch: a kernel launched by LaunchPdl may be scheduled while the previous kernel on
 // its stream drains. It calls PdlWait() before reading anything an earlier kernel wrote (the wait returns once that

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/nereus_b200.h"
+#include "nb_batch.cuh"
 #include "nb_device.cuh"
 
 namespace nb
@@ -60,6 +61,12 @@ template <typename T>
 void LaunchTail(const LevelView *levels, int nlev, const T *rIn, T *eOut, int pre, int post, int coarseSweeps,
                 const unsigned *lists, const int *counts, cudaStream_t st);
 
+// the batched coarse end (nb_batch.cu): one request's TailArgs<float> for the batch's table (sizes first with
+// out = null), and the launch (grid z = the capacity; smem: the largest request's dynamic shared memory)
+void TailArgsFor(const LevelView *levels, int nlev, const float *rIn, float *eOut, int pre, int post,
+                 int coarseSweeps, const unsigned *lists, const int *counts, void *out, size_t *bytes, size_t *smem);
+void LaunchBatchTail(const BatchReq *rq, BatchList a, int cap, size_t smem, cudaStream_t st);
+
 // ---- nb_pairs.cu: FP32 kernels for 3D levels of a uniform grid with Nz even (cell pairs, unmasked stencil) ----
 bool PairLevelShape(const LevelView &v);
 void LaunchBuildDu(const LevelView &v, uint8_t *du, cudaStream_t st);
@@ -89,6 +96,8 @@ void LaunchPairRefine64(const LevelView &v, const uint8_t *du, const double *b, 
                         cudaStream_t st);
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
                   int baseOdd, cudaStream_t st);
+void LaunchBatchLinXR(const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a, int cap, int baseEven,
+                      int baseOdd, int slotN, int slotPQ, int slotRR, cudaStream_t st);
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,
                  const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int slotN, int singular,
                  int slotPQ, int slotRR, cudaStream_t st);
@@ -117,6 +126,20 @@ void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, fl
                        int singular, int slotPQ, cudaStream_t st);
 void LaunchSplitScaleSum(const LevelView &v, const double *b, float *r, double sfac, const Reducer &R, int slot,
                          cudaStream_t st);
+// the batched forms (nb_batch.cu): kind NB_BK_*; S the march length of the non-reducing kernels; coarse: the next
+// coarser level (restriction, prolongation); mode: the restriction's kernel (1 per coarse cell, else per 4)
+enum : int { NB_BK_FIRST = 0, NB_BK_HALF, NB_BK_RESIDUAL, NB_BK_RESTRICT, NB_BK_PROLONG, NB_BK_COUNT };
+int SplitDefaultS(const LevelView &v, int kind);
+void LaunchBatchSplit(int kind, const LevelView &v, const LevelView *coarse, int S, int mode, const BatchLevel *lv,
+                      int ls, int l, const BatchReq *rq, BatchList a, int cap, int colour, cudaStream_t st);
+void LaunchBatchSplitHalfDot(const LevelView &v, const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a,
+                             int cap, int colour, bool last, int baseEven, int baseOdd, int partSlot, cudaStream_t st);
+void LaunchBatchSplitPApply(const LevelView &v, const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a,
+                            int cap, int baseEven, int baseOdd, int slotN, int slotPQ, cudaStream_t st);
+void LaunchBatchSplitScaleSum(const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a, int cap, int slot,
+                              cudaStream_t st);
+void LaunchBatchSplitRefine64(const LevelView &v, const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a,
+                              int cap, const int *parity, int slot, cudaStream_t st);
 void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
                          double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
                          cudaStream_t st);

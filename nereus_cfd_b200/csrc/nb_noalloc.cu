@@ -10,8 +10,9 @@
 // exists once per device, for the lifetime of the process.
 //
 // Set-up: the first call on a device looks up that device's address of the scratch array (cudaGetSymbolAddress),
-// with the device current. That lookup may load this library's device code onto the device, so make the first call
-// on each device before any stream capture begins.
+// with the device current, and notes the context it belongs to; a call that finds another context current (the
+// device was reset since) looks the address up again. That lookup may load this library's device code onto the
+// device, so make the first call on each device, and the first after a reset, before any stream capture begins.
 //
 // The scratch is shared by all callers on a device: two calls that overlap in time on one device (from different
 // streams or host threads) race on it and corrupt each other's results. Calls that follow each other on one stream
@@ -37,18 +38,41 @@ static __device__ __align__(256) int g_numberingScratch[kScratchInts];
 constexpr int kMaxDevices = 64;
 std::mutex g_setupMutex;
 int *g_scratchAddr[kMaxDevices] = {};
+void *g_scratchCtx[kMaxDevices] = {}; // the context the address belongs to
 
-// The current device's address of the scratch array, looked up on the first call for the device.
+// The driver context current on this thread (cuCtxGetCurrent, reached through the runtime's entry-point query so
+// that the library needs no link to the driver library), or null when it cannot be read.
+void *CurrentContext()
+{
+    typedef int (*GetCurrent)(void **);
+    static GetCurrent fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (GetCurrent)f;
+    }();
+    void *c = nullptr;
+    if (!fn || fn(&c) != 0) return nullptr;
+    return c;
+}
+
+// The current device's address of the scratch array, looked up on the first call for the device, and again when
+// the device's context is no longer the one it was looked up in (after a cudaDeviceReset the old address would
+// point into a context that no longer exists).
 int *ScratchAddress(int device)
 {
     if (device < 0 || device >= kMaxDevices) throw InputError("device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_setupMutex);
-    if (!g_scratchAddr[device])
+    void *ctx = CurrentContext();
+    if (!g_scratchAddr[device] || !ctx || ctx != g_scratchCtx[device])
     {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_numberingScratch);
         if (e != cudaSuccess) throw CudaError("cudaGetSymbolAddress(numbering scratch)", e);
         g_scratchAddr[device] = (int *)p;
+        g_scratchCtx[device] = CurrentContext();
     }
     return g_scratchAddr[device];
 }

@@ -795,22 +795,21 @@ __global__ void __launch_bounds__(256) k_lin_dot(long long cells, const float *_
 }
 
 // alpha = rz / pq; x += alpha p; r -= alpha q; sum r.r; the last block advances the iteration counter
-__global__ void __launch_bounds__(256) k_lin_xr(long long cells, float *__restrict__ x, float *__restrict__ r,
-                                                const float *p0, const float *p1, const float *__restrict__ q,
-                                                Reducer R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
-                                                int singular, int slotPQ, int slotRR)
+// bx of gx: this block among the launch's blocks (a grid-stride loop)
+__device__ __forceinline__ void LinXR(long long cells, float *__restrict__ x, float *__restrict__ r, const float *p0,
+                                      const float *p1, const float *__restrict__ q, const Reducer &R, const double *S,
+                                      int *it, int baseEven, int baseOdd, int slotN, int singular, int slotPQ,
+                                      int slotRR, int bx, int gx)
 {
-    PdlWait();
-    PdlTrigger();
     const int par = *it & 1;
     const float *__restrict__ p = par ? p0 : p1;
     const int base = par ? baseOdd : baseEven;
     const float a = (float)(RzEffP(S, base, S[slotN], singular) / S[slotPQ]);
     double acc[1] = {0.0};
-    const long long n4 = cells >> 2, stride = (long long)gridDim.x * blockDim.x;
+    const long long n4 = cells >> 2, stride = (long long)gx * blockDim.x;
     float4 *x4 = reinterpret_cast<float4 *>(x), *r4 = reinterpret_cast<float4 *>(r);
     const float4 *p4 = reinterpret_cast<const float4 *>(p), *q4 = reinterpret_cast<const float4 *>(q);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4; t += stride)
+    for (long long t = bx * (long long)blockDim.x + threadIdx.x; t < n4; t += stride)
     {
         const float4 pv = p4[t], qv = q4[t];
         float4 xv = x4[t], rv = r4[t];
@@ -820,14 +819,39 @@ __global__ void __launch_bounds__(256) k_lin_xr(long long cells, float *__restri
         r4[t] = rv;
         acc[0] += ((double)rv.x * rv.x + (double)rv.y * rv.y) + ((double)rv.z * rv.z + (double)rv.w * rv.w);
     }
-    for (long long t = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells; t += stride)
+    for (long long t = 4 * n4 + bx * (long long)blockDim.x + threadIdx.x; t < cells; t += stride)
     {
         x[t] += a * p[t];
         const float rn = r[t] - a * q[t];
         r[t] = rn;
         acc[0] += (double)rn * rn;
     }
-    GridReduce<1>(R, acc, slotRR, 0, it);
+    GridReduceB<1>(R, acc, slotRR, (unsigned)bx, (unsigned)gx, 0, it);
+}
+
+__global__ void __launch_bounds__(256) k_lin_xr(long long cells, float *__restrict__ x, float *__restrict__ r,
+                                                const float *p0, const float *p1, const float *__restrict__ q,
+                                                Reducer R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
+                                                int singular, int slotPQ, int slotRR)
+{
+    PdlWait();
+    PdlTrigger();
+    LinXR(cells, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, singular, slotPQ, slotRR, (int)blockIdx.x,
+          (int)gridDim.x);
+}
+
+// batched (nb_batch.cu): block z runs the request at list[z]; r is its level 0's r
+__global__ void __launch_bounds__(256) kb_lin_xr(const BatchLevel *__restrict__ lv, int ls,
+                                                 const BatchReq *__restrict__ rq, BatchList a, int baseEven,
+                                                 int baseOdd, int slotN, int slotPQ, int slotRR)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchReq Q = rq[q];
+    LinXR(Q.vecLen, Q.x, lv[q * ls].r, Q.p0, Q.p1, Q.q, Q.red, Q.red.out, Q.it, baseEven, baseOdd, slotN, Q.singular,
+          slotPQ, slotRR, (int)blockIdx.x, (int)gridDim.x);
 }
 
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
@@ -835,6 +859,14 @@ void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer
 {
     NB_COUNT_LAUNCH();
     k_lin_dot<<<kLinBlocks, 256, 0, st>>>(cells, r, z, R, it, baseEven, baseOdd);
+}
+
+void LaunchBatchLinXR(const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a, int cap, int baseEven,
+                      int baseOdd, int slotN, int slotPQ, int slotRR, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    LaunchPdl(kb_lin_xr, dim3(kLinBlocks, 1, cap), dim3(256), 0, st, lv, ls, rq, a, baseEven, baseOdd, slotN, slotPQ,
+              slotRR);
 }
 
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,

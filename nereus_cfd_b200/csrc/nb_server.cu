@@ -126,9 +126,6 @@ void nb_server::Slot(int dev)
                 nb_options o = opt.solver;
                 o.device = devices[(size_t)dev];
                 o.stream = nullptr;
-                // concurrent slots: one graph per CG iteration (measured 6% faster than device-side loops when 8
-                // slots share a GPU)
-                if (o.use_graphs > 1) o.use_graphs = 1;
                 ctx = std::make_unique<nb::Context>(o);
             }
             nb::Context &C = *ctx;

@@ -501,6 +501,22 @@ void Context::ReadSlots(int s, int count)
     NB_CK(cudaStreamSynchronize(st));
 }
 
+// Every byte <= 5 (the six cell types), eight at a time: a byte b >= 6 has bit 7 set in b + 0x7A or in b itself.
+static bool TypesInRange(const uint8_t *t, size_t n)
+{
+    const uint64_t k7A = 0x7A7A7A7A7A7A7A7AULL, k80 = 0x8080808080808080ULL;
+    size_t c = 0;
+    uint64_t bad = 0;
+    for (; c + 8 <= n; c += 8)
+    {
+        uint64_t x;
+        std::memcpy(&x, t + c, 8);
+        bad |= (x | ((x & 0x7F7F7F7F7F7F7F7FULL) + k7A)) & k80;
+    }
+    for (; c < n; c++) bad |= t[c] > 5 ? 1u : 0u;
+    return bad == 0;
+}
+
 void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *types, const double *const width[3],
                         const double *const gap[3], int nonUniform, double dh_)
 {
@@ -512,8 +528,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
         if (!width[a] || !gap[a]) throw InputError("null spacing table");
     if (!nonUniform && !(dh_ > 0.0)) throw InputError("uniform grid needs dh > 0");
     const size_t cells = (size_t)Nx_ * Ny_ * Nz_;
-    for (size_t c = 0; c < cells; c++)
-        if (types[c] > 5) throw InputError("cell type out of range");
+    if (!TypesInRange(types, cells)) throw InputError("cell type out of range");
     const int N[3] = {Nx_, Ny_, Nz_};
     bool same = built && dim_ == dim && Nx_ == Nx && Ny_ == Ny && Nz_ == Nz && (nonUniform != 0) == nonuniform &&
                 dh_ == dh && layout.size() == cells && std::memcmp(layout.data(), types, cells) == 0;
@@ -535,12 +550,47 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
         shapeSame = wt[a].size() == nw && gt[a].size() == ng && std::memcmp(wt[a].data(), width[a], nw * 8) == 0 &&
                     std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
     }
+    // a uniform grid of the same sizes at another dh: the hierarchy keeps its shape (the FP32 levels see gamma, not
+    // dh); the spacing tables and the scale are replaced in the arrays they have, so the captured iterations stay
+    const bool rescale = !shapeSame && built && !nonUniform && !nonuniform && dim_ == dim && Nx_ == Nx &&
+                         Ny_ == Ny && Nz_ == Nz && layout.size() == cells;
     NB_CK(cudaStreamSynchronize(st));
     const bool wasSingular = singular;
     built = false;
     idpValid = false;
     layout.assign(types, types + cells);
-    if (shapeSame)
+    if (rescale)
+    {
+        dh = dh_;
+        scale = 1.0 / (dh * dh); // MatrixScale3D (PressureSolver3D.cpp:34-37)
+        for (int a = 0; a < (dim == 3 ? 3 : 2); a++)
+        {
+            std::vector<double> w(width[a], width[a] + N[a] + 2), g(gap[a], gap[a] + N[a] + 1);
+            for (double x : w)
+                if (!(x > 0.0) || !std::isfinite(x)) throw InputError("width table entries must be positive");
+            for (double x : g)
+                if (!(x > 0.0) || !std::isfinite(x)) throw InputError("gap table entries must be positive");
+            wt[a] = w;
+            gt[a] = g;
+        }
+        if (dim == 2)
+        {
+            wt[2].assign(3, wt[0][1]);
+            gt[2].assign(2, wt[0][1]);
+        }
+        for (int a = 0; a < 3; a++) { L[0].w[a] = wt[a]; L[0].g[a] = gt[a]; }
+        for (size_t l = 1; l < L.size(); l++)
+        {
+            LevelData &F = L[l - 1], &C = L[l];
+            CoarseAxis(F.w[0], F.Nx, C.Nx, C.w[0], C.g[0]);
+            CoarseAxis(F.w[1], F.Ny, C.Ny, C.w[1], C.g[1]);
+            if (dim == 3) CoarseAxis(F.w[2], F.Nz, C.Nz, C.w[2], C.g[2]);
+            else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }
+        }
+        for (auto &Lv : L) UploadTables(Lv, st); // same sizes: the same device arrays
+        RefillHierarchy();
+    }
+    else if (shapeSame)
         RefillHierarchy();
     else
     {
@@ -575,7 +625,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
     ReadSlots(S_RES, 2);
     n = (int)hostSlots[S_RES];
     singular = hostSlots[S_RES + 1] == 0.0;
-    if (shapeSame && singular != wasSingular)
+    if ((shapeSame || rescale) && singular != wasSingular)
         for (auto &g : graphs) g.Release(); // the iteration's kernels depend on the flag
     hostSlots[S_NUNK] = (double)n;
     NB_CK(cudaMemcpyAsync(slots.p + S_NUNK, hostSlots + S_NUNK, sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1244,6 +1294,33 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
     out->status = status;
     lastIterations = out->iters_inner;
     return status;
+}
+
+void Context::BatchBegin(double *u, double *v, double *w, double *p, double rho, double dt, int compat)
+{
+    if (!built) throw InputError("set_layout has not been called");
+    if (!u || !v || !p || (dim == 3 && !w)) throw InputError("null field pointer");
+    if (!(rho > 0.0) || !(dt > 0.0)) throw InputError("rho and dt must be positive");
+    const LevelView v0 = L[0].view();
+    LaunchRing(v0, p, st);
+    LaunchRhs(v0, u, v, w, p, rho / dt, scale, dh, b.p, st);
+    if (compat && singular && n > 0)
+        for (int pass = 0; pass < 2; pass++) // b -= mean(b), twice (PressureSolver3D.cpp:300-307)
+        {
+            LaunchSumUnknowns(v0, b.p, red, S_SUM, st);
+            LaunchSubMeanScatter(v0, b.p, slots.p + S_SUM, n, 1, nullptr, st);
+        }
+}
+
+void Context::BatchEnd(double *x, double *u, double *v, double *w, double *p, double rho, double dt, int compat)
+{
+    const LevelView v0 = L[0].view();
+    const bool level = compat && singular && n > 0;
+    if (level) LaunchSumUnknowns(v0, x, red, S_SUM, st);
+    LaunchSubMeanScatter(v0, x, slots.p + S_SUM, n, level ? 1 : 0, p, st);
+    LaunchRing(v0, p, st);
+    LaunchProject(v0, u, v, w, p, dt / rho, st);
+    LaunchMaxDiv(v0, u, v, w, dh, red, S_DIV, st);
 }
 
 int Context::SolveLaplacian(const double *f, double *xh, double tol, nb_result *out)

@@ -226,6 +226,11 @@ struct Context
                       nb_result *out, bool solve = true, bool correct = true, const double *pPrev = nullptr,
                       int scheme = NB_SCHEME_CHORIN, bool warm = false);
     int SolveLaplacian(const double *f, double *x, double tol, nb_result *out);
+    // A batch's halves of the Chorin step around its solve (nb_batch.cu), on this context's stream: Begin checks the
+    // call and runs the ring, the right-hand side and the compatibility step; End levels x, scatters it into p, runs
+    // the ring and the velocity correction and leaves max |div u| in slot S_DIV.
+    void BatchBegin(double *u, double *v, double *w, double *p, double rho, double dt, int compat);
+    void BatchEnd(double *x, double *u, double *v, double *w, double *p, double rho, double dt, int compat);
     void Rhs(const double *u, const double *v, const double *w, const double *p, double rho, double dt, double *bOut);
     void ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnz, int *singularOut);
     void GetIdp(int32_t *out);
@@ -237,6 +242,7 @@ struct Context
     size_t Cells() const { return (size_t)Nx * Ny * Nz; }
 
   private:
+    friend struct Batch;
     void BuildHierarchy();
     void RefillHierarchy();
     void BuildPairData();

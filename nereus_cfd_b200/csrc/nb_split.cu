@@ -68,18 +68,18 @@ struct QuadPos
     long long off; // element of the quad on plane i0, within one colour
 };
 
-__device__ __forceinline__ QuadPos QuadStart(const LevelView &v)
+__device__ __forceinline__ QuadPos QuadStart(const LevelView &v, const Blk &b)
 {
     QuadPos p;
     const int Q = v.sRS >> 2, nq = v.Nx * Q;
     p.lane = threadIdx.x & 31;
-    int t = blockIdx.x * kPairThreads + threadIdx.x;
+    int t = b.x * kPairThreads + threadIdx.x;
     p.valid = t < nq;
     if (!p.valid) t = nq - 1;
     // grid.y splits the Ny-2 interior planes into chunks of S (the host sized it); a block past the last plane starts
     // at the ring plane and marches none
-    const int S = (v.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
-    p.i0 = min(1 + (int)blockIdx.y * S, v.Ny - 1);
+    const int S = (v.Ny - 2 + b.gy - 1) / b.gy;
+    p.i0 = min(1 + b.y * S, v.Ny - 1);
     p.i1 = min(p.i0 + S, v.Ny - 1);
     p.RS = v.sRS;
     p.PS = v.sPS;
@@ -119,6 +119,14 @@ inline int SmCount()
 // 92%-full wave of 16-plane chunks beats two waves of 8 (and 1.03 waves of 15 runs at half speed). With no such S,
 // the best-filled one (a small level fills no wave: S = 1, all the parallelism there is).
 constexpr int kQuadMaxS = 16;
+
+// A quad kernel's grid with a march of S planes (S > 0), or sized as above (S = 0).
+inline dim3 QuadGridS(const LevelView &v, int S)
+{
+    const long long nq = (long long)v.Nx * (v.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
+    const long long planes = v.Ny - 2 > 0 ? v.Ny - 2 : 1;
+    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
+}
 
 inline dim3 QuadGrid(const LevelView &v, int resident)
 {
@@ -174,14 +182,12 @@ constexpr int kSplitReduceS = 16;
 // The first red-black sweep from a zero iterate on a uniform level, one launch: red e = r / diag, then black
 // e = (r + gamma * sum of the red neighbours) / diag with the red neighbours formed from r and the bytes. A thread
 // owns one quad position and writes the red and the black quad there.
-__global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const uint8_t *__restrict__ du,
-                                                              const float *__restrict__ r, float *__restrict__ e)
+__device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__restrict__ du,
+                                           const float *__restrict__ r, float *__restrict__ e, const Blk &blk)
 {
-    PdlWait();
-    PdlTrigger();
     __shared__ float inv[32];
     FillInv(inv, v.gamma);
-    const QuadPos P = QuadStart(v);
+    const QuadPos P = QuadStart(v, blk);
     const float g = (float)v.gamma;
     const long long hb = v.sHalf;
     const float *R0 = r + P.off, *R1 = r + hb + P.off;
@@ -223,22 +229,28 @@ __global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const
     }
 }
 
+__global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const uint8_t *__restrict__ du,
+                                                              const float *__restrict__ r, float *__restrict__ e)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitFirst(v, du, r, e, ThisBlk());
+}
+
 // One colour of a red-black sweep: e_c = (r_c + gamma * sum of the other colour's six neighbours) / diag_c.
 // kDot 1: (sum r.e, sum e, sum r) of this colour into out[partSlot..]; kDot 2: the same plus the totals already in
 // out[partSlot..], into the scalar block of the iteration's parity (the CG's r.z, sum z, sum r of the V-cycle's z).
 // du, r: this colour's halves; eo, ec: the other colour's and this colour's halves of e (disjoint).
 template <int kDot>
-__global__ void __launch_bounds__(kPairThreads)
-    k_split_half(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ r,
-                 const float *__restrict__ eo, float *__restrict__ ec, int colour, Reducer R, const int *it,
-                 int baseEven, int baseOdd, int partSlot)
+__device__ __forceinline__ void SplitHalf(const LevelView &v, const uint8_t *__restrict__ du,
+                                          const float *__restrict__ r, const float *__restrict__ eo,
+                                          float *__restrict__ ec, int colour, const Reducer &R, const int *it,
+                                          int baseEven, int baseOdd, int partSlot, const Blk &blk)
 {
-    PdlWait();
-    PdlTrigger();
     float facc[3] = {0.f, 0.f, 0.f}; // a thread's terms in FP32, the block and grid sums in FP64
     __shared__ float inv[32];
     FillInv(inv, v.gamma);
-    const QuadPos P = QuadStart(v);
+    const QuadPos P = QuadStart(v, blk);
     const float g = (float)v.gamma;
     const float *O = eo + P.off;
     const float *Rr = r + P.off;
@@ -300,13 +312,24 @@ __global__ void __launch_bounds__(kPairThreads)
     if (kDot == 1)
     {
         double acc[3] = {facc[0], facc[1], facc[2]};
-        GridReduce<3>(R, acc, partSlot);
+        GridReduceB<3>(R, acc, partSlot, BlkId(blk), BlkCount(blk));
     }
     else if (kDot == 2)
     {
         double acc[3] = {facc[0], facc[1], facc[2]};
-        GridReduce<3>(R, acc, (*it & 1) ? baseOdd : baseEven, 0, nullptr, partSlot);
+        GridReduceB<3>(R, acc, (*it & 1) ? baseOdd : baseEven, BlkId(blk), BlkCount(blk), 0, nullptr, partSlot);
     }
+}
+
+template <int kDot>
+__global__ void __launch_bounds__(kPairThreads)
+    k_split_half(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ r,
+                 const float *__restrict__ eo, float *__restrict__ ec, int colour, Reducer R, const int *it,
+                 int baseEven, int baseOdd, int partSlot)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitHalf<kDot>(v, du, r, eo, ec, colour, R, it, baseEven, baseOdd, partSlot, ThisBlk());
 }
 
 // the arguments of k_split_half for colour c: its halves of du and r, the other colour's and its own halves of e
@@ -342,13 +365,11 @@ void LaunchSplitHalfDot(const LevelView &v, const uint8_t *du, const float *r, f
 
 // res = r - M e on the red cells (colour 0), into the first half of `res`; the black residual after a black
 // half-sweep is zero.
-__global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, const uint8_t *__restrict__ du,
-                                                                 const float *__restrict__ r,
-                                                                 const float *__restrict__ e, float *__restrict__ res)
+__device__ __forceinline__ void SplitResidual(const LevelView &v, const uint8_t *__restrict__ du,
+                                              const float *__restrict__ r, const float *__restrict__ e,
+                                              float *__restrict__ res, const Blk &blk)
 {
-    PdlWait();
-    PdlTrigger();
-    const QuadPos P = QuadStart(v);
+    const QuadPos P = QuadStart(v, blk);
     const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
     const float *O = e + v.sHalf + P.off;
     const float *Xr = e + P.off;
@@ -377,6 +398,15 @@ __global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, co
         oM = oC;
         oC = oP;
     }
+}
+
+__global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, const uint8_t *__restrict__ du,
+                                                                 const float *__restrict__ r,
+                                                                 const float *__restrict__ e, float *__restrict__ res)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitResidual(v, du, r, e, res, ThisBlk());
 }
 
 void LaunchSplitResidual(const LevelView &v, const uint8_t *du, const float *r, const float *e, float *res,
@@ -442,19 +472,17 @@ __device__ __forceinline__ void CoarsePlaneRows(const LevelView &cv, const float
     }
 }
 
-__global__ void __launch_bounds__(kPairThreads) k_split_prolong(LevelView fv, LevelView cv,
-                                                                const uint8_t *__restrict__ pext,
-                                                                const float *__restrict__ ec, float *__restrict__ ef)
+__device__ __forceinline__ void SplitProlong(const LevelView &fv, const LevelView &cv,
+                                             const uint8_t *__restrict__ pext, const float *__restrict__ ec,
+                                             float *__restrict__ ef, const Blk &blk)
 {
-    PdlWait();
-    PdlTrigger();
     const int Q = fv.sRS >> 2, nrow = cv.Nx - 2, nq = nrow * Q;
-    int t = blockIdx.x * kPairThreads + threadIdx.x;
+    int t = blk.x * kPairThreads + threadIdx.x;
     const bool valid = t < nq;
     if (!valid) t = nq - 1;
     const int B = 1 + t / Q, m0 = 4 * (t - (B - 1) * Q);
-    const int S = (cv.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
-    const int A0 = min(1 + (int)blockIdx.y * S, cv.Ny - 1), A1 = min(A0 + S, cv.Ny - 1);
+    const int S = (cv.Ny - 2 + blk.gy - 1) / blk.gy;
+    const int A0 = min(1 + blk.y * S, cv.Ny - 1), A1 = min(A0 + S, cv.Ny - 1);
     if (!valid || A0 >= A1) return;
     float yM0[5], yM1[5], yC0[5], yC1[5], pC[5], pD[5];
     CoarsePlaneRows(cv, ec, A0 - 1, B, m0, yM0, yM1, pD);
@@ -507,8 +535,24 @@ __global__ void __launch_bounds__(kPairThreads) k_split_prolong(LevelView fv, Le
     }
 }
 
+__global__ void __launch_bounds__(kPairThreads) k_split_prolong(LevelView fv, LevelView cv,
+                                                                const uint8_t *__restrict__ pext,
+                                                                const float *__restrict__ ec, float *__restrict__ ef)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitProlong(fv, cv, pext, ec, ef, ThisBlk());
+}
+
 // The grid of k_split_prolong: threads over (coarse row, fine quad), grid.y chunks of coarse planes sized like
 // QuadGrid's (the longest march with a full last wave).
+inline dim3 ProlongGridS(const LevelView &fine, const LevelView &coarse, int S)
+{
+    const long long nq = (long long)(coarse.Nx - 2) * (fine.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
+    const long long planes = coarse.Ny - 2 > 0 ? coarse.Ny - 2 : 1;
+    return dim3((unsigned)perPlane, (unsigned)((planes + S - 1) / S));
+}
+
 inline dim3 ProlongGrid(const LevelView &fine, const LevelView &coarse, int resident)
 {
     const long long nq = (long long)(coarse.Nx - 2) * (fine.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
@@ -587,18 +631,16 @@ __device__ __forceinline__ void SplitRestrictPlane(const LevelView &fv, const ui
     for (int x = 0; x < 4; x++) X[x] *= 1.0f / 64.0f;
 }
 
-__global__ void __launch_bounds__(kPairThreads) k_split_restrict(LevelView fv, LevelView cv,
-                                                                 const uint8_t *__restrict__ pext,
-                                                                 const float *__restrict__ res, float *__restrict__ rc)
+__device__ __forceinline__ void SplitRestrictQ(const LevelView &fv, const LevelView &cv,
+                                               const uint8_t *__restrict__ pext, const float *__restrict__ res,
+                                               float *__restrict__ rc, const Blk &blk)
 {
-    PdlWait();
-    PdlTrigger();
     const int nq = (cv.Nz - 2 + 3) / 4, nt = (cv.Nx - 2) * nq;
-    const int t = blockIdx.x * kPairThreads + threadIdx.x;
+    const int t = blk.x * kPairThreads + threadIdx.x;
     if (t >= nt) return;
     const int J = 1 + t / nq, K0 = 1 + 4 * (t - (J - 1) * nq);
-    const int S = (cv.Ny - 2 + (int)gridDim.y - 1) / (int)gridDim.y;
-    const int I0 = 1 + (int)blockIdx.y * S, I1 = min(I0 + S, cv.Ny - 1);
+    const int S = (cv.Ny - 2 + blk.gy - 1) / blk.gy;
+    const int I0 = 1 + blk.y * S, I1 = min(I0 + S, cv.Ny - 1);
     if (I0 >= I1) return;
     const bool five = K0 + 3 <= cv.Nz - 2; // element K0+3 is read only for coarse cell K0+3
     float Tm2[4], Tm1[4], Xm1[4], Xd[4];
@@ -621,6 +663,15 @@ __global__ void __launch_bounds__(kPairThreads) k_split_restrict(LevelView fv, L
             Xm1[x] = X1[x];
         }
     }
+}
+
+__global__ void __launch_bounds__(kPairThreads) k_split_restrict(LevelView fv, LevelView cv,
+                                                                 const uint8_t *__restrict__ pext,
+                                                                 const float *__restrict__ res, float *__restrict__ rc)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitRestrictQ(fv, cv, pext, res, rc, ThisBlk());
 }
 
 // The same restriction with one thread per coarse cell (K along the 32 lanes, J across the 8 warps), for the smaller
@@ -646,15 +697,15 @@ __device__ __forceinline__ void SplitRestrictPlane1(const LevelView &fv, const u
     X *= 1.0f / 64.0f;
 }
 
-__global__ void __launch_bounds__(256) k_split_restrict1(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
-                                                        const float *__restrict__ res, float *__restrict__ rc)
+// bx, by: the K and J tiles; bz of gz: the chunk of coarse planes
+__device__ __forceinline__ void SplitRestrict1(const LevelView &fv, const LevelView &cv,
+                                               const uint8_t *__restrict__ pext, const float *__restrict__ res,
+                                               float *__restrict__ rc, int bx, int by, int bz, int gz)
 {
-    PdlWait();
-    PdlTrigger();
-    const int K = 1 + blockIdx.x * 32 + threadIdx.x, J = 1 + blockIdx.y * 8 + threadIdx.y;
+    const int K = 1 + bx * 32 + threadIdx.x, J = 1 + by * 8 + threadIdx.y;
     if (K > cv.Nz - 2 || J > cv.Nx - 2) return;
-    const int S = (cv.Ny - 2 + (int)gridDim.z - 1) / (int)gridDim.z;
-    const int I0 = 1 + (int)blockIdx.z * S, I1 = min(I0 + S, cv.Ny - 1);
+    const int S = (cv.Ny - 2 + gz - 1) / gz;
+    const int I0 = 1 + bz * S, I1 = min(I0 + S, cv.Ny - 1);
     if (I0 >= I1) return;
     float Tm2, Tm1, Xm1, Xdummy;
     SplitRestrictPlane1(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
@@ -671,6 +722,14 @@ __global__ void __launch_bounds__(256) k_split_restrict1(LevelView fv, LevelView
         Tm1 = T1;
         Xm1 = X1;
     }
+}
+
+__global__ void __launch_bounds__(256) k_split_restrict1(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
+                                                        const float *__restrict__ res, float *__restrict__ rc)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitRestrict1(fv, cv, pext, res, rc, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)gridDim.z);
 }
 
 // Coarse levels with at least kRestrictQuadCells cells take the quad kernel (4x fewer loads per coarse cell), the
@@ -726,13 +785,11 @@ __device__ __forceinline__ double SplitRzEff(const double *S, int base, double n
 
 // p_new = U (z - mean + beta p_old), q = M p_new, sum p_new.q, both colours at a thread's quad position.
 template <bool kSingular>
-__global__ void __launch_bounds__(kPairThreads, 4)
-    k_split_papply(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ z, float *p0, float *p1,
-                   float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd,
-                   int slotN, int slotPQ)
+__device__ __forceinline__ void SplitPApply(const LevelView &v, const uint8_t *__restrict__ du,
+                                            const float *__restrict__ z, float *p0, float *p1, float *__restrict__ q,
+                                            const Reducer &R, const double *S, const int *it, int baseEven,
+                                            int baseOdd, int slotN, int slotPQ, const Blk &blk)
 {
-    PdlWait();
-    PdlTrigger();
     const int iter = *it, par = iter & 1;
     const float *__restrict__ pIn = par ? p1 : p0;
     float *__restrict__ pOut = par ? p0 : p1;
@@ -742,7 +799,7 @@ __global__ void __launch_bounds__(kPairThreads, 4)
         iter == 0 ? 0.0 : SplitRzEff(S, baseNew, n, kSingular) / SplitRzEff(S, baseOld, n, kSingular);
     const float bt = (float)beta;
     const float mean = kSingular ? (float)(S[baseNew + 1] / n) : 0.f;
-    const QuadPos P = QuadStart(v);
+    const QuadPos P = QuadStart(v, blk);
     const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
     const long long hb = v.sHalf;
     auto pn = [&](long long base) {
@@ -812,7 +869,18 @@ __global__ void __launch_bounds__(kPairThreads, 4)
         C1 = P1;
     }
     double acc[1] = {facc};
-    GridReduce<1>(R, acc, slotPQ);
+    GridReduceB<1>(R, acc, slotPQ, BlkId(blk), BlkCount(blk));
+}
+
+template <bool kSingular>
+__global__ void __launch_bounds__(kPairThreads, 4)
+    k_split_papply(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ z, float *p0, float *p1,
+                   float *__restrict__ q, Reducer R, const double *S, const int *it, int baseEven, int baseOdd,
+                   int slotN, int slotPQ)
+{
+    PdlWait();
+    PdlTrigger();
+    SplitPApply<kSingular>(v, du, z, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, slotPQ, ThisBlk());
 }
 
 void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, float *p0, float *p1, float *q,
@@ -832,14 +900,15 @@ void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, fl
 // the FP64 side of level 0: FP64 arrays in the grid layout, the FP32 vectors colour-split
 // ---------------------------------------------------------------------------------------------------------------
 // r = sfac * b (split) and (sum b^2, sum b): the residual of a zero iterate. One thread per cell pair (k0 even).
-__global__ void __launch_bounds__(256) k_split_scale_sum(LevelView v, const double *__restrict__ b,
-                                                         float *__restrict__ r, double sfac, Reducer R, int slot)
+// bx of gx: this block among the launch's blocks (a grid-stride loop)
+__device__ __forceinline__ void SplitScaleSum(const LevelView &v, const double *__restrict__ b, float *__restrict__ r,
+                                              double sfac, const Reducer &R, int slot, int bx, int gx)
 {
     double acc[2] = {0.0, 0.0};
-    const long long pairs = v.cells >> 1, stride = (long long)gridDim.x * blockDim.x;
+    const long long pairs = v.cells >> 1, stride = (long long)gx * blockDim.x;
     const int H = v.Nz >> 1;
     const double2 *b2 = reinterpret_cast<const double2 *>(b);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < pairs; t += stride)
+    for (long long t = bx * (long long)blockDim.x + threadIdx.x; t < pairs; t += stride)
     {
         const double2 x = b2[t];
         const long long row = t / H; // i * Nx + j
@@ -852,14 +921,22 @@ __global__ void __launch_bounds__(256) k_split_scale_sum(LevelView v, const doub
         acc[0] += x.x * x.x + x.y * x.y;
         acc[1] += x.x + x.y;
     }
-    GridReduce<2>(R, acc, slot);
+    GridReduceB<2>(R, acc, slot, (unsigned)bx, (unsigned)gx);
+}
+
+constexpr int kScaleSumBlocks = 148 * 8;
+
+__global__ void __launch_bounds__(256) k_split_scale_sum(LevelView v, const double *__restrict__ b,
+                                                         float *__restrict__ r, double sfac, Reducer R, int slot)
+{
+    SplitScaleSum(v, b, r, sfac, R, slot, (int)blockIdx.x, (int)gridDim.x);
 }
 
 void LaunchSplitScaleSum(const LevelView &v, const double *b, float *r, double sfac, const Reducer &R, int slot,
                          cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_split_scale_sum<<<148 * 8, 256, 0, st>>>(v, b, r, sfac, R, slot);
+    k_split_scale_sum<<<kScaleSumBlocks, 256, 0, st>>>(v, b, r, sfac, R, slot);
 }
 
 // The FP64 refinement step on a uniform split level 0 (k_pair_refine64's, with e read and r written split):
@@ -868,12 +945,13 @@ void LaunchSplitScaleSum(const LevelView &v, const double *b, float *r, double s
 __device__ __forceinline__ double2 Ld2d(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
 // 3 resident blocks (80 registers, no spill) beat 4 with a 64-register cap that spills (measured 115 vs 122 us)
-__global__ void __launch_bounds__(kPairThreads, 3)
-    k_split_refine64(LevelView v, const uint8_t *__restrict__ du, const double *__restrict__ b,
-                     const double *__restrict__ xin, const float *__restrict__ e, double *__restrict__ xout,
-                     float *__restrict__ r, double scale, double sfac, Reducer R, int slot)
+__device__ __forceinline__ void SplitRefine64(const LevelView &v, const uint8_t *__restrict__ du,
+                                              const double *__restrict__ b, const double *__restrict__ xin,
+                                              const float *__restrict__ e, double *__restrict__ xout,
+                                              float *__restrict__ r, double scale, double sfac, const Reducer &R,
+                                              int slot, const Blk &blk)
 {
-    const PairPos P = PairStart(v);
+    const PairPos P = PairStart(v, blk.x, blk.y, blk.gy);
     const long long sb = (long long)P.i0 * v.sPS + (long long)P.j * v.sRS + (P.k0 >> 1);
     // the thread's element on plane i0 in colour 0 and colour 1
     const float *e0 = e + sb, *e1 = e + v.sHalf + sb;
@@ -920,7 +998,15 @@ __global__ void __launch_bounds__(kPairThreads, 3)
         XM = XC;
         XC = XP;
     }
-    GridReduce<2>(R, acc, slot);
+    GridReduceB<2>(R, acc, slot, BlkId(blk), BlkCount(blk));
+}
+
+__global__ void __launch_bounds__(kPairThreads, 3)
+    k_split_refine64(LevelView v, const uint8_t *__restrict__ du, const double *__restrict__ b,
+                     const double *__restrict__ xin, const float *__restrict__ e, double *__restrict__ xout,
+                     float *__restrict__ r, double scale, double sfac, Reducer R, int slot)
+{
+    SplitRefine64(v, du, b, xin, e, xout, r, scale, sfac, R, slot, ThisBlk());
 }
 
 void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
@@ -932,6 +1018,249 @@ void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b,
                                                                            slot);
 }
 
+
+// ---------------------------------------------------------------------------------------------------------------
+// batched launches (nb_batch.cu): grid z = the batch's capacity, block z runs the request at list[z] on the x, y tiles
+// of its own grid. The launches that end in a grid-wide sum keep the grid a single solve uses, so each request's sums
+// (and so its whole solve) are bit for bit the ones it gets alone; the others take the march length S the caller
+// chose (it changes which planes a thread visits, not what a cell gets).
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kPairThreads) kb_split_first(const BatchLevel *__restrict__ lv, int ls, int l,
+                                                               BatchList a)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &L = lv[q * ls + l];
+    SplitFirst(L.v, L.du, L.r, L.e, ThisBlk());
+}
+
+template <int kDot>
+__global__ void __launch_bounds__(kPairThreads)
+    kb_split_half(const BatchLevel *__restrict__ lv, int ls, int l, const BatchReq *__restrict__ rq, BatchList a,
+                  int colour, int baseEven, int baseOdd, int partSlot)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &L = lv[q * ls + l];
+    const long long h = L.v.sHalf;
+    if (kDot)
+        SplitHalf<kDot>(L.v, L.du + colour * h, L.r + colour * h, L.e + (colour ^ 1) * h, L.e + colour * h, colour,
+                        rq[q].red, rq[q].it, baseEven, baseOdd, partSlot, ThisBlk());
+    else
+        SplitHalf<kDot>(L.v, L.du + colour * h, L.r + colour * h, L.e + (colour ^ 1) * h, L.e + colour * h, colour,
+                        Reducer{}, nullptr, baseEven, baseOdd, partSlot, ThisBlk());
+}
+
+__global__ void __launch_bounds__(kPairThreads) kb_split_residual(const BatchLevel *__restrict__ lv, int ls, int l,
+                                                                  BatchList a)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &L = lv[q * ls + l];
+    SplitResidual(L.v, L.du, L.r, L.e, L.res, ThisBlk());
+}
+
+__global__ void __launch_bounds__(kPairThreads) kb_split_prolong(const BatchLevel *__restrict__ lv, int ls, int l,
+                                                                 BatchList a)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &F = lv[q * ls + l], &C = lv[q * ls + l + 1];
+    SplitProlong(F.v, C.v, F.pext, C.e, F.e, ThisBlk());
+}
+
+__global__ void __launch_bounds__(kPairThreads) kb_split_restrict(const BatchLevel *__restrict__ lv, int ls, int l,
+                                                                  BatchList a)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &F = lv[q * ls + l], &C = lv[q * ls + l + 1];
+    SplitRestrictQ(F.v, C.v, F.pext, F.res, C.r, ThisBlk());
+}
+
+// grid (K tiles, J tiles x gz plane chunks, capacity)
+__global__ void __launch_bounds__(256) kb_split_restrict1(const BatchLevel *__restrict__ lv, int ls, int l,
+                                                         BatchList a, int gyJ, int gz)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &F = lv[q * ls + l], &C = lv[q * ls + l + 1];
+    const int by = (int)blockIdx.y % gyJ, bz = (int)blockIdx.y / gyJ;
+    SplitRestrict1(F.v, C.v, F.pext, F.res, C.r, (int)blockIdx.x, by, bz, gz);
+}
+
+// form -1: every request in its own form; 0 / 1: only the requests of that form (singular = 1)
+__global__ void __launch_bounds__(kPairThreads, 4)
+    kb_split_papply(const BatchLevel *__restrict__ lv, int ls, const BatchReq *__restrict__ rq, BatchList a,
+                    int baseEven, int baseOdd, int slotN, int slotPQ, int form)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &L = lv[q * ls];
+    const BatchReq &Q = rq[q];
+    if (form >= 0 && (Q.singular != 0) != (form == 1)) return;
+    if (Q.singular)
+        SplitPApply<true>(L.v, L.du, L.e, Q.p0, Q.p1, Q.q, Q.red, Q.red.out, Q.it, baseEven, baseOdd, slotN, slotPQ,
+                          ThisBlk());
+    else
+        SplitPApply<false>(L.v, L.du, L.e, Q.p0, Q.p1, Q.q, Q.red, Q.red.out, Q.it, baseEven, baseOdd, slotN, slotPQ,
+                           ThisBlk());
+}
+
+__global__ void __launch_bounds__(256) kb_split_scale_sum(const BatchLevel *__restrict__ lv, int ls,
+                                                          const BatchReq *__restrict__ rq, BatchList a, int slot)
+{
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &L = lv[q * ls];
+    const BatchReq &Q = rq[q];
+    SplitScaleSum(L.v, Q.b, L.r, Q.sfac, Q.red, slot, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// parity[q]: this pass reads x from xin (0) or xout (1) and writes the other
+__global__ void __launch_bounds__(kPairThreads, 3)
+    kb_split_refine64(const BatchLevel *__restrict__ lv, int ls, const BatchReq *__restrict__ rq, BatchList a,
+                      const int *__restrict__ parity, int slot)
+{
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    const BatchLevel &L = lv[q * ls];
+    const BatchReq &Q = rq[q];
+    const bool odd = parity[q] & 1;
+    SplitRefine64(L.v, L.du, Q.b, odd ? Q.xout : Q.xin, Q.x, odd ? Q.xin : Q.xout, L.r, Q.scale, Q.sfac, Q.red, slot,
+                  ThisBlk());
+}
+
+namespace
+{
+inline dim3 WithZ(dim3 g, int cap)
+{
+    g.z = (unsigned)cap;
+    return g;
+}
+} // namespace
+
+// the march length a quad kernel's single launch takes on this colour-split level (the default of the batched
+// smoothing and residual launches)
+int SplitDefaultS(const LevelView &v, int kind)
+{
+    int occ = 1;
+    switch (kind)
+    {
+    case NB_BK_FIRST: occ = Occ<k_split_first>(); break;
+    case NB_BK_HALF: occ = Occ<k_split_half<0>>(); break;
+    default: occ = Occ<k_split_residual>(); break;
+    }
+    const long long planes = v.Ny - 2 > 0 ? v.Ny - 2 : 1;
+    const dim3 g = QuadGrid(v, occ);
+    return (int)((planes + g.y - 1) / g.y);
+}
+
+void LaunchBatchSplit(int kind, const LevelView &v, const LevelView *coarse, int S, int mode,
+                      const BatchLevel *lv, int ls, int l, const BatchReq *rq, BatchList a, int cap, int colour,
+                      cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    S = S < 1 ? 1 : S;
+    switch (kind)
+    {
+    case NB_BK_FIRST:
+        LaunchPdl(kb_split_first, WithZ(QuadGridS(v, S), cap), kPairThreads, 0, st, lv, ls, l, a);
+        break;
+    case NB_BK_HALF:
+        LaunchPdl(kb_split_half<0>, WithZ(QuadGridS(v, S), cap), kPairThreads, 0, st, lv, ls, l, rq, a, colour, 0, 0,
+                  0);
+        break;
+    case NB_BK_RESIDUAL:
+        LaunchPdl(kb_split_residual, WithZ(QuadGridS(v, S), cap), kPairThreads, 0, st, lv, ls, l, a);
+        break;
+    case NB_BK_PROLONG:
+        LaunchPdl(kb_split_prolong, WithZ(ProlongGridS(v, *coarse, S), cap), kPairThreads, 0, st, lv, ls, l, a);
+        break;
+    case NB_BK_RESTRICT:
+    {
+        const LevelView &c = *coarse;
+        const long long planes = c.Ny - 2 > 0 ? c.Ny - 2 : 1;
+        const int gz = (int)((planes + S - 1) / S);
+        if (mode == 1)
+        {
+            const int gx = (c.Nz - 2 + 31) / 32, gyJ = (c.Nx - 2 + 7) / 8;
+            LaunchPdl(kb_split_restrict1, dim3((unsigned)gx, (unsigned)(gyJ * gz), (unsigned)cap), dim3(32, 8), 0,
+                      st, lv, ls, l, a, gyJ, gz);
+        }
+        else
+        {
+            const long long nt = (long long)(c.Nx - 2) * ((c.Nz - 2 + 3) / 4);
+            const long long perPlane = (nt + kPairThreads - 1) / kPairThreads;
+            LaunchPdl(kb_split_restrict, dim3((unsigned)perPlane, (unsigned)gz, (unsigned)cap), kPairThreads, 0, st,
+                      lv, ls, l, a);
+        }
+        break;
+    }
+    default: break;
+    }
+}
+
+// The launches that end in a grid-wide sum, on the grids a single solve of the level uses.
+void LaunchBatchSplitHalfDot(const LevelView &v, const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a,
+                             int cap, int colour, bool last, int baseEven, int baseOdd, int partSlot, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    if (last)
+        LaunchPdl(kb_split_half<2>, WithZ(QuadGrid(v, Occ<k_split_half<2>>()), cap), kPairThreads, 0, st, lv, ls, 0,
+                  rq, a, colour, baseEven, baseOdd, partSlot);
+    else
+        LaunchPdl(kb_split_half<1>, WithZ(QuadGrid(v, Occ<k_split_half<1>>()), cap), kPairThreads, 0, st, lv, ls, 0,
+                  rq, a, colour, baseEven, baseOdd, partSlot);
+}
+
+void LaunchBatchSplitPApply(const LevelView &v, const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a,
+                            int cap, int baseEven, int baseOdd, int slotN, int slotPQ, cudaStream_t st)
+{
+    // a single solve launches its form (singular or not) on that form's grid; both have the same occupancy unless
+    // the compiler gave them different register counts, and then each form gets a launch on its own grid
+    const dim3 gs = QuadGrid(v, Occ<k_split_papply<true>>()), gn = QuadGrid(v, Occ<k_split_papply<false>>());
+    if (gs.x == gn.x && gs.y == gn.y)
+    {
+        NB_COUNT_LAUNCH();
+        LaunchPdl(kb_split_papply, WithZ(gn, cap), kPairThreads, 0, st, lv, ls, rq, a, baseEven, baseOdd, slotN,
+                  slotPQ, -1);
+        return;
+    }
+    NB_COUNT_LAUNCHES(2);
+    LaunchPdl(kb_split_papply, WithZ(gn, cap), kPairThreads, 0, st, lv, ls, rq, a, baseEven, baseOdd, slotN, slotPQ,
+              0);
+    LaunchPdl(kb_split_papply, WithZ(gs, cap), kPairThreads, 0, st, lv, ls, rq, a, baseEven, baseOdd, slotN, slotPQ,
+              1);
+}
+
+void LaunchBatchSplitScaleSum(const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a, int cap, int slot,
+                              cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    kb_split_scale_sum<<<dim3(kScaleSumBlocks, 1, cap), 256, 0, st>>>(lv, ls, rq, a, slot);
+}
+
+void LaunchBatchSplitRefine64(const LevelView &v, const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a,
+                              int cap, const int *parity, int slot, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    kb_split_refine64<<<WithZ(PairGrid(v, kSplitReduceS), cap), kPairThreads, 0, st>>>(lv, ls, rq, a, parity, slot);
+}
 
 // The occupancy of every split kernel, read outside any stream capture (the launchers size their grids from it).
 void PrepareSplitKernels()

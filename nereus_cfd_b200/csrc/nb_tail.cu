@@ -14,6 +14,8 @@
 //   between their phases instead of a block-wide barrier.
 #include "nb_kernels.h"
 
+#include <cstring>
+
 namespace nb
 {
 
@@ -329,10 +331,8 @@ template <typename T, bool kWarp> __device__ void TUp(const SmemLevel<T> &F, con
     }
 }
 
-template <typename T> __global__ void __launch_bounds__(kTailThreads) k_tail(TailArgs<T> A)
+template <typename T> __device__ __forceinline__ void TailBody(const TailArgs<T> &A)
 {
-    PdlWait();
-    PdlTrigger();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double sInv[kMaxTailLevels][32];
     __shared__ int sCount[kMaxTailLevels][2];
@@ -418,6 +418,33 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_tail(Tai
     for (long long c = threadIdx.x; c < A.lv[0].v.cells; c += blockDim.x) A.eOut[c] = F0.e[c];
 }
 
+template <typename T> __global__ void __launch_bounds__(kTailThreads) k_tail(TailArgs<T> A)
+{
+    PdlWait();
+    PdlTrigger();
+    TailBody<T>(A);
+}
+
+// batched (nb_batch.cu): block z runs the coarse end of the request at list[z], its arguments copied from global
+// memory into shared memory first
+__global__ void __launch_bounds__(kTailThreads) kb_tail(const BatchReq *__restrict__ rq, BatchList a)
+{
+    PdlWait();
+    PdlTrigger();
+    const int q = BatchReqOf(a);
+    if (q < 0) return;
+    __shared__ TailArgs<float> sA;
+    const TailArgs<float> *g = static_cast<const TailArgs<float> *>(rq[q].tail);
+    {
+        const int n = (int)(sizeof(TailArgs<float>) / sizeof(int));
+        const int *src = reinterpret_cast<const int *>(g);
+        int *dst = reinterpret_cast<int *>(&sA);
+        for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+    }
+    __syncthreads();
+    TailBody<float>(sA);
+}
+
 // The per-colour lists of every tail level's unknowns, once per layout: entries packed (i << 20 | j << 10 | k), red
 // ones from the front of the level's segment, black ones from the back; their order within a colour does not matter
 // (the cells of one colour are updated independently).
@@ -480,8 +507,45 @@ template <typename T> size_t TailSmemBytes(const LevelView *levels, int nlev)
 template <typename T> bool PrepareTail(size_t bytes)
 {
     if (bytes > kTailMaxSmem) return false;
+    if (sizeof(T) == 4 &&
+        cudaFuncSetAttribute(kb_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTailMaxSmem) != cudaSuccess)
+        return false;
     return cudaFuncSetAttribute(k_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTailMaxSmem) ==
            cudaSuccess;
+}
+
+// The coarse end's arguments of one request (FP32), for a batch's table in device memory: *bytes = their size,
+// and when out is not null they are written there; *smem = the dynamic shared memory of its launch.
+void TailArgsFor(const LevelView *levels, int nlev, const float *rIn, float *eOut, int pre, int post,
+                 int coarseSweeps, const unsigned *lists, const int *counts, void *out, size_t *bytes, size_t *smem)
+{
+    TailArgs<float> A{};
+    unsigned off = 0, listOff = 0;
+    for (int l = 0; l < nlev; l++)
+    {
+        A.lv[l].v = levels[l];
+        A.lv[l].off = off;
+        A.lv[l].listOff = listOff;
+        off += LevelBytes<float>(levels[l].cells);
+        listOff += (unsigned)levels[l].cells;
+    }
+    A.nlev = nlev;
+    A.rIn = rIn;
+    A.eOut = eOut;
+    A.pre = pre < 1 ? 1 : pre;
+    A.post = post < 1 ? 1 : post;
+    A.coarseSweeps = coarseSweeps < 1 ? 1 : coarseSweeps;
+    A.lists = lists;
+    A.counts = counts;
+    *bytes = sizeof(A);
+    *smem = off;
+    if (out) std::memcpy(out, &A, sizeof(A));
+}
+
+void LaunchBatchTail(const BatchReq *rq, BatchList a, int cap, size_t smem, cudaStream_t st)
+{
+    NB_COUNT_LAUNCH();
+    LaunchPdl(kb_tail, dim3(1, 1, cap), dim3(kTailThreads), smem, st, rq, a);
 }
 
 template <typename T>

@@ -96,6 +96,88 @@ def plan(costs: Sequence[float], k: int) -> List[int]:
     return [out[i] for i in range(n)]
 
 
+class Batch:
+    """nereus_b200_batch_*: one pressure step for each of up to ``capacity`` grids of the same shape, advanced by
+    the same launches (mixed precision, uniform 3D). Slot i takes jobs[i]; a slot keeps its hierarchy while its
+    layout bytes are unchanged. Each job's result is bit for bit its solo solve's."""
+
+    def __init__(self, capacity: int, device: int = 0, stream: Optional[int] = None, **solver_options):
+        self.lib = capi.load()
+        self.opts = capi.default_options(device=device, precision=capi.PRECISION_MIXED, **solver_options)
+        if stream is not None:
+            self.opts.stream = ctypes.c_void_p(stream)
+        self.capacity = capacity
+        self.h = ctypes.c_void_p()
+        capi.check(self.lib.nereus_b200_batch_create(ctypes.byref(self.h), ctypes.byref(self.opts), capacity))
+        self._tables = {}
+
+    def set_layout(self, slot: int, grid: MACGrid):
+        g = grid.grid
+        widths = [np.ascontiguousarray(w) for w in g.width_tables()]
+        gaps = [np.ascontiguousarray(x) for x in g.gap_tables()]
+        types = np.ascontiguousarray(grid.types, dtype=np.uint8)
+        self._tables[slot] = (widths, gaps, types)
+        W = (capi._dp * 3)(*[capi.ptr(a) for a in widths])
+        G = (capi._dp * 3)(*[capi.ptr(a) for a in gaps])
+        capi.check(self.lib.nereus_b200_batch_set_layout(self.h, slot, g.dim, g.Nx, g.Ny, g.Nz,
+                                                         capi.ptr(types, capi._u8), W, G, int(g.nonuniform), g.dh))
+
+    def items(self, jobs: Sequence[Job]):
+        arr = (capi.BatchItem * len(jobs))()
+        for i, j in enumerate(jobs):
+            f = j.device_fields
+            arr[i].u, arr[i].v, arr[i].w, arr[i].p = (f[k].data_ptr() for k in ("u", "v", "w", "p"))
+            arr[i].rho, arr[i].dt = j.grid.rho, j.grid.dt
+            arr[i].needs_compat = int(j.needs_compat)
+            arr[i].tol = j.tol
+        return arr
+
+    def project(self, jobs: Sequence[Job], items=None, allow=(capi.NB_OK, capi.NB_NOT_CONVERGED)):
+        """The step of jobs[0 .. n-1] in slots 0 .. n-1 (their layouts set), fields on the device, in place."""
+        n = len(jobs)
+        res = (capi.Result * n)()
+        items = self.items(jobs) if items is None else items
+        capi.check(self.lib.nereus_b200_batch_project_device(self.h, n, items, res), allow=allow)
+        for j, r in zip(jobs, res):
+            j.result = r.as_dict()
+            j.status = r.status
+        return [r.as_dict() for r in res]
+
+    def info(self) -> dict:
+        i = capi.BatchInfo()
+        capi.check(self.lib.nereus_b200_batch_info(self.h, ctypes.byref(i)))
+        return i.as_dict()
+
+    def close(self):
+        if self.h:
+            self.lib.nereus_b200_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tune_cache_dump() -> str:
+    lib = capi.load()
+    n = lib.nereus_b200_tune_cache_dump(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.nereus_b200_tune_cache_dump(buf, n + 1)
+    return buf.value.decode()
+
+
+def tune_cache_load(text: str) -> int:
+    return capi.check(capi.load().nereus_b200_tune_cache_load(text.encode()), allow=range(0, 1 << 30))
+
+
 class Server:
     """nereus_b200_server_*: submit jobs, poll or wait for them, read the server's statistics."""
 
