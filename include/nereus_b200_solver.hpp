@@ -211,4 +211,41 @@ class BoundaryReplay
     nb_bc *bc_ = nullptr;
 };
 
+// Many pressure systems of one grid shape stepped together (nereus_b200_batch_*): where the reference makes one
+// SolvePressureSystem call per system (src/Methods/PPESolver/PressureSettings.h:578-624), slot i of a batch holds
+// system i's layout and one Project call runs the Chorin step of slots 0 .. n-1 on their device fields. Each system's
+// result is bit for bit the one a PressureSolver with the same options gives it alone.
+class BatchSolver
+{
+  public:
+    explicit BatchSolver(int capacity, int device = 0, bool autotune = true)
+    {
+        nb_options o;
+        nereus_b200_default_options(&o);
+        o.device = device;
+        o.autotune = autotune ? 1 : 0;
+        const int st = nereus_b200_batch_create(&b_, &o, capacity);
+        if (st != NB_OK) throw Error(st, nereus_b200_last_error());
+    }
+    ~BatchSolver() { nereus_b200_batch_destroy(b_); }
+    BatchSolver(const BatchSolver &) = delete;
+    BatchSolver &operator=(const BatchSolver &) = delete;
+
+    // the layout of slot i (unchanged bytes keep its hierarchy, as PressureLayoutChanged)
+    void SetLayout(int slot, const GridView &g)
+    {
+        Check(nereus_b200_batch_set_layout(b_, slot, g.dim, g.Nx, g.Ny, g.Nz, g.cellTypes, g.width, g.gap,
+                                           g.nonUniform ? 1 : 0, g.dh));
+    }
+    // the step of slots 0 .. items.size()-1; results[i] is slot i's report
+    void Project(const std::vector<nb_batch_item> &items, std::vector<nb_result> &results)
+    {
+        results.assign(items.size(), nb_result{});
+        Check(nereus_b200_batch_project_device(b_, (int)items.size(), items.data(), results.data()));
+    }
+
+  private:
+    nb_batch *b_ = nullptr;
+};
+
 } // namespace nereus_b200
