@@ -325,6 +325,7 @@ def run_b200(args, rank, world, dist):
         s.DestroyPressureSolver()
 
     stretched = run_stretched(args, dev) if args.stretched_steps > 0 and world == 1 else None
+    box2d = run_box2d(args, dev) if args.box2d_steps > 0 and world == 1 else None
     tanks = run_tanks(args, rank, world, dist, dev) if args.tanks > 0 else None
     trace = run_trace(args, dev) if args.trace > 0 and world == 1 else None
     relabel = None
@@ -346,17 +347,18 @@ def run_b200(args, rank, world, dist):
         "latency_ms": {"p50": round(percentile(lat, 0.5), 3), "p99": round(percentile(lat, 0.99), 3)},
         "solve": {k: mixed_res[k] for k in ("iters_outer", "iters_inner", "rel_res", "max_div", "status")},
         "parity": parity, "fp64_plain": fp64, "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": int(launches),
-        "stretched_cylinder": stretched, "batched_tanks": tanks, "serving_trace": trace, "flip_relabel": relabel,
+        "stretched_cylinder": stretched, "closed_box_2d": box2d, "batched_tanks": tanks, "serving_trace": trace, "flip_relabel": relabel,
     }
     return out
 
 
 def run_trace(args, dev):
-    """The served form: `trace` requests of mixed dimension (3D side log-U[32, 256], 2D side log-U[64, 1024]), mask
-    (closed, obstacle + outlet, free surface) and spacing (uniform, 1.04-stretched), fields drawn on the device, each
-    to 1e-8. A closed loop (all submitted at once) gives the capacity; Poisson arrivals at 0.5x and 0.9x of it give
-    p50/p99 latency from arrival to completion; the first `trace_fp64` requests are also solved one at a time in plain
-    FP64 on the device (the one-at-a-time path)."""
+    """The served form (cfg5): `trace` requests of mixed dimension (3D side log-U[32, 256], 2D side log-U[64, 1024]),
+    mask (closed, obstacle + outlet, free surface) and spacing (uniform, 1.04-stretched), fields drawn on the device
+    just before use (a bounded number ahead, so the trace's memory stays bounded), each to 1e-8 through the server.
+    A closed loop (16 requests in flight) gives the capacity; Poisson arrivals at each fraction of it in
+    `trace_rates` give p50/p99 latency (the middle rate twice, for its run-to-run spread). The same requests one at a
+    time in plain FP64 on one context (the single-solve form) are the comparison; host wall clock throughout."""
     import torch
 
     from nereus_cfd_b200 import capi, serving
@@ -364,25 +366,27 @@ def run_trace(args, dev):
 
     rng = np.random.default_rng(5)
     cases = [serving.trace_case(rng, i) for i in range(args.trace)]
-    fresh = lambda cs: [serving.device_job(c, dev, TOL) for c in cs]
+    rates = [float(x) for x in args.trace_rates.split(",") if x]
     out = {"requests": len(cases), "slots_per_device": args.slots, "hbm_budget_gb": 150.0,
            "mix": {"3d": sum(c.grid.dim == 3 for c in cases), "2d": sum(c.grid.dim == 2 for c in cases),
                    "stretched": sum(c.grid.nonuniform for c in cases)}}
+    biggest = sorted(cases, key=lambda c: -c.grid.cells)[: args.slots]
     with serving.Server(devices=(dev,), slots_per_device=args.slots, hbm_budget_gb=150.0, **args.solver_opts) as srv:
         # warm-up: the largest requests first, so that every slot's device arrays hold the trace's biggest shapes
-        biggest = sorted(cases, key=lambda c: -c.grid.cells)[: args.slots]
-        serving.serve_jobs(fresh(biggest), srv)
-        closed = serving.serve_jobs(fresh(cases), srv)
-        cap = closed["completed"] / closed["seconds"]
-        out["closed_loop"] = {"solves_per_s": round(cap, 3), "seconds": round(closed["seconds"], 4),
-                              "p50_ms": round(closed["p50_ms"], 3), "p99_ms": round(closed["p99_ms"], 3)}
-        out["poisson"] = [serving.run_trace(srv, fresh(cases), f * cap, seed=11 + k)
-                          for k, f in enumerate((0.5, 0.9))]
-        # the first `trace_fp64` requests served again (the server as warmed above) ...
-        k = min(args.trace_fp64, len(cases))
-        same = serving.serve_jobs(fresh(cases[:k]), srv)
-    # ... and one at a time in plain FP64, its context warmed the same way (on the largest request first)
-    sample = fresh(cases[:k])
+        serving.serve_jobs([serving.device_job(c, dev, TOL) for c in biggest], srv)
+        closed = serving.stream_serve(srv, cases, dev, TOL, rate=None, inflight=2 * args.slots)
+        cap = closed["solves_per_s"]
+        out["closed_loop"] = closed
+        out["poisson"] = [serving.stream_serve(srv, cases, dev, TOL, rate=f * cap, seed=11 + k)
+                          for k, f in enumerate(rates)]
+        if rates:
+            m = len(rates) // 2
+            again = serving.stream_serve(srv, cases, dev, TOL, rate=rates[m] * cap, seed=11 + m)
+            first = out["poisson"][m]
+            out["poisson_repeat"] = again
+            out["repeat_spread"] = {q: round(abs(again[q] - first[q]) / max(first[q], 1e-9), 3)
+                                    for q in ("p50_ms", "p99_ms")}
+    # one at a time in plain FP64 on one context, the same requests made the same way, warmed on the largest
     s = PressureSolver("fp64", device=dev, **args.solver_opts)
     lib = capi.load()
 
@@ -392,54 +396,57 @@ def run_trace(args, dev):
         capi.check(lib.nereus_b200_project_device(s.ctx, f["u"].data_ptr(), f["v"].data_ptr(), f["w"].data_ptr(),
                                                   f["p"].data_ptr(), j.grid.rho, j.grid.dt, int(j.needs_compat), TOL,
                                                   ctypes.byref(res)), allow=(0, 1))
+        torch.cuda.synchronize()
+        j.device_fields = None
 
-    warm = fresh([max(cases[:k], key=lambda c: c.grid.cells)])[0]
+    warm = serving.device_job(biggest[0], dev, TOL)
     s.InitializePressureSolver(warm.grid)
     one(warm)
-    torch.cuda.synchronize()
+    stream = serving.JobStream(cases, dev, TOL)
     t0 = time.perf_counter()
-    for j in sample:
+    for j in stream:
         one(j)
-    torch.cuda.synchronize()
-    fp64_rate = k / (time.perf_counter() - t0)
+    fp64_sec = time.perf_counter() - t0
     s.DestroyPressureSolver()
-    out["fp64_one_at_a_time"] = {"value": round(fp64_rate, 3), "unit": "solves/s", "requests": k}
-    out["served_same_requests"] = {"value": round(same["completed"] / same["seconds"], 3), "unit": "solves/s",
-                                   "requests": k}
-    out["speedup_over_fp64_one_at_a_time"] = round(same["completed"] / same["seconds"] / fp64_rate, 3)
-    out["timing"] = "host wall clock; latency from submission (arrival) to completion"
+    fp64_rate = len(cases) / fp64_sec
+    out["fp64_one_at_a_time"] = {"value": round(fp64_rate, 3), "unit": "solves/s", "requests": len(cases),
+                                 "seconds": round(fp64_sec, 3), "make_seconds": round(stream.make_seconds, 3)}
+    out["speedup_over_fp64_one_at_a_time"] = round(cap / fp64_rate, 3)
+    out["timing"] = ("host wall clock; latency from submission to completion (and from the arrival time under "
+                     "Poisson arrivals); fields made on the device by a producer thread a bounded number ahead")
     return out
 
 
-def run_stretched(args, dev):
-    """The stretched workload: 192x128x128 on [0,2.2]x[0,0.41]^2, widths x 1.04 per cell away from a 24-cell band
-    at x = 0.5, a solid cylinder along z, inflow at x = 0, p = 0 outlet at x = 2.2, seeded N(0,1) faces; mixed and
-    plain FP64 to 1e-8, fields device-resident and restored each step, CUDA events."""
+def run_case_leg(args, dev, case, tol, compat, steps, name):
+    """One workload solved again and again, mixed and plain FP64, fields device-resident and restored from a copy
+    each step (inside the timed step), CUDA events around each step after three warm-up steps."""
     import torch
 
-    from nereus_cfd_b200 import capi, workloads as W
+    from nereus_cfd_b200 import capi
     from nereus_cfd_b200.pressure import MACGrid, PressureSolver
 
     lib = capi.load()
-    case = W.stretched_cylinder_3d(192, 128, 128, seed=3)
     types = capi.label_cells(case.grid, case.scene)
-    u, v, w = W.face_velocities(case.grid, types, case.seed)
+    from nereus_cfd_b200 import workloads as W
+
+    u, v, w = W.face_velocities(case.grid, types, case.seed, case.velocity_rule, case.fp32_velocity)
     td = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to("cuda")
-    orig = [td(u), td(v), td(w), torch.zeros(case.grid.cells, dtype=torch.float64, device="cuda")]
+    wz = w if case.grid.dim == 3 else np.zeros(1)
+    orig = [td(u), td(v), td(wz), torch.zeros(case.grid.cells, dtype=torch.float64, device="cuda")]
     work = [t.clone() for t in orig]
-    out = {"workload": "stretched_cylinder_192x128x128", "unknowns": None}
+    out = {"workload": name, "unknowns": None, "tol": tol}
     for prec in ("mixed", "fp64"):
         s = PressureSolver(prec, device=dev, **args.solver_opts)
-        s.InitializePressureSolver(MACGrid.from_case(case, types, u, v, w))
+        s.InitializePressureSolver(MACGrid.from_case(case, types, u, v, wz))
         res = capi.Result()
         evs = []
-        for k in range(3 + args.stretched_steps):
+        for k in range(3 + steps):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             for x, y in zip(work, orig):
                 x.copy_(y)
-            capi.check(lib.nereus_b200_project_device(s.ctx, *[t.data_ptr() for t in work], case.rho, case.dt, 0,
-                                                      TOL, ctypes.byref(res)), allow=(0, 1))
+            capi.check(lib.nereus_b200_project_device(s.ctx, *[t.data_ptr() for t in work], case.rho, case.dt,
+                                                      int(compat), tol, ctypes.byref(res)), allow=(0, 1))
             b.record()
             if k >= 3:
                 evs.append((a, b))
@@ -447,11 +454,30 @@ def run_stretched(args, dev):
         ms = [a.elapsed_time(b) for a, b in evs]
         out[prec] = {"value": round(1e3 / statistics.mean(ms), 3), "unit": "solves/s",
                      "p50_ms": round(percentile(ms, 0.5), 3), "iters_inner": res.iters_inner,
-                     "iters_outer": res.iters_outer, "rel_res": res.rel_res, "steps": len(ms)}
+                     "iters_outer": res.iters_outer, "rel_res": res.rel_res, "max_div": res.max_div,
+                     "status": res.status, "steps": len(ms)}
         out["unknowns"] = res.n
         s.DestroyPressureSolver()
     out["speedup_mixed_over_fp64"] = round(out["mixed"]["value"] / out["fp64"]["value"], 3)
     return out
+
+
+def run_stretched(args, dev):
+    """The stretched workload (cfg3): 192x128x128 on [0,2.2]x[0,0.41]^2, widths x 1.04 per cell away from a 24-cell
+    band at x = 0.5, a solid cylinder along z, inflow at x = 0, p = 0 outlet at x = 2.2, seeded N(0,1) faces; mixed
+    and plain FP64 to 1e-8."""
+    from nereus_cfd_b200 import workloads as W
+
+    return run_case_leg(args, dev, W.stretched_cylinder_3d(192, 128, 128, seed=3), TOL, False, args.stretched_steps,
+                        "stretched_cylinder_192x128x128")
+
+
+def run_box2d(args, dev):
+    """The 2D closed box (cfg1): 128^2 uniform on the unit square, all fluid, no-slip walls (all-Neumann, the
+    compatibility condition on), seeded N(0,1) faces; mixed and plain FP64 to 1e-10."""
+    from nereus_cfd_b200 import workloads as W
+
+    return run_case_leg(args, dev, W.closed_box_2d(128, seed=1), 1e-10, True, args.box2d_steps, "closed_box_2d_128")
 
 
 def run_relabel(args, dev):
@@ -815,9 +841,11 @@ def main():
     ap.add_argument("--tank-size", type=int, default=128)
     ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device of the serving trace")
     ap.add_argument("--tank-steps", type=int, default=5, help="batched steps at least (the timed region >= 1 s)")
-    ap.add_argument("--trace", type=int, default=200, help="requests of the serving trace (0: skip)")
+    ap.add_argument("--trace", type=int, default=2000, help="requests of the serving trace (0: skip)")
+    ap.add_argument("--trace-rates", default="0.4,0.6,0.8,1.0",
+                    help="Poisson arrival rates of the trace as fractions of the closed-loop capacity")
     ap.add_argument("--stretched-steps", type=int, default=5, help="steps of the stretched workload (0: skip)")
-    ap.add_argument("--trace-fp64", type=int, default=40, help="trace requests solved one at a time in plain FP64")
+    ap.add_argument("--box2d-steps", type=int, default=10, help="steps of the 2D 128^2 closed box (0: skip)")
     ap.add_argument("--relabel-steps", type=int, default=10, help="timed steps of FLIP's re-labelling (0: skip)")
     ap.add_argument("--relabel-size", type=int, default=256)
     args = ap.parse_args()

@@ -81,6 +81,9 @@ typedef struct nb_options
     int autotune;        /* batches: 1 (default): the launch shapes of the smoothing, residual and transfer kernels
                             are timed on the batch's first step and the fastest kept (cached per grid, level, kernel
                             and capacity); 0: the shapes a single solve takes. Neither changes a result */
+    int skip_idle_tiles; /* 1 (default): on colour-split levels a block whose cells hold no unknown (the air of a
+                            free-surface tank, a solid) skips its loads and stores; 0: every block works. Both give the
+                            same result */
 } nb_options;
 
 typedef struct nb_result

@@ -30,7 +30,7 @@ class Options(ctypes.Structure):
                 ("post_sweeps", ctypes.c_int), ("coarse_sweeps", ctypes.c_int), ("max_levels", ctypes.c_int),
                 ("stream", ctypes.c_void_p), ("use_graphs", ctypes.c_int), ("transfer_kernels", ctypes.c_int),
                 ("pair_kernels", ctypes.c_int), ("tail_cells", ctypes.c_int), ("stretched_sweeps", ctypes.c_int),
-                ("autotune", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("skip_idle_tiles", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):

@@ -43,6 +43,7 @@ void nereus_b200_default_options(nb_options *o)
     o->tail_cells = 2048;
     o->stretched_sweeps = 2;
     o->autotune = 1;
+    o->skip_idle_tiles = 1;
 }
 
 const char *nereus_b200_last_error(void) { return g_error.c_str(); }

@@ -46,6 +46,11 @@ struct LevelView
     // hold the Nz/2 cells of that colour, padded with zeros to a multiple of 4.
     int sRS, sPS;
     long long sHalf;
+    // Colour-split level: act[i * actTiles + t] != 0 when tile t of plane i (elements 1024 t .. 1024 t + 1023 of
+    // either colour's plane, the cells one block of a quad kernel owns on that plane) holds an unknown; null: every
+    // tile counts as holding one. A block whose planes' tiles hold none skips its work: its cells stay zero.
+    const uint8_t *act;
+    int actTiles;
 };
 
 // Index of cell (i, j, k) in a level vector of the level's layout.

@@ -126,6 +126,10 @@ void LaunchSplitPApply(const LevelView &v, const uint8_t *du, const float *z, fl
                        int singular, int slotPQ, cudaStream_t st);
 void LaunchSplitScaleSum(const LevelView &v, const double *b, float *r, double sfac, const Reducer &R, int slot,
                          cudaStream_t st);
+// the tiles of a plane of a colour-split level (1024 elements each, the cells one quad-kernel block owns), and the
+// activity bytes of every (plane, tile): nonzero where a tile holds an unknown of either colour (LevelView::act)
+int SplitActivityTiles(const LevelView &v);
+void LaunchSplitActivity(const LevelView &v, const uint8_t *du, uint8_t *act, int tiles, cudaStream_t st);
 // the batched forms (nb_batch.cu): kind NB_BK_*; S the march length of the non-reducing kernels; coarse: the next
 // coarser level (restriction, prolongation); mode: the restriction's kernel (1 per coarse cell, else per 4)
 enum : int { NB_BK_FIRST = 0, NB_BK_HALF, NB_BK_RESIDUAL, NB_BK_RESTRICT, NB_BK_PROLONG, NB_BK_COUNT };

@@ -57,6 +57,8 @@ LevelView LevelData::view() const
     v.sRS = sRS;
     v.sPS = sPS;
     v.sHalf = sHalf;
+    v.act = sRS && actTiles ? act.p : nullptr;
+    v.actTiles = sRS ? actTiles : 0;
     v.stretched = stretched ? 1 : 0;
     v.gamma = gamma;
     for (int a = 0; a < 3; a++)
@@ -241,6 +243,17 @@ void Context::BuildPairData()
                 Lv.du.alloc((size_t)(2 * Lv.sHalf));
                 Lv.du.zero(st); // the padding
                 LaunchBuildDu(v, Lv.du.p, st);
+                if (opt.skip_idle_tiles)
+                {
+                    Lv.actTiles = SplitActivityTiles(v);
+                    Lv.act.alloc((size_t)Lv.Ny * Lv.actTiles);
+                    LaunchSplitActivity(v, Lv.du.p, Lv.act.p, Lv.actTiles, st);
+                }
+                else
+                {
+                    Lv.actTiles = 0;
+                    Lv.act.release();
+                }
             }
             else
             {

@@ -105,6 +105,8 @@ struct LevelData
                                           // Colour-split level: in that layout, and the codes on a stretched level
     DevArray<uint8_t> pext;               // unknown flag + moved prolongation weight toward the next coarser level
                                           // (colour-split level: the red cells only)
+    DevArray<uint8_t> act;                // colour-split level: which (plane, tile) holds an unknown (LevelView::act)
+    int actTiles = 0;
     // the colour-split layout of the FP32 vectors (nb_split.cu); sRS = 0: the grid layout
     int sRS = 0, sPS = 0;
     long long sHalf = 0;

@@ -89,6 +89,16 @@ __device__ __forceinline__ QuadPos QuadStart(const LevelView &v, const Blk &b)
     return p;
 }
 
+// True when no tile this block owns on planes [i0, i1) holds an unknown (LevelView::act): the block's cells are
+// all zero in every vector and stay so, so it has nothing to compute, load or store.
+__device__ __forceinline__ bool TileIdle(const LevelView &v, int bx, int i0, int i1)
+{
+    if (!v.act) return false;
+    for (int i = i0; i < i1; i++)
+        if (v.act[(long long)i * v.actTiles + bx]) return false;
+    return true;
+}
+
 // Resident blocks of a kernel per SM at kPairThreads threads (its registers and shared memory decide), and the SM
 // count of the current device.
 inline int ResidentBlocks(const void *fn)
@@ -188,6 +198,7 @@ __device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__
     __shared__ float inv[32];
     FillInv(inv, v.gamma);
     const QuadPos P = QuadStart(v, blk);
+    if (TileIdle(v, blk.x, P.i0, P.i1)) return;
     const float g = (float)v.gamma;
     const long long hb = v.sHalf;
     const float *R0 = r + P.off, *R1 = r + hb + P.off;
@@ -250,7 +261,12 @@ __device__ __forceinline__ void SplitHalf(const LevelView &v, const uint8_t *__r
     float facc[3] = {0.f, 0.f, 0.f}; // a thread's terms in FP32, the block and grid sums in FP64
     __shared__ float inv[32];
     FillInv(inv, v.gamma);
-    const QuadPos P = QuadStart(v, blk);
+    QuadPos P = QuadStart(v, blk);
+    if (TileIdle(v, blk.x, P.i0, P.i1))
+    {
+        if (!kDot) return;
+        P.i1 = P.i0; // nothing to sweep; the block still adds its zero terms to the sums
+    }
     const float g = (float)v.gamma;
     const float *O = eo + P.off;
     const float *Rr = r + P.off;
@@ -370,6 +386,7 @@ __device__ __forceinline__ void SplitResidual(const LevelView &v, const uint8_t 
                                               float *__restrict__ res, const Blk &blk)
 {
     const QuadPos P = QuadStart(v, blk);
+    if (TileIdle(v, blk.x, P.i0, P.i1)) return;
     const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
     const float *O = e + v.sHalf + P.off;
     const float *Xr = e + P.off;
@@ -800,6 +817,12 @@ __device__ __forceinline__ void SplitPApply(const LevelView &v, const uint8_t *_
     const float bt = (float)beta;
     const float mean = kSingular ? (float)(S[baseNew + 1] / n) : 0.f;
     const QuadPos P = QuadStart(v, blk);
+    if (TileIdle(v, blk.x, P.i0, P.i1))
+    {
+        double zero[1] = {0.0}; // p and q stay zero on these cells; the block adds its zero term to p.q
+        GridReduceB<1>(R, zero, slotPQ, BlkId(blk), BlkCount(blk));
+        return;
+    }
     const float g = (float)v.gamma, hg = 0.5f * (float)v.gamma;
     const long long hb = v.sHalf;
     auto pn = [&](long long base) {
@@ -1260,6 +1283,36 @@ void LaunchBatchSplitRefine64(const LevelView &v, const BatchLevel *lv, int ls, 
 {
     NB_COUNT_LAUNCH();
     kb_split_refine64<<<WithZ(PairGrid(v, kSplitReduceS), cap), kPairThreads, 0, st>>>(lv, ls, rq, a, parity, slot);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// tile activity: one thread per (plane, tile), ORing the unknown bits of the tile's diagonal bytes in both colours
+// ---------------------------------------------------------------------------------------------------------------
+constexpr int kTileElems = 4 * kPairThreads;
+
+int SplitActivityTiles(const LevelView &v) { return (v.sPS + kTileElems - 1) / kTileElems; }
+
+__global__ void __launch_bounds__(256) k_split_activity(LevelView v, const uint8_t *__restrict__ du,
+                                                        uint8_t *__restrict__ act, int tiles)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)v.Ny * tiles) return;
+    const int i = (int)(t / tiles), tile = (int)(t - (long long)i * tiles);
+    const int e0 = tile * kTileElems, e1 = min(e0 + kTileElems, v.sPS);
+    unsigned any = 0;
+    for (int c = 0; c < 2; c++)
+    {
+        const uint8_t *row = du + (long long)c * v.sHalf + (long long)i * v.sPS;
+        for (int e = e0; e < e1; e += 4) any |= LdU4(row + e); // sPS and e0 are multiples of 4
+    }
+    act[t] = (any & 0x80808080u) ? 1 : 0;
+}
+
+void LaunchSplitActivity(const LevelView &v, const uint8_t *du, uint8_t *act, int tiles, cudaStream_t st)
+{
+    const long long n = (long long)v.Ny * tiles;
+    NB_COUNT_LAUNCH();
+    k_split_activity<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(v, du, act, tiles);
 }
 
 // The occupancy of every split kernel, read outside any stream capture (the launchers size their grids from it).

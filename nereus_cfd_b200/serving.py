@@ -404,7 +404,119 @@ def device_job(case, device: int = 0, tol: float = 1e-8) -> Job:
     m = MACGrid(g, types, np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0), case.rho, case.dt)
     job = Job(m, tol=tol, needs_compat=case.needs_compat)
     job.device_fields = fields
+    torch.cuda.current_stream(d).synchronize()  # the fields are written before any slot's stream reads them
     return job
+
+
+class JobStream:
+    """The device jobs of a list of cases, made by a background thread a bounded number ahead of use (so a long
+    trace never holds more than `ahead` unsubmitted requests' fields on the device). Iterate to take them in order."""
+
+    def __init__(self, cases: Sequence, device: int = 0, tol: float = 1e-8, ahead: int = 16):
+        import queue
+        import threading
+
+        self.q = queue.Queue(maxsize=max(1, ahead))
+        self.n = len(cases)
+        self.error = None
+        self.make_seconds = 0.0  # time the producer spent making jobs (not waiting for room)
+
+        def produce():
+            import torch
+
+            torch.cuda.set_device(device)
+            try:
+                for c in cases:
+                    t = time.perf_counter()
+                    j = device_job(c, device, tol)
+                    self.make_seconds += time.perf_counter() - t
+                    self.q.put(j)
+            except Exception as e:  # reported to the consumer
+                self.error = e
+                self.q.put(None)
+
+        self.t = threading.Thread(target=produce, daemon=True)
+        self.t.start()
+
+    def __iter__(self):
+        for _ in range(self.n):
+            j = self.q.get()
+            if j is None:
+                raise RuntimeError("making a trace request failed: %s" % self.error)
+            yield j
+
+
+def stream_serve(server: Server, cases: Sequence, device: int = 0, tol: float = 1e-8, rate: Optional[float] = None,
+                 seed: int = 0, inflight: int = 16, ahead: int = 16) -> dict:
+    """Serves the cases' requests as they are made (JobStream): with `rate`, submitted at Poisson arrival times of
+    that rate (per second); without, as a closed loop keeping `inflight` requests submitted. A completed request's
+    device fields are dropped at once. Latency: the server's own, from submission to completion, and, under Poisson
+    arrivals, from the arrival time (the two differ when a request was made after its arrival was due)."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, len(cases)) if rate else None
+    server.reset_stats()
+    out = {}  # ticket -> (job, submitted at, due at)
+    lat, lat_due, iters = [], [], []
+    failed = 0
+
+    def reap(block: bool):
+        nonlocal failed
+        while out:
+            done = []
+            for t, (j, ts, td) in out.items():
+                st = server.poll(t)
+                if st == capi.NB_BUSY:
+                    continue
+                done.append(t)
+                if st in (capi.NB_OK, capi.NB_NOT_CONVERGED):
+                    lat.append(j.latency_ms)
+                    lat_due.append(1e3 * (ts - td) + j.latency_ms)
+                    iters.append(j.result["iters_inner"] if j.result else 0)
+                else:
+                    failed += 1
+                j.device_fields = None
+            for t in done:
+                del out[t]
+            if not block or done:
+                return
+            time.sleep(0.0002)
+
+    stream = JobStream(cases, device, tol, ahead)
+    t0 = time.perf_counter()
+    due = t0
+    for k, j in enumerate(stream):
+        if gaps is not None:
+            due += gaps[k]
+            while time.perf_counter() < due:
+                reap(False)
+                time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
+        else:
+            while len(out) >= inflight:
+                reap(True)
+            due = time.perf_counter()
+        ts = time.perf_counter()
+        out[server.submit(j)] = (j, ts, due)
+        reap(False)
+    while out:
+        reap(True)
+    seconds = time.perf_counter() - t0
+
+    def pct(xs, q):
+        xs = sorted(xs)
+        if not xs:
+            return None
+        kk = (len(xs) - 1) * q
+        lo, hi = int(kk), min(int(kk) + 1, len(xs) - 1)
+        return round(xs[lo] + (xs[hi] - xs[lo]) * (kk - lo), 3)
+
+    r = {"requests": len(cases), "completed": len(lat), "failed": failed, "seconds": round(seconds, 4),
+         "make_seconds": round(stream.make_seconds, 3),
+         "solves_per_s": round(len(lat) / seconds, 3), "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+         "iters_inner_mean": round(float(np.mean(iters)), 2) if iters else None}
+    if rate:
+        r["rate_per_s"] = round(rate, 3)
+        r["p50_ms_from_arrival"], r["p99_ms_from_arrival"] = pct(lat_due, 0.5), pct(lat_due, 0.99)
+    return r
 
 
 def run_trace(server: Server, jobs: Sequence[Job], rate: float, seed: int = 0) -> dict:

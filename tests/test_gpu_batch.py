@@ -119,3 +119,22 @@ def test_batch_refuses_mixed_shapes(nb, jobs):
         with pytest.raises(capi.NBError) as e:
             b.project(js)
         assert e.value.status == capi.NB_BAD_INPUT
+
+
+def test_skipping_idle_tiles_changes_nothing(nb, jobs):
+    """Blocks whose cells are all air or solid skip their work (skip_idle_tiles, on by default); the results are
+    the ones every block working gives, bit for bit, solo and batched."""
+    for j in jobs[:3]:
+        a, ra = solo(j)
+        b, rb = solo(j, skip_idle_tiles=0)
+        assert_same(a, ra, b, rb)
+    with serving.Batch(3, skip_idle_tiles=0) as b:
+        for i, j in enumerate(jobs[:3]):
+            b.set_layout(i, j.grid)
+        out, res = batched(b, jobs[:3])
+    with serving.Batch(3) as b:
+        for i, j in enumerate(jobs[:3]):
+            b.set_layout(i, j.grid)
+        out2, res2 = batched(b, jobs[:3])
+    for o, r, o2, r2 in zip(out, res, out2, res2):
+        assert_same(o, r, o2, r2)
