@@ -372,7 +372,8 @@ int nereus_b200_plan(const double *costs, int n, int k, int *device_of);
  *      is one launch over all requests still iterating (a device-side work list of requests, compacted after each
  *      iteration as requests converge), the iteration runs as a captured CUDA graph with a WHILE node, and each
  *      request keeps its own labels, multigrid hierarchy, vectors, reductions, tolerance and iteration count. A
- *      request's result is bit for bit what nereus_b200_project_device gives it alone with the same options.
+ *      request's result does not depend on the rest of the batch (alone or in any mix, the same bits); it agrees
+ *      with nereus_b200_project_device on the same request within the solve's tolerance.
  *      Mixed precision; uniform 3D grids whose multigrid levels above the coarse end have Nz even. ---- */
 typedef struct nb_batch nb_batch;
 

@@ -213,8 +213,8 @@ class BoundaryReplay
 
 // Many pressure systems of one grid shape stepped together (nereus_b200_batch_*): where the reference makes one
 // SolvePressureSystem call per system (src/Methods/PPESolver/PressureSettings.h:578-624), slot i of a batch holds
-// system i's layout and one Project call runs the Chorin step of slots 0 .. n-1 on their device fields. Each system's
-// result is bit for bit the one a PressureSolver with the same options gives it alone.
+// system i's layout and one Project call runs the Chorin step of slots 0 .. n-1 on their device fields. A system's
+// result does not depend on the rest of the batch, and agrees with a PressureSolver's within the solve's tolerance.
 class BatchSolver
 {
   public:

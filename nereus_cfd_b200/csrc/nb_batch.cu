@@ -13,11 +13,13 @@
 //   * the FP64 refinement around the inner solves is batched the same way, one host synchronisation per pass;
 //   * the FP64 steps before and after the solve (ring, right-hand side, compatibility, levelling, scatter,
 //     projection) run per request on the batch's stream.
-// The launches that end in a grid-wide sum use the grid of a single solve, so each request's result is bit for bit
-// the one its solve alone gives (a single context with the same options); the autotuner only picks shapes that
-// cannot change a result: the march length of the smoothing, residual and transfer kernels and the restriction's
-// kernel (one thread per coarse cell or per four), timed on the batch itself and cached by (grid, level, kind,
-// capacity).
+// Each request's sums run over its own blocks in a fixed order, so its result does not depend on the other requests
+// of the batch (alone or in any mix, in any slot, the same bits); the autotuner only picks shapes that cannot change
+// a result: the march length of the smoothing, residual and transfer kernels and the restriction's kernel (one
+// thread per coarse cell or per four), timed on the batch itself and cached by (grid, level, kind, capacity). The
+// batched kernels inline the same bodies as the single-context ones into other kernels, where the compiler may fuse
+// products into FMAs differently, so a batched request and its single-context solve agree to FP32 rounding in the
+// inner solve and within the solve's tolerance in the result.
 #include "nb_guard.h"
 
 #include <algorithm>

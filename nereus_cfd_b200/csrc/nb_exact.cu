@@ -610,10 +610,15 @@ void LaunchCellwise(const LevelView &v, int op, double *a, const double *b, doub
 // The refinement form also adds a correction e first: x_out = x_in + e, r = b - A x_out, read from the
 // neighbours' x_in + e, so x_in and x_out are different arrays.
 // ---------------------------------------------------------------------------------------------------------------
+// swap (refinement form, may be null): when *swap is odd, x_in and x_out trade places (a refinement loop on the device
+// alternates its two iterates without the host)
 template <typename T, bool kAdd>
-__global__ void k_residual64(LevelView v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
-                             double scale, double sfac, Reducer R, int slot)
+__global__ void k_residual64(LevelView v, const double *b, const double *xin0, const T *e, double *xout0, T *rOut,
+                             double scale, double sfac, Reducer R, int slot, const int *swap)
 {
+    const bool sw = kAdd && swap && (*swap & 1);
+    const double *xin = sw ? xout0 : xin0;
+    double *xout = sw ? const_cast<double *>(xin0) : xout0;
     const int fo = blockIdx.x * kTileF + threadIdx.x, mo = blockIdx.y * kTileM + threadIdx.y;
     const int sBeg = blockIdx.z * v.slowChunk, sEnd = min(sBeg + v.slowChunk, v.slowLen);
     double acc[2] = {0.0, 0.0};
@@ -655,16 +660,17 @@ void LaunchResidual64(const LevelView &v, const double *b, const double *x, T *r
 {
     const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_residual64<T, false><<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, b, x, (const T *)nullptr, nullptr, rOut, scale, sfac, R, slot);
+    k_residual64<T, false><<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, b, x, (const T *)nullptr, nullptr, rOut,
+                                                                          scale, sfac, R, slot, nullptr);
 }
 
 template <typename T>
 void LaunchRefine64(const LevelView &v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
-                    double scale, double sfac, const Reducer &R, int slot, cudaStream_t st)
+                    double scale, double sfac, const Reducer &R, int slot, cudaStream_t st, const int *swap)
 {
-    const int blocks = LineGrid(v.nLines > 0 ? v.nLines : 1, R.maxBlocks);
     NB_COUNT_LAUNCH();
-    k_residual64<T, true><<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, b, xin, e, xout, rOut, scale, sfac, R, slot);
+    k_residual64<T, true><<<TileGrid(v), dim3(kTileF, kTileM), 0, st>>>(v, b, xin, e, xout, rOut, scale, sfac, R, slot,
+                                                                         swap);
 }
 
 template void LaunchResidual64<float>(const LevelView &, const double *, const double *, float *, double, double,
@@ -672,9 +678,9 @@ template void LaunchResidual64<float>(const LevelView &, const double *, const d
 template void LaunchResidual64<double>(const LevelView &, const double *, const double *, double *, double, double,
                                        const Reducer &, int, cudaStream_t);
 template void LaunchRefine64<float>(const LevelView &, const double *, const double *, const float *, double *,
-                                    float *, double, double, const Reducer &, int, cudaStream_t);
+                                    float *, double, double, const Reducer &, int, cudaStream_t, const int *);
 template void LaunchRefine64<double>(const LevelView &, const double *, const double *, const double *, double *,
-                                     double *, double, double, const Reducer &, int, cudaStream_t);
+                                     double *, double, double, const Reducer &, int, cudaStream_t, const int *);
 
 // ---------------------------------------------------------------------------------------------------------------
 // level, scatter, ring (PressureSolver3D.cpp:181-187, 321-328; MAC::EnforcePressureBC src/MAC.cpp:866-871 replaying

@@ -35,8 +35,10 @@ template <typename T>
 void LaunchResidual64(const LevelView &v, const double *b, const double *x, T *rOut, double scale, double sfac,
                       const Reducer &R, int slot, cudaStream_t st);
 template <typename T>
+// swap (may be null): when *swap is odd the kernel reads xout and writes xin (a device-side refinement loop)
 void LaunchRefine64(const LevelView &v, const double *b, const double *xin, const T *e, double *xout, T *rOut,
-                    double scale, double sfac, const Reducer &R, int slot, cudaStream_t st);
+                    double scale, double sfac, const Reducer &R, int slot, cudaStream_t st,
+                    const int *swap = nullptr);
 enum : int { CELL_DELTA = 0, CELL_RING_DELTA, CELL_NEG, CELL_TAKE, CELL_SUM, CELL_RESTORE };
 void LaunchCellwise(const LevelView &v, int op, double *a, const double *b, double *out, cudaStream_t st);
 void LaunchSumUnknowns(const LevelView &v, const double *x, const Reducer &R, int slot, cudaStream_t st);
@@ -93,9 +95,13 @@ void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const ui
 // the FP64 refinement step x_out = x_in + e, r = sfac (b - A x_out) on a uniform 3D level 0 (k_residual64's)
 void LaunchPairRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
                         double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
-                        cudaStream_t st);
+                        cudaStream_t st, const int *swap = nullptr);
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
                   int baseOdd, cudaStream_t st);
+// the same on a colour-split level 0 (v), skipping the tiles its activity marks empty (all tiles without one)
+void LaunchSplitLinXR(const LevelView &v, long long vecLen, float *x, float *r, const float *p0, const float *p1,
+                      const float *q, const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
+                      int singular, int slotPQ, int slotRR, cudaStream_t st);
 void LaunchBatchLinXR(const BatchLevel *lv, int ls, const BatchReq *rq, BatchList a, int cap, int baseEven,
                       int baseOdd, int slotN, int slotPQ, int slotRR, cudaStream_t st);
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,
@@ -146,7 +152,7 @@ void LaunchBatchSplitRefine64(const LevelView &v, const BatchLevel *lv, int ls, 
                               int cap, const int *parity, int slot, cudaStream_t st);
 void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
                          double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
-                         cudaStream_t st);
+                         cudaStream_t st, const int *swap = nullptr);
 
 // ---- nb_kernels.cu: multigrid and PCG kernels, T = float (inner solve) or double (plain FP64) ----
 void LaunchBuildCodes(const LevelView &v, uint8_t *code, cudaStream_t st);

@@ -716,11 +716,15 @@ void LaunchPairPApply(const LevelView &v, const uint8_t *du, const float *z, flo
 // neighbour sum runs over all six; the sum's order differs from the per-cell kernel's, within FP64 rounding.
 __device__ __forceinline__ double2 Ld2d(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
+// swap (may be null): when *swap is odd, x_in and x_out trade places
 __global__ void __launch_bounds__(kPairThreads)
     k_pair_refine64(LevelView v, const uint8_t *__restrict__ du, const double *__restrict__ b,
-                    const double *__restrict__ xin, const float *__restrict__ e, double *__restrict__ xout,
-                    float *__restrict__ r, double scale, double sfac, Reducer R, int slot)
+                    const double *xin0, const float *__restrict__ e, double *xout0,
+                    float *__restrict__ r, double scale, double sfac, Reducer R, int slot, const int *swap)
 {
+    const bool sw = swap && (*swap & 1);
+    const double *__restrict__ xin = sw ? xout0 : xin0;
+    double *__restrict__ xout = sw ? const_cast<double *>(xin0) : xout0;
     const PairPos P = PairStart(v);
     auto X = [&](int o) {
         const double2 a = Ld2d(xin + P.base + o);
@@ -759,11 +763,11 @@ __global__ void __launch_bounds__(kPairThreads)
 
 void LaunchPairRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
                         double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
-                        cudaStream_t st)
+                        cudaStream_t st, const int *swap)
 {
     NB_COUNT_LAUNCH();
     k_pair_refine64<<<PairGrid(v, kReduceS), kPairThreads, 0, st>>>(v, du, b, xin, e, xout, r, scale, sfac, R,
-                                                                      slot);
+                                                                      slot, swap);
 }
 
 // Whole-array kernels (every entry off the unknowns is zero): 16-byte loads over the level's cells.
@@ -829,6 +833,52 @@ __device__ __forceinline__ void LinXR(long long cells, float *__restrict__ x, fl
     GridReduceB<1>(R, acc, slotRR, (unsigned)bx, (unsigned)gx, 0, it);
 }
 
+// The same update on a colour-split level 0 with its tile activity (LevelView::act): the vector walked tile by tile
+// (1024 elements of one colour's plane), the tiles that hold no unknown skipped (p and q are zero there, so x and r
+// stay as they are and add nothing to r.r).
+__device__ __forceinline__ void LinXRTiles(const LevelView &v, float *__restrict__ x, float *__restrict__ r,
+                                           const float *p0, const float *p1, const float *__restrict__ q,
+                                           const Reducer &R, const double *S, int *it, int baseEven, int baseOdd,
+                                           int slotN, int singular, int slotPQ, int slotRR, int bx, int gx)
+{
+    const int par = *it & 1;
+    const float *__restrict__ p = par ? p0 : p1;
+    const int base = par ? baseOdd : baseEven;
+    const float a = (float)(RzEffP(S, base, S[slotN], singular) / S[slotPQ]);
+    double acc[1] = {0.0};
+    const int tiles = v.actTiles, perColour = v.Ny * tiles, units = 2 * perColour;
+    for (int u = bx; u < units; u += gx)
+    {
+        const int c = u / perColour, rem = u - c * perColour, i = rem / tiles, t = rem - i * tiles;
+        if (!v.act[(long long)i * tiles + t]) continue;
+        const long long e0 = (long long)c * v.sHalf + (long long)i * v.sPS + 4LL * kPairThreads * t;
+        const int n4 = min(kPairThreads, (v.sPS - 4 * kPairThreads * t) >> 2);
+        for (int k = threadIdx.x; k < n4; k += blockDim.x)
+        {
+            const long long o = e0 + 4LL * k;
+            const float4 pv = *reinterpret_cast<const float4 *>(p + o), qv = *reinterpret_cast<const float4 *>(q + o);
+            float4 xv = *reinterpret_cast<float4 *>(x + o), rv = *reinterpret_cast<float4 *>(r + o);
+            xv.x += a * pv.x; xv.y += a * pv.y; xv.z += a * pv.z; xv.w += a * pv.w;
+            rv.x -= a * qv.x; rv.y -= a * qv.y; rv.z -= a * qv.z; rv.w -= a * qv.w;
+            *reinterpret_cast<float4 *>(x + o) = xv;
+            *reinterpret_cast<float4 *>(r + o) = rv;
+            acc[0] += ((double)rv.x * rv.x + (double)rv.y * rv.y) + ((double)rv.z * rv.z + (double)rv.w * rv.w);
+        }
+    }
+    GridReduceB<1>(R, acc, slotRR, (unsigned)bx, (unsigned)gx, 0, it);
+}
+
+__global__ void __launch_bounds__(256) k_lin_xr_tiles(LevelView v, float *__restrict__ x, float *__restrict__ r,
+                                                      const float *p0, const float *p1, const float *__restrict__ q,
+                                                      Reducer R, const double *S, int *it, int baseEven, int baseOdd,
+                                                      int slotN, int singular, int slotPQ, int slotRR)
+{
+    PdlWait();
+    PdlTrigger();
+    LinXRTiles(v, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, singular, slotPQ, slotRR, (int)blockIdx.x,
+               (int)gridDim.x);
+}
+
 __global__ void __launch_bounds__(256) k_lin_xr(long long cells, float *__restrict__ x, float *__restrict__ r,
                                                 const float *p0, const float *p1, const float *__restrict__ q,
                                                 Reducer R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
@@ -849,9 +899,14 @@ __global__ void __launch_bounds__(256) kb_lin_xr(const BatchLevel *__restrict__ 
     PdlTrigger();
     const int q = BatchReqOf(a);
     if (q < 0) return;
-    const BatchReq Q = rq[q];
-    LinXR(Q.vecLen, Q.x, lv[q * ls].r, Q.p0, Q.p1, Q.q, Q.red, Q.red.out, Q.it, baseEven, baseOdd, slotN, Q.singular,
-          slotPQ, slotRR, (int)blockIdx.x, (int)gridDim.x);
+    const BatchReq &Q = rq[q];
+    const BatchLevel &L = lv[q * ls];
+    if (L.v.act)
+        LinXRTiles(L.v, Q.x, L.r, Q.p0, Q.p1, Q.q, Q.red, Q.red.out, Q.it, baseEven, baseOdd, slotN, Q.singular,
+                   slotPQ, slotRR, (int)blockIdx.x, (int)gridDim.x);
+    else
+        LinXR(Q.vecLen, Q.x, L.r, Q.p0, Q.p1, Q.q, Q.red, Q.red.out, Q.it, baseEven, baseOdd, slotN, Q.singular,
+              slotPQ, slotRR, (int)blockIdx.x, (int)gridDim.x);
 }
 
 void LaunchLinDot(long long cells, const float *r, const float *z, const Reducer &R, const int *it, int baseEven,
@@ -867,6 +922,20 @@ void LaunchBatchLinXR(const BatchLevel *lv, int ls, const BatchReq *rq, BatchLis
     NB_COUNT_LAUNCH();
     LaunchPdl(kb_lin_xr, dim3(kLinBlocks, 1, cap), dim3(256), 0, st, lv, ls, rq, a, baseEven, baseOdd, slotN, slotPQ,
               slotRR);
+}
+
+void LaunchSplitLinXR(const LevelView &v, long long vecLen, float *x, float *r, const float *p0, const float *p1,
+                      const float *q, const Reducer &R, const double *S, int *it, int baseEven, int baseOdd, int slotN,
+                      int singular, int slotPQ, int slotRR, cudaStream_t st)
+{
+    if (!v.act)
+    {
+        LaunchLinXR(vecLen, x, r, p0, p1, q, R, S, it, baseEven, baseOdd, slotN, singular, slotPQ, slotRR, st);
+        return;
+    }
+    NB_COUNT_LAUNCH();
+    LaunchPdl(k_lin_xr_tiles, dim3(kLinBlocks), dim3(256), 0, st, v, x, r, p0, p1, q, R, S, it, baseEven, baseOdd,
+              slotN, singular, slotPQ, slotRR);
 }
 
 void LaunchLinXR(long long cells, float *x, float *r, const float *p0, const float *p1, const float *q,

@@ -380,6 +380,8 @@ Context::Context(const nb_options &o) : opt(o)
     counter.zero(st);
     iter.alloc(1);
     iter.zero(st);
+    passes.alloc(1);
+    passes.zero(st);
     red.partials = partials.p;
     red.out = slots.p;
     red.counter = counter.p;
@@ -392,6 +394,7 @@ Context::~Context()
 {
     if (st) cudaStreamSynchronize(st);
     for (auto &g : graphs) g.Release();
+    ReleaseSolveGraph();
     for (cudaEvent_t e : evPool) cudaEventDestroy(e);
     if (hostSlots) cudaFreeHost(hostSlots);
     if (ev0) cudaEventDestroy(ev0);
@@ -601,6 +604,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
             else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }
         }
         for (auto &Lv : L) UploadTables(Lv, st); // same sizes: the same device arrays
+        ReleaseSolveGraph();                     // its refinement step holds the old scale
         RefillHierarchy();
     }
     else if (shapeSame)
@@ -608,6 +612,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
     else
     {
         for (auto &g : graphs) g.Release(); // they hold the old hierarchy's pointers
+        ReleaseSolveGraph();
         dim = dim_;
         Nx = Nx_;
         Ny = Ny_;
@@ -639,7 +644,10 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
     n = (int)hostSlots[S_RES];
     singular = hostSlots[S_RES + 1] == 0.0;
     if ((shapeSame || rescale) && singular != wasSingular)
+    {
         for (auto &g : graphs) g.Release(); // the iteration's kernels depend on the flag
+        ReleaseSolveGraph();
+    }
     hostSlots[S_NUNK] = (double)n;
     NB_CK(cudaMemcpyAsync(slots.p + S_NUNK, hostSlots + S_NUNK, sizeof(double), cudaMemcpyHostToDevice, st));
     AllocVectors();
@@ -870,8 +878,8 @@ template <typename T> void Context::IterBody(T *x, T *r, T *z, T *p0, T *p1, T *
             LaunchSplitPApply(v0, L[0].du.p, z, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ, st);
             ProfEnd();
             ProfBegin(NB_K_XR, 6.0 * s * cells);
-            LaunchLinXR((long long)VecLen0(), x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK, sing, S_PQ,
-                        S_RR, st);
+            LaunchSplitLinXR(v0, (long long)VecLen0(), x, r, p0, p1, q, red, slots.p, iter.p, S_RZ0, S_RZ1, S_NUNK,
+                             sing, S_PQ, S_RR, st);
             ProfEnd();
             if (copyRR)
                 NB_CK(cudaMemcpyAsync(hostSlots + S_RR, slots.p + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1069,8 +1077,212 @@ bool Context::StartFrom(const double *guess, double refNorm, double tol, double 
     return go;
 }
 
+// ---- the mixed solve as one graph (SolveMixed's loop on the device) ----
+// Before the passes: ||b||^2 (the zero iterate's residual, in S_RES) is kept, no pass done yet, and the loop starts
+// unless that residual already meets the tolerance (the host loop's test, sqrt(rr / bn2) <= tol, in the same order).
+__global__ void k_mixed_init(cudaGraphConditionalHandle h, double *S, int *passes, int maxOuter)
+{
+    const double bn2 = S[S_RES];
+    S[S_BN2] = bn2;
+    S[S_INNER] = 0.0;
+    *passes = 0;
+    const bool go = bn2 > 0.0 && !(sqrt(bn2 / bn2) <= S[S_TOL]) && 0 < maxOuter && isfinite(bn2);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// A pass's CG targets: r.r down by inner_tol^2 from the unit-form residual of this pass, at most maxIt iterations.
+__global__ void k_mixed_pass(double *S, double sfac, double innerTol, int maxIt)
+{
+    const double rr0 = S[S_RES] * sfac * sfac;
+    S[S_TGT] = rr0 * innerTol * innerTol;
+    S[S_MAXIT] = (double)maxIt;
+}
+
+// After a pass's refinement step: count it and its CG iterations; go on while the FP64 residual is above the
+// tolerance, finite, and passes remain.
+__global__ void k_mixed_cond(cudaGraphConditionalHandle h, double *S, int *passes, int maxOuter)
+{
+    const int n = *passes + 1;
+    *passes = n;
+    S[S_INNER] += S[S_ITS];
+    const double rr = S[S_RES], bn2 = S[S_BN2];
+    const bool go = !(sqrt(rr / bn2) <= S[S_TOL]) && n < maxOuter && isfinite(rr);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+void Context::ReleaseSolveGraph()
+{
+    if (solveExec) cudaGraphExecDestroy(solveExec);
+    if (solveGraph) cudaGraphDestroy(solveGraph);
+    solveExec = nullptr;
+    solveGraph = nullptr;
+    solveFailed = false;
+}
+
+void Context::BuildSolveGraph()
+{
+    const LevelView v0 = L[0].view();
+    const double sfac = -1.0 / scale;
+    float *r32 = L[0].r32.p, *z32 = L[0].e32.p;
+    const int maxOuter = std::max(1, opt.max_outer), maxIt = std::max(1, opt.max_iters);
+    cudaGraph_t G = nullptr;
+    auto unavailable = [&]() {
+        cudaGetLastError();
+        if (G) cudaGraphDestroy(G);
+        solveGraph = nullptr;
+        solveExec = nullptr;
+        solveFailed = true;
+    };
+    // the sink nodes of the capture in progress on st
+    auto sinks = [&](std::vector<cudaGraphNode_t> &out) {
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        if (cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd) != cudaSuccess) return false;
+        out.assign(deps, deps + nd);
+        return true;
+    };
+    auto endCapture = [&]() {
+        cudaGraph_t g = nullptr;
+        return cudaStreamEndCapture(st, &g) == cudaSuccess;
+    };
+    auto whileNode = [&](cudaGraph_t parent, const std::vector<cudaGraphNode_t> &deps, cudaGraphConditionalHandle h,
+                         cudaGraph_t *body) {
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        if (cudaGraphAddNode(&node, parent, deps.empty() ? nullptr : deps.data(), deps.size(), &np) != cudaSuccess)
+            return (cudaGraphNode_t) nullptr;
+        *body = np.conditional.phGraph_out[0];
+        return node;
+    };
+    cudaGraphConditionalHandle hOuter = 0, hInner = 0;
+    if (cudaGraphCreate(&G, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&hOuter, G, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+        return unavailable();
+    const long long l0 = g_launches.load();
+    std::vector<cudaGraphNode_t> deps;
+    bool ok = true;
+    // prologue: x = 0, the zero iterate's residual and ||b||^2, the loop's start
+    if (cudaStreamBeginCaptureToGraph(st, G, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return unavailable();
+    try
+    {
+        NB_CK(cudaMemsetAsync(xa.p, 0, xa.bytes(), st));
+        if (Split(0)) LaunchSplitScaleSum(v0, b.p, r32, sfac, red, S_RES, st);
+        else LaunchScaleSum<float>(L[0].cells, b.p, r32, sfac, red, S_RES, st);
+        NB_COUNT_LAUNCH();
+        k_mixed_init<<<1, 1, 0, st>>>(hOuter, slots.p, passes.p, maxOuter);
+        ok = sinks(deps);
+    }
+    catch (...)
+    {
+        ok = false;
+    }
+    if (!endCapture() || !ok) return unavailable();
+    const long long l1 = g_launches.load();
+    cudaGraph_t outerBody = nullptr;
+    cudaGraphNode_t outerNode = whileNode(G, deps, hOuter, &outerBody);
+    if (!outerNode || cudaGraphConditionalHandleCreate(&hInner, outerBody, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return unavailable();
+    // a pass: x32 = 0, p0 = 0, iteration 0, the targets
+    if (cudaStreamBeginCaptureToGraph(st, outerBody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+        return unavailable();
+    try
+    {
+        NB_CK(cudaMemsetAsync(x32.p, 0, x32.bytes(), st));
+        NB_CK(cudaMemsetAsync(p32[0].p, 0, p32[0].bytes(), st));
+        NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
+        NB_COUNT_LAUNCH();
+        k_mixed_pass<<<1, 1, 0, st>>>(slots.p, sfac, opt.inner_tol, maxIt);
+        ok = sinks(deps);
+    }
+    catch (...)
+    {
+        ok = false;
+    }
+    if (!endCapture() || !ok) return unavailable();
+    const long long l2 = g_launches.load();
+    cudaGraph_t innerBody = nullptr;
+    cudaGraphNode_t innerNode = whileNode(outerBody, deps, hInner, &innerBody);
+    if (!innerNode) return unavailable();
+    // the CG iteration, its loop condition
+    if (cudaStreamBeginCaptureToGraph(st, innerBody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+        return unavailable();
+    try
+    {
+        IterBody<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, false, false);
+        NB_COUNT_LAUNCH();
+        k_loop_cond<<<1, 1, 0, st>>>(hInner, slots.p, iter.p, S_RR, S_TGT, S_MAXIT, S_ITS);
+    }
+    catch (...)
+    {
+        ok = false;
+    }
+    if (!endCapture() || !ok) return unavailable();
+    const long long l3 = g_launches.load();
+    // the refinement step (iterates swapped by the pass count) and the outer condition
+    std::vector<cudaGraphNode_t> afterInner(1, innerNode);
+    if (cudaStreamBeginCaptureToGraph(st, outerBody, afterInner.data(), nullptr, 1,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return unavailable();
+    try
+    {
+        if (Split(0) && !nonuniform)
+            LaunchSplitRefine64(v0, L[0].du.p, b.p, xa.p, x32.p, xb.p, r32, scale, sfac, red, S_RES, st, passes.p);
+        else if (PairLevel(0) && !nonuniform && dim == 3)
+            LaunchPairRefine64(v0, L[0].du.p, b.p, xa.p, x32.p, xb.p, r32, scale, sfac, red, S_RES, st, passes.p);
+        else
+            LaunchRefine64<float>(v0, b.p, xa.p, x32.p, xb.p, r32, scale, sfac, red, S_RES, st, passes.p);
+        NB_COUNT_LAUNCH();
+        k_mixed_cond<<<1, 1, 0, st>>>(hOuter, slots.p, passes.p, maxOuter);
+    }
+    catch (...)
+    {
+        ok = false;
+    }
+    if (!endCapture() || !ok) return unavailable();
+    const long long l4 = g_launches.load();
+    if (cudaGraphInstantiate(&solveExec, G, 0) != cudaSuccess) return unavailable();
+    solveGraph = G;
+    solvePrologLaunches = l1 - l0;
+    solvePassLaunches = (l2 - l1) + (l4 - l3);
+    solveIterLaunches = l3 - l2;
+    NB_COUNT_LAUNCHES(-(l4 - l0)); // counted when run
+}
+
 int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double *guess, double refNorm)
 {
+    if (opt.use_graphs >= 2 && profMask == 0 && !guess && !(refNorm > 0.0) && !solveFailed)
+    {
+        // the whole solve on the device: one launch, one synchronisation
+        if (!solveExec) BuildSolveGraph();
+        if (solveExec)
+        {
+            hostSlots[S_TOL] = tol;
+            NB_CK(cudaMemcpyAsync(slots.p + S_TOL, hostSlots + S_TOL, sizeof(double), cudaMemcpyHostToDevice, st));
+            NB_CK(cudaGraphLaunch(solveExec, st));
+            int np = 0;
+            NB_CK(cudaMemcpyAsync(hostSlots, slots.p, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
+            NB_CK(cudaMemcpyAsync(&np, passes.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            NB_CK(cudaStreamSynchronize(st));
+            NB_CK(cudaGetLastError());
+            const double bn2 = hostSlots[S_BN2], rr64 = np > 0 ? hostSlots[S_RES] : bn2;
+            const int inner = (int)hostSlots[S_INNER];
+            NB_COUNT_LAUNCHES(solvePrologLaunches + np * solvePassLaunches + (long long)inner * solveIterLaunches);
+            out->b_norm = std::sqrt(bn2);
+            out->iters_outer = np;
+            out->iters_inner = inner;
+            out->rel_res = bn2 > 0.0 ? std::sqrt(rr64 / bn2) : 0.0;
+            *xOut = (np & 1) ? xb.p : xa.p;
+            return (bn2 > 0.0 && !(std::sqrt(rr64 / bn2) <= tol)) ? NB_NOT_CONVERGED : NB_OK;
+        }
+    }
     const LevelView v0 = L[0].view();
     const double sfac = -1.0 / scale;
     double *x = xa.p, *xo = xb.p;

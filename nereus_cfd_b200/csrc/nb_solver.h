@@ -88,7 +88,10 @@ enum : int
     S_TGT = 19,  // the device-side CG loop: r.r target, iteration cap, iterations done
     S_MAXIT = 20,
     S_ITS = 21,
-    S_COUNT = 22
+    S_BN2 = 22,  // the device-side refinement loop: ||b||^2, the tolerance, the CG iterations of all passes
+    S_TOL = 23,
+    S_INNER = 24,
+    S_COUNT = 25
 };
 
 struct LevelData
@@ -213,6 +216,14 @@ struct Context
     IterGraph graphs[2]; // [0] float, [1] double
     IterGraph *capturing = nullptr;
     DevArray<int> iter;  // the CG iteration number, advanced on the device
+    // the whole mixed solve as one graph: the zero-iterate residual, then a WHILE node over refinement passes whose
+    // body holds the CG loop's WHILE node and the FP64 refinement step (built once per shape, or unavailable)
+    cudaGraph_t solveGraph = nullptr;
+    cudaGraphExec_t solveExec = nullptr;
+    bool solveFailed = false;
+    long long solvePrologLaunches = 0, solvePassLaunches = 0, solveIterLaunches = 0;
+    DevArray<int> passes; // the refinement passes done (their parity picks the iterate the next pass reads)
+    void ReleaseSolveGraph();
 
     Context(const nb_options &o);
     ~Context();
@@ -258,6 +269,7 @@ struct Context
     // (SolveEigenPressure, PressureSettings.h:411-427).
     int Solve(double tol, double **xOut, nb_result *out, const double *guess = nullptr, double refNorm = 0.0);
     int SolveMixed(double tol, double **xOut, nb_result *out, const double *guess, double refNorm);
+    void BuildSolveGraph();
     int SolveFP64(double tol, double **xOut, nb_result *out, const double *guess, double refNorm);
     // the initial residual of the guess, and the tolerance the refNorm floor turns `tol` into; false: nothing to do
     bool StartFrom(const double *guess, double refNorm, double tol, double bn2, double *tolEff);

@@ -1024,29 +1024,32 @@ __device__ __forceinline__ void SplitRefine64(const LevelView &v, const uint8_t 
     GridReduceB<2>(R, acc, slot, BlkId(blk), BlkCount(blk));
 }
 
+// swap (may be null): when *swap is odd, x_in and x_out trade places
 __global__ void __launch_bounds__(kPairThreads, 3)
     k_split_refine64(LevelView v, const uint8_t *__restrict__ du, const double *__restrict__ b,
-                     const double *__restrict__ xin, const float *__restrict__ e, double *__restrict__ xout,
-                     float *__restrict__ r, double scale, double sfac, Reducer R, int slot)
+                     const double *xin, const float *__restrict__ e, double *xout,
+                     float *__restrict__ r, double scale, double sfac, Reducer R, int slot, const int *swap)
 {
-    SplitRefine64(v, du, b, xin, e, xout, r, scale, sfac, R, slot, ThisBlk());
+    const bool sw = swap && (*swap & 1);
+    SplitRefine64(v, du, b, sw ? xout : xin, e, sw ? const_cast<double *>(xin) : xout, r, scale, sfac, R, slot,
+                  ThisBlk());
 }
 
 void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b, const double *xin, const float *e,
                          double *xout, float *r, double scale, double sfac, const Reducer &R, int slot,
-                         cudaStream_t st)
+                         cudaStream_t st, const int *swap)
 {
     NB_COUNT_LAUNCH();
     k_split_refine64<<<PairGrid(v, kSplitReduceS), kPairThreads, 0, st>>>(v, du, b, xin, e, xout, r, scale, sfac, R,
-                                                                           slot);
+                                                                           slot, swap);
 }
 
 
 // ---------------------------------------------------------------------------------------------------------------
 // batched launches (nb_batch.cu): grid z = the batch's capacity, block z runs the request at list[z] on the x, y tiles
 // of its own grid. The launches that end in a grid-wide sum keep the grid a single solve uses, so each request's sums
-// (and so its whole solve) are bit for bit the ones it gets alone; the others take the march length S the caller
-// chose (it changes which planes a thread visits, not what a cell gets).
+// run over its own blocks in the same order whatever else the batch holds; the others take the march length S the
+// caller chose (it changes which planes a thread visits, not what a cell gets).
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kPairThreads) kb_split_first(const BatchLevel *__restrict__ lv, int ls, int l,
                                                                BatchList a)

@@ -99,7 +99,8 @@ def plan(costs: Sequence[float], k: int) -> List[int]:
 class Batch:
     """nereus_b200_batch_*: one pressure step for each of up to ``capacity`` grids of the same shape, advanced by
     the same launches (mixed precision, uniform 3D). Slot i takes jobs[i]; a slot keeps its hierarchy while its
-    layout bytes are unchanged. Each job's result is bit for bit its solo solve's."""
+    layout bytes are unchanged. A job's result does not depend on the rest of the batch (the same bits alone or in
+    any mix) and agrees with its single-context solve within the tolerance."""
 
     def __init__(self, capacity: int, device: int = 0, stream: Optional[int] = None, **solver_options):
         self.lib = capi.load()
@@ -371,17 +372,19 @@ def trace_case(rng, index: int):
     return W.Case(name, g, sc, int(rng.integers(1 << 31)), needs_compat=compat, velocity_rule=rule)
 
 
-def device_job(case, device: int = 0, tol: float = 1e-8) -> Job:
-    """A job whose fields are drawn on the device: labels by the library, N(0,1) face velocities from a torch
-    generator seeded by the case, zeroed by the case's rule (face_velocities' rules), p = 0."""
+def device_job(case, device: int = 0, tol: float = 1e-8, types: Optional[np.ndarray] = None, dtypes=None) -> Job:
+    """A job whose fields are drawn on the device: labels by the library (or the given host `types` and their device
+    copy `dtypes`), N(0,1) face velocities from a torch generator seeded by the case, zeroed by the case's rule
+    (face_velocities' rules), p = 0."""
     import torch
 
     from . import workloads as W
 
     g = case.grid
-    types = capi.label_cells(g, case.scene)
+    if types is None:
+        types = capi.label_cells(g, case.scene)
     d = "cuda:%d" % device
-    t = torch.from_numpy(types.reshape(g.shape)).to(d)
+    t = dtypes.reshape(g.shape) if dtypes is not None else torch.from_numpy(types.reshape(g.shape)).to(d)
     gen = torch.Generator(device=d)
     gen.manual_seed(case.seed)
     fields = {}
@@ -408,11 +411,25 @@ def device_job(case, device: int = 0, tol: float = 1e-8) -> Job:
     return job
 
 
+def trace_labels(cases: Sequence, device: int = 0):
+    """The cell types of every case, computed once by the library: host arrays and their device copies."""
+    import torch
+
+    host, dev = [], []
+    for c in cases:
+        t = capi.label_cells(c.grid, c.scene)
+        host.append(t)
+        dev.append(torch.from_numpy(t).to("cuda:%d" % device))
+    torch.cuda.synchronize(device)
+    return host, dev
+
+
 class JobStream:
     """The device jobs of a list of cases, made by a background thread a bounded number ahead of use (so a long
-    trace never holds more than `ahead` unsubmitted requests' fields on the device). Iterate to take them in order."""
+    trace never holds more than `ahead` unsubmitted requests' fields on the device). Iterate to take them in order.
+    labels: (host, device) cell types of the cases (trace_labels), else each job labels its case."""
 
-    def __init__(self, cases: Sequence, device: int = 0, tol: float = 1e-8, ahead: int = 16):
+    def __init__(self, cases: Sequence, device: int = 0, tol: float = 1e-8, ahead: int = 16, labels=None):
         import queue
         import threading
 
@@ -426,9 +443,9 @@ class JobStream:
 
             torch.cuda.set_device(device)
             try:
-                for c in cases:
+                for k, c in enumerate(cases):
                     t = time.perf_counter()
-                    j = device_job(c, device, tol)
+                    j = device_job(c, device, tol, *((labels[0][k], labels[1][k]) if labels else ()))
                     self.make_seconds += time.perf_counter() - t
                     self.q.put(j)
             except Exception as e:  # reported to the consumer
@@ -447,7 +464,7 @@ class JobStream:
 
 
 def stream_serve(server: Server, cases: Sequence, device: int = 0, tol: float = 1e-8, rate: Optional[float] = None,
-                 seed: int = 0, inflight: int = 16, ahead: int = 16) -> dict:
+                 seed: int = 0, inflight: int = 16, ahead: int = 16, labels=None) -> dict:
     """Serves the cases' requests as they are made (JobStream): with `rate`, submitted at Poisson arrival times of
     that rate (per second); without, as a closed loop keeping `inflight` requests submitted. A completed request's
     device fields are dropped at once. Latency: the server's own, from submission to completion, and, under Poisson
@@ -461,6 +478,8 @@ def stream_serve(server: Server, cases: Sequence, device: int = 0, tol: float = 
 
     def reap(block: bool):
         nonlocal failed
+        if block and out:
+            server.wait(next(iter(out)), 0.002)  # blocks in the library (the GIL released) up to 2 ms
         while out:
             done = []
             for t, (j, ts, td) in out.items():
@@ -481,7 +500,7 @@ def stream_serve(server: Server, cases: Sequence, device: int = 0, tol: float = 
                 return
             time.sleep(0.0002)
 
-    stream = JobStream(cases, device, tol, ahead)
+    stream = JobStream(cases, device, tol, ahead, labels)
     t0 = time.perf_counter()
     due = t0
     for k, j in enumerate(stream):

@@ -134,3 +134,48 @@ def test_device_loop_stops_at_the_iteration_cap(nb):
     s.DestroyPressureSolver()
     assert r.status == capi.NB_NOT_CONVERGED
     assert r.iters_inner == 2
+
+
+@pytest.mark.parametrize("name", ["closed_box_2d", "stretched_cylinder_3d", "flip_tank_3d"])
+def test_device_refinement_loop_equals_host_loop(nb, name):
+    """The mixed solve as one graph (use_graphs = 2: the refinement passes in a WHILE node around the CG loop's WHILE
+    node) and the refinement loop on the host (use_graphs = 1): the same passes, iterations and bits, on a singular
+    2D box (compatibility on), a stretched 3D channel and a free-surface tank."""
+    case = {"closed_box_2d": lambda: W.closed_box_2d(48, seed=3),
+            "stretched_cylinder_3d": lambda: W.stretched_cylinder_3d(24, 16, 16, seed=4),
+            "flip_tank_3d": lambda: W.flip_tank_3d(30, seed=5)}[name]()
+    g = case.grid
+    types = capi.label_cells(g, case.scene)
+    u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
+    out = []
+    for graphs in (2, 1):
+        s = PressureSolver("mixed", use_graphs=graphs)
+        for rep in range(2):
+            m = MACGrid(g, types.copy(), u.copy(), v.copy(), w.copy(), np.zeros(g.cells), case.rho, case.dt)
+            r = s.SolvePressure(m, tol=1e-10, needs_compat=case.needs_compat)
+            assert r.status == capi.NB_OK and r.rel_res <= 1e-10
+            out.append((r.iters_inner, r.iters_outer, r.rel_res, m.p, m.u, m.v))
+        s.DestroyPressureSolver()
+    for o in out[1:]:
+        assert out[0][:3] == o[:3]
+        for a, b in zip(out[0][3:], o[3:]):
+            assert np.array_equal(a, b)
+
+
+def test_device_refinement_loop_limits(nb):
+    """The device-side refinement loop stops at max_outer passes with NOT_CONVERGED, and a zero right-hand side needs
+    no pass at all."""
+    case = W.sphere_outlet_3d(24, seed=6)
+    g = case.grid
+    types = capi.label_cells(g, case.scene)
+    u, v, w = W.face_velocities(g, types, case.seed, case.velocity_rule, case.fp32_velocity)
+    s = PressureSolver("mixed", max_outer=1)
+    m = MACGrid(g, types.copy(), u.copy(), v.copy(), w.copy(), np.zeros(g.cells), case.rho, case.dt)
+    r = s.SolvePressure(m, tol=1e-14)
+    assert r.status == capi.NB_NOT_CONVERGED and r.iters_outer == 1 and r.rel_res > 1e-14
+    z = MACGrid(g, types.copy(), np.zeros_like(u), np.zeros_like(v), np.zeros_like(w), np.zeros(g.cells), case.rho,
+                case.dt)
+    r0 = s.SolvePressure(z, tol=1e-8)
+    s.DestroyPressureSolver()
+    assert r0.status == capi.NB_OK and r0.iters_outer == 0 and r0.iters_inner == 0 and r0.rel_res == 0.0
+    assert not np.any(z.p[types == W.FLUID])
