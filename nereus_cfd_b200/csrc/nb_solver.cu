@@ -1090,12 +1090,15 @@ __global__ void k_mixed_init(cudaGraphConditionalHandle h, double *S, int *passe
     cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
-// A pass's CG targets: r.r down by inner_tol^2 from the unit-form residual of this pass, at most maxIt iterations.
-__global__ void k_mixed_pass(double *S, double sfac, double innerTol, int maxIt)
+// A pass's CG targets: r.r down by inner_tol^2 from the unit-form residual of this pass, at most maxIt iterations;
+// the CG loop's condition set to run (a handle's default value is applied when the whole graph is launched, not when
+// an enclosing loop's body starts again).
+__global__ void k_mixed_pass(cudaGraphConditionalHandle hInner, double *S, double sfac, double innerTol, int maxIt)
 {
     const double rr0 = S[S_RES] * sfac * sfac;
     S[S_TGT] = rr0 * innerTol * innerTol;
     S[S_MAXIT] = (double)maxIt;
+    cudaGraphSetConditional(hInner, 1u);
 }
 
 // After a pass's refinement step: count it and its CG iterations; go on while the FP64 residual is above the
@@ -1198,7 +1201,7 @@ void Context::BuildSolveGraph()
         NB_CK(cudaMemsetAsync(p32[0].p, 0, p32[0].bytes(), st));
         NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
         NB_COUNT_LAUNCH();
-        k_mixed_pass<<<1, 1, 0, st>>>(slots.p, sfac, opt.inner_tol, maxIt);
+        k_mixed_pass<<<1, 1, 0, st>>>(hInner, slots.p, sfac, opt.inner_tol, maxIt);
         ok = sinks(deps);
     }
     catch (...)

@@ -272,29 +272,9 @@ __device__ __forceinline__ void SplitHalf(const LevelView &v, const uint8_t *__r
     const float *Rr = r + P.off;
     const uint8_t *D = du + P.off;
     float *C = ec + P.off;
-    // the next plane's streamed values are loaded one iteration ahead
-    F4 oM{}, oC{}, oP{}, rr{};
-    unsigned d = 0;
-    if (P.i0 < P.i1)
-    {
-        rr = L4(Rr);
-        d = LdU4(D);
-        oM = L4(O - P.PS);
-        oC = L4(O);
-        oP = L4(O + P.PS);
-    }
-    long long o = 0;
-    for (int i = P.i0; i < P.i1; i++, o += P.PS)
-    {
-        F4 oPn{}, rrn{};
-        unsigned dn = 0;
-        if (i + 1 < P.i1)
-        {
-            oPn = L4(O + o + 2 * P.PS);
-            rrn = L4(Rr + o + P.PS);
-            dn = LdU4(D + o + P.PS);
-        }
-        const F4 oJp = L4(O + o + P.RS), oJm = L4(O + o - P.RS);
+    // one plane: the six other-colour neighbours, r and the bytes given, the new values stored (and summed)
+    auto plane = [&](int i, long long o, const F4 &oM, const F4 &oC, const F4 &oP, const F4 &jp, const F4 &jm,
+                     const F4 &rr, unsigned d) {
         float prevW, nextX;
         Edges(P, oC, O + o, prevW, nextX);
         const F4 sh = KShift(oC, prevW, nextX, (i + P.j + colour) & 1);
@@ -302,7 +282,7 @@ __device__ __forceinline__ void SplitHalf(const LevelView &v, const uint8_t *__r
 #pragma unroll
         for (int x = 0; x < 4; x++)
         {
-            const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
+            const float s = ((oP.v[x] + oM.v[x]) + (jp.v[x] + jm.v[x])) + (oC.v[x] + sh.v[x]);
             nv.v[x] = (rr.v[x] + g * s) * inv[Byte(d, x) & 0x7Fu];
         }
         if (P.valid)
@@ -319,11 +299,29 @@ __device__ __forceinline__ void SplitHalf(const LevelView &v, const uint8_t *__r
                 }
             }
         }
-        oM = oC;
-        oC = oP;
-        oP = oPn;
-        rr = rrn;
-        d = dn;
+    };
+    // two planes per trip: all the streamed values of both (the other colour up to two planes ahead, the j rows,
+    // r and the bytes) are loaded before either is computed, twice the loads in flight of a plane-by-plane march
+    F4 oM{}, oC{};
+    if (P.i0 < P.i1)
+    {
+        oM = L4(O - P.PS);
+        oC = L4(O);
+    }
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i += 2, o += 2 * P.PS)
+    {
+        const bool two = i + 1 < P.i1;
+        const F4 oP = L4(O + o + P.PS);
+        const F4 oPP = two ? L4(O + o + 2 * P.PS) : F4{};
+        const F4 r0 = L4(Rr + o), r1 = two ? L4(Rr + o + P.PS) : F4{};
+        const unsigned d0 = LdU4(D + o), d1 = two ? LdU4(D + o + P.PS) : 0u;
+        const F4 jp0 = L4(O + o + P.RS), jm0 = L4(O + o - P.RS);
+        const F4 jp1 = two ? L4(O + o + P.PS + P.RS) : F4{}, jm1 = two ? L4(O + o + P.PS - P.RS) : F4{};
+        plane(i, o, oM, oC, oP, jp0, jm0, r0, d0);
+        if (two) plane(i + 1, o + P.PS, oC, oP, oPP, jp1, jm1, r1, d1);
+        oM = oP;
+        oC = oPP;
     }
     if (kDot == 1)
     {
@@ -337,8 +335,9 @@ __device__ __forceinline__ void SplitHalf(const LevelView &v, const uint8_t *__r
     }
 }
 
+// 4 resident blocks (64 registers): the two-plane march measured 12% faster there than at 3 (73 registers)
 template <int kDot>
-__global__ void __launch_bounds__(kPairThreads)
+__global__ void __launch_bounds__(kPairThreads, 4)
     k_split_half(LevelView v, const uint8_t *__restrict__ du, const float *__restrict__ r,
                  const float *__restrict__ eo, float *__restrict__ ec, int colour, Reducer R, const int *it,
                  int baseEven, int baseOdd, int partSlot)
@@ -393,13 +392,8 @@ __device__ __forceinline__ void SplitResidual(const LevelView &v, const uint8_t 
     const float *Rr = r + P.off;
     const uint8_t *D = du + P.off;
     float *Out = res + P.off;
-    F4 oM = L4(O - P.PS), oC = L4(O);
-    long long o = 0;
-    for (int i = P.i0; i < P.i1; i++, o += P.PS)
-    {
-        const F4 oP = L4(O + o + P.PS), oJp = L4(O + o + P.RS), oJm = L4(O + o - P.RS);
-        const F4 xc = L4(Xr + o), rr = L4(Rr + o);
-        const unsigned d = LdU4(D + o);
+    auto plane = [&](int i, long long o, const F4 &oM, const F4 &oC, const F4 &oP, const F4 &jp, const F4 &jm,
+                     const F4 &xc, const F4 &rr, unsigned d) {
         float prevW, nextX;
         Edges(P, oC, O + o, prevW, nextX);
         const F4 sh = KShift(oC, prevW, nextX, (i + P.j) & 1);
@@ -408,16 +402,31 @@ __device__ __forceinline__ void SplitResidual(const LevelView &v, const uint8_t 
         for (int x = 0; x < 4; x++)
         {
             const unsigned b = Byte(d, x);
-            const float s = ((oP.v[x] + oM.v[x]) + (oJp.v[x] + oJm.v[x])) + (oC.v[x] + sh.v[x]);
+            const float s = ((oP.v[x] + oM.v[x]) + (jp.v[x] + jm.v[x])) + (oC.v[x] + sh.v[x]);
             out.v[x] = (b & 0x80u) ? rr.v[x] - (hg * (float)(b & 0x7Fu) * xc.v[x] - g * s) : 0.f;
         }
         if (P.valid) S4(Out + o, out);
-        oM = oC;
-        oC = oP;
+    };
+    // two planes per trip, all their streamed values loaded first (as in the half-sweep)
+    F4 oM = L4(O - P.PS), oC = L4(O);
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i += 2, o += 2 * P.PS)
+    {
+        const bool two = i + 1 < P.i1;
+        const F4 oP = L4(O + o + P.PS), oPP = two ? L4(O + o + 2 * P.PS) : F4{};
+        const F4 jp0 = L4(O + o + P.RS), jm0 = L4(O + o - P.RS);
+        const F4 jp1 = two ? L4(O + o + P.PS + P.RS) : F4{}, jm1 = two ? L4(O + o + P.PS - P.RS) : F4{};
+        const F4 x0 = L4(Xr + o), r0 = L4(Rr + o), x1 = two ? L4(Xr + o + P.PS) : F4{},
+                 r1 = two ? L4(Rr + o + P.PS) : F4{};
+        const unsigned d0 = LdU4(D + o), d1 = two ? LdU4(D + o + P.PS) : 0u;
+        plane(i, o, oM, oC, oP, jp0, jm0, x0, r0, d0);
+        if (two) plane(i + 1, o + P.PS, oC, oP, oPP, jp1, jm1, x1, r1, d1);
+        oM = oP;
+        oC = oPP;
     }
 }
 
-__global__ void __launch_bounds__(kPairThreads) k_split_residual(LevelView v, const uint8_t *__restrict__ du,
+__global__ void __launch_bounds__(kPairThreads, 4) k_split_residual(LevelView v, const uint8_t *__restrict__ du,
                                                                  const float *__restrict__ r,
                                                                  const float *__restrict__ e, float *__restrict__ res)
 {
@@ -1063,7 +1072,7 @@ __global__ void __launch_bounds__(kPairThreads) kb_split_first(const BatchLevel 
 }
 
 template <int kDot>
-__global__ void __launch_bounds__(kPairThreads)
+__global__ void __launch_bounds__(kPairThreads, kDot ? 3 : 4)
     kb_split_half(const BatchLevel *__restrict__ lv, int ls, int l, const BatchReq *__restrict__ rq, BatchList a,
                   int colour, int baseEven, int baseOdd, int partSlot)
 {
@@ -1081,7 +1090,7 @@ __global__ void __launch_bounds__(kPairThreads)
                         Reducer{}, nullptr, baseEven, baseOdd, partSlot, ThisBlk());
 }
 
-__global__ void __launch_bounds__(kPairThreads) kb_split_residual(const BatchLevel *__restrict__ lv, int ls, int l,
+__global__ void __launch_bounds__(kPairThreads, 3) kb_split_residual(const BatchLevel *__restrict__ lv, int ls, int l,
                                                                   BatchList a)
 {
     PdlWait();
