@@ -608,11 +608,25 @@ def run_tanks(args, rank, world, dist, dev):
         if not jobs:
             return {"seconds": 0.0, "completed": 0, "latencies": []}
         keys = ("u", "v", "w", "p")
-        orig = [{k: j.device_fields[k].clone() for k in keys} for j in jobs]
+        # every tank's field k is a slice of one buffer, so a step restores all tanks with one copy per field
+        big, orig_big = {}, {}
+        for k in keys:
+            n = jobs[0].device_fields[k].numel()
+            big[k] = torch.empty(n * len(jobs), dtype=torch.float64, device="cuda")
+            for i, j in enumerate(jobs):
+                big[k][i * n:(i + 1) * n].copy_(j.device_fields[k])
+                j.device_fields[k] = big[k][i * n:(i + 1) * n]
+            orig_big[k] = big[k].clone()
+        orig = [{k: orig_big[k][i * big[k].numel() // len(jobs):(i + 1) * big[k].numel() // len(jobs)]
+                 for k in keys} for i in range(len(jobs))]
 
         def restore(i):
             for k in keys:
                 jobs[i].device_fields[k].copy_(orig[i][k])
+
+        def restore_all():
+            for k in keys:
+                big[k].copy_(orig_big[k])
 
         def events():
             return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -624,8 +638,7 @@ def run_tanks(args, rank, world, dist, dev):
         items = batch.items(jobs)
 
         def step():
-            for i in range(len(jobs)):
-                restore(i)
+            restore_all()
             return batch.project(jobs, items=items)
 
         for _ in range(2):  # the first call tunes and captures

@@ -99,6 +99,19 @@ __device__ __forceinline__ bool TileIdle(const LevelView &v, int bx, int i0, int
     return true;
 }
 
+// The same for a block of a grid-layout pair kernel (PairStart): its rows j0 .. j1 of planes [i0, i1), checked
+// through the split tiles that hold those rows' cells in either colour.
+__device__ __forceinline__ bool RowsIdle(const LevelView &v, int j0, int j1, int i0, int i1)
+{
+    if (!v.act) return false;
+    const int t0 = (int)(((long long)j0 * v.sRS) / (4 * kPairThreads));
+    const int t1 = min(v.actTiles - 1, (int)(((long long)(j1 + 1) * v.sRS - 1) / (4 * kPairThreads)));
+    for (int i = i0; i < i1; i++)
+        for (int t = t0; t <= t1; t++)
+            if (v.act[(long long)i * v.actTiles + t]) return false;
+    return true;
+}
+
 // Resident blocks of a kernel per SM at kPairThreads threads (its registers and shared memory decide), and the SM
 // count of the current device.
 inline int ResidentBlocks(const void *fn)
@@ -212,13 +225,9 @@ __device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__
         return a;
     };
     auto red1 = [&](long long o) { return R0[o] * inv[D0[o] & 0x7Fu]; };
-    F4 RM = red(-P.PS), RC = red(0);
-    long long o = 0;
-    for (int i = P.i0; i < P.i1; i++, o += P.PS)
-    {
-        const F4 RP = red(o + P.PS), RJp = red(o + P.RS), RJm = red(o - P.RS);
-        const F4 rb = L4(R1 + o);
-        const unsigned db = LdU4(D1 + o);
+    // one plane: red from r, black from the red neighbours
+    auto plane = [&](int i, long long o, const F4 &RM, const F4 &RC, const F4 &RP, const F4 &RJp, const F4 &RJm,
+                     const F4 &rb, unsigned db) {
         float prevW = __shfl_up_sync(0xffffffffu, RC.v[3], 1), nextX = __shfl_down_sync(0xffffffffu, RC.v[0], 1);
         if (P.lane == 0) prevW = P.m0 > 0 ? red1(o - 1) : 0.f;
         if (P.lane == 31) nextX = P.m0 + 4 < P.RS ? red1(o + 4) : 0.f;
@@ -235,12 +244,26 @@ __device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__
             S4(X0 + o, RC);
             S4(X1 + o, nb);
         }
-        RM = RC;
-        RC = RP;
+    };
+    // two planes per trip, all their streamed values loaded first (as in the half-sweep)
+    F4 RM = red(-P.PS), RC = red(0);
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i += 2, o += 2 * P.PS)
+    {
+        const bool two = i + 1 < P.i1;
+        const F4 RP = red(o + P.PS), RPP = two ? red(o + 2 * P.PS) : F4{};
+        const F4 RJp0 = red(o + P.RS), RJm0 = red(o - P.RS);
+        const F4 RJp1 = two ? red(o + P.PS + P.RS) : F4{}, RJm1 = two ? red(o + P.PS - P.RS) : F4{};
+        const F4 rb0 = L4(R1 + o), rb1 = two ? L4(R1 + o + P.PS) : F4{};
+        const unsigned db0 = LdU4(D1 + o), db1 = two ? LdU4(D1 + o + P.PS) : 0u;
+        plane(i, o, RM, RC, RP, RJp0, RJm0, rb0, db0);
+        if (two) plane(i + 1, o + P.PS, RC, RP, RPP, RJp1, RJm1, rb1, db1);
+        RM = RP;
+        RC = RPP;
     }
 }
 
-__global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const uint8_t *__restrict__ du,
+__global__ void __launch_bounds__(kPairThreads, 4) k_split_first(LevelView v, const uint8_t *__restrict__ du,
                                                               const float *__restrict__ r, float *__restrict__ e)
 {
     PdlWait();
@@ -984,6 +1007,18 @@ __device__ __forceinline__ void SplitRefine64(const LevelView &v, const uint8_t 
                                               int slot, const Blk &blk)
 {
     const PairPos P = PairStart(v, blk.x, blk.y, blk.gy);
+    if (v.act)
+    {
+        // the block's pairs lie in rows j0 .. j1; with no unknown there, x_out = x_in + e and r stay zero
+        const long long c0 = 2LL * kPairThreads * blk.x;
+        const int j0 = (int)(c0 / v.Nz), j1 = min(v.Nx - 1, (int)((c0 + 2 * kPairThreads - 1) / v.Nz));
+        if (RowsIdle(v, j0, j1, P.i0, P.i1))
+        {
+            double zero[2] = {0.0, 0.0};
+            GridReduceB<2>(R, zero, slot, BlkId(blk), BlkCount(blk));
+            return;
+        }
+    }
     const long long sb = (long long)P.i0 * v.sPS + (long long)P.j * v.sRS + (P.k0 >> 1);
     // the thread's element on plane i0 in colour 0 and colour 1
     const float *e0 = e + sb, *e1 = e + v.sHalf + sb;
@@ -1060,7 +1095,7 @@ void LaunchSplitRefine64(const LevelView &v, const uint8_t *du, const double *b,
 // run over its own blocks in the same order whatever else the batch holds; the others take the march length S the
 // caller chose (it changes which planes a thread visits, not what a cell gets).
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPairThreads) kb_split_first(const BatchLevel *__restrict__ lv, int ls, int l,
+__global__ void __launch_bounds__(kPairThreads, 4) kb_split_first(const BatchLevel *__restrict__ lv, int ls, int l,
                                                                BatchList a)
 {
     PdlWait();

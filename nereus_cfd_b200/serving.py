@@ -442,12 +442,16 @@ class JobStream:
             import torch
 
             torch.cuda.set_device(device)
+            # a high-priority stream: the requests' fields are drawn while the solves keep the GPU busy
+            lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+            stream = torch.cuda.Stream(device=device, priority=min(lo, hi))
             try:
-                for k, c in enumerate(cases):
-                    t = time.perf_counter()
-                    j = device_job(c, device, tol, *((labels[0][k], labels[1][k]) if labels else ()))
-                    self.make_seconds += time.perf_counter() - t
-                    self.q.put(j)
+                with torch.cuda.stream(stream):
+                    for k, c in enumerate(cases):
+                        t = time.perf_counter()
+                        j = device_job(c, device, tol, *((labels[0][k], labels[1][k]) if labels else ()))
+                        self.make_seconds += time.perf_counter() - t
+                        self.q.put(j)
             except Exception as e:  # reported to the consumer
                 self.error = e
                 self.q.put(None)
