@@ -55,7 +55,9 @@ typedef struct nb_options
     int precision;       /* NB_PRECISION_FP64 or NB_PRECISION_MIXED */
     int max_iters;       /* FP64: PCG iterations; mixed: inner PCG iterations per refinement step */
     int max_outer;       /* mixed: refinement steps */
-    double inner_tol;    /* mixed: relative residual reduction asked of each inner solve */
+    double inner_tol;    /* mixed: relative residual reduction asked of each inner solve; for a tolerance below
+                            inner_tol^2 each inner solve is asked for sqrt(tolerance) instead (at least 1e-6), so
+                            that two refinement passes reach it */
     int pre_sweeps;      /* red-black Gauss-Seidel sweeps before the coarse correction */
     int post_sweeps;     /* ... and after it */
     int coarse_sweeps;   /* symmetric sweep pairs on the coarsest level */
@@ -345,6 +347,8 @@ typedef struct nb_server_stats
     double mean_ms;
     double admitted_gb;      /* estimated device memory of the running requests */
     long long device_completed[8]; /* completions per served device (the first 8) */
+    double layout_s;         /* slots' host seconds in set_layout (hierarchy builds), summed over slots */
+    double project_s;        /* slots' host seconds in the step itself (solve, projection, copies), summed */
 } nb_server_stats;
 
 void nereus_b200_default_server_options(nb_server_options *o);

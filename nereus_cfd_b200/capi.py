@@ -64,7 +64,8 @@ class ServerStats(ctypes.Structure):
                 ("queued", ctypes.c_longlong), ("running", ctypes.c_longlong), ("seconds", ctypes.c_double),
                 ("solves_per_s", ctypes.c_double), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("admitted_gb", ctypes.c_double),
-                ("device_completed", ctypes.c_longlong * 8)]
+                ("device_completed", ctypes.c_longlong * 8), ("layout_s", ctypes.c_double),
+                ("project_s", ctypes.c_double)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "device_completed"}

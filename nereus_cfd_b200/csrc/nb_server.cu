@@ -79,6 +79,7 @@ struct nb_server
     std::vector<double> used;        // admitted bytes per device
     std::vector<long long> doneOn;   // completions per device
     std::vector<double> latencies;   // ms
+    double layoutSeconds = 0.0, projectSeconds = 0.0; // slots' host time in set_layout and in the step
     long long submitted = 0, completed = 0, failed = 0, running = 0;
     uint64_t nextTicket = 1;
     bool started = false, stop = false;
@@ -119,6 +120,7 @@ void nb_server::Slot(int dev)
         nb_result res{};
         int status = NB_OK;
         std::string err;
+        double tLayout = 0.0, tProject = 0.0;
         try
         {
             if (!ctx)
@@ -132,7 +134,9 @@ void nb_server::Slot(int dev)
             const nb_request &r = q->r;
             const double *W[3] = {q->tables[0].data(), q->tables[1].data(), q->tables[2].data()};
             const double *G[3] = {q->tables[3].data(), q->tables[4].data(), q->tables[5].data()};
+            const auto t0 = nb::Clock::now();
             C.SetLayout(r.dim, r.Nx, r.Ny, r.Nz, q->types.data(), W, G, r.non_uniform, r.dh);
+            tLayout = std::chrono::duration<double>(nb::Clock::now() - t0).count();
             if (r.fields_on_device)
             {
                 // the caller's device fields, in place
@@ -155,6 +159,7 @@ void nb_server::Slot(int dev)
                 NB_CK(cudaMemcpyAsync(r.p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
             }
             NB_CK(cudaStreamSynchronize(C.st));
+            tProject = std::chrono::duration<double>(nb::Clock::now() - t0).count() - tLayout;
         }
         catch (...)
         {
@@ -170,6 +175,8 @@ void nb_server::Slot(int dev)
             std::lock_guard<std::mutex> lock(mu);
             used[(size_t)dev] -= q->bytes;
             running--;
+            layoutSeconds += tLayout;
+            projectSeconds += tProject;
             nb::Record &rec = records[q->ticket];
             rec.state = 2;
             rec.status = status;
@@ -364,6 +371,8 @@ int nereus_b200_server_stats(nb_server *srv, nb_server_stats *st)
     double adm = 0.0;
     for (double u : srv->used) adm += u;
     st->admitted_gb = adm / 1e9;
+    st->layout_s = srv->layoutSeconds;
+    st->project_s = srv->projectSeconds;
     for (size_t d = 0; d < srv->doneOn.size() && d < 8; d++) st->device_completed[d] = srv->doneOn[d];
     return (int)NB_OK;
 }
@@ -375,6 +384,7 @@ int nereus_b200_server_reset_stats(nb_server *srv)
     srv->submitted = (long long)srv->queue.size() + srv->running;
     srv->completed = srv->failed = 0;
     srv->latencies.clear();
+    srv->layoutSeconds = srv->projectSeconds = 0.0;
     std::fill(srv->doneOn.begin(), srv->doneOn.end(), 0LL);
     srv->started = false;
     return (int)NB_OK;

@@ -1093,9 +1093,9 @@ __global__ void k_mixed_init(cudaGraphConditionalHandle h, double *S, int *passe
 // A pass's CG targets: r.r down by inner_tol^2 from the unit-form residual of this pass, at most maxIt iterations;
 // the CG loop's condition set to run (a handle's default value is applied when the whole graph is launched, not when
 // an enclosing loop's body starts again).
-__global__ void k_mixed_pass(cudaGraphConditionalHandle hInner, double *S, double sfac, double innerTol, int maxIt)
+__global__ void k_mixed_pass(cudaGraphConditionalHandle hInner, double *S, double sfac, int maxIt)
 {
-    const double rr0 = S[S_RES] * sfac * sfac;
+    const double rr0 = S[S_RES] * sfac * sfac, innerTol = S[S_INTOL];
     S[S_TGT] = rr0 * innerTol * innerTol;
     S[S_MAXIT] = (double)maxIt;
     cudaGraphSetConditional(hInner, 1u);
@@ -1201,7 +1201,7 @@ void Context::BuildSolveGraph()
         NB_CK(cudaMemsetAsync(p32[0].p, 0, p32[0].bytes(), st));
         NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
         NB_COUNT_LAUNCH();
-        k_mixed_pass<<<1, 1, 0, st>>>(hInner, slots.p, sfac, opt.inner_tol, maxIt);
+        k_mixed_pass<<<1, 1, 0, st>>>(hInner, slots.p, sfac, maxIt);
         ok = sinks(deps);
     }
     catch (...)
@@ -1268,7 +1268,11 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
         if (solveExec)
         {
             hostSlots[S_TOL] = tol;
-            NB_CK(cudaMemcpyAsync(slots.p + S_TOL, hostSlots + S_TOL, sizeof(double), cudaMemcpyHostToDevice, st));
+            hostSlots[S_TOL + 1] = 0.0; // S_INNER, set on the device
+            hostSlots[S_INTOL] = InnerTol(tol);
+            static_assert(S_INTOL == S_TOL + 2, "the solve's host-set slots are contiguous");
+            NB_CK(cudaMemcpyAsync(slots.p + S_TOL, hostSlots + S_TOL, 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                  st));
             NB_CK(cudaGraphLaunch(solveExec, st));
             int np = 0;
             NB_CK(cudaMemcpyAsync(hostSlots, slots.p, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
@@ -1319,8 +1323,9 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
             x32.zero(st);
             double rrEnd = 0.0;
             const double rr0 = rr64 * sfac * sfac;
-            inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0,
-                                   rr0 * opt.inner_tol * opt.inner_tol, std::max(1, opt.max_iters), false, &rrEnd);
+            const double it = InnerTol(tolEff);
+            inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0, rr0 * it * it,
+                                   std::max(1, opt.max_iters), false, &rrEnd);
             ProfBegin(NB_K_REFINE, (8.0 + 4.0 + 8.0 + 1.0 + 8.0 + 4.0) * (double)Cells());
             if (Split(0) && !nonuniform)
                 LaunchSplitRefine64(v0, L[0].du.p, b.p, x, x32.p, xo, r32, scale, sfac, red, S_RES, st);

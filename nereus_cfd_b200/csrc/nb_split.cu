@@ -225,9 +225,13 @@ __device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__
         return a;
     };
     auto red1 = [&](long long o) { return R0[o] * inv[D0[o] & 0x7Fu]; };
-    // one plane: red from r, black from the red neighbours
-    auto plane = [&](int i, long long o, const F4 &RM, const F4 &RC, const F4 &RP, const F4 &RJp, const F4 &RJm,
-                     const F4 &rb, unsigned db) {
+    F4 RM = red(-P.PS), RC = red(0);
+    long long o = 0;
+    for (int i = P.i0; i < P.i1; i++, o += P.PS)
+    {
+        const F4 RP = red(o + P.PS), RJp = red(o + P.RS), RJm = red(o - P.RS);
+        const F4 rb = L4(R1 + o);
+        const unsigned db = LdU4(D1 + o);
         float prevW = __shfl_up_sync(0xffffffffu, RC.v[3], 1), nextX = __shfl_down_sync(0xffffffffu, RC.v[0], 1);
         if (P.lane == 0) prevW = P.m0 > 0 ? red1(o - 1) : 0.f;
         if (P.lane == 31) nextX = P.m0 + 4 < P.RS ? red1(o + 4) : 0.f;
@@ -244,26 +248,12 @@ __device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__
             S4(X0 + o, RC);
             S4(X1 + o, nb);
         }
-    };
-    // two planes per trip, all their streamed values loaded first (as in the half-sweep)
-    F4 RM = red(-P.PS), RC = red(0);
-    long long o = 0;
-    for (int i = P.i0; i < P.i1; i += 2, o += 2 * P.PS)
-    {
-        const bool two = i + 1 < P.i1;
-        const F4 RP = red(o + P.PS), RPP = two ? red(o + 2 * P.PS) : F4{};
-        const F4 RJp0 = red(o + P.RS), RJm0 = red(o - P.RS);
-        const F4 RJp1 = two ? red(o + P.PS + P.RS) : F4{}, RJm1 = two ? red(o + P.PS - P.RS) : F4{};
-        const F4 rb0 = L4(R1 + o), rb1 = two ? L4(R1 + o + P.PS) : F4{};
-        const unsigned db0 = LdU4(D1 + o), db1 = two ? LdU4(D1 + o + P.PS) : 0u;
-        plane(i, o, RM, RC, RP, RJp0, RJm0, rb0, db0);
-        if (two) plane(i + 1, o + P.PS, RC, RP, RPP, RJp1, RJm1, rb1, db1);
-        RM = RP;
-        RC = RPP;
+        RM = RC;
+        RC = RP;
     }
 }
 
-__global__ void __launch_bounds__(kPairThreads, 4) k_split_first(LevelView v, const uint8_t *__restrict__ du,
+__global__ void __launch_bounds__(kPairThreads) k_split_first(LevelView v, const uint8_t *__restrict__ du,
                                                               const float *__restrict__ r, float *__restrict__ e)
 {
     PdlWait();

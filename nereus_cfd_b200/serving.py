@@ -536,6 +536,8 @@ def stream_serve(server: Server, cases: Sequence, device: int = 0, tol: float = 
          "make_seconds": round(stream.make_seconds, 3),
          "solves_per_s": round(len(lat) / seconds, 3), "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
          "iters_inner_mean": round(float(np.mean(iters)), 2) if iters else None}
+    st = server.stats()
+    r["slot_layout_s"], r["slot_project_s"] = round(st["layout_s"], 3), round(st["project_s"], 3)
     if rate:
         r["rate_per_s"] = round(rate, 3)
         r["p50_ms_from_arrival"], r["p99_ms_from_arrival"] = pct(lat_due, 0.5), pct(lat_due, 0.99)
