@@ -680,8 +680,7 @@ struct Batch
                 }
                 const double sf = -1.0 / ctx[i]->scale, rr0 = s.rr64 * sf * sf;
                 hInt[np++] = i;
-                const double it = ctx[i]->InnerTol(items[i].tol);
-                hOut[2 * i] = rr0 * it * it;
+                hOut[2 * i] = Context::InnerTarget(rr0, ctx[i]->InnerTol(s.tolEff), s.tolEff, s.bn2, sf);
                 hOut[2 * i + 1] = (double)std::max(1, opt.max_iters);
                 hInt[2 * cap + 2 + i] = s.parity;
             }

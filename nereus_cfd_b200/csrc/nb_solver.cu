@@ -556,6 +556,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
                std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
     }
     if (same) return; // PressureLayoutChanged: nothing moved
+    BlockCacheScope blocks(&blockCache);
     // the same shape (sizes, spacing tables, dh): only the cell types moved, the hierarchy is refilled in place
     bool shapeSame = built && dim_ == dim && Nx_ == Nx && Ny_ == Ny && Nz_ == Nz &&
                      (nonUniform != 0) == nonuniform && dh_ == dh && layout.size() == cells;
@@ -1095,8 +1096,8 @@ __global__ void k_mixed_init(cudaGraphConditionalHandle h, double *S, int *passe
 // an enclosing loop's body starts again).
 __global__ void k_mixed_pass(cudaGraphConditionalHandle hInner, double *S, double sfac, int maxIt)
 {
-    const double rr0 = S[S_RES] * sfac * sfac, innerTol = S[S_INTOL];
-    S[S_TGT] = rr0 * innerTol * innerTol;
+    const double rr0 = S[S_RES] * sfac * sfac, innerTol = S[S_INTOL], q = 0.25 * S[S_TOL] * sfac;
+    S[S_TGT] = fmax(rr0 * innerTol * innerTol, q * q * S[S_BN2]); // as Context::InnerTarget
     S[S_MAXIT] = (double)maxIt;
     cudaGraphSetConditional(hInner, 1u);
 }
@@ -1323,8 +1324,8 @@ int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double 
             x32.zero(st);
             double rrEnd = 0.0;
             const double rr0 = rr64 * sfac * sfac;
-            const double it = InnerTol(tolEff);
-            inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0, rr0 * it * it,
+            const double tgt = InnerTarget(rr0, InnerTol(tolEff), tolEff, bn2, sfac);
+            inner += RunPCG<float>(x32.p, r32, z32, p32[0].p, p32[1].p, q32.p, rr0, tgt,
                                    std::max(1, opt.max_iters), false, &rrEnd);
             ProfBegin(NB_K_REFINE, (8.0 + 4.0 + 8.0 + 1.0 + 8.0 + 4.0) * (double)Cells());
             if (Split(0) && !nonuniform)
@@ -1637,6 +1638,7 @@ void Context::ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnzO
 void Context::EnsureIdp()
 {
     if (idpValid) return;
+    BlockCacheScope blocks(&blockCache);
     const LevelView v0 = L[0].view();
     idp.alloc(Cells());
     lineCounts.alloc((size_t)std::max(v0.nLines, 0) + 1);

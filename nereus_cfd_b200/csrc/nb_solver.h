@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -33,19 +34,83 @@ struct InputError : std::runtime_error
         if (e_ != cudaSuccess) throw ::nb::CudaError(#x, e_);                                                      \
     } while (0)
 
+// The device blocks a context's arrays gave back, kept for the context's later allocations instead of cudaFree'd:
+// cudaFree waits for the whole device, every other context's queued work included, which a server whose slots change
+// shape from request to request cannot afford. A context allocates and launches on its one stream, so the work that
+// used a block is ordered before the block's next use. A block serves requests of half its size and up; the cache
+// holds at most `limit` bytes (the rest is freed), and everything it holds is freed with it or when a cudaMalloc
+// finds the device full.
+struct BlockCache
+{
+    std::multimap<size_t, void *> blocks; // size in bytes -> block
+    size_t cached = 0, limit = (size_t)4 << 30;
+    BlockCache() = default;
+    BlockCache(const BlockCache &) = delete;
+    BlockCache &operator=(const BlockCache &) = delete;
+    ~BlockCache() { flush(); }
+    // a cached block of `bytes` .. 2 `bytes` (its size in *got), or null
+    void *get(size_t bytes, size_t *got)
+    {
+        auto it = blocks.lower_bound(bytes);
+        if (it == blocks.end() || it->first / 2 > bytes) return nullptr;
+        void *p = it->second;
+        *got = it->first;
+        cached -= it->first;
+        blocks.erase(it);
+        return p;
+    }
+    void put(void *p, size_t bytes)
+    {
+        if (cached + bytes > limit)
+        {
+            cudaFree(p);
+            return;
+        }
+        blocks.emplace(bytes, p);
+        cached += bytes;
+    }
+    void flush()
+    {
+        for (auto &b : blocks) cudaFree(b.second);
+        blocks.clear();
+        cached = 0;
+    }
+};
+
+// the cache that DevArray allocations made on this thread draw on (set by a Context around its layout work)
+inline thread_local BlockCache *t_blockCache = nullptr;
+struct BlockCacheScope
+{
+    BlockCache *prev;
+    explicit BlockCacheScope(BlockCache *c) : prev(t_blockCache) { t_blockCache = c; }
+    ~BlockCacheScope() { t_blockCache = prev; }
+};
+
 // A device array that keeps its allocation: a smaller or equal size reuses it (no cudaFree, which would synchronize
-// the device, and no cudaMalloc), a larger one replaces it.
+// the device, and no cudaMalloc), a larger one replaces it. Allocated under a BlockCacheScope, it takes its blocks
+// from that cache and gives them back to it.
 template <typename T> struct DevArray
 {
     T *p = nullptr;
     size_t n = 0, cap = 0;
+    BlockCache *cache = nullptr;
     DevArray() = default;
     DevArray(const DevArray &) = delete;
     DevArray &operator=(const DevArray &) = delete;
-    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n), cap(o.cap) { o.p = nullptr; o.n = o.cap = 0; }
+    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n), cap(o.cap), cache(o.cache)
+    {
+        o.p = nullptr;
+        o.n = o.cap = 0;
+        o.cache = nullptr;
+    }
     DevArray &operator=(DevArray &&o) noexcept
     {
-        if (this != &o) { release(); p = o.p; n = o.n; cap = o.cap; o.p = nullptr; o.n = o.cap = 0; }
+        if (this != &o)
+        {
+            release();
+            p = o.p; n = o.n; cap = o.cap; cache = o.cache;
+            o.p = nullptr; o.n = o.cap = 0; o.cache = nullptr;
+        }
         return *this;
     }
     ~DevArray() { release(); }
@@ -53,9 +118,24 @@ template <typename T> struct DevArray
     {
         if (count == 0) { n = 0; return; }
         if (p && count <= cap) { n = count; return; }
+        BlockCache *c = t_blockCache ? t_blockCache : cache;
         release();
+        cache = c;
+        size_t got = 0;
+        if (c && (p = (T *)c->get(count * sizeof(T), &got)) != nullptr)
+        {
+            n = count;
+            cap = got / sizeof(T);
+            return;
+        }
         cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
-        if (e != cudaSuccess) { p = nullptr; throw CudaError("cudaMalloc", e); }
+        if (e == cudaErrorMemoryAllocation && c && c->cached)
+        {
+            cudaGetLastError();
+            c->flush();
+            e = cudaMalloc((void **)&p, count * sizeof(T));
+        }
+        if (e != cudaSuccess) { p = nullptr; cache = nullptr; throw CudaError("cudaMalloc", e); }
         n = cap = count;
     }
     void zero(cudaStream_t st) { if (p && n) NB_CK(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
@@ -66,7 +146,11 @@ template <typename T> struct DevArray
     }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p)
+        {
+            if (cache) cache->put(p, cap * sizeof(T));
+            else cudaFree(p);
+        }
         p = nullptr;
         n = cap = 0;
     }
@@ -125,6 +209,7 @@ struct LevelData
 
 struct Context
 {
+    BlockCache blockCache; // first, so that it outlives every array that gives its block back to it
     nb_options opt{};
     int device = 0;
     cudaStream_t st = nullptr;
@@ -276,6 +361,14 @@ struct Context
     double InnerTol(double tol) const
     {
         return tol >= opt.inner_tol * opt.inner_tol ? opt.inner_tol : std::max(1e-6, std::sqrt(tol));
+    }
+    // The squared residual, in the inner solve's scaling (rr0 = the pass's starting residual there, sfac the FP64 ->
+    // inner factor), at which a pass's CG loop stops: the pass's relative reduction, or a quarter of the outer
+    // tolerance once that is the looser bound, so that the last pass does no more than the tolerance needs.
+    static double InnerTarget(double rr0, double innerTol, double tol, double bn2, double sfac)
+    {
+        const double q = 0.25 * tol * sfac;
+        return std::max(rr0 * innerTol * innerTol, q * q * bn2);
     }
     void BuildSolveGraph();
     int SolveFP64(double tol, double **xOut, nb_result *out, const double *guess, double refNorm);
