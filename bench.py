@@ -796,6 +796,14 @@ def reference_parity(args, ref_1e8, P, res, idp_mask):
         out["max_div_ref_1e8"] = ref_1e8.max_div
         out["max_div_ratio"] = res.max_div / max(ref_1e8.max_div, 1e-300)
         out["max_div_bar"] = 10.0
+        if ref_1e8.p is not None and ref_1e8.p.size == r12.p.size:
+            # for context: the reference's own solve at the same 1e-8 against its 1e-12 solve
+            x8 = ref_1e8.p[idp_mask]
+            x12 = r12.p[idp_mask]
+            if r12.singular:
+                x8, x12 = x8 - x8.mean(), x12 - x12.mean()
+            out["reference_1e8_pressure_rel_l2"] = float(np.linalg.norm(x8 - x12) / max(np.linalg.norm(x12), 1e-300))
+            out["reference_1e8_rel_res"] = ref_1e8.rel_res
     out["ok"] = bool(err <= 1e-6 and res.rel_res <= TOL and out.get("max_div_ratio", 0.0) <= 10.0)
     return out
 

@@ -63,10 +63,10 @@ LevelView LevelData::view() const
     v.gamma = gamma;
     for (int a = 0; a < 3; a++)
     {
-        v.w[a] = dw[a].p;
-        v.g[a] = dg[a].p;
-        v.w32[a] = dw32[a].p;
-        v.ig32[a] = dig32[a].p;
+        v.w[a] = dw[a];
+        v.g[a] = dg[a];
+        v.w32[a] = dw32[a];
+        v.ig32[a] = dig32[a];
     }
     return v;
 }
@@ -78,18 +78,64 @@ template <> double *LevelData::e<double>() { return e64.p; }
 template <> float *LevelData::res<float>() { return res32.p; }
 template <> double *LevelData::res<double>() { return res64.p; }
 
-static void UploadTables(LevelData &Lv, cudaStream_t st)
+// Every level's spacing tables (Width and FaceGap in FP64, Width and 1/FaceGap in FP32, per axis) packed into one
+// pinned staging buffer and sent in one copy into one device array; the level views point into it. A layout
+// change thus costs one transfer instead of twelve per level. The staging buffer is rewritten only by the next
+// layout, which starts with the stream idle.
+void Context::UploadTables()
 {
-    for (int a = 0; a < 3; a++)
+    auto pad = [](size_t b) { return (b + 15) & ~size_t(15); };
+    size_t bytes = 0;
+    for (const LevelData &Lv : L)
+        for (int a = 0; a < 3; a++)
+            bytes += 2 * pad(Lv.w[a].size() * 8) + 2 * pad(Lv.g[a].size() * 8);
+    if (bytes > tablesHostCap)
     {
-        Lv.dw[a].upload(Lv.w[a].data(), Lv.w[a].size(), st);
-        Lv.dg[a].upload(Lv.g[a].data(), Lv.g[a].size(), st);
-        std::vector<float> w32(Lv.w[a].begin(), Lv.w[a].end()), ig32(Lv.g[a].size());
-        for (size_t q = 0; q < ig32.size(); q++) ig32[q] = (float)(1.0 / Lv.g[a][q]);
-        Lv.dw32[a].upload(w32.data(), w32.size(), st);
-        Lv.dig32[a].upload(ig32.data(), ig32.size(), st);
+        if (tablesHost) NB_CK(cudaFreeHost(tablesHost));
+        tablesHost = nullptr;
+        tablesHostCap = 0;
+        NB_CK(cudaMallocHost((void **)&tablesHost, bytes));
+        tablesHostCap = bytes;
     }
-    NB_CK(cudaStreamSynchronize(st)); // the host vectors above are temporaries
+    tables.alloc(bytes);
+    size_t off = 0;
+    auto put = [&](const void *src, size_t n) {
+        std::memcpy(tablesHost + off, src, n);
+        const size_t at = off;
+        off += pad(n);
+        return at;
+    };
+    struct Off
+    {
+        size_t w, g, w32, ig32;
+    };
+    std::vector<Off> offs(L.size() * 3);
+    for (size_t l = 0; l < L.size(); l++)
+        for (int a = 0; a < 3; a++)
+        {
+            const LevelData &Lv = L[l];
+            Off &o = offs[l * 3 + a];
+            o.w = put(Lv.w[a].data(), Lv.w[a].size() * 8);
+            o.g = put(Lv.g[a].data(), Lv.g[a].size() * 8);
+            float *w32 = (float *)(tablesHost + off);
+            for (size_t q = 0; q < Lv.w[a].size(); q++) w32[q] = (float)Lv.w[a][q];
+            o.w32 = off;
+            off += pad(Lv.w[a].size() * 4);
+            float *ig32 = (float *)(tablesHost + off);
+            for (size_t q = 0; q < Lv.g[a].size(); q++) ig32[q] = (float)(1.0 / Lv.g[a][q]);
+            o.ig32 = off;
+            off += pad(Lv.g[a].size() * 4);
+        }
+    NB_CK(cudaMemcpyAsync(tables.p, tablesHost, off, cudaMemcpyHostToDevice, st));
+    for (size_t l = 0; l < L.size(); l++)
+        for (int a = 0; a < 3; a++)
+        {
+            const Off &o = offs[l * 3 + a];
+            L[l].dw[a] = (const double *)(tables.p + o.w);
+            L[l].dg[a] = (const double *)(tables.p + o.g);
+            L[l].dw32[a] = (const float *)(tables.p + o.w32);
+            L[l].dig32[a] = (const float *)(tables.p + o.ig32);
+        }
 }
 
 // Coarse padded tables of one axis: interior widths summed in pairs, the ring mirroring its neighbour
@@ -142,8 +188,6 @@ void Context::BuildHierarchy()
         for (int a = 0; a < 3; a++) { L0.w[a] = wt[a]; L0.g[a] = gt[a]; }
         L0.types.upload(layout.data(), layout.size(), st);
         L0.code.alloc(layout.size());
-        UploadTables(L0, st);
-        LaunchBuildCodes(L0.view(), L0.code.p, st);
         L.push_back(std::move(L0));
     }
     const int maxLevels = std::max(1, opt.max_levels);
@@ -171,10 +215,15 @@ void Context::BuildHierarchy()
         else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }
         C.types.alloc((size_t)C.cells);
         C.code.alloc((size_t)C.cells);
-        UploadTables(C, st);
-        LaunchCoarsenTypes(F.view(), C.view(), C.types.p, st);
-        LaunchBuildCodes(C.view(), C.code.p, st);
         L.push_back(std::move(C));
+    }
+    // the levels' tables, then their cell types and codes, level by level
+    UploadTables();
+    LaunchBuildCodes(L[0].view(), L[0].code.p, st);
+    for (size_t l = 1; l < L.size(); l++)
+    {
+        LaunchCoarsenTypes(L[l - 1].view(), L[l].view(), L[l].types.p, st);
+        LaunchBuildCodes(L[l].view(), L[l].code.p, st);
     }
     NB_CK(cudaGetLastError());
     // The tail: the first level from which every coarser level has at most opt.tail_cells cells and all of them fit
@@ -395,8 +444,13 @@ Context::~Context()
     if (st) cudaStreamSynchronize(st);
     for (auto &g : graphs) g.Release();
     ReleaseSolveGraph();
+    if (cst) cudaStreamSynchronize(cst);
     for (cudaEvent_t e : evPool) cudaEventDestroy(e);
+    if (evP) cudaEventDestroy(evP);
+    if (evPDone) cudaEventDestroy(evPDone);
+    if (cst) cudaStreamDestroy(cst);
     if (hostSlots) cudaFreeHost(hostSlots);
+    if (tablesHost) cudaFreeHost(tablesHost);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     L.clear();
@@ -604,7 +658,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
             if (dim == 3) CoarseAxis(F.w[2], F.Nz, C.Nz, C.w[2], C.g[2]);
             else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }
         }
-        for (auto &Lv : L) UploadTables(Lv, st); // same sizes: the same device arrays
+        UploadTables(); // same sizes: the same device array
         ReleaseSolveGraph();                     // its refinement step holds the old scale
         RefillHierarchy();
     }
@@ -1096,8 +1150,10 @@ __global__ void k_mixed_init(cudaGraphConditionalHandle h, double *S, int *passe
 // an enclosing loop's body starts again).
 __global__ void k_mixed_pass(cudaGraphConditionalHandle hInner, double *S, double sfac, int maxIt)
 {
-    const double rr0 = S[S_RES] * sfac * sfac, innerTol = S[S_INTOL], q = 0.25 * S[S_TOL] * sfac;
-    S[S_TGT] = fmax(rr0 * innerTol * innerTol, q * q * S[S_BN2]); // as Context::InnerTarget
+    // as Context::InnerTarget
+    const double rr0 = S[S_RES] * sfac * sfac, innerTol = S[S_INTOL], q = S[S_TOL] * sfac;
+    const double t = rr0 * innerTol * innerTol, goal = q * q * S[S_BN2];
+    S[S_TGT] = t > goal ? t : fmin(fmax(t, 0.01 * goal), 0.25 * goal);
     S[S_MAXIT] = (double)maxIt;
     cudaGraphSetConditional(hInner, 1u);
 }
@@ -1500,6 +1556,18 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
     LaunchSubMeanScatter(v0, x, slots.p + S_SUM, n, level ? 1 : 0, p, st);
     LaunchRing(v0, p, st);
     if (incr) LaunchCellwise(v0, CELL_RING_DELTA, p, pPrev, nullptr, st); // the ring carries phi (:321-328)
+    if (hostP && !incr)
+    {
+        // p is final: its copy to the host runs beside the velocity correction
+        if (!cst) NB_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
+        if (!evP) NB_CK(cudaEventCreateWithFlags(&evP, cudaEventDisableTiming));
+        if (!evPDone) NB_CK(cudaEventCreateWithFlags(&evPDone, cudaEventDisableTiming));
+        NB_CK(cudaEventRecord(evP, st));
+        NB_CK(cudaStreamWaitEvent(cst, evP, 0));
+        NB_CK(cudaMemcpyAsync(hostP, p, Cells() * sizeof(double), cudaMemcpyDeviceToHost, cst));
+        NB_CK(cudaEventRecord(evPDone, cst));
+        hostPIssued = true;
+    }
     if (correct)
     {
         ProfBegin(NB_K_PROJECT, (8.0 + 1.0 + 6.0 * 8.0) * (double)Cells());

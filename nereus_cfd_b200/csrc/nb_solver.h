@@ -186,8 +186,9 @@ struct LevelData
     bool stretched = false;
     double gamma = 1.0;
     std::vector<double> w[3], g[3];
-    DevArray<double> dw[3], dg[3];
-    DevArray<float> dw32[3], dig32[3];
+    // the device copies of w, g (FP64) and of w, 1/g (FP32): pointers into the context's packed table array
+    const double *dw[3] = {}, *dg[3] = {};
+    const float *dw32[3] = {}, *dig32[3] = {};
     DevArray<uint8_t> types, code;
     DevArray<uint8_t> du;                 // diagonal units for the pair kernels (nb_pairs.cu); empty elsewhere.
                                           // Colour-split level: in that layout, and the codes on a stretched level
@@ -224,6 +225,9 @@ struct Context
     std::vector<double> wt[3], gt[3];
     std::vector<LevelData> L;
     int tailStart = 0;                       // levels from here down run in one shared-memory block (nb_tail.cu)
+    DevArray<uint8_t> tables;                // every level's spacing tables, packed (UploadTables)
+    uint8_t *tablesHost = nullptr;           // their pinned staging buffer
+    size_t tablesHostCap = 0;
     DevArray<unsigned> tailLists;            // the tail levels' per-colour lists of unknowns (built per layout)
     DevArray<int> tailCounts;
     DevArray<int32_t> idp;
@@ -249,6 +253,13 @@ struct Context
     double *hostSlots = nullptr; // pinned
     Reducer red{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // host-buffer projection (nereus_b200_project): when hostP is set, ProjectDevice copies the final p there on the
+    // copy stream cst as soon as it is final, beside the velocity correction, and sets hostPIssued; evPDone marks the
+    // copy's end
+    double *hostP = nullptr;
+    bool hostPIssued = false;
+    cudaStream_t cst = nullptr;
+    cudaEvent_t evP = nullptr, evPDone = nullptr;
 
     int lastIterations = 0;
 
@@ -363,12 +374,15 @@ struct Context
         return tol >= opt.inner_tol * opt.inner_tol ? opt.inner_tol : std::max(1e-6, std::sqrt(tol));
     }
     // The squared residual, in the inner solve's scaling (rr0 = the pass's starting residual there, sfac the FP64 ->
-    // inner factor), at which a pass's CG loop stops: the pass's relative reduction, or a quarter of the outer
-    // tolerance once that is the looser bound, so that the last pass does no more than the tolerance needs.
+    // inner factor), at which a pass's CG loop stops: the pass's relative reduction. A pass whose reduction already
+    // reaches the outer tolerance (the last one) stops between a tenth and a half of it instead: no further than a
+    // tenth (a warm start's last pass starts far below the first pass's residual), and not above a half, so that the
+    // solution's distance from the exact one does not hang on where the last CG step lands just under the tolerance.
     static double InnerTarget(double rr0, double innerTol, double tol, double bn2, double sfac)
     {
-        const double q = 0.25 * tol * sfac;
-        return std::max(rr0 * innerTol * innerTol, q * q * bn2);
+        const double t = rr0 * innerTol * innerTol, q = tol * sfac, goal = q * q * bn2;
+        if (t > goal) return t;
+        return std::min(std::max(t, 0.01 * goal), 0.25 * goal);
     }
     void BuildSolveGraph();
     int SolveFP64(double tol, double **xOut, nb_result *out, const double *guess, double refNorm);
@@ -386,6 +400,7 @@ struct Context
     size_t VecLen0() const { return L[0].VecLen(); }
     void VCyclePairs(int l, float *r, float *e);
     void VCycleSplit(int l, float *r, float *e);
+    void UploadTables();
     void AssignSplit();
     void BuildTailLists();
     // copyRR: end with the copy of r.r to the host (not inside the device-side loop)

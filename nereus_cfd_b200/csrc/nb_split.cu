@@ -143,6 +143,27 @@ inline int SmCount()
 // the best-filled one (a small level fills no wave: S = 1, all the parallelism there is).
 constexpr int kQuadMaxS = 16;
 
+// The march length S (planes per thread, 1 .. kQuadMaxS) for a grid of perPlane x ceil(planes / S) blocks on `slots`
+// resident blocks, by the rule above.
+inline long long BestMarch(long long perPlane, long long planes, long long slots)
+{
+    long long bestS = 1;
+    double bestU = -1.0;
+    for (long long S = kQuadMaxS; S >= 1; S--)
+    {
+        const long long blocks = perPlane * ((planes + S - 1) / S);
+        const long long waves = (blocks + slots - 1) / slots;
+        const double u = (double)blocks / (double)(waves * slots);
+        if (u >= 0.9) return S;
+        if (u > bestU + 1e-9)
+        {
+            bestU = u;
+            bestS = S;
+        }
+    }
+    return bestS;
+}
+
 // A quad kernel's grid with a march of S planes (S > 0), or sized as above (S = 0).
 inline dim3 QuadGridS(const LevelView &v, int S)
 {
@@ -155,25 +176,7 @@ inline dim3 QuadGrid(const LevelView &v, int resident)
 {
     const long long nq = (long long)v.Nx * (v.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
     const long long planes = v.Ny - 2 > 0 ? v.Ny - 2 : 1;
-    const long long slots = (long long)SmCount() * (resident > 0 ? resident : 1);
-    long long bestS = 1;
-    double bestU = -1.0;
-    for (long long S = kQuadMaxS; S >= 1; S--)
-    {
-        const long long blocks = perPlane * ((planes + S - 1) / S);
-        const long long waves = (blocks + slots - 1) / slots;
-        const double u = (double)blocks / (double)(waves * slots);
-        if (u >= 0.9)
-        {
-            bestS = S;
-            break;
-        }
-        if (u > bestU + 1e-9)
-        {
-            bestU = u;
-            bestS = S;
-        }
-    }
+    const long long bestS = BestMarch(perPlane, planes, (long long)SmCount() * (resident > 0 ? resident : 1));
     return dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS));
 }
 
@@ -596,25 +599,7 @@ inline dim3 ProlongGrid(const LevelView &fine, const LevelView &coarse, int resi
 {
     const long long nq = (long long)(coarse.Nx - 2) * (fine.sRS / 4), perPlane = (nq + kPairThreads - 1) / kPairThreads;
     const long long planes = coarse.Ny - 2 > 0 ? coarse.Ny - 2 : 1;
-    const long long slots = (long long)SmCount() * (resident > 0 ? resident : 1);
-    long long bestS = 1;
-    double bestU = -1.0;
-    for (long long S = kQuadMaxS; S >= 1; S--)
-    {
-        const long long blocks = perPlane * ((planes + S - 1) / S);
-        const long long waves = (blocks + slots - 1) / slots;
-        const double u = (double)blocks / (double)(waves * slots);
-        if (u >= 0.9)
-        {
-            bestS = S;
-            break;
-        }
-        if (u > bestU + 1e-9)
-        {
-            bestU = u;
-            bestS = S;
-        }
-    }
+    const long long bestS = BestMarch(perPlane, planes, (long long)SmCount() * (resident > 0 ? resident : 1));
     return dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS));
 }
 
@@ -791,25 +776,7 @@ void LaunchSplitRestrict(const LevelView &fine, const LevelView &coarse, const u
     }
     const long long nt = (long long)(coarse.Nx - 2) * ((coarse.Nz - 2 + 3) / 4);
     const long long perPlane = (nt + kPairThreads - 1) / kPairThreads, planes = coarse.Ny - 2 > 0 ? coarse.Ny - 2 : 1;
-    const long long slots = (long long)SmCount() * Occ<k_split_restrict>();
-    long long bestS = 1;
-    double bestU = -1.0;
-    for (long long S = kQuadMaxS; S >= 1; S--)
-    {
-        const long long blocks = perPlane * ((planes + S - 1) / S);
-        const long long waves = (blocks + slots - 1) / slots;
-        const double u = (double)blocks / (double)(waves * slots);
-        if (u >= 0.9)
-        {
-            bestS = S;
-            break;
-        }
-        if (u > bestU + 1e-9)
-        {
-            bestU = u;
-            bestS = S;
-        }
-    }
+    const long long bestS = BestMarch(perPlane, planes, (long long)SmCount() * Occ<k_split_restrict>());
     LaunchPdl(k_split_restrict, dim3((unsigned)perPlane, (unsigned)((planes + bestS - 1) / bestS)), kPairThreads, 0,
               st, fine, coarse, pext, resFine, rCoarse);
 }
