@@ -356,7 +356,7 @@ def run_trace(args, dev):
     """The served form (cfg5): `trace` requests of mixed dimension (3D side log-U[32, 256], 2D side log-U[64, 1024]),
     mask (closed, obstacle + outlet, free surface) and spacing (uniform, 1.04-stretched), fields drawn on the device
     just before use (a bounded number ahead, so the trace's memory stays bounded), each to 1e-8 through the server.
-    A closed loop (16 requests in flight) gives the capacity; Poisson arrivals at each fraction of it in
+    A closed loop (two requests in flight per slot) gives the capacity; Poisson arrivals at each fraction of it in
     `trace_rates` give p50/p99 latency (the middle rate twice, for its run-to-run spread). The same requests one at a
     time in plain FP64 on one context (the single-solve form) are the comparison; host wall clock throughout."""
     import torch
@@ -866,10 +866,10 @@ def main():
     ap.add_argument("--opt", action="append", default=[], help="solver option key=value (nb_options field)")
     ap.add_argument("--tanks", type=int, default=64, help="batched tanks (0: skip the batched form)")
     ap.add_argument("--tank-size", type=int, default=128)
-    ap.add_argument("--slots", type=int, default=8, help="concurrent solves per device of the serving trace")
+    ap.add_argument("--slots", type=int, default=4, help="concurrent solves per device of the serving trace")
     ap.add_argument("--tank-steps", type=int, default=5, help="batched steps at least (the timed region >= 1 s)")
     ap.add_argument("--trace", type=int, default=2000, help="requests of the serving trace (0: skip)")
-    ap.add_argument("--trace-rates", default="0.4,0.6,0.8,1.0",
+    ap.add_argument("--trace-rates", default="0.2,0.4,0.6,0.8,1.0",
                     help="Poisson arrival rates of the trace as fractions of the closed-loop capacity")
     ap.add_argument("--stretched-steps", type=int, default=5, help="steps of the stretched workload (0: skip)")
     ap.add_argument("--box2d-steps", type=int, default=10, help="steps of the 2D 128^2 closed box (0: skip)")

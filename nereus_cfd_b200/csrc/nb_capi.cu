@@ -125,24 +125,36 @@ int nereus_b200_project(nb_ctx *ctx, double *u, double *v, double *w, double *p,
         C.dv.upload(v, C.FieldSizeV(), C.st);
         if (C.dim == 3) C.dw.upload(w, C.FieldSizeW(), C.st);
         C.dp.upload(p, C.Cells(), C.st);
-        // p goes back to the host on the context's copy stream once final, beside the velocity correction
-        struct HostP
+        // p and then u, v, w go back to the host on the context's copy stream as soon as each is final, beside the
+        // velocity correction and the divergence check
+        struct HostFields
         {
             nb::Context &C;
-            HostP(nb::Context &c, double *p) : C(c) { C.hostP = p; C.hostPIssued = false; }
-            ~HostP()
+            HostFields(nb::Context &c, double *u, double *v, double *w, double *p) : C(c)
             {
-                if (C.hostPIssued) cudaStreamSynchronize(C.cst); // an error path must not leave the copy running
-                C.hostP = nullptr;
+                C.hostU = u;
+                C.hostV = v;
+                C.hostW = w;
+                C.hostP = p;
+                C.hostCopied = false;
             }
-        } hp(C, p);
+            ~HostFields()
+            {
+                if (C.hostCopied) cudaStreamSynchronize(C.cst); // an error path must not leave the copies running
+                C.hostP = C.hostU = C.hostV = C.hostW = nullptr;
+            }
+        } hf(C, u, v, w, p);
         const int status = C.ProjectDevice(C.du.p, C.dv.p, C.dim == 3 ? C.dw.p : C.du.p, C.dp.p, rho, dt,
                                            needsCompat, tol, r);
-        NB_CK(cudaMemcpyAsync(u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
-        NB_CK(cudaMemcpyAsync(v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
-        if (C.dim == 3) NB_CK(cudaMemcpyAsync(w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
-        if (C.hostPIssued) NB_CK(cudaStreamWaitEvent(C.st, C.evPDone, 0));
-        else NB_CK(cudaMemcpyAsync(p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+        if (C.hostCopied)
+            NB_CK(cudaStreamWaitEvent(C.st, C.evPDone, 0));
+        else
+        {
+            NB_CK(cudaMemcpyAsync(u, C.du.p, C.du.bytes(), cudaMemcpyDeviceToHost, C.st));
+            NB_CK(cudaMemcpyAsync(v, C.dv.p, C.dv.bytes(), cudaMemcpyDeviceToHost, C.st));
+            if (C.dim == 3) NB_CK(cudaMemcpyAsync(w, C.dw.p, C.dw.bytes(), cudaMemcpyDeviceToHost, C.st));
+            NB_CK(cudaMemcpyAsync(p, C.dp.p, C.dp.bytes(), cudaMemcpyDeviceToHost, C.st));
+        }
         NB_CK(cudaStreamSynchronize(C.st));
         return status;
     });

@@ -421,6 +421,7 @@ Context::Context(const nb_options &o) : opt(o)
         NB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         ownStream = true;
     }
+    arrays.Init(device, st);
     red.maxBlocks = 1 << 16; // partial sums per reduction launch (the tile grids stay well below)
     partials.alloc((size_t)red.maxBlocks * 4);
     slots.alloc(S_COUNT);
@@ -454,6 +455,7 @@ Context::~Context()
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     L.clear();
+    arrays.st = nullptr; // the arrays still to go are freed after the stream, on the legacy one (nothing runs now)
     if (ownStream && st) cudaStreamDestroy(st);
 }
 
@@ -610,7 +612,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
                std::memcmp(gt[a].data(), gap[a], ng * 8) == 0;
     }
     if (same) return; // PressureLayoutChanged: nothing moved
-    BlockCacheScope blocks(&blockCache);
+    ArrayPoolScope pooled(&arrays);
     // the same shape (sizes, spacing tables, dh): only the cell types moved, the hierarchy is refilled in place
     bool shapeSame = built && dim_ == dim && Nx_ == Nx && Ny_ == Ny && Nz_ == Nz &&
                      (nonUniform != 0) == nonuniform && dh_ == dh && layout.size() == cells;
@@ -1556,7 +1558,8 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
     LaunchSubMeanScatter(v0, x, slots.p + S_SUM, n, level ? 1 : 0, p, st);
     LaunchRing(v0, p, st);
     if (incr) LaunchCellwise(v0, CELL_RING_DELTA, p, pPrev, nullptr, st); // the ring carries phi (:321-328)
-    if (hostP && !incr)
+    const bool toHost = hostP && !incr && correct;
+    if (toHost)
     {
         // p is final: its copy to the host runs beside the velocity correction
         if (!cst) NB_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
@@ -1565,14 +1568,24 @@ int Context::ProjectDevice(double *u, double *v, double *w, double *p, double rh
         NB_CK(cudaEventRecord(evP, st));
         NB_CK(cudaStreamWaitEvent(cst, evP, 0));
         NB_CK(cudaMemcpyAsync(hostP, p, Cells() * sizeof(double), cudaMemcpyDeviceToHost, cst));
-        NB_CK(cudaEventRecord(evPDone, cst));
-        hostPIssued = true;
+        hostCopied = true;
     }
     if (correct)
     {
         ProfBegin(NB_K_PROJECT, (8.0 + 1.0 + 6.0 * 8.0) * (double)Cells());
         LaunchProject(v0, u, v, w, p, dt / rho, st);
         ProfEnd();
+        if (toHost)
+        {
+            // u, v, w are final: their copies follow p's, beside the divergence check
+            NB_CK(cudaEventRecord(evP, st));
+            NB_CK(cudaStreamWaitEvent(cst, evP, 0));
+            NB_CK(cudaMemcpyAsync(hostU, u, FieldSizeU() * sizeof(double), cudaMemcpyDeviceToHost, cst));
+            NB_CK(cudaMemcpyAsync(hostV, v, FieldSizeV() * sizeof(double), cudaMemcpyDeviceToHost, cst));
+            if (dim == 3)
+                NB_CK(cudaMemcpyAsync(hostW, w, FieldSizeW() * sizeof(double), cudaMemcpyDeviceToHost, cst));
+            NB_CK(cudaEventRecord(evPDone, cst));
+        }
         LaunchMaxDiv(v0, u, v, w, dh, red, S_DIV, st);
     }
     if (incr)
@@ -1706,7 +1719,7 @@ void Context::ExportMatrix(int32_t *rowptr, int32_t *col, double *val, int *nnzO
 void Context::EnsureIdp()
 {
     if (idpValid) return;
-    BlockCacheScope blocks(&blockCache);
+    ArrayPoolScope pooled(&arrays);
     const LevelView v0 = L[0].view();
     idp.alloc(Cells());
     lineCounts.alloc((size_t)std::max(v0.nLines, 0) + 1);

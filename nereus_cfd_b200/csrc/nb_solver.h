@@ -4,7 +4,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -34,82 +33,89 @@ struct InputError : std::runtime_error
         if (e_ != cudaSuccess) throw ::nb::CudaError(#x, e_);                                                      \
     } while (0)
 
-// The device blocks a context's arrays gave back, kept for the context's later allocations instead of cudaFree'd:
-// cudaFree waits for the whole device, every other context's queued work included, which a server whose slots change
-// shape from request to request cannot afford. A context allocates and launches on its one stream, so the work that
-// used a block is ordered before the block's next use. A block serves requests of half its size and up; the cache
-// holds at most `limit` bytes (the rest is freed), and everything it holds is freed with it or when a cudaMalloc
-// finds the device full.
-struct BlockCache
+// The device memory a context's layout-dependent arrays live in: a stream-ordered pool of the context's own
+// (cudaMemPool, nothing released back until the context goes), allocated from and freed to on the context's stream,
+// so the work that used memory is ordered before its next use. A layout change reuses what the context already holds,
+// suballocated by the driver for any size. Plain allocation was measured stalling a busy server: with 4 slots each
+// changing shape per request, cudaMalloc took 10-66 ms even for a few hundred bytes, and every request in flight
+// waited with it (up to 300 ms); cudaFree waits for the whole device.
+struct ArrayPool
 {
-    std::multimap<size_t, void *> blocks; // size in bytes -> block
-    size_t cached = 0, limit = (size_t)4 << 30;
-    BlockCache() = default;
-    BlockCache(const BlockCache &) = delete;
-    BlockCache &operator=(const BlockCache &) = delete;
-    ~BlockCache() { flush(); }
-    // a cached block of `bytes` .. 2 `bytes` (its size in *got), or null
-    void *get(size_t bytes, size_t *got)
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr; // allocations and frees are ordered on it (null: the legacy stream)
+    ArrayPool() = default;
+    ArrayPool(const ArrayPool &) = delete;
+    ArrayPool &operator=(const ArrayPool &) = delete;
+    ~ArrayPool()
     {
-        auto it = blocks.lower_bound(bytes);
-        if (it == blocks.end() || it->first / 2 > bytes) return nullptr;
-        void *p = it->second;
-        *got = it->first;
-        cached -= it->first;
-        blocks.erase(it);
+        if (pool) cudaMemPoolDestroy(pool); // its memory is released once every allocation from it is freed
+    }
+    void Init(int device, cudaStream_t s)
+    {
+        cudaMemPoolProps pr = {};
+        pr.allocType = cudaMemAllocationTypePinned;
+        pr.location.type = cudaMemLocationTypeDevice;
+        pr.location.id = device;
+        NB_CK(cudaMemPoolCreate(&pool, &pr));
+        unsigned long long keep = ~0ull; // the attribute is a 64-bit unsigned
+        NB_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        st = s;
+    }
+    // null when the stream is being captured (the caller allocates plainly then)
+    void *Get(size_t bytes)
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (!pool || cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+        void *p = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, st);
+        if (e == cudaErrorMemoryAllocation)
+        {
+            // memory the pool keeps but nothing uses goes back to the device, then once more
+            cudaGetLastError();
+            cudaStreamSynchronize(st);
+            cudaMemPoolTrimTo(pool, 0);
+            e = cudaMallocFromPoolAsync(&p, bytes, pool, st);
+        }
+        if (e != cudaSuccess) throw CudaError("cudaMallocFromPoolAsync", e);
+        NB_CK(cudaMemsetAsync(p, 0, bytes, st)); // as fresh device memory reads: no earlier owner's values
         return p;
     }
-    void put(void *p, size_t bytes)
-    {
-        if (cached + bytes > limit)
-        {
-            cudaFree(p);
-            return;
-        }
-        blocks.emplace(bytes, p);
-        cached += bytes;
-    }
-    void flush()
-    {
-        for (auto &b : blocks) cudaFree(b.second);
-        blocks.clear();
-        cached = 0;
-    }
+    void Put(void *p) { cudaFreeAsync(p, st); }
 };
 
-// the cache that DevArray allocations made on this thread draw on (set by a Context around its layout work)
-inline thread_local BlockCache *t_blockCache = nullptr;
-struct BlockCacheScope
+// the pool that DevArray allocations made on this thread draw on (set by a Context around its layout work)
+inline thread_local ArrayPool *t_arrayPool = nullptr;
+struct ArrayPoolScope
 {
-    BlockCache *prev;
-    explicit BlockCacheScope(BlockCache *c) : prev(t_blockCache) { t_blockCache = c; }
-    ~BlockCacheScope() { t_blockCache = prev; }
+    ArrayPool *prev;
+    explicit ArrayPoolScope(ArrayPool *c) : prev(t_arrayPool) { t_arrayPool = c; }
+    ~ArrayPoolScope() { t_arrayPool = prev; }
 };
 
 // A device array that keeps its allocation: a smaller or equal size reuses it (no cudaFree, which would synchronize
-// the device, and no cudaMalloc), a larger one replaces it. Allocated under a BlockCacheScope, it takes its blocks
-// from that cache and gives them back to it.
+// the device, and no cudaMalloc), a larger one replaces it. Allocated under an ArrayPoolScope, it takes its memory
+// from that pool and gives it back there.
 template <typename T> struct DevArray
 {
     T *p = nullptr;
     size_t n = 0, cap = 0;
-    BlockCache *cache = nullptr;
+    ArrayPool *pool = nullptr; // where p came from (null: cudaMalloc)
     DevArray() = default;
     DevArray(const DevArray &) = delete;
     DevArray &operator=(const DevArray &) = delete;
-    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n), cap(o.cap), cache(o.cache)
+    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n), cap(o.cap), pool(o.pool)
     {
         o.p = nullptr;
         o.n = o.cap = 0;
-        o.cache = nullptr;
+        o.pool = nullptr;
     }
     DevArray &operator=(DevArray &&o) noexcept
     {
         if (this != &o)
         {
             release();
-            p = o.p; n = o.n; cap = o.cap; cache = o.cache;
-            o.p = nullptr; o.n = o.cap = 0; o.cache = nullptr;
+            p = o.p; n = o.n; cap = o.cap; pool = o.pool;
+            o.p = nullptr; o.n = o.cap = 0; o.pool = nullptr;
         }
         return *this;
     }
@@ -118,24 +124,17 @@ template <typename T> struct DevArray
     {
         if (count == 0) { n = 0; return; }
         if (p && count <= cap) { n = count; return; }
-        BlockCache *c = t_blockCache ? t_blockCache : cache;
+        ArrayPool *c = t_arrayPool ? t_arrayPool : pool;
         release();
-        cache = c;
-        size_t got = 0;
-        if (c && (p = (T *)c->get(count * sizeof(T), &got)) != nullptr)
+        if (c && (p = (T *)c->Get(count * sizeof(T))) != nullptr)
         {
-            n = count;
-            cap = got / sizeof(T);
+            pool = c;
+            n = cap = count;
             return;
         }
+        pool = nullptr;
         cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
-        if (e == cudaErrorMemoryAllocation && c && c->cached)
-        {
-            cudaGetLastError();
-            c->flush();
-            e = cudaMalloc((void **)&p, count * sizeof(T));
-        }
-        if (e != cudaSuccess) { p = nullptr; cache = nullptr; throw CudaError("cudaMalloc", e); }
+        if (e != cudaSuccess) { p = nullptr; throw CudaError("cudaMalloc", e); }
         n = cap = count;
     }
     void zero(cudaStream_t st) { if (p && n) NB_CK(cudaMemsetAsync(p, 0, n * sizeof(T), st)); }
@@ -148,7 +147,7 @@ template <typename T> struct DevArray
     {
         if (p)
         {
-            if (cache) cache->put(p, cap * sizeof(T));
+            if (pool) pool->Put(p);
             else cudaFree(p);
         }
         p = nullptr;
@@ -210,7 +209,7 @@ struct LevelData
 
 struct Context
 {
-    BlockCache blockCache; // first, so that it outlives every array that gives its block back to it
+    ArrayPool arrays; // first, so that it outlives every array that gives its memory back to it
     nb_options opt{};
     int device = 0;
     cudaStream_t st = nullptr;
@@ -254,10 +253,10 @@ struct Context
     Reducer red{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host-buffer projection (nereus_b200_project): when hostP is set, ProjectDevice copies the final p there on the
-    // copy stream cst as soon as it is final, beside the velocity correction, and sets hostPIssued; evPDone marks the
-    // copy's end
-    double *hostP = nullptr;
-    bool hostPIssued = false;
+    // copy stream cst as soon as it is final, beside the velocity correction, then u, v, w to hostU, hostV, hostW as
+    // soon as they are corrected, beside the divergence check, and sets hostCopied; evPDone marks the copies' end
+    double *hostP = nullptr, *hostU = nullptr, *hostV = nullptr, *hostW = nullptr;
+    bool hostCopied = false;
     cudaStream_t cst = nullptr;
     cudaEvent_t evP = nullptr, evPDone = nullptr;
 
