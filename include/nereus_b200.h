@@ -63,11 +63,12 @@ typedef struct nb_options
     int coarse_sweeps;   /* symmetric sweep pairs on the coarsest level */
     int max_levels;      /* multigrid levels at most (>= 1) */
     void *stream;        /* cudaStream_t to launch on; NULL: the context makes its own */
-    int use_graphs;      /* 2 (default): each refinement pass's CG loop runs as one captured CUDA graph, a WHILE
-                            node whose condition the device sets after every iteration (one host synchronisation
-                            per pass); 1: one captured graph per CG iteration (V-cycle included), the loop on the
-                            host; 0: plain launches. The server's slots run 2 as 1: with several slots on one GPU
-                            the per-iteration graphs were measured 6% faster */
+    int use_graphs;      /* 2 (default): the mixed solve runs as one captured CUDA graph, WHILE nodes over the
+                            refinement passes and the CG iterations whose conditions the device sets (one host
+                            synchronisation per solve; the FP64 form: one per restart); 1: one captured graph per
+                            CG iteration (V-cycle included), the loop on the host; 0: plain launches. Graphs are
+                            captured from a layout's second solve on: the first solve after a change of shape
+                            launches plainly (capturing costs more than it saves once). All give the same result */
     int transfer_kernels; /* the restriction of colour-split levels: 0 (default): one thread per 4 coarse cells
                              where the coarse level has at least 2^20 cells, else one thread per coarse cell;
                              1: one thread per coarse cell everywhere; 2: one thread per 4 coarse cells everywhere.

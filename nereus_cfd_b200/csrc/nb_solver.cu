@@ -662,6 +662,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
         }
         UploadTables(); // same sizes: the same device array
         ReleaseSolveGraph();                     // its refinement step holds the old scale
+        solvesOnShape = 0;
         RefillHierarchy();
     }
     else if (shapeSame)
@@ -670,6 +671,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
     {
         for (auto &g : graphs) g.Release(); // they hold the old hierarchy's pointers
         ReleaseSolveGraph();
+        solvesOnShape = 0;
         dim = dim_;
         Nx = Nx_;
         Ny = Ny_;
@@ -704,6 +706,7 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
     {
         for (auto &g : graphs) g.Release(); // the iteration's kernels depend on the flag
         ReleaseSolveGraph();
+        solvesOnShape = 0;
     }
     hostSlots[S_NUNK] = (double)n;
     NB_CK(cudaMemcpyAsync(slots.p + S_NUNK, hostSlots + S_NUNK, sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1037,7 +1040,7 @@ int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double
 {
     NB_CK(cudaMemsetAsync(p0, 0, sizeof(T) * VecLen0(), st));
     NB_CK(cudaMemsetAsync(iter.p, 0, sizeof(int), st));
-    if (opt.use_graphs >= 2 && profMask == 0)
+    if (GraphMode() >= 2 && profMask == 0)
     {
         // the whole loop on the device: one launch, one synchronisation
         IterGraph *L = &graphs[sizeof(T) == 8 ? 1 : 0];
@@ -1064,7 +1067,7 @@ int Context::RunPCG(T *x, T *r, T *z, T *p0, T *p1, T *q, double rrStart, double
         }
     }
     IterGraph *G = nullptr;
-    if (opt.use_graphs)
+    if (GraphMode())
     {
         G = &graphs[sizeof(T) == 8 ? 1 : 0];
         if (G->exec && G->mask != profMask) G->Release();
@@ -1320,7 +1323,7 @@ void Context::BuildSolveGraph()
 
 int Context::SolveMixed(double tol, double **xOut, nb_result *out, const double *guess, double refNorm)
 {
-    if (opt.use_graphs >= 2 && profMask == 0 && !guess && !(refNorm > 0.0) && !solveFailed)
+    if (GraphMode() >= 2 && profMask == 0 && !guess && !(refNorm > 0.0) && !solveFailed)
     {
         // the whole solve on the device: one launch, one synchronisation
         if (!solveExec) BuildSolveGraph();
@@ -1467,8 +1470,10 @@ int Context::Solve(double tol, double **xOut, nb_result *out, const double *gues
         out->iters_inner = out->iters_outer = 0;
         return NB_OK;
     }
-    return opt.precision == NB_PRECISION_MIXED ? SolveMixed(tol, xOut, out, guess, refNorm)
-                                               : SolveFP64(tol, xOut, out, guess, refNorm);
+    const int status = opt.precision == NB_PRECISION_MIXED ? SolveMixed(tol, xOut, out, guess, refNorm)
+                                                           : SolveFP64(tol, xOut, out, guess, refNorm);
+    solvesOnShape++;
+    return status;
 }
 
 // ---------------------------------------------------------------------------------------------------------------

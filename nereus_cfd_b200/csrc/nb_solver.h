@@ -77,7 +77,9 @@ struct ArrayPool
             e = cudaMallocFromPoolAsync(&p, bytes, pool, st);
         }
         if (e != cudaSuccess) throw CudaError("cudaMallocFromPoolAsync", e);
-        NB_CK(cudaMemsetAsync(p, 0, bytes, st)); // as fresh device memory reads: no earlier owner's values
+        // zeroed: a batched solve was measured to differ with the memory's earlier contents once it was recycled
+        // (some cells are read that no kernel of the layout writes), as it never did from fresh cudaMalloc memory
+        NB_CK(cudaMemsetAsync(p, 0, bytes, st));
         return p;
     }
     void Put(void *p) { cudaFreeAsync(p, st); }
@@ -368,6 +370,12 @@ struct Context
     // The relative tolerance asked of each FP32 inner solve for a solve to `tol`: opt.inner_tol, or sqrt(tol) (at
     // least 1e-6) when tol is below opt.inner_tol^2, so that two refinement passes reach it (measured on the 2D
     // 128^2 box to 1e-10: 2 passes and 13 iterations instead of 3 and 17, 1.09 instead of 1.40 ms).
+    // Solves since the last layout change that dropped the captured graphs. The graphs (use_graphs) are captured
+    // from a layout's second solve on: a first solve on a new shape launches plainly, since capturing and
+    // instantiating them costs more than they save once (measured: a 4-slot server whose requests all change shape
+    // served 393 solves/s without them, 225 with them).
+    int solvesOnShape = 0;
+    int GraphMode() const { return solvesOnShape > 0 ? opt.use_graphs : 0; }
     double InnerTol(double tol) const
     {
         return tol >= opt.inner_tol * opt.inner_tol ? opt.inner_tol : std::max(1e-6, std::sqrt(tol));

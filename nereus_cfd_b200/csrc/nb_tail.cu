@@ -15,6 +15,8 @@
 #include "nb_kernels.h"
 
 #include <cstring>
+#include <mutex>
+#include <set>
 
 namespace nb
 {
@@ -504,9 +506,8 @@ template <typename T> size_t TailSmemBytes(const LevelView *levels, int nlev)
     return bytes;
 }
 
-template <typename T> bool PrepareTail(size_t bytes)
+template <typename T> static bool PrepareTailOnce()
 {
-    if (bytes > kTailMaxSmem) return false;
     if (sizeof(T) == 4 &&
         cudaFuncSetAttribute(kb_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTailMaxSmem) != cudaSuccess)
         return false;
@@ -514,6 +515,22 @@ template <typename T> bool PrepareTail(size_t bytes)
            cudaSuccess;
 }
 
+// Once per device and precision: changing a kernel's attribute on every layout change would take the driver's
+// locks under a server's running solves.
+template <typename T> bool PrepareTail(size_t bytes)
+{
+    if (bytes > kTailMaxSmem) return false;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    static std::mutex mu;
+    static std::set<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    const int key = 2 * dev + (sizeof(T) == 4 ? 0 : 1);
+    if (done.count(key)) return true;
+    if (!PrepareTailOnce<T>()) return false;
+    done.insert(key);
+    return true;
+}
 // The coarse end's arguments of one request (FP32), for a batch's table in device memory: *bytes = their size,
 // and when out is not null they are written there; *smem = the dynamic shared memory of its launch.
 void TailArgsFor(const LevelView *levels, int nlev, const float *rIn, float *eOut, int pre, int post,

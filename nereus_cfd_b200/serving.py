@@ -433,6 +433,12 @@ class JobStream:
         import queue
         import threading
 
+        # device memory for the fields and their temporaries (about 48 B per cell), reserved up front in the
+        # producer stream's cache: a cudaMalloc while solves run holds up every thread on the device (measured: tens
+        # to hundreds of ms), so making a request must not call it
+        sizes = sorted((c.grid.cells for c in cases), reverse=True)[: ahead + 4]
+        reserve = 48 * sum(sizes)
+
         self.q = queue.Queue(maxsize=max(1, ahead))
         self.n = len(cases)
         self.error = None
@@ -447,6 +453,8 @@ class JobStream:
             stream = torch.cuda.Stream(device=device, priority=min(lo, hi))
             try:
                 with torch.cuda.stream(stream):
+                    block = torch.empty(reserve, dtype=torch.uint8, device="cuda:%d" % device)
+                    del block  # stays in this stream's cache; the requests' tensors are carved out of it
                     for k, c in enumerate(cases):
                         t = time.perf_counter()
                         j = device_job(c, device, tol, *((labels[0][k], labels[1][k]) if labels else ()))
