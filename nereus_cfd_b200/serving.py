@@ -424,6 +424,9 @@ def trace_labels(cases: Sequence, device: int = 0):
     return host, dev
 
 
+_PRODUCERS = {}  # device -> (the job producers' stream, bytes reserved in its cache)
+
+
 class JobStream:
     """The device jobs of a list of cases, made by a background thread a bounded number ahead of use (so a long
     trace never holds more than `ahead` unsubmitted requests' fields on the device). Iterate to take them in order.
@@ -448,13 +451,18 @@ class JobStream:
             import torch
 
             torch.cuda.set_device(device)
-            # a high-priority stream: the requests' fields are drawn while the solves keep the GPU busy
-            lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
-            stream = torch.cuda.Stream(device=device, priority=min(lo, hi))
+            # a high-priority stream, one per device for every stream of jobs (torch caches memory per stream, so the
+            # reservation below serves later streams too): the fields are drawn while the solves keep the GPU busy
+            stream, held = _PRODUCERS.get(device, (None, 0))
+            if stream is None:
+                lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+                stream = torch.cuda.Stream(device=device, priority=min(lo, hi))
             try:
                 with torch.cuda.stream(stream):
-                    block = torch.empty(reserve, dtype=torch.uint8, device="cuda:%d" % device)
-                    del block  # stays in this stream's cache; the requests' tensors are carved out of it
+                    if reserve > held:
+                        block = torch.empty(reserve, dtype=torch.uint8, device="cuda:%d" % device)
+                        del block  # stays in this stream's cache; the requests' tensors are carved out of it
+                    _PRODUCERS[device] = (stream, max(held, reserve))
                     for k, c in enumerate(cases):
                         t = time.perf_counter()
                         j = device_job(c, device, tol, *((labels[0][k], labels[1][k]) if labels else ()))
