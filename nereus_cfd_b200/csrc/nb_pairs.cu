@@ -264,12 +264,74 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_residual(LevelView v, con
 // off the unknowns), weighted per direction. The first sweep from zero is a red pass writing r/diag (and zero on
 // black) followed by a black pass.
 // ---------------------------------------------------------------------------------------------------------------
-// sum_q c_q x_q over the six neighbours of unknown cell (i, j, k) and its diagonal; neighbours in NbrOffset order
-__device__ __forceinline__ float StSum(const LevelView &v, int i, int j, int k, long long c, unsigned code, float nP,
-                                       float nM, float nJp, float nJm, float nKp, float nKm, float &diag)
+// The table entries of a pair's two cells (i, j, k0 + h) that do not change along a thread's march over the planes
+// i: Width x of row j and 1/FaceGap x on its sides, Width z of both cells and 1/FaceGap z on their sides. With them
+// a plane costs two table reads (Width y and the upper 1/FaceGap y; the lower one is the plane before's upper) where
+// LevelCoefs reads nine; the products are LevelCoefs' own, in its order.
+struct StPair
+{
+    float wx, igx0, igx1;
+    float wz[2], igz[3];
+};
+
+__device__ __forceinline__ StPair StPairOf(const LevelView &v, int j, int k0)
+{
+    StPair S;
+    S.wx = v.w32[0][j + 1];
+    S.igx0 = v.ig32[0][j];
+    S.igx1 = v.ig32[0][j + 1];
+    S.wz[0] = v.w32[2][k0 + 1];
+    S.wz[1] = v.w32[2][k0 + 2];
+    S.igz[0] = v.ig32[2][k0];
+    S.igz[1] = v.ig32[2][k0 + 1];
+    S.igz[2] = v.ig32[2][k0 + 2];
+    return S;
+}
+
+// LevelCoefs of cell (i, j, k0 + h) from the pair's entries and plane i's Width y and 1/FaceGap y below and above
+__device__ __forceinline__ void StCoefs(const StPair &S, int h, float wy, float igyLo, float igyHi, float c[6])
+{
+    const float wz = S.wz[h];
+    const float ax = wy * wz, ay = S.wx * wz, az = S.wx * wy;
+    c[0] = ay * igyHi;
+    c[1] = ay * igyLo;
+    c[2] = ax * S.igx1;
+    c[3] = ax * S.igx0;
+    c[4] = az * S.igz[h + 1];
+    c[5] = az * S.igz[h];
+}
+
+// CodeStencil's diagonal from given coefficients: the FLUID neighbours' coefficients, then the Dirichlet ones (a
+// ring neighbour's weighted by the ring factor)
+__device__ __forceinline__ float StDiag(const LevelView &v, int i, int j, int k, long long c, unsigned code,
+                                        const float cq[6])
+{
+    const unsigned m = code & CODE_FLUID_MASK;
+    float d = 0.f;
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        if (m >> q & 1u) d += cq[q];
+    if (code & CODE_DIRICHLET)
+        for (int q = 0; q < 6; q++)
+        {
+            const int t = v.types[c + NbrOffset(v, q)];
+            if (IsDirichlet(t))
+            {
+                const int ni = i + (q == 0) - (q == 1), nj = j + (q == 2) - (q == 3), nk = k + (q == 4) - (q == 5);
+                d += OnRing(v, ni, nj, nk) ? cq[q] * LevelRingFactor<float>(v, i, j, k, q) : cq[q];
+            }
+        }
+    return d;
+}
+
+// sum_q c_q x_q over the six neighbours of unknown cell (i, j, k0 + h) and its diagonal; neighbours in NbrOffset order
+__device__ __forceinline__ float StSum(const LevelView &v, const StPair &S, int h, float wy, float igyLo, float igyHi,
+                                       int i, int j, int k, long long c, unsigned code, float nP, float nM, float nJp,
+                                       float nJm, float nKp, float nKm, float &diag)
 {
     float cq[6];
-    CodeStencil<float>(v, i, j, k, c, code, cq, diag);
+    StCoefs(S, h, wy, igyLo, igyHi, cq);
+    diag = StDiag(v, i, j, k, c, code, cq);
     return ((cq[0] * nP + cq[1] * nM) + (cq[2] * nJp + cq[3] * nJm)) + (cq[4] * nKp + cq[5] * nKm);
 }
 
@@ -284,9 +346,12 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_half_st(LevelView v, cons
     const uint8_t *cp = v.code + P.base;
     float *ep = e + P.base;
     float2 eM = kFirst ? make_float2(0.f, 0.f) : Ld2(ep - P.sI), eC = kFirst ? make_float2(0.f, 0.f) : Ld2(ep);
+    const StPair SP = StPairOf(v, P.j, P.k0);
+    float igyLo = v.ig32[1][P.i0];
     int off = 0;
     for (int i = P.i0; i < P.i1; i++, off += P.sI)
     {
+        const float wy = v.w32[1][i + 1], igyHi = v.ig32[1][i + 1];
         float2 eP = make_float2(0.f, 0.f), eJp = eP, eJm = eP;
         if (!kFirst)
         {
@@ -315,12 +380,13 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_half_st(LevelView v, cons
             if (kFirst)
             {
                 float cq[6];
-                CodeStencil<float>(v, i, P.j, k, c, code, cq, diag);
+                StCoefs(SP, h, wy, igyLo, igyHi, cq);
+                diag = StDiag(v, i, P.j, k, c, code, cq);
             }
             else if (second)
-                s = StSum(v, i, P.j, k, c, code, eP.y, eM.y, eJp.y, eJm.y, right, eC.x, diag);
+                s = StSum(v, SP, h, wy, igyLo, igyHi, i, P.j, k, c, code, eP.y, eM.y, eJp.y, eJm.y, right, eC.x, diag);
             else
-                s = StSum(v, i, P.j, k, c, code, eP.x, eM.x, eJp.x, eJm.x, eC.y, left, diag);
+                s = StSum(v, SP, h, wy, igyLo, igyHi, i, P.j, k, c, code, eP.x, eM.x, eJp.x, eJm.x, eC.y, left, diag);
             nv = diag != 0.f ? ((second ? rc.y : rc.x) + s) / diag : 0.f;
         }
         if (P.valid)
@@ -339,6 +405,7 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_half_st(LevelView v, cons
         }
         eM = eC;
         eC = eP;
+        igyLo = igyHi;
     }
     if (kDot)
     {
@@ -357,9 +424,12 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_residual_st(LevelView v, 
     const uint8_t *cp = v.code + P.base;
     float *op = res + P.base;
     float2 eM = Ld2(ep - P.sI), eC = Ld2(ep);
+    const StPair SP = StPairOf(v, P.j, P.k0);
+    float igyLo = v.ig32[1][P.i0];
     int off = 0;
     for (int i = P.i0; i < P.i1; i++, off += P.sI)
     {
+        const float wy = v.w32[1][i + 1], igyHi = v.ig32[1][i + 1];
         const float2 eP = Ld2(ep + off + P.sI);
         const float2 eJp = Ld2(ep + off + P.sJ), eJm = Ld2(ep + off - P.sJ);
         const float2 rc = Ld2(rp + off);
@@ -375,19 +445,21 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_residual_st(LevelView v, 
             float diag;
             if (d & 0x80u)
             {
-                const float s = StSum(v, i, P.j, P.k0, c, d & 0xFFu, eP.x, eM.x, eJp.x, eJm.x, eC.y, left, diag);
+                const float s = StSum(v, SP, 0, wy, igyLo, igyHi, i, P.j, P.k0, c, d & 0xFFu, eP.x, eM.x, eJp.x,
+                                      eJm.x, eC.y, left, diag);
                 o.x = rc.x - (diag * eC.x - s);
             }
             if (d & 0x8000u)
             {
-                const float s = StSum(v, i, P.j, P.k0 + 1, c + 1, (d >> 8) & 0xFFu, eP.y, eM.y, eJp.y, eJm.y, right,
-                                      eC.x, diag);
+                const float s = StSum(v, SP, 1, wy, igyLo, igyHi, i, P.j, P.k0 + 1, c + 1, (d >> 8) & 0xFFu, eP.y,
+                                      eM.y, eJp.y, eJm.y, right, eC.x, diag);
                 o.y = rc.y - (diag * eC.y - s);
             }
             *reinterpret_cast<float2 *>(op + off) = o;
         }
         eM = eC;
         eC = eP;
+        igyLo = igyHi;
     }
 }
 
@@ -636,9 +708,17 @@ __global__ void __launch_bounds__(kPairThreads)
     };
     float2 NM = pnew(-P.sI), NC = pnew(0);
     float facc = 0.f;
+    StPair SP{};
+    float igyLo = 0.f;
+    if (kSt)
+    {
+        SP = StPairOf(v, P.j, P.k0);
+        igyLo = v.ig32[1][P.i0];
+    }
     int off = 0;
     for (int i = P.i0; i < P.i1; i++, off += P.sI)
     {
+        const float wy = kSt ? v.w32[1][i + 1] : 0.f, igyHi = kSt ? v.ig32[1][i + 1] : 0.f;
         const float2 NP = pnew(off + P.sI);
         const float2 NJp = pnew(off + P.sJ), NJm = pnew(off - P.sJ);
         const unsigned d = LdDu(dp + off);
@@ -655,14 +735,14 @@ __global__ void __launch_bounds__(kPairThreads)
             float diag;
             if (d & 0x80u)
             {
-                const float s = StSum(v, i, P.j, P.k0, P.base + off, d & 0xFFu, NP.x, NM.x, NJp.x, NJm.x, NC.y, left,
-                                      diag);
+                const float s = StSum(v, SP, 0, wy, igyLo, igyHi, i, P.j, P.k0, P.base + off, d & 0xFFu, NP.x, NM.x,
+                                      NJp.x, NJm.x, NC.y, left, diag);
                 qq.x = diag * NC.x - s;
             }
             if (d & 0x8000u)
             {
-                const float s = StSum(v, i, P.j, P.k0 + 1, P.base + off + 1, (d >> 8) & 0xFFu, NP.y, NM.y, NJp.y,
-                                      NJm.y, right, NC.x, diag);
+                const float s = StSum(v, SP, 1, wy, igyLo, igyHi, i, P.j, P.k0 + 1, P.base + off + 1, (d >> 8) & 0xFFu,
+                                      NP.y, NM.y, NJp.y, NJm.y, right, NC.x, diag);
                 qq.y = diag * NC.y - s;
             }
         }
@@ -679,6 +759,7 @@ __global__ void __launch_bounds__(kPairThreads)
         }
         NM = NC;
         NC = NP;
+        igyLo = igyHi;
     }
     double acc[1] = {facc};
     GridReduce<1>(R, acc, slotPQ);
