@@ -462,7 +462,7 @@ Context::~Context()
 // ---- per-kernel timing: events from a pool, bracketing launches of the selected kernel ids ----
 void Context::ProfBegin(int id, double bytes, int launches)
 {
-    if (!(profMask >> id & 1u)) return;
+    if (profQuiet || !(profMask >> id & 1u)) return;
     cudaEvent_t a;
     if (capturing)
     {
@@ -488,9 +488,10 @@ void Context::ProfBegin(int id, double bytes, int launches)
     profLaunches = launches;
 }
 
-void Context::ProfEnd()
+void Context::ProfEnd(int launches)
 {
-    if (profOpen < 0) return;
+    if (profQuiet || profOpen < 0) return;
+    if (launches >= 0) profLaunches = launches;
     cudaEvent_t b;
     if (capturing)
     {
@@ -718,6 +719,20 @@ void Context::SetLayout(int dim_, int Nx_, int Ny_, int Nz_, const uint8_t *type
 // ---------------------------------------------------------------------------------------------------------------
 // multigrid V-cycle and PCG
 // ---------------------------------------------------------------------------------------------------------------
+// The levels below level 0 of one V-cycle under one bracket of the per-kernel timing (NB_K_COARSE): their dozens
+// of short kernels then overlap their dependent launches as in an unprofiled solve, where a bracket of events around
+// each (a few us apiece) would both inflate and serialise them.
+template <typename T> void Context::CoarseBracket(int l, T *r, T *e)
+{
+    const long long n0 = g_launches.load();
+    ProfBegin(NB_K_COARSE, 0.0);
+    const bool quiet = profQuiet;
+    profQuiet = true;
+    VCycle<T>(l, r, e);
+    profQuiet = quiet;
+    ProfEnd((int)(g_launches.load() - n0));
+}
+
 template <typename T> void Context::VCycle(int l, T *r, T *e)
 {
     LevelData &Lv = L[l];
@@ -783,7 +798,8 @@ template <typename T> void Context::VCycle(int l, T *r, T *e)
     prof(NB_K_RESTRICT0, s + s / 8.0);
     LaunchRestrict<T>(v, vc, res, Lc.r<T>(), st);
     ProfEnd();
-    VCycle<T>(l + 1, Lc.r<T>(), Lc.e<T>());
+    if (l == 0) CoarseBracket<T>(l + 1, Lc.r<T>(), Lc.e<T>());
+    else VCycle<T>(l + 1, Lc.r<T>(), Lc.e<T>());
     prof(NB_K_PROLONG0, 2.0 * s + s / 8.0 + 1.0);
     LaunchProlong<T>(v, vc, Lc.e<T>(), e, st);
     ProfEnd();
@@ -845,7 +861,8 @@ void Context::VCyclePairs(int l, float *r, float *e)
     prof(NB_K_RESTRICT0, s + s / 8.0);
     LaunchPairRestrict(v, vc, Lv.pext.p, res, Lc.r<float>(), st);
     ProfEnd();
-    VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
+    if (l == 0) CoarseBracket<float>(l + 1, Lc.r<float>(), Lc.e<float>());
+    else VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
     prof(NB_K_PROLONG0, 2.0 * s + s / 8.0 + 1.0);
     LaunchPairProlong(v, vc, Lv.pext.p, Lc.e<float>(), e, st);
     ProfEnd();
@@ -903,7 +920,8 @@ void Context::VCycleSplit(int l, float *r, float *e)
     prof(NB_K_RESTRICT0, (s + 1.0) / 2.0 + s / 8.0);
     LaunchSplitRestrict(v, vc, Lv.pext.p, res, Lc.r<float>(), opt.transfer_kernels, st);
     ProfEnd();
-    VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
+    if (l == 0) CoarseBracket<float>(l + 1, Lc.r<float>(), Lc.e<float>());
+    else VCycle<float>(l + 1, Lc.r<float>(), Lc.e<float>());
     prof(NB_K_PROLONG0, s + 0.5 + s / 8.0); // reads and writes red e, reads the red bytes and the coarse e
     LaunchSplitProlong(v, vc, Lv.pext.p, Lc.e<float>(), e, st);
     ProfEnd();

@@ -289,7 +289,9 @@ struct Context
     int profLaunches = 1;
     // events around the next `launches` launches of kernel `id` (back to back on the stream), `bytes` in all
     void ProfBegin(int id, double bytes, int launches = 1);
-    void ProfEnd();
+    void ProfEnd(int launches = -1); // launches >= 0: the bracket's kernel count, set at its end
+    bool profQuiet = false;          // inside a bracket that covers several kernels: their own brackets are skipped
+    template <typename T> void CoarseBracket(int l, T *r, T *e);
     void ProfClear();
     void ProfFlush();
     void ProfRead(int id, int *launches, double *ms, double *bytesPerLaunch);
