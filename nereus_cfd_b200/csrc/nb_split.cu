@@ -439,9 +439,9 @@ __device__ __forceinline__ void SplitResidual(const LevelView &v, const uint8_t 
         const F4 oP = L4(O + o + P.PS), oPP = two ? L4(O + o + 2 * P.PS) : F4{};
         const F4 jp0 = L4(O + o + P.RS), jm0 = L4(O + o - P.RS);
         const F4 jp1 = two ? L4(O + o + P.PS + P.RS) : F4{}, jm1 = two ? L4(O + o + P.PS - P.RS) : F4{};
-        const F4 x0 = L4(Xr + o), r0 = L4(Rr + o), x1 = two ? L4(Xr + o + P.PS) : F4{},
-                 r1 = two ? L4(Rr + o + P.PS) : F4{};
-        const unsigned d0 = LdU4(D + o), d1 = two ? LdU4(D + o + P.PS) : 0u;
+        const F4 x0 = L4(Xr + o), r0 = L4Once(Rr + o), x1 = two ? L4(Xr + o + P.PS) : F4{},
+                 r1 = two ? L4Once(Rr + o + P.PS) : F4{};
+        const unsigned d0 = LdU4Once(D + o), d1 = two ? LdU4Once(D + o + P.PS) : 0u;
         plane(i, o, oM, oC, oP, jp0, jm0, x0, r0, d0);
         if (two) plane(i + 1, o + P.PS, oC, oP, oPP, jp1, jm1, x1, r1, d1);
         oM = oP;
