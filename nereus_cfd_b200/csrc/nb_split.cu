@@ -240,8 +240,8 @@ __device__ __forceinline__ void SplitFirst(const LevelView &v, const uint8_t *__
     for (int i = P.i0; i < P.i1; i++, o += P.PS)
     {
         const F4 RP = red(o + P.PS), RJp = red(o + P.RS), RJm = red(o - P.RS);
-        const F4 rb = L4(R1 + o);
-        const unsigned db = LdU4(D1 + o);
+        const F4 rb = L4Once(R1 + o);
+        const unsigned db = LdU4Once(D1 + o);
         float prevW = __shfl_up_sync(0xffffffffu, RC.v[3], 1), nextX = __shfl_down_sync(0xffffffffu, RC.v[0], 1);
         if (P.lane == 0) prevW = P.m0 > 0 ? red1(o - 1) : 0.f;
         if (P.lane == 31) nextX = P.m0 + 4 < P.RS ? red1(o + 4) : 0.f;
