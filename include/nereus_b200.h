@@ -413,7 +413,8 @@ int nereus_b200_batch_project_device(nb_batch *batch, int count, const nb_batch_
 int nereus_b200_batch_info(nb_batch *batch, nb_batch_info *info);
 /* The autotuner (host only). choose: the candidate index to keep given the candidates' times (the fastest, unless
  * the fallback is within 3% of it; ties within 0.5% to the earlier one). key: the cache key of a (grid, level,
- * kernel kind 0-4, capacity) into buf, returning its length. The cache holds one line per key, "key|S|mode|us":
+ * kernel kind 0-4, capacity) into buf, returning its length. The cache holds one line per key, "key|S|mode|us"
+ * (mode records a restriction level's kernel; it is not tuned and a loaded mode is not applied, only S is):
  * dump writes it into buf (returning its full length), load adds lines of that form (returning the count, or
  * NB_BAD_INPUT for a malformed text), clear empties it. */
 int nereus_b200_tune_choose(int n, const double *times, int fallback);

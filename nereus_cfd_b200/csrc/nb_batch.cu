@@ -15,8 +15,9 @@
 //     projection) run per request on the batch's stream.
 // Each request's sums run over its own blocks in a fixed order, so its result does not depend on the other requests
 // of the batch (alone or in any mix, in any slot, the same bits); the autotuner only picks shapes that cannot change
-// a result: the march length of the smoothing, residual and transfer kernels and the restriction's kernel (one
-// thread per coarse cell or per four), timed on the batch itself and cached by (grid, level, kind, capacity). The
+// a result: the march length of the smoothing, residual and transfer kernels, timed on the batch itself and cached
+// by (grid, level, kind, capacity). The restriction's kernel (one thread per coarse cell or per four) is not tuned:
+// inlined into the batched kernels the two round differently, so it follows the fixed rule of the single solve. The
 // batched kernels inline the same bodies as the single-context ones into other kernels, where the compiler may fuse
 // products into FMAs differently, so a batched request and its single-context solve agree to FP32 rounding in the
 // inner solve and within the solve's tolerance in the result.
@@ -41,7 +42,7 @@ namespace tune
 struct Choice
 {
     int S = 0;    // march length (planes per thread)
-    int mode = 0; // restriction: 1 one thread per coarse cell, 2 one per four
+    int mode = 0; // restriction: the kernel the level ran (1 per coarse cell, 2 per four); recorded, not chosen
     double us = 0.0;
 };
 std::mutex g_mu;
@@ -509,7 +510,7 @@ struct Batch
         NB_COUNT_LAUNCHES(-loopLaunches);
     }
 
-    // ---- the autotuner: per level and kind the march length (and the restriction's kernel), on this batch ----
+    // ---- the autotuner: per level and kind the march length, on this batch ----
     void Tune(int count)
     {
         tuning.assign(nLev, LevelTune{});
@@ -551,41 +552,33 @@ struct Batch
                 const LevelView &v = views[l];
                 const std::string key = tune::Key(v.Nx, v.Ny, v.Nz, l, k, cap);
                 tune::Choice c;
+                // a cached entry gives the march only: the restriction's kernel stays the fixed rule's, whatever an
+                // entry records, since the two kernels do not give the same bits in the batched form
                 if (tune::Find(key, &c))
                 {
                     T.S[k] = c.S;
-                    if (k == NB_BK_RESTRICT && c.mode) T.mode = c.mode;
                     continue;
                 }
-                // candidates: the default shape first, then marches of 1 .. 32 planes; both restriction kernels
-                struct Cand
+                // candidates: the default march first, then marches of 1 .. 32 planes
+                const int mode = k == NB_BK_RESTRICT ? T.mode : 0;
+                std::vector<int> cands{T.S[k]};
+                for (int S = 1; S <= 32; S *= 2)
                 {
-                    int S, mode;
-                };
-                std::vector<Cand> cands;
-                cands.push_back({T.S[k], k == NB_BK_RESTRICT ? T.mode : 0});
-                const int modes = k == NB_BK_RESTRICT && opt.transfer_kernels == 0 ? 2 : 1;
-                for (int m = 0; m < modes; m++)
-                    for (int S = 1; S <= 32; S *= 2)
-                    {
-                        if (S > planes && S != 1) break;
-                        const int mode = k == NB_BK_RESTRICT ? (modes == 2 ? m + 1 : T.mode) : 0;
-                        if (S == cands[0].S && mode == cands[0].mode) continue;
-                        cands.push_back({S, mode});
-                    }
+                    if (S > planes && S != 1) break;
+                    if (S != cands[0]) cands.push_back(S);
+                }
                 std::vector<double> times;
-                for (const Cand &cd : cands)
+                for (const int S : cands)
                     times.push_back(timeIt([&] {
                         const LevelView *coarse = (k == NB_BK_RESTRICT || k == NB_BK_PROLONG) ? &views[l + 1] : nullptr;
-                        LaunchBatchSplit(k, views[l], coarse, cd.S, cd.mode, dLev.p, ls, l, dReq.p, a, cap, 0, st);
+                        LaunchBatchSplit(k, views[l], coarse, S, mode, dLev.p, ls, l, dReq.p, a, cap, 0, st);
                     }));
                 const int pick = tune::Choose((int)times.size(), times.data(), 0);
-                c.S = cands[pick].S;
-                c.mode = cands[pick].mode;
+                c.S = cands[pick];
+                c.mode = mode;
                 c.us = times[pick];
                 tune::Put(key, c);
                 T.S[k] = c.S;
-                if (k == NB_BK_RESTRICT) T.mode = c.mode;
             }
         }
         NB_CK(cudaEventRecord(c1, st));
