@@ -70,9 +70,9 @@ typedef struct nb_options
                             captured from a layout's second solve on: the first solve after a change of shape
                             launches plainly (capturing costs more than it saves once). All give the same result */
     int transfer_kernels; /* the restriction of colour-split levels: 0 (default): one thread per 4 coarse cells
-                             where the coarse level has at least 2^20 cells, else one thread per coarse cell;
-                             1: one thread per coarse cell everywhere; 2: one thread per 4 coarse cells everywhere.
-                             All three give the same result */
+                             where the coarse level has at least 2^20 cells, else one thread per coarse cell (a
+                             batch: per 4 everywhere); 1: one thread per coarse cell everywhere; 2: one thread per 4
+                             coarse cells everywhere. All three give the same result in a single solve */
     int pair_kernels;    /* FP32 kernels of the mixed form on 3D levels with Nz even (uniform or stretched):
                             2 (default): the colour-split layout, red and black cells in separate arrays, so that
                             one colour's sweep moves half the bytes; 1: cell pairs in the grid layout; 0: the
