@@ -87,6 +87,11 @@ typedef struct nb_options
     int skip_idle_tiles; /* 1 (default): on colour-split levels a block whose cells hold no unknown (the air of a
                             free-surface tank, a solid) skips its loads and stores; 0: every block works. Both give the
                             same result */
+    int x_groups;        /* stretched 3D grids: 1 (default): coarsening pairs two x cells only where the pair is at
+                            most 1.5 times as wide as a coarse y/z cell, and keeps the others whole, on every level
+                            above the coarse end (the coarse cells stay near cubes, so point smoothing holds on
+                            strongly stretched x); 0: every axis coarsened by two. y and z are always coarsened by
+                            two. The iteration counts differ, the tolerance is met either way */
 } nb_options;
 
 typedef struct nb_result
@@ -418,6 +423,11 @@ int nereus_b200_batch_info(nb_batch *batch, nb_batch_info *info);
  * dump writes it into buf (returning its full length), load adds lines of that form (returning the count, or
  * NB_BAD_INPUT for a malformed text), clear empties it. */
 int nereus_b200_tune_choose(int n, const double *times, int fallback);
+/* The x groups a stretched 3D level's coarsening makes (x_groups = 1; host only): n interior x widths, yz_min the
+ * thinnest interior y or z width. Left to right, two cells form one coarse cell when together they are at most
+ * 1.5 coarse y/z cells (3 yz_min) wide, else a cell stays whole. Writes each group's cell count (1 or 2) into
+ * counts (room for n) and returns the number of groups, or NB_BAD_INPUT. */
+int nereus_b200_x_groups(const double *widths, int n, double yz_min, int32_t *counts);
 int nereus_b200_tune_key(int Nx, int Ny, int Nz, int level, int kind, int capacity, char *buf, int size);
 int nereus_b200_tune_cache_dump(char *buf, int size);
 int nereus_b200_tune_cache_load(const char *text);

@@ -30,7 +30,8 @@ class Options(ctypes.Structure):
                 ("post_sweeps", ctypes.c_int), ("coarse_sweeps", ctypes.c_int), ("max_levels", ctypes.c_int),
                 ("stream", ctypes.c_void_p), ("use_graphs", ctypes.c_int), ("transfer_kernels", ctypes.c_int),
                 ("pair_kernels", ctypes.c_int), ("tail_cells", ctypes.c_int), ("stretched_sweeps", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("skip_idle_tiles", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("skip_idle_tiles", ctypes.c_int),
+                ("x_groups", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -205,6 +206,7 @@ SIGNATURES = {
                                                         ctypes.POINTER(Result)]),
     "nereus_b200_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchInfo)]),
     "nereus_b200_tune_choose": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int]),
+    "nereus_b200_x_groups": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_double, _ip]),
     "nereus_b200_tune_key": (ctypes.c_int, [ctypes.c_int] * 6 + [ctypes.c_char_p, ctypes.c_int]),
     "nereus_b200_tune_cache_dump": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "nereus_b200_tune_cache_load": (ctypes.c_int, [ctypes.c_char_p]),

@@ -44,6 +44,7 @@ void nereus_b200_default_options(nb_options *o)
     o->stretched_sweeps = 2;
     o->autotune = 1;
     o->skip_idle_tiles = 1;
+    o->x_groups = 1;
 }
 
 const char *nereus_b200_last_error(void) { return g_error.c_str(); }
@@ -573,6 +574,15 @@ int nereus_b200_label_cells(int dim, int Nx, int Ny, int Nz, const double *cx, c
         cudaStreamDestroy(st);
         return (int)NB_OK;
     });
+}
+
+int nereus_b200_x_groups(const double *widths, int n, double yz_min, int32_t *counts)
+{
+    if (!widths || !counts || n < 1 || !(yz_min > 0.0)) return Fail(NB_BAD_INPUT, "bad x widths");
+    std::vector<int> c;
+    nb::PlanXGroups(widths, n, yz_min, c);
+    for (size_t g = 0; g < c.size(); g++) counts[g] = c[g];
+    return (int)c.size();
 }
 
 } // extern "C"

@@ -51,7 +51,34 @@ struct LevelView
     // tile counts as holding one. A block whose planes' tiles hold none skips its work: its cells stay zero.
     const uint8_t *act;
     int actTiles;
+    // The x (mid-axis) groups of the transfer from this level to the next coarser one, where that coarsening keeps
+    // some x cells whole (a stretched 3D level); null: cells 2J-1 and 2J under coarse J, as along the other axes.
+    // xp[j] per fine j: parent J (bits 0-14), the other x contributor (bits 15-29; J itself when the parent has one
+    // child) and bit 30 when the parent has one child (x weights 1 and 0, else 3/4 and 1/4).
+    // xr[J] per coarse J: first child (bits 0-14), bit 15 when J has two children, bit 16 when the group before J
+    // has two (its second child gives J a quarter), bit 17 when the group after J has two (its first child does).
+    const int *xp, *xr;
 };
+
+__device__ __forceinline__ int XpParent(int x) { return x & 0x7FFF; }
+__device__ __forceinline__ int XpOther(int x) { return (x >> 15) & 0x7FFF; }
+__device__ __forceinline__ bool XpSingle(int x) { return (x >> 30) & 1; }
+
+// The fine x cells that coarse J gathers from, with their weights (zero weight: an unused slot at a valid index);
+// slots 1 and 2 are J's children (slot 2 only when it has two)
+template <typename T> __device__ __forceinline__ void XrTaps(int x, int (&b)[4], T (&w)[4], bool &two)
+{
+    const int f0 = x & 0x7FFF;
+    two = (x >> 15) & 1;
+    b[0] = (x >> 16) & 1 ? f0 - 1 : f0;
+    w[0] = (x >> 16) & 1 ? (T)0.25 : (T)0;
+    b[1] = f0;
+    w[1] = two ? (T)0.75 : (T)1;
+    b[2] = two ? f0 + 1 : f0;
+    w[2] = two ? (T)0.75 : (T)0;
+    b[3] = (x >> 17) & 1 ? f0 + (two ? 2 : 1) : f0;
+    w[3] = (x >> 17) & 1 ? (T)0.25 : (T)0;
+}
 
 // Index of cell (i, j, k) in a level vector of the level's layout.
 __device__ __forceinline__ long long VecIdx(const LevelView &v, int i, int j, int k)

@@ -201,7 +201,14 @@ __global__ void k_coarsen_types(LevelView f, LevelView cv, uint8_t *ct)
             if (2 * C <= Nf - 2) out[cnt++] = 2 * C;
         };
         kids(I, cv.Ny, f.Ny, ia, ni);
-        kids(J, cv.Nx, f.Nx, ja, nj);
+        if (f.xr)
+        {
+            const int x = f.xr[J];
+            ja[0] = x & 0x7FFF;
+            ja[1] = ja[0] + 1;
+            nj = (x >> 15) & 1 ? 2 : 1;
+        }
+        else kids(J, cv.Nx, f.Nx, ja, nj);
         if (cv.dim == 3) kids(K, cv.Nz, f.Nz, ka, nk);
         else { ka[0] = 0; nk = 1; }
         bool anyDir = false, anyFluid = false;
@@ -381,13 +388,117 @@ __global__ void __launch_bounds__(256) k_restrict(LevelView fv, LevelView cv, co
     }
 }
 
+// The same two operators where the coarsening keeps some x cells whole (3D, LevelView::xp / xr): along x a fine cell
+// gives its parent 1 (a parent of one child) or 3/4 and the neighbouring coarse cell on its side 1/4; along y and z
+// 3/4 and 1/4 as above. SolidWeightX: the weight the prolongation moves onto the parent of fine cell (., b, .) from
+// its SOLID contributors (si, sk: the directions of its other contributors along i and k).
+template <typename T>
+__device__ __forceinline__ T SolidWeightX(const LevelView &fv, const LevelView &cv, int I, int J, int K, int si, int b,
+                                          int sk)
+{
+    const int x = fv.xp[b];
+    const bool one = XpSingle(x);
+    const int J2 = XpOther(x);
+    const T wv[2] = {(T)0.75, (T)0.25};
+    const T wj[2] = {one ? (T)1 : (T)0.75, (T)0.25};
+    T extra = (T)0;
+    for (int di = 0; di < 2; di++)
+        for (int dj = 0; dj < (one ? 1 : 2); dj++)
+            for (int dk = 0; dk < 2; dk++)
+            {
+                if (!(di | dj | dk)) continue;
+                const long long cc = (long long)(I + di * si) * cv.sI + (long long)(dj ? J2 : J) * cv.sJ + K + dk * sk;
+                if (cv.types[cc] == SOLID) extra += wv[di] * wj[dj] * wv[dk];
+            }
+    return extra;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict_x(LevelView fv, LevelView cv, const T *__restrict__ res,
+                                                    T *__restrict__ rc)
+{
+    NB_TILE_LOOP(cv)
+    {
+        int I, J, K;
+        long long c;
+        if (!TileCell(cv, fo, mo, s, I, J, K, c)) continue;
+        if (!(cv.code[c] & CODE_UNKNOWN)) continue;
+        int bq[4];
+        T wq[4];
+        bool two;
+        XrTaps<T>(fv.xr[J], bq, wq, two);
+        const T wt[4] = {(T)0.25, (T)0.75, (T)0.75, (T)0.25};
+        T acc = (T)0;
+        for (int di = 0; di < 4; di++)
+        {
+            const int a = 2 * I - 2 + di;
+            if (a > fv.Ny - 1) continue;
+            for (int dj = 0; dj < 4; dj++)
+            {
+                if (wq[dj] == (T)0) continue;
+                const long long rowBase = (long long)a * fv.sI + (long long)bq[dj] * fv.sJ;
+                T t = (T)0;
+#pragma unroll
+                for (int dk = 0; dk < 4; dk++)
+                {
+                    const int d = 2 * K - 2 + dk;
+                    if (d <= fv.Nz - 1) t += wt[dk] * res[rowBase + d];
+                }
+                acc += (wt[di] * wq[dj]) * t;
+            }
+        }
+        for (int ci = 0; ci < 2; ci++)
+            for (int cj = 0; cj < (two ? 2 : 1); cj++)
+                for (int ck = 0; ck < 2; ck++)
+                {
+                    const int a = 2 * I - 1 + ci, b = bq[1] + cj, d = 2 * K - 1 + ck;
+                    if (a > fv.Ny - 2 || d > fv.Nz - 2) continue;
+                    const T extra = SolidWeightX<T>(fv, cv, I, J, K, ci ? 1 : -1, b, ck ? 1 : -1);
+                    if (extra != (T)0) acc += extra * res[(long long)a * fv.sI + (long long)b * fv.sJ + d];
+                }
+        rc[c] = acc;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_x(LevelView fv, LevelView cv, const T *__restrict__ ec, T *ef)
+{
+    NB_TILE_LOOP(fv)
+    {
+        int a, b, d;
+        long long c;
+        if (!TileCell(fv, fo, mo, s, a, b, d, c)) continue;
+        if (!(fv.code[c] & CODE_UNKNOWN)) continue;
+        const int A = (a + 1) >> 1, D = (d + 1) >> 1;
+        const int si = (a & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
+        const int x = fv.xp[b];
+        const int B = XpParent(x), B2 = XpOther(x);
+        const bool one = XpSingle(x);
+        const T wv[2] = {(T)0.75, (T)0.25};
+        const T wj[2] = {one ? (T)1 : (T)0.75, (T)0.25};
+        const long long parent = (long long)A * cv.sI + (long long)B * cv.sJ + D;
+        T acc = (T)0, extra = (T)0;
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < (one ? 1 : 2); dj++)
+                for (int dk = 0; dk < 2; dk++)
+                {
+                    const long long cc = (long long)(A + di * si) * cv.sI + (long long)(dj ? B2 : B) * cv.sJ + D + dk * sk;
+                    const T w = wv[di] * wj[dj] * wv[dk];
+                    if ((di | dj | dk) && cv.types[cc] == SOLID) extra += w; // Neumann: the parent's value
+                    else acc += w * ec[cc];
+                }
+        ef[c] += acc + extra * ec[parent];
+    }
+}
+
 template <typename T>
 void LaunchRestrict(const LevelView &fine, const LevelView &coarse, const T *resFine, T *rCoarse, cudaStream_t st)
 {
     if (coarse.fastLen <= 0 || coarse.midLen <= 0) return;
     const LevelView o = OnePlane(coarse);
     NB_COUNT_LAUNCH();
-    k_restrict<T><<<TileGrid(o), kTile, 0, st>>>(fine, o, resFine, rCoarse);
+    if (fine.xr) k_restrict_x<T><<<TileGrid(o), kTile, 0, st>>>(fine, o, resFine, rCoarse);
+    else k_restrict<T><<<TileGrid(o), kTile, 0, st>>>(fine, o, resFine, rCoarse);
 }
 
 template <typename T>
@@ -425,7 +536,8 @@ void LaunchProlong(const LevelView &fine, const LevelView &coarse, const T *eCoa
     if (fine.fastLen <= 0 || fine.midLen <= 0) return;
     const LevelView o = OnePlane(fine);
     NB_COUNT_LAUNCH();
-    k_prolong<T><<<TileGrid(o), kTile, 0, st>>>(o, coarse, eCoarse, eFine);
+    if (fine.xp) k_prolong_x<T><<<TileGrid(o), kTile, 0, st>>>(o, coarse, eCoarse, eFine);
+    else k_prolong<T><<<TileGrid(o), kTile, 0, st>>>(o, coarse, eCoarse, eFine);
 }
 
 // ---------------------------------------------------------------------------------------------------------------

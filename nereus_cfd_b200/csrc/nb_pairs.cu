@@ -531,18 +531,28 @@ __global__ void k_build_pext(LevelView fv, LevelView cv, uint8_t *pext)
         const long long o = VecIdx(fv, a, b, d);
         const bool interior = a > 0 && a < fv.Ny - 1 && b > 0 && b < fv.Nx - 1 && d > 0 && d < fv.Nz - 1;
         if (!interior || fv.types[c] != FLUID) { pext[o] = 0; continue; }
-        const int A = (a + 1) >> 1, B = (b + 1) >> 1, D = (d + 1) >> 1;
-        const int si = (a & 1) ? -1 : 1, sj = (b & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
-        const int w[2] = {3, 1};
+        const int A = (a + 1) >> 1, D = (d + 1) >> 1;
+        const int si = (a & 1) ? -1 : 1, sk = (d & 1) ? -1 : 1;
+        // along x (j): the parent and the neighbour on the cell's side, 3/4 and 1/4; with x groups (xp) a parent of
+        // one child takes all of it
+        int B = (b + 1) >> 1, B2 = B + ((b & 1) ? -1 : 1), wj0 = 3, wj1 = 1;
+        if (fv.xp)
+        {
+            const int x = fv.xp[b];
+            B = XpParent(x);
+            B2 = XpOther(x);
+            if (XpSingle(x)) { wj0 = 4; wj1 = 0; }
+        }
+        const int w[2] = {3, 1}, wj[2] = {wj0, wj1};
         unsigned extra = 0;
         for (int di = 0; di < 2; di++)
             for (int dj = 0; dj < 2; dj++)
                 for (int dk = 0; dk < 2; dk++)
                 {
                     if (!(di | dj | dk)) continue;
-                    const long long cc = (long long)(A + di * si) * cv.sI + (long long)(B + dj * sj) * cv.sJ +
+                    const long long cc = (long long)(A + di * si) * cv.sI + (long long)(dj ? B2 : B) * cv.sJ +
                                          (D + dk * sk);
-                    if (cv.types[cc] == SOLID) extra += (unsigned)(w[di] * w[dj] * w[dk]);
+                    if (cv.types[cc] == SOLID) extra += (unsigned)(w[di] * wj[dj] * w[dk]);
                 }
         pext[o] = (uint8_t)(0x80u | extra);
     }
@@ -558,6 +568,8 @@ void LaunchBuildPext(const LevelView &fine, const LevelView &coarse, uint8_t *pe
 }
 
 // e_f += P e_c on the fine unknowns; one thread per fine pair (k0 even: parents k0/2 and k0/2 + 1 along k).
+// kX: the coarsening keeps some x cells whole (LevelView::xp gives the x parent, the other contributor, their weights)
+template <bool kX>
 __global__ void __launch_bounds__(kPairThreads) k_pair_prolong(LevelView fv, LevelView cv,
                                                                const uint8_t *__restrict__ pext,
                                                                const float *__restrict__ ec, float *ef)
@@ -571,14 +583,36 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_prolong(LevelView fv, Lev
         if (!P.valid || !(x & 0x8080u)) continue;
         const int b = P.j;
         const int A = (a + 1) >> 1, A2 = A + ((a & 1) ? -1 : 1);
-        const int B = (b + 1) >> 1, B2 = B + ((b & 1) ? -1 : 1);
+        int B = (b + 1) >> 1, B2 = B + ((b & 1) ? -1 : 1);
+        bool one = false;
+        if constexpr (kX)
+        {
+            const int xq = fv.xp[b];
+            B = XpParent(xq);
+            B2 = XpOther(xq);
+            one = XpSingle(xq);
+        }
         const float *r00 = ec + (long long)A * cv.sI + (long long)B * cv.sJ + m;
         const float *r01 = ec + (long long)A * cv.sI + (long long)B2 * cv.sJ + m;
         const float *r10 = ec + (long long)A2 * cv.sI + (long long)B * cv.sJ + m;
         const float *r11 = ec + (long long)A2 * cv.sI + (long long)B2 * cv.sJ + m;
         // rows weighted 3/4 (parent's row and plane) and 1/4 across i and j, then along k
-        const float lo = 0.5625f * r00[0] + 0.1875f * (r01[0] + r10[0]) + 0.0625f * r11[0];
-        const float hi = 0.5625f * r00[1] + 0.1875f * (r01[1] + r10[1]) + 0.0625f * r11[1];
+        float lo, hi;
+        if (!kX)
+        {
+            lo = 0.5625f * r00[0] + 0.1875f * (r01[0] + r10[0]) + 0.0625f * r11[0];
+            hi = 0.5625f * r00[1] + 0.1875f * (r01[1] + r10[1]) + 0.0625f * r11[1];
+        }
+        else if (one) // one x child: the parent's row and column only along x
+        {
+            lo = 0.75f * r00[0] + 0.25f * r10[0];
+            hi = 0.75f * r00[1] + 0.25f * r10[1];
+        }
+        else
+        {
+            lo = 0.75f * (0.75f * r00[0] + 0.25f * r01[0]) + 0.25f * (0.75f * r10[0] + 0.25f * r11[0]);
+            hi = 0.75f * (0.75f * r00[1] + 0.25f * r01[1]) + 0.25f * (0.75f * r10[1] + 0.25f * r11[1]);
+        }
         float2 v = *reinterpret_cast<float2 *>(ef + P.base + off);
         if (x & 0x80u) v.x += (0.75f * lo + 0.25f * hi) + (float)(x & 0x3Fu) * (1.0f / 64.0f) * r00[0];
         if (x & 0x8000u) v.y += (0.75f * hi + 0.25f * lo) + (float)((x >> 8) & 0x3Fu) * (1.0f / 64.0f) * r00[1];
@@ -590,7 +624,8 @@ void LaunchPairProlong(const LevelView &fine, const LevelView &coarse, const uin
                        float *eFine, cudaStream_t st)
 {
     NB_COUNT_LAUNCH();
-    k_pair_prolong<<<PairGrid(fine), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+    if (fine.xp) k_pair_prolong<true><<<PairGrid(fine), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
+    else k_pair_prolong<false><<<PairGrid(fine), kPairThreads, 0, st>>>(fine, coarse, pext, eCoarse, eFine);
 }
 
 // r_c = R res_f = P^T res_f at the coarse unknowns. A thread owns one coarse cell (K along the 32 lanes, J across
@@ -622,6 +657,30 @@ __device__ __forceinline__ void RestrictPlane(const LevelView &fv, const uint8_t
     X *= 1.0f / 64.0f;
 }
 
+// The same plane sum where the coarsening keeps some x cells whole: the x taps of coarse J (XrTaps) replace the
+// fixed 2J-2 .. 2J+1; a warp holds one J, so the skipped taps do not diverge.
+__device__ __forceinline__ void RestrictPlaneX(const LevelView &fv, const uint8_t *pext, const float *res, int a,
+                                               int K, const int (&bq)[4], const float (&wq)[4], bool two, float &T,
+                                               float &X)
+{
+    T = 0.f;
+    X = 0.f;
+    if (a > fv.Ny - 1) return;
+#pragma unroll
+    for (int dj = 0; dj < 4; dj++)
+    {
+        if (wq[dj] == 0.f) continue;
+        const long long row = (long long)a * fv.sI + (long long)bq[dj] * fv.sJ + 2 * K - 2;
+        const float2 u = *reinterpret_cast<const float2 *>(res + row);
+        const float2 w = *reinterpret_cast<const float2 *>(res + row + 2);
+        T += wq[dj] * ((0.25f * u.x + 0.75f * u.y) + (0.75f * w.x + 0.25f * w.y));
+        if (dj == 1 || (dj == 2 && two))
+            X += (float)(pext[row + 1] & 0x3Fu) * u.y + (float)(pext[row + 2] & 0x3Fu) * w.x;
+    }
+    X *= 1.0f / 64.0f;
+}
+
+template <bool kX>
 __global__ void __launch_bounds__(256) k_pair_restrict(LevelView fv, LevelView cv, const uint8_t *__restrict__ pext,
                                                        const float *__restrict__ res, float *__restrict__ rc)
 {
@@ -631,14 +690,22 @@ __global__ void __launch_bounds__(256) k_pair_restrict(LevelView fv, LevelView c
     const int S = (cv.Ny - 2 + (int)gridDim.z - 1) / (int)gridDim.z;
     const int I0 = 1 + (int)blockIdx.z * S, I1 = min(I0 + S, cv.Ny - 1);
     if (I0 >= I1) return;
+    int bq[4] = {0, 0, 0, 0};
+    float wq[4] = {0.f, 0.f, 0.f, 0.f};
+    bool two = false;
+    if constexpr (kX) XrTaps<float>(fv.xr[J], bq, wq, two);
+    auto plane = [&](int a, float &T, float &X) {
+        if constexpr (kX) RestrictPlaneX(fv, pext, res, a, K, bq, wq, two, T, X);
+        else RestrictPlane(fv, pext, res, a, J, K, T, X);
+    };
     float Tm2, Tm1, Xm1, Xdummy;
-    RestrictPlane(fv, pext, res, 2 * I0 - 2, J, K, Tm2, Xdummy);
-    RestrictPlane(fv, pext, res, 2 * I0 - 1, J, K, Tm1, Xm1);
+    plane(2 * I0 - 2, Tm2, Xdummy);
+    plane(2 * I0 - 1, Tm1, Xm1);
     for (int I = I0; I < I1; I++)
     {
         float T0, X0, T1, X1;
-        RestrictPlane(fv, pext, res, 2 * I, J, K, T0, X0);
-        RestrictPlane(fv, pext, res, 2 * I + 1, J, K, T1, X1);
+        plane(2 * I, T0, X0);
+        plane(2 * I + 1, T1, X1);
         const long long c = (long long)I * cv.sI + (long long)J * cv.sJ + K;
         if (cv.code[c] & CODE_UNKNOWN)
             rc[c] = ((0.25f * Tm2 + 0.75f * Tm1) + (0.75f * T0 + 0.25f * T1)) + (Xm1 + X0);
@@ -656,7 +723,8 @@ void LaunchPairRestrict(const LevelView &fine, const LevelView &coarse, const ui
     const dim3 grid((unsigned)((coarse.Nz - 2 + 31) / 32), (unsigned)((coarse.Nx - 2 + 7) / 8),
                     (unsigned)((coarse.Ny - 2 + S - 1) / S));
     NB_COUNT_LAUNCH();
-    k_pair_restrict<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
+    if (fine.xr) k_pair_restrict<true><<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
+    else k_pair_restrict<false><<<grid, dim3(32, 8), 0, st>>>(fine, coarse, pext, resFine, rCoarse);
 }
 
 // ---------------------------------------------------------------------------------------------------------------

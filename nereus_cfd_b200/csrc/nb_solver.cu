@@ -61,6 +61,8 @@ LevelView LevelData::view() const
     v.actTiles = sRS ? actTiles : 0;
     v.stretched = stretched ? 1 : 0;
     v.gamma = gamma;
+    v.xp = dxp;
+    v.xr = dxr;
     for (int a = 0; a < 3; a++)
     {
         v.w[a] = dw[a];
@@ -87,8 +89,11 @@ void Context::UploadTables()
     auto pad = [](size_t b) { return (b + 15) & ~size_t(15); };
     size_t bytes = 0;
     for (const LevelData &Lv : L)
+    {
         for (int a = 0; a < 3; a++)
             bytes += 2 * pad(Lv.w[a].size() * 8) + 2 * pad(Lv.g[a].size() * 8);
+        bytes += pad(Lv.xp.size() * 4) + pad(Lv.xr.size() * 4);
+    }
     if (bytes > tablesHostCap)
     {
         if (tablesHost) NB_CK(cudaFreeHost(tablesHost));
@@ -100,7 +105,7 @@ void Context::UploadTables()
     tables.alloc(bytes);
     size_t off = 0;
     auto put = [&](const void *src, size_t n) {
-        std::memcpy(tablesHost + off, src, n);
+        if (n) std::memcpy(tablesHost + off, src, n);
         const size_t at = off;
         off += pad(n);
         return at;
@@ -126,6 +131,12 @@ void Context::UploadTables()
             o.ig32 = off;
             off += pad(Lv.g[a].size() * 4);
         }
+    std::vector<size_t> xOff(2 * L.size());
+    for (size_t l = 0; l < L.size(); l++)
+    {
+        xOff[2 * l] = put(L[l].xp.data(), L[l].xp.size() * 4);
+        xOff[2 * l + 1] = put(L[l].xr.data(), L[l].xr.size() * 4);
+    }
     NB_CK(cudaMemcpyAsync(tables.p, tablesHost, off, cudaMemcpyHostToDevice, st));
     for (size_t l = 0; l < L.size(); l++)
         for (int a = 0; a < 3; a++)
@@ -136,6 +147,11 @@ void Context::UploadTables()
             L[l].dw32[a] = (const float *)(tables.p + o.w32);
             L[l].dig32[a] = (const float *)(tables.p + o.ig32);
         }
+    for (size_t l = 0; l < L.size(); l++)
+    {
+        L[l].dxp = L[l].xp.empty() ? nullptr : (const int *)(tables.p + xOff[2 * l]);
+        L[l].dxr = L[l].xr.empty() ? nullptr : (const int *)(tables.p + xOff[2 * l + 1]);
+    }
 }
 
 // Coarse padded tables of one axis: interior widths summed in pairs, the ring mirroring its neighbour
@@ -164,6 +180,77 @@ static void CoarseAxis(const std::vector<double> &wFine, int Nf, int Nc, std::ve
     }
 }
 
+// The x groups of a stretched 3D level's coarsening: left to right, two interior x cells form one coarse cell when
+// together they are at most 1.5 coarse y/z cells wide (twice the thinnest interior y or z cell), else a cell stays
+// whole. Returns false when that is every cell paired by two (the regular coarsening); otherwise the padded coarse x
+// tables (as CoarseAxis), the coarse extent and the transfer maps of LevelView::xp / xr.
+void PlanXGroups(const double *w, int n, double yzMin, std::vector<int> &count)
+{
+    const double target = 1.5 * 2.0 * yzMin;
+    count.clear();
+    for (int j = 0; j < n;)
+    {
+        const bool two = j + 1 < n && w[j] + w[j + 1] <= target;
+        count.push_back(two ? 2 : 1);
+        j += two ? 2 : 1;
+    }
+}
+
+static bool XGroups(const LevelData &F, int &Nc, std::vector<double> &wOut, std::vector<double> &gOut,
+                    std::vector<int> &xp, std::vector<int> &xr)
+{
+    const int nf = F.Nx - 2;
+    double yz = 1e300;
+    for (int a = 1; a <= 2; a++)
+    {
+        const int n = (a == 1 ? F.Ny : F.Nz) - 2;
+        for (int q = 0; q < n; q++) yz = std::min(yz, F.w[a][q + 2]);
+    }
+    std::vector<int> first, count; // interior groups: first fine cell (grid index), children
+    PlanXGroups(F.w[0].data() + 2, nf, yz, count);
+    for (size_t g = 0, j = 1; g < count.size(); j += count[g], g++) first.push_back((int)j);
+    const int m = (int)first.size();
+    bool regular = true;
+    for (int g = 0; g < m; g++)
+        if (count[g] != 2 && !(g == m - 1 && first[g] == nf)) regular = false;
+    if (regular) return false;
+    if (std::max(F.Nx, m + 2) > 0x7FFF) return false; // the maps pack indices in 15 bits
+    Nc = m + 2;
+    std::vector<double> size(Nc);
+    for (int g = 0; g < m; g++) size[g + 1] = F.w[0][first[g] + 1] + (count[g] == 2 ? F.w[0][first[g] + 2] : 0.0);
+    size[0] = size[1];
+    size[Nc - 1] = size[m];
+    wOut.resize(Nc + 2);
+    for (int q = -1; q <= Nc; q++) wOut[q + 1] = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
+    gOut.resize(Nc + 1);
+    for (int q = -1; q <= Nc - 1; q++)
+    {
+        const double a = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
+        const double b = size[q + 1 >= Nc ? Nc - 1 : q + 1];
+        gOut[q + 1] = 0.5 * (a + b);
+    }
+    // fine j -> parent, other contributor, single; the rings map onto the rings
+    xp.assign(F.Nx, 0);
+    xp[0] = 0 | (0 << 15) | (1 << 30);
+    xp[F.Nx - 1] = (Nc - 1) | ((Nc - 1) << 15) | (1 << 30);
+    xr.assign(Nc, 0);
+    xr[0] = 0;
+    xr[Nc - 1] = F.Nx - 1;
+    for (int g = 0; g < m; g++)
+    {
+        const int J = g + 1;
+        if (count[g] == 1) xp[first[g]] = J | (J << 15) | (1 << 30);
+        else
+        {
+            xp[first[g]] = J | ((J - 1) << 15);
+            xp[first[g] + 1] = J | ((J + 1) << 15);
+        }
+        const bool before = g > 0 && count[g - 1] == 2, after = g + 1 < m && count[g + 1] == 2;
+        xr[J] = first[g] | ((count[g] == 2) << 15) | (before << 16) | (after << 17);
+    }
+    return true;
+}
+
 void Context::BuildHierarchy()
 {
     // the previous levels lend their device arrays to the new ones of the same index (a DevArray keeps its
@@ -174,6 +261,9 @@ void Context::BuildHierarchy()
     auto take = [&](size_t l) {
         LevelData X = l < old.size() ? std::move(old[l]) : LevelData();
         for (int a = 0; a < 3; a++) { X.w[a].clear(); X.g[a].clear(); }
+        X.xp.clear();
+        X.xr.clear();
+        X.dxp = X.dxr = nullptr;
         return X;
     };
     {
@@ -193,7 +283,7 @@ void Context::BuildHierarchy()
     const int maxLevels = std::max(1, opt.max_levels);
     while ((int)L.size() < maxLevels)
     {
-        const LevelData &F = L.back();
+        LevelData &F = L.back();
         const int nx = F.Nx - 2, ny = F.Ny - 2, nz = dim == 3 ? F.Nz - 2 : 1;
         const int mn = dim == 3 ? std::min(nx, std::min(ny, nz)) : std::min(nx, ny);
         const long long interior = (long long)nx * ny * nz;
@@ -203,13 +293,17 @@ void Context::BuildHierarchy()
         if (mn < 8 || interior <= 64) break;
         LevelData C = take(L.size());
         C.dim = dim;
-        C.Nx = (nx + 1) / 2 + 2;
+        // x kept whole where a pair would be much wider than the coarse y/z cells (not on the coarse end's levels,
+        // whose transfers pair every axis)
+        const bool grouped = dim == 3 && F.stretched && opt.x_groups && F.cells > (long long)opt.tail_cells &&
+                             XGroups(F, C.Nx, C.w[0], C.g[0], F.xp, F.xr);
+        if (!grouped) C.Nx = (nx + 1) / 2 + 2;
         C.Ny = (ny + 1) / 2 + 2;
         C.Nz = dim == 3 ? (nz + 1) / 2 + 2 : 1;
         C.cells = (long long)C.Nx * C.Ny * C.Nz;
         C.stretched = F.stretched;
         C.gamma = F.gamma * (dim == 3 ? 2.0 : 1.0);
-        CoarseAxis(F.w[0], F.Nx, C.Nx, C.w[0], C.g[0]);
+        if (!grouped) CoarseAxis(F.w[0], F.Nx, C.Nx, C.w[0], C.g[0]);
         CoarseAxis(F.w[1], F.Ny, C.Ny, C.w[1], C.g[1]);
         if (dim == 3) CoarseAxis(F.w[2], F.Nz, C.Nz, C.w[2], C.g[2]);
         else { C.w[2] = F.w[2]; C.g[2] = F.g[2]; }

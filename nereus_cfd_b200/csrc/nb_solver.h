@@ -190,6 +190,10 @@ struct LevelData
     // the device copies of w, g (FP64) and of w, 1/g (FP32): pointers into the context's packed table array
     const double *dw[3] = {}, *dg[3] = {};
     const float *dw32[3] = {}, *dig32[3] = {};
+    // the x groups of the transfer to the next coarser level (LevelView::xp, xr) and their device copies in the
+    // packed table array; empty: x cells paired by two like the other axes
+    std::vector<int> xp, xr;
+    const int *dxp = nullptr, *dxr = nullptr;
     DevArray<uint8_t> types, code;
     DevArray<uint8_t> du;                 // diagonal units for the pair kernels (nb_pairs.cu); empty elsewhere.
                                           // Colour-split level: in that layout, and the codes on a stretched level
@@ -437,6 +441,11 @@ void UpdateFluidCellsDevice(int dim, int Nx, int Ny, int Nz, double ox, double o
 // Boundary-condition replay (nb_bc.cu): the reference's lists as leveled device write programs.
 struct BcReplay;
 // Checks the lists on the host (every index inside its field); throws InputError on a bad list.
+// The x groups of a stretched level's coarsening from its n interior x widths: left to right, two cells form one
+// coarse cell when together they are at most 1.5 coarse y/z cells wide (twice yzMin), else a cell stays whole.
+// count gets each group's cell count (1 or 2).
+void PlanXGroups(const double *w, int n, double yzMin, std::vector<int> &count);
+
 void CheckBcLists(const nb_bc_lists &lists);
 // The level of each operation of the two replays, in list order (solid faces of u, v, w, prescribed entries, copies;
 // ring entries), on the host.
