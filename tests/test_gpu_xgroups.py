@@ -4,7 +4,9 @@ The stretched cylinder's x widths run from 0.0013 in its band to 0.066 at its en
 every axis leaves coarse cells up to 20 times longer in x than across, where red-black point smoothing stalls; keeping
 the wide x cells whole (and pairing the thin ones) keeps the coarse cells near cubes. Each solve below must meet its
 tolerance with the reference's FP64 residual; the grouped hierarchy must need far fewer CG iterations than the halved
-one, in both precisions and every FP32 kernel family, and the two hierarchies' pressures agree to the tolerance.
+one, in both precisions and every FP32 kernel family. Solved to 1e-11 the two hierarchies' pressures agree within
+1e-5: at 1e-8 they differ by about 5e-4 (measured), since the cylinder's stretched operator is ill-conditioned and a
+relative residual of 1e-8 bounds the pressure's error only to its condition number times that.
 """
 import numpy as np
 import pytest
@@ -43,10 +45,15 @@ def test_groups_cut_iterations_on_the_cylinder(nb, cylinder, precision):
     # measured on a B200: 16 against 74 (mixed), 16 against 73 (fp64)
     assert rg.iters_inner <= 20, rg.as_dict()
     assert rh.iters_inner >= 2 * rg.iters_inner, (rg.as_dict(), rh.as_dict())
+    assert rg.max_div <= 10.0 * rh.max_div + 1e-12
+    tight = 1e-11
+    rg, mg = solve(case, types, u, v, w, precision, tight)
+    rh, mh = solve(case, types, u, v, w, precision, tight, x_groups=0)
+    for r in (rg, rh):
+        assert r.status == capi.NB_OK and r.rel_res <= tight, r.as_dict()
     fluid = types.reshape(-1) == W.FLUID
     pg, ph = mg.p.reshape(-1)[fluid], mh.p.reshape(-1)[fluid]
-    assert np.linalg.norm(pg - ph) / np.linalg.norm(ph) <= 1e-6
-    assert rg.max_div <= 10.0 * rh.max_div + 1e-12
+    assert np.linalg.norm(pg - ph) / np.linalg.norm(ph) <= 1e-5
 
 
 @pytest.mark.parametrize("family", [0, 1])
@@ -58,10 +65,13 @@ def test_groups_in_every_fp32_family(nb, cylinder, family):
     r, m = solve(case, types, u, v, w, "mixed", tol, pair_kernels=family)
     assert r.status == capi.NB_OK and r.rel_res <= tol, r.as_dict()
     assert r.iters_inner <= 20, r.as_dict()
-    ref, mref = solve(case, types, u, v, w, "mixed", tol)
+    tight = 1e-11
+    r, m = solve(case, types, u, v, w, "mixed", tight, pair_kernels=family)
+    ref, mref = solve(case, types, u, v, w, "mixed", tight)
+    assert r.rel_res <= tight and ref.rel_res <= tight
     fluid = types.reshape(-1) == W.FLUID
     a, b = m.p.reshape(-1)[fluid], mref.p.reshape(-1)[fluid]
-    assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-6
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5
 
 
 def test_groups_on_a_graded_tank(nb):
