@@ -5,9 +5,13 @@ every axis leaves coarse cells up to 20 times longer in x than across, where red
 the wide x cells whole (and pairing the thin ones) keeps the coarse cells near cubes. Each solve below must meet its
 tolerance with the reference's FP64 residual; the grouped hierarchy must need far fewer CG iterations than the halved
 one, in both precisions and every FP32 kernel family. Solved to 1e-11 the two hierarchies' pressures agree within
-1e-5: at 1e-8 they differ by about 5e-4 (measured), since the cylinder's stretched operator is ill-conditioned and a
-relative residual of 1e-8 bounds the pressure's error only to its condition number times that.
+1e-5. At 1e-8 the mixed solves lie further apart (measured against the reference's 1e-12 solve: 4.7e-4 grouped,
+1.7e-5 halved; the FP64 ones 6.9e-8 and 3.9e-7): the cylinder's operator is ill-conditioned, so a relative residual
+of 1e-8 bounds the pressure's error only loosely, and how much error the residual leaves in the smooth modes depends
+on the Krylov space that made it (two short FP32 passes in the mixed form, one FP64 space in the plain one).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -90,3 +94,40 @@ def test_groups_on_a_graded_tank(nb):
     assert (r1.iters_inner, r1.rel_res) == (r2.iters_inner, r2.rel_res)
     assert np.array_equal(m1.p, m2.p)
     assert r1.iters_inner <= r0.iters_inner
+
+
+@pytest.fixture(scope="module")
+def reference(cylinder):
+    """The reference's own solves of the cylinder (oracle/_ref/ref_harness: AMGCL SA+SPAI0 CG, run on this host, the
+    way tests/suite_pressure.cpp:104-141 drives it) to 1e-12 and to 1e-8."""
+    from oracle import refcase
+
+    if not refcase.available():
+        pytest.skip("oracle/_ref/ref_harness is not built")
+    case, types, u, v, w = cylinder
+    threads = os.cpu_count() or 1
+    run = lambda tol: refcase.run(case, u, v, w, label_mode=1, types=types, solver=refcase.SOLVER_AMG, tol=tol,
+                                  threads=threads, timeout=1800, lean=True)
+    return run(1e-12), run(1e-8)
+
+
+def test_cylinder_against_reference(nb, cylinder, reference):
+    """The full 192x128x128 cylinder against the reference's solve at 1e-12 (the reference's own 1e-8 solve lies
+    5.3e-8 from it, measured):
+    - plain FP64 to 1e-8: pressure within 1e-6 relative L2 on the fluid cells (measured 6.9e-8);
+    - mixed to 1e-8: the residual bar holds, but its pressure lies 4.7e-4 from the reference's (measured): two
+      refinement passes of 8 FP32 CG iterations leave the smooth modes' error that one FP64 Krylov space of 16
+      iterations removes, so the bar is 1e-3 here and 1e-6 only from a solve to 1e-11 (measured 1.4e-6 at 1e-10);
+    - max |div u| within 10x of the reference's own at 1e-8 for both."""
+    case, types, u, v, w = cylinder
+    r12, r8 = reference
+    assert r12.rel_res <= 1e-11 and r8.rel_res <= 1e-8
+    fluid = types.reshape(-1) == W.FLUID
+    ref = r12.p.reshape(-1)[fluid]
+    err = lambda m: float(np.linalg.norm(m.p.reshape(-1)[fluid] - ref) / np.linalg.norm(ref))
+    for precision, tol, bar in (("fp64", 1e-8, 1e-6), ("mixed", 1e-8, 1e-3), ("mixed", 1e-11, 1e-6)):
+        r, m = solve(case, types, u, v, w, precision, tol)
+        assert r.status == capi.NB_OK and r.rel_res <= tol, r.as_dict()
+        assert r.n == r12.n and r.singular == int(r12.singular)
+        assert err(m) <= bar, (precision, tol, err(m))
+        assert r.max_div <= 10.0 * r8.max_div, (r.max_div, r8.max_div)
