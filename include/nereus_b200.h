@@ -428,6 +428,12 @@ int nereus_b200_tune_choose(int n, const double *times, int fallback);
  * 1.5 coarse y/z cells (3 yz_min) wide, else a cell stays whole. Writes each group's cell count (1 or 2) into
  * counts (room for n) and returns the number of groups, or NB_BAD_INPUT. */
 int nereus_b200_x_groups(const double *widths, int n, double yz_min, int32_t *counts);
+/* The same groups as the transfer maps the kernels read (host only): xp[j] for the fine x index j = 0 .. n+1 (rings
+ * included): parent (bits 0-14), other contributor (bits 15-29), bit 30 when the parent has one child; xr[J] for the
+ * coarse x index J: first child (bits 0-14), bit 15 two children, bit 16 / 17 the group before / after has two.
+ * Returns the coarse extent Nc (rings included; xr needs room for n + 2), 0 when the groups are the regular pairing
+ * of every axis (nothing written), or NB_BAD_INPUT. */
+int nereus_b200_x_maps(const double *widths, int n, double yz_min, int32_t *xp, int32_t *xr);
 int nereus_b200_tune_key(int Nx, int Ny, int Nz, int level, int kind, int capacity, char *buf, int size);
 int nereus_b200_tune_cache_dump(char *buf, int size);
 int nereus_b200_tune_cache_load(const char *text);

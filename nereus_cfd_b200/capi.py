@@ -207,6 +207,7 @@ SIGNATURES = {
     "nereus_b200_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchInfo)]),
     "nereus_b200_tune_choose": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int]),
     "nereus_b200_x_groups": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_double, _ip]),
+    "nereus_b200_x_maps": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_double, _ip, _ip]),
     "nereus_b200_tune_key": (ctypes.c_int, [ctypes.c_int] * 6 + [ctypes.c_char_p, ctypes.c_int]),
     "nereus_b200_tune_cache_dump": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "nereus_b200_tune_cache_load": (ctypes.c_int, [ctypes.c_char_p]),

@@ -585,4 +585,16 @@ int nereus_b200_x_groups(const double *widths, int n, double yz_min, int32_t *co
     return (int)c.size();
 }
 
+int nereus_b200_x_maps(const double *widths, int n, double yz_min, int32_t *xp, int32_t *xr)
+{
+    if (!widths || !xp || !xr || n < 1 || !(yz_min > 0.0)) return Fail(NB_BAD_INPUT, "bad x widths");
+    int Nc = 0;
+    std::vector<double> size;
+    std::vector<int> p, r;
+    if (!nb::XMaps(widths, n, yz_min, Nc, size, p, r)) return 0;
+    for (size_t q = 0; q < p.size(); q++) xp[q] = p[q];
+    for (size_t q = 0; q < r.size(); q++) xr[q] = r[q];
+    return Nc;
+}
+
 } // extern "C"

@@ -180,10 +180,7 @@ static void CoarseAxis(const std::vector<double> &wFine, int Nf, int Nc, std::ve
     }
 }
 
-// The x groups of a stretched 3D level's coarsening: left to right, two interior x cells form one coarse cell when
-// together they are at most 1.5 coarse y/z cells wide (twice the thinnest interior y or z cell), else a cell stays
-// whole. Returns false when that is every cell paired by two (the regular coarsening); otherwise the padded coarse x
-// tables (as CoarseAxis), the coarse extent and the transfer maps of LevelView::xp / xr.
+// x groups of stretched coarsening (declared with their rule in nb_solver.h)
 void PlanXGroups(const double *w, int n, double yzMin, std::vector<int> &count)
 {
     const double target = 1.5 * 2.0 * yzMin;
@@ -196,46 +193,30 @@ void PlanXGroups(const double *w, int n, double yzMin, std::vector<int> &count)
     }
 }
 
-static bool XGroups(const LevelData &F, int &Nc, std::vector<double> &wOut, std::vector<double> &gOut,
-                    std::vector<int> &xp, std::vector<int> &xr)
+bool XMaps(const double *w, int nf, double yzMin, int &Nc, std::vector<double> &size, std::vector<int> &xp,
+           std::vector<int> &xr)
 {
-    const int nf = F.Nx - 2;
-    double yz = 1e300;
-    for (int a = 1; a <= 2; a++)
-    {
-        const int n = (a == 1 ? F.Ny : F.Nz) - 2;
-        for (int q = 0; q < n; q++) yz = std::min(yz, F.w[a][q + 2]);
-    }
     std::vector<int> first, count; // interior groups: first fine cell (grid index), children
-    PlanXGroups(F.w[0].data() + 2, nf, yz, count);
+    PlanXGroups(w, nf, yzMin, count);
     for (size_t g = 0, j = 1; g < count.size(); j += count[g], g++) first.push_back((int)j);
     const int m = (int)first.size();
     bool regular = true;
     for (int g = 0; g < m; g++)
         if (count[g] != 2 && !(g == m - 1 && first[g] == nf)) regular = false;
     if (regular) return false;
-    if (std::max(F.Nx, m + 2) > 0x7FFF) return false; // the maps pack indices in 15 bits
+    if (nf + 2 > 0x7FFF) return false; // the maps pack indices in 15 bits
     Nc = m + 2;
-    std::vector<double> size(Nc);
-    for (int g = 0; g < m; g++) size[g + 1] = F.w[0][first[g] + 1] + (count[g] == 2 ? F.w[0][first[g] + 2] : 0.0);
+    size.assign(Nc, 0.0);
+    for (int g = 0; g < m; g++) size[g + 1] = w[first[g] - 1] + (count[g] == 2 ? w[first[g]] : 0.0);
     size[0] = size[1];
     size[Nc - 1] = size[m];
-    wOut.resize(Nc + 2);
-    for (int q = -1; q <= Nc; q++) wOut[q + 1] = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
-    gOut.resize(Nc + 1);
-    for (int q = -1; q <= Nc - 1; q++)
-    {
-        const double a = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
-        const double b = size[q + 1 >= Nc ? Nc - 1 : q + 1];
-        gOut[q + 1] = 0.5 * (a + b);
-    }
     // fine j -> parent, other contributor, single; the rings map onto the rings
-    xp.assign(F.Nx, 0);
+    xp.assign(nf + 2, 0);
     xp[0] = 0 | (0 << 15) | (1 << 30);
-    xp[F.Nx - 1] = (Nc - 1) | ((Nc - 1) << 15) | (1 << 30);
+    xp[nf + 1] = (Nc - 1) | ((Nc - 1) << 15) | (1 << 30);
     xr.assign(Nc, 0);
     xr[0] = 0;
-    xr[Nc - 1] = F.Nx - 1;
+    xr[Nc - 1] = nf + 1;
     for (int g = 0; g < m; g++)
     {
         const int J = g + 1;
@@ -247,6 +228,31 @@ static bool XGroups(const LevelData &F, int &Nc, std::vector<double> &wOut, std:
         }
         const bool before = g > 0 && count[g - 1] == 2, after = g + 1 < m && count[g + 1] == 2;
         xr[J] = first[g] | ((count[g] == 2) << 15) | (before << 16) | (after << 17);
+    }
+    return true;
+}
+
+// The x groups of a stretched 3D level's next coarsening (XMaps with the level's thinnest interior y or z width),
+// with the coarse level's padded x tables (as CoarseAxis makes them) and its extent; false: the regular pairing.
+static bool XGroups(const LevelData &F, int &Nc, std::vector<double> &wOut, std::vector<double> &gOut,
+                    std::vector<int> &xp, std::vector<int> &xr)
+{
+    double yz = 1e300;
+    for (int a = 1; a <= 2; a++)
+    {
+        const int n = (a == 1 ? F.Ny : F.Nz) - 2;
+        for (int q = 0; q < n; q++) yz = std::min(yz, F.w[a][q + 2]);
+    }
+    std::vector<double> size;
+    if (!XMaps(F.w[0].data() + 2, F.Nx - 2, yz, Nc, size, xp, xr)) return false;
+    wOut.resize(Nc + 2);
+    for (int q = -1; q <= Nc; q++) wOut[q + 1] = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
+    gOut.resize(Nc + 1);
+    for (int q = -1; q <= Nc - 1; q++)
+    {
+        const double a = size[q < 0 ? 0 : (q >= Nc ? Nc - 1 : q)];
+        const double b = size[q + 1 >= Nc ? Nc - 1 : q + 1];
+        gOut[q + 1] = 0.5 * (a + b);
     }
     return true;
 }

@@ -445,6 +445,11 @@ struct BcReplay;
 // coarse cell when together they are at most 1.5 coarse y/z cells wide (twice yzMin), else a cell stays whole.
 // count gets each group's cell count (1 or 2).
 void PlanXGroups(const double *w, int n, double yzMin, std::vector<int> &count);
+// Those groups as the transfer maps of LevelView::xp (nf + 2 entries, the rings included) and xr (Nc entries), with
+// the coarse cell widths (Nc entries, each ring as wide as its neighbour); false (nothing written) when the groups
+// are the regular pairing of every axis.
+bool XMaps(const double *w, int nf, double yzMin, int &Nc, std::vector<double> &size, std::vector<int> &xp,
+           std::vector<int> &xr);
 
 void CheckBcLists(const nb_bc_lists &lists);
 // The level of each operation of the two replays, in list order (solid faces of u, v, w, prescribed entries, copies;

@@ -58,3 +58,81 @@ def test_bad_input():
         capi.NB_BAD_INPUT
     assert lib.nereus_b200_x_groups(w.ctypes.data_as(capi._dp), 4, 0.0, out.ctypes.data_as(capi._ip)) == \
         capi.NB_BAD_INPUT
+
+
+def maps(widths, yz):
+    lib = capi.load()
+    w = np.ascontiguousarray(widths, dtype=np.float64)
+    n = len(w)
+    xp = np.zeros(n + 2, dtype=np.int32)
+    xr = np.zeros(n + 2, dtype=np.int32)
+    nc = lib.nereus_b200_x_maps(w.ctypes.data_as(capi._dp), n, float(yz), xp.ctypes.data_as(capi._ip),
+                                xr.ctypes.data_as(capi._ip))
+    assert nc >= 0
+    return nc, xp, xr[:nc]
+
+
+def prolongation_1d(xp, nc):
+    """P along x as the prolongation kernels read xp: a fine cell gives its parent 1 (one child) or 3/4, and the
+    other contributor 1/4."""
+    P = np.zeros((len(xp), nc))
+    for j, x in enumerate(xp):
+        parent, other, single = x & 0x7FFF, (x >> 15) & 0x7FFF, (x >> 30) & 1
+        if single:
+            assert other == parent
+            P[j, parent] += 1.0
+        else:
+            assert abs(other - parent) == 1
+            P[j, parent] += 0.75
+            P[j, other] += 0.25
+    return P
+
+
+def restriction_taps_1d(xr, nf):
+    """R along x as the restriction kernels read xr (the taps of XrTaps), rows for the interior coarse cells."""
+    R = np.zeros((len(xr), nf))
+    for J in range(1, len(xr) - 1):
+        x = int(xr[J])
+        f0, two, before, after = x & 0x7FFF, (x >> 15) & 1, (x >> 16) & 1, (x >> 17) & 1
+        if before:
+            R[J, f0 - 1] += 0.25
+        R[J, f0] += 0.75 if two else 1.0
+        if two:
+            R[J, f0 + 1] += 0.75
+        if after:
+            R[J, f0 + (2 if two else 1)] += 0.25
+    return R
+
+
+@pytest.mark.parametrize("case", ["cylinder", "random0", "random1", "random2"])
+def test_maps_restrict_with_the_transpose(case):
+    """The restriction taps are the transpose of the prolongation weights on every interior coarse cell, each fine
+    interior cell has exactly one parent whose children include it, and the groups are the planner's."""
+    if case == "cylinder":
+        wx, yz = W.stretched_cylinder_3d(192, 128, 128).grid.interior_widths[0], 0.41 / 128
+    else:
+        rng = np.random.default_rng(int(case[-1]))
+        wx, yz = rng.uniform(0.3, 2.5, size=int(rng.integers(8, 200))), 1.0
+    nc, xp, xr = maps(wx, yz)
+    counts = plan(wx, yz)
+    if nc == 0:
+        assert all(c == 2 for c in counts[:-1])
+        return
+    assert nc == len(counts) + 2
+    nf = len(wx) + 2
+    P = prolongation_1d(xp, nc)
+    R = restriction_taps_1d(xr, nf)
+    assert np.array_equal(R[1:nc - 1], P.T[1:nc - 1])
+    # children: xr's children of J are exactly the fine cells whose parent is J
+    for J in range(1, nc - 1):
+        f0, two = int(xr[J]) & 0x7FFF, (int(xr[J]) >> 15) & 1
+        kids = [f0, f0 + 1] if two else [f0]
+        assert [j for j in range(nf) if (int(xp[j]) & 0x7FFF) == J] == kids
+        assert len(kids) == counts[J - 1]
+    # the rings map onto the rings
+    assert int(xp[0]) & 0x7FFF == 0 and int(xp[-1]) & 0x7FFF == nc - 1
+
+
+def test_maps_regular_pairing_is_left_to_the_plain_kernels():
+    nc, _, _ = maps(np.full(12, 0.5), 1.0)
+    assert nc == 0
